@@ -1,0 +1,77 @@
+"""numpy mirrors of the record layouts declared in include/exg.h.
+
+The host-side arrays built with these dtypes are passed by pointer to the C ABI; their
+byte layout must equal the C structs (checked against the library at load time).
+"""
+import numpy as np
+
+BODY_DTYPE = np.dtype(
+    [
+        ("pose", "<f8", (8,)),
+        ("momentum", "<f8", (6,)),
+        ("mass", "<f8"),
+        ("inertia", "<f8", (9,)),
+        ("size", "<f8"),
+        ("kinematic", "<i4"),
+        ("diagonal", "<i4"),
+    ],
+    align=True,
+)
+
+JOINT_DTYPE = np.dtype(
+    [("law", "<i4"), ("a", "<i4"), ("b", "<i4"), ("reserved", "<i4"), ("params", "<f8", (10,))],
+    align=True,
+)
+
+
+STEP_PARAMS_DTYPE = np.dtype(
+    [
+        ("integrator", "<i4"),
+        ("gravity_law", "<i4"),
+        ("precision", "<i4"),
+        ("reserved0", "<i4"),
+        ("G", "<f8"),
+        ("softening", "<f8"),
+        ("dt", "<f8"),
+        ("warp", "<f8"),
+        ("tol", "<f8"),
+        ("max_newton", "<i4"),
+        ("reserved1", "<i4"),
+    ],
+    align=True,
+)
+
+WORLD_STATS_DTYPE = np.dtype(
+    [
+        ("steps", "<i8"),
+        ("last_spans", "<i4"),
+        ("last_newton_iterations", "<i4"),
+        ("max_depth_reached", "<i4"),
+        ("fatal", "<i4"),
+        ("last_residual", "<f8"),
+    ],
+    align=True,
+)
+
+# Law ids and names (crates/newton/src/accelerator/mod.rs:118-132).
+LAW_NAMES = ("SimpleSpringDamper", "CriticallyDampedWarped", "PerpendicularDamperWarped", "TorsionalDamperWarped")
+LAW_N_PARAMS = (10, 10, 2, 1)
+
+EXPLICIT_EULER, SYMPLECTIC_EULER, LIE_EULER, NEWTON = 0, 1, 2, 3
+GRAVITY_OFF, GRAVITY_SIZE_CORE, GRAVITY_PLUMMER = 0, 1, 2
+PRECISION_F64, PRECISION_MIXED = 0, 1
+
+
+def step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, precision=PRECISION_F64, G=1.0, softening=0.0,
+                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32):
+    p = np.zeros((), dtype=STEP_PARAMS_DTYPE)
+    p["integrator"] = integrator
+    p["gravity_law"] = gravity_law
+    p["precision"] = precision
+    p["G"] = G
+    p["softening"] = softening
+    p["dt"] = dt
+    p["warp"] = warp
+    p["tol"] = tol
+    p["max_newton"] = max_newton
+    return p

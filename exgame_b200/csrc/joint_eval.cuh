@@ -1,0 +1,76 @@
+// Per-joint evaluation routines shared by the joint kernels.
+//
+// Plain:    the 12 wrench components [force a, torque a, force b, torque b] at (pose, twist)
+//           (crates/newton/build.rs:938-973).
+// Jacobian: value + partials w.r.t. 24 axes — pose A, pose B (retraction exp(delta) * pose,
+//           unit Motor::exp, no half), world twist A, world twist B, each lin xyz then ang xyz
+//           (crates/newton/build.rs:673-768, crates/clifford/src/pga3/ad.rs:119-150).
+//           The 24 axes are evaluated as four 6-axis dual slices; slice s seeds axes
+//           6s..6s+5. With the pose seed's value at zero, exp(delta) = 1 + delta exactly to
+//           first order (the Study forms take their Taylor arm at u = 0), so the seeded pose
+//           is (1 + delta) * pose.
+// The wrench on b is the negation of the wrench on a for every law, so only a is evaluated.
+#pragma once
+#include "laws.cuh"
+
+namespace exg {
+
+// poses: 8 motor components in slot order; twists: 6 physical components (lin, ang).
+template <class R>
+EXG_HD void joint_plain(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a, const R* vel_b, double dt,
+                        double warp, R* out12) {
+  R ta[6], tb[6], wa[6];
+  screw_from6(vel_a, ta);
+  screw_from6(vel_b, tb);
+  law_wrench(law, prm, pose_a, pose_b, ta, tb, dt, warp, wa);
+  R w6[6];
+  screw_to6(wa, w6);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { out12[i] = w6[i]; out12[6 + i] = -w6[i]; }
+}
+
+// One slice: value[6] of the wrench on a and d[6][6] = d(wrench on a component r)/d(axis 6s+c),
+// stored d[r*6 + c].
+template <class R>
+EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
+                                 const R* vel_b, double dt, double warp, int slice, R* value6, R* d36) {
+  using D = Dual<6, R>;
+  D ma[8], mb[8], va[6], vb[6];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) { ma[i] = D(0.0); ma[i].v = pose_a[i]; mb[i] = D(0.0); mb[i].v = pose_b[i]; }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { va[i] = D(0.0); va[i].v = vel_a[i]; vb[i] = D(0.0); vb[i].v = vel_b[i]; }
+  if (slice < 2) {
+    // pose seed: (1 + delta) * base with delta = Twist(seed lin, seed ang), value 0
+    D seed6[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { seed6[i] = D(0.0); seed6[i].g[i] = R(1); }
+    D delta[6], one_delta[8];
+    screw_from6(seed6, delta);
+    one_delta[0] = D(1.0);
+    one_delta[7] = D(0.0);
+    static_for<0, 6>([&](auto i) { one_delta[slot_of(EVEN, BIV[i])] = delta[i]; });
+    D* base = (slice == 0) ? ma : mb;
+    D moved[8];
+    gp<EVEN, EVEN, EVEN>(one_delta, base, moved);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) base[i] = moved[i];
+  } else {
+    D* v = (slice == 2) ? va : vb;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) v[i].g[i] = R(1);
+  }
+  D ta[6], tb[6], wa[6], w6[6];
+  screw_from6(va, ta);
+  screw_from6(vb, tb);
+  law_wrench(law, prm, ma, mb, ta, tb, dt, warp, wa);
+  screw_to6(wa, w6);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    value6[r] = w6[r].v;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) d36[r * 6 + c] = w6[r].g[c];
+  }
+}
+
+}  // namespace exg

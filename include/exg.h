@@ -1,0 +1,174 @@
+/*
+ * exg.h — C ABI of the B200 per-step dynamics path (all-pairs gravity, joint force laws,
+ * implicit mid-point Newton step).
+ *
+ * This is the drop-in boundary a host binds instead of the reference's Vulkan device layer
+ * and GPU-resident world storage. Every entry point takes plain pointers and sizes and
+ * returns an `int` status (EXG_OK = 0, negative = error; `exg_status_string` names it).
+ * Host arrays are ordinary CPU memory; entry points whose parameter is named `d_*` take
+ * device pointers on the device the handle was created on.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   - rembrandt::GpuAccelerator (crates/rembrandt/src/lib.rs:77-243)      -> exg_device_*
+ *   - aristotle::World storage + WorldKey slots (crates/aristotle/src/world.rs:400-650)
+ *                                                                        -> exg_world_* (device buffers)
+ *   - newton::Accelerator stage calls (crates/newton/src/accelerator/mod.rs:649-964)
+ *                                                                        -> exg_eval_joints, exg_gravity_forces
+ *   - Mechanism::step / Driver::step (crates/newton/src/mechanism/mechanism.rs:526,
+ *     crates/newton/src/driver.rs:76)                                    -> exg_world_step, exg_batch_step
+ *   - joint-law registration by shader name (crates/newton/src/accelerator/mod.rs:118-132,
+ *     crates/joints/src/lib.rs:246-253)                                  -> exg_law_lookup
+ *   - EvalError / StructureError (crates/newton/src/error.rs:11-28,
+ *     crates/newton/src/mechanism/mechanism.rs:21-58)                    -> exg_status codes
+ */
+#ifndef EXG_H
+#define EXG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXG_ABI_VERSION 1
+
+/* ── status codes ─────────────────────────────────────────────────────────── */
+typedef enum {
+  EXG_OK = 0,
+  /* EvalError (crates/newton/src/error.rs:11-28) */
+  EXG_ERR_NO_SHADER = -1,       /* NoShader: unknown joint-law name or id */
+  EXG_ERR_TRAP = -2,            /* Trap: a kernel refused its input */
+  EXG_ERR_FATAL = -3,           /* Fatal: a guarded site fired (non-finite state) */
+  EXG_ERR_WORKER_GONE = -4,     /* WorkerGone: the request loop has shut down */
+  EXG_ERR_BACKEND = -5,         /* Backend: a CUDA call failed */
+  /* StructureError (crates/newton/src/mechanism/mechanism.rs:21-58) */
+  EXG_ERR_EPOCH_IN_PROGRESS = -10,
+  EXG_ERR_ALREADY_OWNED = -11,
+  EXG_ERR_FOREIGN_ACCELERATOR = -12,
+  EXG_ERR_DUPLICATE_MECHANISM = -13,
+  /* storage misuse, which panics in the reference (crates/aristotle/src/world.rs:246-264) */
+  EXG_ERR_INVALID_ARGUMENT = -20,
+  EXG_ERR_OUT_OF_MEMORY = -21,
+  EXG_ERR_UNSUPPORTED = -22,
+  EXG_ERR_TIMEOUT = -23,
+  EXG_ERR_NO_DEVICE = -24
+} exg_status;
+
+/* ── records (host layout == device layout) ───────────────────────────────── */
+
+/* One rigid body (crates/newton/src/body.rs:32-63). `pose` is the motor in the reference's
+ * slot order (even blades by increasing bitmask: 1, e12, e13, e23, e1e0, e2e0, e3e0, e123e0 in
+ * bit terms 0,3,5,6,9,10,12,15; crates/clifford/src/pga3/motor.rs:119-147). `momentum` is the
+ * BODY-frame momentum (force xyz, torque xyz). `inertia` is the 3x3 angular tensor, row-major
+ * (crates/newton/src/inertia.rs:145-156); `diagonal` = 1 reads only its diagonal. `size` is the
+ * gravity core radius, (mass/4)^(1/3) by default (body.rs:70-77). A kinematic body has a
+ * prescribed velocity equal to its momentum read as a twist (inertia.rs:160-170). */
+typedef struct {
+  double pose[8];
+  double momentum[6];
+  double mass;
+  double inertia[9];
+  double size;
+  int32_t kinematic;
+  int32_t diagonal;
+} exg_body_t;
+
+/* One joint edge (crates/joints/src/lib.rs:47-60): law id, the two body indices and the law's
+ * parameters in its canonical flatten order (crates/joints/src/lib.rs:273-298). */
+typedef struct {
+  int32_t law;
+  int32_t a;
+  int32_t b;
+  int32_t reserved;
+  double params[10];
+} exg_joint_t;
+
+typedef enum {
+  EXG_LAW_SIMPLE_SPRING_DAMPER = 0,        /* "SimpleSpringDamper", 10 params */
+  EXG_LAW_CRITICALLY_DAMPED_WARPED = 1,    /* "CriticallyDampedWarped", 10 params */
+  EXG_LAW_PERPENDICULAR_DAMPER_WARPED = 2, /* "PerpendicularDamperWarped", 2 params */
+  EXG_LAW_TORSIONAL_DAMPER_WARPED = 3      /* "TorsionalDamperWarped", 1 param */
+} exg_law;
+
+typedef enum { EXG_EXPLICIT_EULER = 0, EXG_SYMPLECTIC_EULER = 1, EXG_LIE_EULER = 2, EXG_NEWTON = 3 } exg_integrator;
+typedef enum { EXG_GRAVITY_OFF = 0, EXG_GRAVITY_SIZE_CORE = 1, EXG_GRAVITY_PLUMMER = 2 } exg_gravity_law;
+/* F64: every stage in double precision (the plain path). MIXED: forces and the linear
+ * solve's inner iterations in FP32, pose/momentum accumulation, the Newton residual and the
+ * final block-inverse correction in FP64. */
+typedef enum { EXG_PRECISION_F64 = 0, EXG_PRECISION_MIXED = 1 } exg_precision;
+
+/* Step configuration: Epoch dt/warp (crates/aristotle/src/epoch.rs:17-60), the integrator
+ * (crates/newton/src/integrator/implicit/mod.rs:44-49), the gravity field and the Newton
+ * tolerance (relative per-block residual; the reference hard-codes 1e-4,
+ * crates/newton/src/integrator/implicit/newton.rs:799-805). */
+typedef struct {
+  int32_t integrator;
+  int32_t gravity_law;
+  int32_t precision;
+  int32_t reserved0;
+  double G;
+  double softening; /* Plummer epsilon */
+  double dt;
+  double warp;
+  double tol;
+  int32_t max_newton; /* per span; the reference uses 32 (newton.rs:355) */
+  int32_t reserved1;
+} exg_step_params_t;
+
+/* Per-world counters of the last step. */
+typedef struct {
+  int64_t steps;
+  int32_t last_spans;            /* dt sub-spans taken (newton.rs:543-683) */
+  int32_t last_newton_iterations;
+  int32_t max_depth_reached;
+  int32_t fatal;                 /* non-zero after a non-finite residual was committed */
+  double last_residual;          /* worst relative residual^2 of the last span */
+} exg_world_stats_t;
+
+typedef struct exg_device_s* exg_device_t;
+typedef struct exg_world_s* exg_world_t;
+
+/* ── device (replaces rembrandt::GpuAccelerator::new, crates/rembrandt/src/lib.rs:98-158) ── */
+int exg_device_create(int32_t ordinal, exg_device_t* out);
+int exg_device_destroy(exg_device_t dev);
+int exg_device_synchronize(exg_device_t dev);
+/* Number of kernels this library launched on the device so far. */
+int exg_device_kernel_launches(exg_device_t dev, uint64_t* out);
+const char* exg_status_string(int status);
+int exg_abi_version(void);
+
+/* ── law registry (MessageKind::from((shader_name, jacobian)), accelerator/mod.rs:118-132) ── */
+int exg_law_lookup(const char* shader_name, int32_t* law_out, int32_t* n_params_out);
+
+/* ── world: device-resident bodies and joints (aristotle::World + Mechanism) ── */
+int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n_bodies, const exg_joint_t* joints,
+                     int32_t n_joints, const exg_step_params_t* params, exg_world_t* out);
+int exg_world_destroy(exg_world_t w);
+/* Advance n_steps steps (Mechanism::step per step; crates/newton/src/mechanism/mechanism.rs:526-602). */
+int exg_world_step(exg_world_t w, int32_t n_steps);
+int exg_world_get_bodies(exg_world_t w, exg_body_t* out, int32_t n_bodies);
+int exg_world_set_bodies(exg_world_t w, const exg_body_t* bodies, int32_t n_bodies);
+int exg_world_stats(exg_world_t w, exg_world_stats_t* out);
+/* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
+int exg_world_energy(exg_world_t w, double* out);
+
+/* ── stage API on device pointers (the Accelerator's stage calls) ─────────── */
+/* Joint kernels K1-K8 (crates/newton/build.rs:874-973): for each joint k, inputs are the two
+ * poses (8 doubles each, d_pose[8*body]), the two WORLD twists (6 doubles each, d_vel[6*body]);
+ * output is d_out[12*k] = [force a, torque a, force b, torque b] when jacobian == 0, or the
+ * 300-double block d_out[300*k] = 12 components x [value, d/d(axis 0..23)] (axes: pose A,
+ * pose B, vel A, vel B; each lin xyz then ang xyz) when jacobian != 0. */
+int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t n_joints, const double* d_pose,
+                    const double* d_vel, double dt, double warp, int32_t jacobian, double* d_out);
+/* All-pairs gravity (crates/newton/src/gravity.rs:110-140, 438-450): d_pos_mass holds
+ * [x, y, z, m] per body, d_size the core radius (SIZE_CORE law), output d_force[3*i] is the
+ * world force on body i. precision MIXED runs the FP32 tile-relative kernel with compensated
+ * accumulation. */
+int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law,
+                       double G, double softening, int32_t precision, double* d_force);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXG_H */

@@ -1,0 +1,43 @@
+// Test harness: compiles the device algebra and force-law headers of the CUDA path for the
+// host so the CPU test suite can compare them with the oracle without a GPU.
+#include "../../exgame_b200/csrc/joint_eval.cuh"
+
+extern "C" {
+void dh_joint_plain(int law, const double* prm, const double* pa, const double* pb, const double* va, const double* vb,
+                    double dt, double warp, double* out12) {
+  exg::joint_plain<double>(law, prm, pa, pb, va, vb, dt, warp, out12);
+}
+void dh_joint_plain_f32(int law, const double* prm, const float* pa, const float* pb, const float* va, const float* vb,
+                        double dt, double warp, float* out12) {
+  exg::joint_plain<float>(law, prm, pa, pb, va, vb, dt, warp, out12);
+}
+// full 12 x 25 block from the four slices
+void dh_joint_jacobian(int law, const double* prm, const double* pa, const double* pb, const double* va, const double* vb,
+                       double dt, double warp, double* out300) {
+  for (int s = 0; s < 4; ++s) {
+    double v[6], d[36];
+    exg::joint_jacobian_slice<double>(law, prm, pa, pb, va, vb, dt, warp, s, v, d);
+    for (int r = 0; r < 6; ++r) {
+      out300[r * 25] = v[r];
+      out300[(6 + r) * 25] = -v[r];
+      for (int c = 0; c < 6; ++c) {
+        out300[r * 25 + 1 + 6 * s + c] = d[r * 6 + c];
+        out300[(6 + r) * 25 + 1 + 6 * s + c] = -d[r * 6 + c];
+      }
+    }
+  }
+}
+void dh_twist_exp(const double* t6, double dt, double* m8) { double b[6]; exg::screw_from6(t6, b); exg::twist_exp(b, dt, m8); }
+void dh_motor_compose(const double* a, const double* b, double* o) { exg::motor_compose(a, b, o); }
+void dh_apply_point(const double* m8, const double* p3, double* o3) { double p[4]; exg::anchor_point(m8, p3, p); exg::point_coords(p, o3); }
+void dh_transport(const double* t6, const double* m8, int co, double* o6) {
+  double b[6], r[6]; exg::screw_from6(t6, b);
+  if (co) exg::wrench_transport(b, m8, r); else exg::twist_transport(b, m8, r);
+  exg::screw_to6(r, o6);
+}
+double dh_power(const double* w6, const double* t6) { double w[6], t[6]; exg::screw_from6(w6, w); exg::screw_from6(t6, t); return exg::screw_power(w, t); }
+void dh_coad(const double* w6, const double* t6, double* o6) {
+  double w[6], t[6], r[6]; exg::screw_from6(w6, w); exg::screw_from6(t6, t); exg::coad_bracket(w, t, r); exg::screw_to6(r, o6);
+}
+void dh_rotation_part(const double* m8, double* o8) { exg::motor_rotation_part(m8, o8); }
+}

@@ -1,0 +1,318 @@
+"""Benchmark of the per-step dynamics path on B200.
+
+`python bench.py --gpus N --steps K --warmup W [--impl ours|reference] [--workload c0|c1|c2]`
+
+A step is one Mechanism::step of the whole workload (every body advanced by dt). `value` is
+body-steps/s from CUDA events on the library's stream with the state resident in HBM; `e2e` is the
+same metric through the public API with host buffers (the step's inputs copied in from host
+memory and its result read back inside the timed region). Under torchrun each rank steps its own
+replica of the workload (independent worlds: weak scaling, no collective in the data path); the
+timing is the max over ranks.
+
+--impl reference times the reference algorithm's CPU implementation on the host cores. The
+reference (a Rust/Vulkan workspace) cannot be built here, so that arm runs the C++ f64
+restatement of its functions (`cpu_baseline.kind = "port"`).
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from exgame_b200 import _lib, scenarios  # noqa: E402
+from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON  # noqa: E402
+
+METRIC = "body-steps/s"
+FP64_FMA_PER_SM_CLK = 64
+FP32_FMA_PER_SM_CLK = 128
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def workload(name, rank):
+    """(label, list of (bodies, joints, params) parts, config dict)"""
+    if name == "c0":
+        b, j, p, _ = scenarios.config0(seed=rank)
+        cfg = {"workload": "1024 point masses, Plummer eps 0.05, LieEuler, dt 1e-3, f64 (config 0)",
+               "bodies": 1024, "dtype": "f64"}
+        return [(b, j, p)], cfg
+    if name == "c1":
+        b, j, p, _ = scenarios.config1(seed=1 + rank)
+        cfg = {"workload": "256-body box chain, 765 joints, implicit Newton tol 1e-10, dt 1e-2, f64 (config 1)",
+               "bodies": 256, "dtype": "f64"}
+        return [(b, j, p)], cfg
+    if name == "c2":
+        (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(seed=2 + rank)
+        cfg = {"workload": "65,536-body gravity (ball R 1000, LieEuler) + 16 x 256-body chains (Newton tol 1e-10), "
+                           "dt 1e-3, f64 (config 2)", "bodies": len(gb) + len(cb), "dtype": "f64"}
+        return [(gb, gj, gp), (cb, cj, cp)], cfg
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [x.strip() for x in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def time_steps(dev, worlds, steps, flush):
+    """Per-step device time (CUDA events on the library stream), L2 flushed between steps."""
+    import torch
+    stream = torch.cuda.ExternalStream(dev.stream())
+    total = 0.0
+    for _ in range(steps):
+        flush()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for w in worlds:
+            w.step(1)
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b) / 1e3
+    return total
+
+
+def dominant_kernel(cfg_name, worlds, parts):
+    """(profile kind, algorithmic flops per launch, bound, label)"""
+    if cfg_name in ("c0", "c2"):
+        n = len(parts[0][0])
+        return 0, 20.0 * n * n, "fp64", f"all-pairs gravity, {n} bodies (20 flop per directed pair)"
+    return 3, None, "fp64", "Newton island step"
+
+
+def run_ours(args, rank, world_size, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = _lib.Device(local_rank)
+    parts, cfg = workload(args.workload, rank)
+    worlds = [_lib.DeviceWorld(dev, b, j, p) for (b, j, p) in parts]
+    n_bodies = sum(len(b) for (b, _, _) in parts)
+    flush_buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def flush():
+        flush_buf.zero_()
+
+    for _ in range(args.warmup):
+        for w in worlds:
+            w.step(1)
+    dev.synchronize()
+    if world_size > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = dev.kernel_launches()
+    with ClockSampler(local_rank) as clk:
+        t_dev = time_steps(dev, worlds, args.steps, flush)
+    launches = dev.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    t = t_dev
+    if world_size > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+        dist.barrier()
+    value = n_bodies * args.steps * world_size / t
+
+    # end to end through the public API: host state in, step, host state out
+    host_in = [np.ascontiguousarray(w.bodies()) for w in worlds]
+    h2d = sum(h.nbytes for h in host_in)
+    dev.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for w, h in zip(worlds, host_in):
+            w.set_bodies(h)
+            w.step(1)
+            h[...] = w.bodies()
+    dev.synchronize()
+    t_e2e = time.perf_counter() - t0
+    if world_size > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = {"value": n_bodies * args.steps * world_size / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(h2d)}
+
+    # dominant kernel, timed live with events on the library stream over a profiled pass
+    kind, flops, bound, label = dominant_kernel(args.workload, worlds, parts)
+    dev.profile(True)
+    for _ in range(args.steps):
+        for w in worlds:
+            w.step(1)
+    ms, nl = dev.profile_read(kind)
+    dev.profile(False)
+    peaks, src = load_peaks()
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    per_clk = FP64_FMA_PER_SM_CLK if bound == "fp64" else FP32_FMA_PER_SM_CLK
+    peak_tflops = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
+    roofline = None
+    if flops and nl:
+        avg_s = ms / 1e3 / nl
+        achieved = flops / avg_s / 1e12
+        roofline = {"bound": bound, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                    "frac": achieved / peak_tflops, "traffic": None, "kernel": label,
+                    "avg_launch_us": avg_s * 1e6, "launches": nl,
+                    "peak_source": f"nominal {per_clk} {bound.upper()} FMA/clk/SM x {sms} SMs at the {src} "
+                                   f"max SM clock {sm_mhz:.0f} MHz (no tensor-core or copy peak applies)"}
+    elif nl:
+        roofline = {"bound": bound, "achieved": None, "peak": peak_tflops, "unit": "TFLOP/s", "frac": None,
+                    "traffic": None, "kernel": label, "avg_launch_us": ms / nl * 1e3, "launches": nl}
+    return {
+        "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
+        "clocks": clk.summary(), "n_bodies": n_bodies,
+    }
+
+
+def cpu_baseline(args, threads):
+    """The oracle (C++ f64 restatement) on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    L = oracle_lib.lib()
+    L.orc_set_threads(int(threads))
+    parts, cfg = workload(args.workload, 0)
+    worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
+    n = sum(w.n for w in worlds)
+    budget = args.cpu_seconds
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        for w in worlds:
+            w.step(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget or steps >= 100000:
+            break
+    return {"value": n * steps / el, "unit": METRIC, "cores": int(threads), "kind": "port",
+            "sample": f"{steps} steps of the same workload ({n} bodies) on {threads} host thread(s), {el:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c0", choices=["c0", "c1", "c2"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        oracle_lib.lib().orc_set_threads(threads)
+        parts, cfg = workload(args.workload, 0)
+        worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
+        n = sum(w.n for w in worlds)
+        for _ in range(args.warmup):
+            for w in worlds:
+                w.step(1)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for w in worlds:
+                w.step(1)
+        el = time.perf_counter() - t0
+        v = n * args.steps / el
+        line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": cfg["dtype"],
+                "data": "synthetic (seeded; the reference publishes no dataset)", "config": cfg,
+                "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                                 "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps, {n} bodies"},
+                "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world_size > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    r = run_ours(args, rank, world_size, local_rank)
+    cpu = cpu_baseline(args, 1) if rank == 0 and world_size == 1 else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["t"] / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": r["cfg"]["dtype"],
+            "data": "synthetic (seeded; the reference publishes no dataset)",
+            "config": dict(r["cfg"], parallelism=f"replicas x{world_size} (independent worlds)",
+                           l2="flushed between timed steps (256 MB write)"),
+            "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
+            "clocks": r["clocks"],
+        }
+        print(json.dumps(line))
+    if world_size > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

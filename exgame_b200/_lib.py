@@ -1,0 +1,229 @@
+"""ctypes binding of libexg.so (include/exg.h).
+
+The library is built in-tree (exgame_b200/libexg.so). Loading fails loudly when it is missing:
+there is no CPU fallback for the compute path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .abi import BODY_DTYPE, JOINT_DTYPE, STEP_PARAMS_DTYPE, WORLD_STATS_DTYPE
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libexg.so")
+
+EXG_OK = 0
+STATUS_NAMES = {
+    0: "EXG_OK", -1: "EXG_ERR_NO_SHADER", -2: "EXG_ERR_TRAP", -3: "EXG_ERR_FATAL", -4: "EXG_ERR_WORKER_GONE",
+    -5: "EXG_ERR_BACKEND", -10: "EXG_ERR_EPOCH_IN_PROGRESS", -11: "EXG_ERR_ALREADY_OWNED",
+    -12: "EXG_ERR_FOREIGN_ACCELERATOR", -13: "EXG_ERR_DUPLICATE_MECHANISM", -20: "EXG_ERR_INVALID_ARGUMENT",
+    -21: "EXG_ERR_OUT_OF_MEMORY", -22: "EXG_ERR_UNSUPPORTED", -23: "EXG_ERR_TIMEOUT", -24: "EXG_ERR_NO_DEVICE",
+}
+
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes); every symbol declared in include/exg.h
+SIGNATURES = {
+    "exg_abi_version": (ctypes.c_int, []),
+    "exg_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "exg_device_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(_vp)]),
+    "exg_device_destroy": (ctypes.c_int, [_vp]),
+    "exg_device_synchronize": (ctypes.c_int, [_vp]),
+    "exg_device_kernel_launches": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
+    "exg_device_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
+    "exg_device_profile": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "exg_device_profile_read": (ctypes.c_int, [_vp, ctypes.c_int32, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "exg_law_lookup": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+    "exg_world_create": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, ctypes.c_int32, _vp, ctypes.POINTER(_vp)]),
+    "exg_world_destroy": (ctypes.c_int, [_vp]),
+    "exg_world_step": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "exg_world_get_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
+    "exg_world_set_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
+    "exg_world_stats": (ctypes.c_int, [_vp, _vp]),
+    "exg_world_energy": (ctypes.c_int, [_vp, _c_double_p]),
+    "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
+    "exg_motor_compose": (ctypes.c_int, [_vp, _vp, _vp]),
+    "exg_motor_inverse": (ctypes.c_int, [_vp, _vp]),
+    "exg_motor_apply_point": (ctypes.c_int, [_vp, _vp, _vp]),
+    "exg_screw_transport": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "exg_eval_joints": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int32, _vp]),
+    "exg_gravity_forces": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int32, _vp]),
+}
+
+
+class ExgError(RuntimeError):
+    """A non-zero status from the C ABI (EvalError / StructureError of the reference)."""
+
+    def __init__(self, status, where=""):
+        self.status = status
+        self.name = STATUS_NAMES.get(status, str(status))
+        msg = lib().exg_status_string(status).decode() if _LIB is not None else ""
+        super().__init__(f"{where}: {self.name} ({msg})" if where else f"{self.name} ({msg})")
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libexg.so is not built ({LIB_PATH}); run `python -m exgame_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(status, where=""):
+    if status != EXG_OK:
+        raise ExgError(status, where)
+
+
+def ptr(a):
+    # data_as keeps a reference to the array, so temporaries outlive the call
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else ctypes.c_void_p(0)
+
+
+def motor_exp(twist, dt=1.0):
+    t = np.ascontiguousarray(twist, dtype=np.float64)
+    out = np.zeros(8)
+    check(lib().exg_motor_exp(ptr(t), float(dt), ptr(out)), "exg_motor_exp")
+    return out
+
+
+def motor_compose(a, b):
+    """'first a, then b' (Motor::compose)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros(8)
+    check(lib().exg_motor_compose(ptr(a), ptr(b), ptr(out)), "exg_motor_compose")
+    return out
+
+
+def motor_inverse(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = np.zeros(8)
+    check(lib().exg_motor_inverse(ptr(a), ptr(out)), "exg_motor_inverse")
+    return out
+
+
+def motor_apply_point(m, p):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    out = np.zeros(3)
+    check(lib().exg_motor_apply_point(ptr(m), ptr(p), ptr(out)), "exg_motor_apply_point")
+    return out
+
+
+def screw_transport(s, m, covariant):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    out = np.zeros(6)
+    check(lib().exg_screw_transport(ptr(s), ptr(m), int(covariant), ptr(out)), "exg_screw_transport")
+    return out
+
+
+def law_lookup(name):
+    law = ctypes.c_int32()
+    n = ctypes.c_int32()
+    check(lib().exg_law_lookup(name.encode(), ctypes.byref(law), ctypes.byref(n)), f"exg_law_lookup({name})")
+    return law.value, n.value
+
+
+class Device:
+    """A CUDA device context (replaces the reference's GpuAccelerator::new)."""
+
+    def __init__(self, ordinal=0):
+        h = ctypes.c_void_p()
+        check(lib().exg_device_create(int(ordinal), ctypes.byref(h)), "exg_device_create")
+        self.handle = h
+        self.ordinal = ordinal
+
+    def kernel_launches(self):
+        v = ctypes.c_uint64()
+        check(lib().exg_device_kernel_launches(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        check(lib().exg_device_synchronize(self.handle))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        check(lib().exg_device_stream(self.handle, ctypes.byref(s)))
+        return s.value
+
+    def profile(self, enable):
+        check(lib().exg_device_profile(self.handle, int(bool(enable))))
+
+    PROF_GRAVITY, PROF_JOINTS, PROF_INTEGRATE, PROF_NEWTON, PROF_BODY_PRE = 0, 1, 2, 3, 4
+
+    def profile_read(self, kind):
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        check(lib().exg_device_profile_read(self.handle, int(kind), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def close(self):
+        if self.handle:
+            lib().exg_device_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceWorld:
+    """A device-resident world of bodies and joints stepped by the CUDA path."""
+
+    def __init__(self, device, bodies, joints, params):
+        self.device = device
+        self.bodies_host = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        self.joints_host = np.ascontiguousarray(joints, dtype=JOINT_DTYPE)
+        self.params = np.ascontiguousarray(params, dtype=STEP_PARAMS_DTYPE).reshape(())
+        h = ctypes.c_void_p()
+        check(lib().exg_world_create(device.handle, ptr(self.bodies_host), len(self.bodies_host), ptr(self.joints_host),
+                                     len(self.joints_host), ptr(self.params), ctypes.byref(h)), "exg_world_create")
+        self.handle = h
+        self.n = len(self.bodies_host)
+
+    def step(self, n_steps=1):
+        check(lib().exg_world_step(self.handle, int(n_steps)), "exg_world_step")
+
+    def bodies(self):
+        out = np.zeros(self.n, dtype=BODY_DTYPE)
+        check(lib().exg_world_get_bodies(self.handle, ptr(out), self.n), "exg_world_get_bodies")
+        return out
+
+    def set_bodies(self, bodies):
+        b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        check(lib().exg_world_set_bodies(self.handle, ptr(b), len(b)), "exg_world_set_bodies")
+
+    def stats(self):
+        s = np.zeros((), dtype=WORLD_STATS_DTYPE)
+        check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
+        return s
+
+    def energy(self):
+        e = ctypes.c_double()
+        check(lib().exg_world_energy(self.handle, ctypes.byref(e)), "exg_world_energy")
+        return e.value
+
+    def close(self):
+        if self.handle:
+            lib().exg_world_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

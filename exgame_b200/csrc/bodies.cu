@@ -1,0 +1,151 @@
+// Per-body kernels of the explicit step (crates/newton/src/integrator/implicit/bridge.rs:19-63):
+//   k_body_pre:          position + mass (gravity charge) and world twist of every body;
+//   k_integrate_explicit: gather of the world wrench (gravity + incident joint wrenches in the
+//                        reference's term order), pull-back to the body frame and one step of
+//                        ExplicitEuler / SymplecticEuler / LieEuler (integrator/explicit/*.rs).
+// Poses and momenta stay FP64 in every precision mode.
+#include "exg_internal.cuh"
+#include "body.cuh"
+
+namespace {
+
+using namespace exg;
+
+__global__ void k_body_pre(BodyView b, double* __restrict__ pos_mass, double* __restrict__ wvel) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.n) return;
+  double pose[8], mom[6], I9[9];
+  load_body(b, i, pose, mom, I9);
+  bool kin = b.kinematic[i] != 0;
+  double p3[3];
+  body_position(pose, p3);
+  double4 pm = make_double4(p3[0], p3[1], p3[2], kin ? 0.0 : b.mass[i]);
+  reinterpret_cast<double4*>(pos_mass)[i] = pm;
+  double wv[6];
+  world_velocity(pose, mom, I9, b.diagonal[i] != 0, kin, b.mass[i], wv);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) wvel[(size_t)c * b.n + i] = wv[c];
+}
+
+template <int SCHEME>
+__global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, double* __restrict__ mom_out,
+                                     const double* __restrict__ pos_mass, const double* __restrict__ grav_partial,
+                                     int splits, int gravity_on, double G, const double* __restrict__ conn, int nj,
+                                     const int* __restrict__ inc_ptr, const int* __restrict__ inc_ref, double dt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b.n) return;
+  if (b.kinematic[i]) return;
+  double pose[8], mom[6], I9[9];
+  load_body(b, i, pose, mom, I9);
+  const bool diag = b.diagonal[i] != 0;
+  const double mass = b.mass[i];
+  // world wrench: gravity (F, p x F) then incident joint wrenches in joint order
+  double tot[6] = {0, 0, 0, 0, 0, 0};
+  if (gravity_on) {
+    double4 pm = reinterpret_cast<const double4*>(pos_mass)[i];
+    double f[3];
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+      for (int s = 0; s < splits; ++s) acc += grav_partial[(size_t)s * 3 * b.n + (size_t)c * b.n + i];
+      f[c] = G * pm.w * acc;
+    }
+    tot[0] = f[0]; tot[1] = f[1]; tot[2] = f[2];
+    tot[3] = pm.y * f[2] - pm.z * f[1];
+    tot[4] = pm.z * f[0] - pm.x * f[2];
+    tot[5] = pm.x * f[1] - pm.y * f[0];
+  }
+  for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; ++q) {
+    int ref = inc_ref[q];
+    int k = ref >> 1, end = ref & 1;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) tot[c] += conn[(size_t)(end * 6 + c) * nj + k];
+  }
+  // pull back to the body frame: transport(pose^-1) under the Co law
+  double wb[6], wbody[6], rev[8], tmp[6];
+  screw_from6(tot, wb);
+  motor_reverse(pose, rev);
+  wrench_transport(wb, rev, tmp);
+  screw_to6(tmp, wbody);
+  if (SCHEME == EXG_LIE_EULER) {  // lie_euler.rs:31-55
+#pragma unroll
+    for (int c = 0; c < 6; ++c) mom[c] += wbody[c] * dt;
+    double v6[6], vb[6], delta[8], drot[8], drot_inv[8], mb[6], mt[6];
+    inertia_inverse(I9, diag, false, mass, mom, v6);
+    screw_from6(v6, vb);
+    twist_exp(vb, dt, delta);
+    motor_rotation_part(delta, drot);
+    motor_reverse(drot, drot_inv);
+    screw_from6(mom, mb);
+    wrench_transport(mb, drot_inv, mt);
+    screw_to6(mt, mom);
+    double np[8];
+    motor_compose(delta, pose, np);  // pose * delta
+#pragma unroll
+    for (int c = 0; c < 8; ++c) pose[c] = np[c];
+  } else {
+    double v6[6], vb[6], mb[6], gy[6], gyro[6];
+    inertia_inverse(I9, diag, false, mass, mom, v6);
+    screw_from6(v6, vb);
+    screw_from6(mom, mb);
+    coad_bracket(mb, vb, gy);
+    screw_to6(gy, gyro);  // gyroscopic = -coad_bracket (body.rs:170-175)
+    if (SCHEME == EXG_SYMPLECTIC_EULER) {  // symplectic_euler.rs:26-41
+#pragma unroll
+      for (int c = 0; c < 6; ++c) mom[c] += (wbody[c] - gyro[c]) * dt;
+      inertia_inverse(I9, diag, false, mass, mom, v6);
+      screw_from6(v6, vb);
+    } else {  // explicit_euler.rs:21-33: the pose moves with the OLD velocity
+#pragma unroll
+      for (int c = 0; c < 6; ++c) mom[c] += (wbody[c] - gyro[c]) * dt;
+    }
+    double e[8], np[8];
+    twist_exp(vb, dt, e);
+    motor_compose(e, pose, np);  // pose * exp
+#pragma unroll
+    for (int c = 0; c < 8; ++c) pose[c] = np[c];
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) pose_out[(size_t)c * b.n + i] = pose[c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) mom_out[(size_t)c * b.n + i] = mom[c];
+}
+
+BodyView view_of(const DeviceWorld& w) {
+  return BodyView{w.pose, w.mom, w.mass, w.inertia, w.kinematic, w.diagonal, w.n};
+}
+
+}  // namespace
+
+int launch_body_pre(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
+  if (w.n <= 0) return EXG_OK;
+  int _tok = prof_begin(dev, PROF_BODY_PRE, s);
+  k_body_pre<<<(w.n + 127) / 128, 128, 0, s>>>(view_of(w), w.pos_mass, w.wvel);
+  prof_end(dev, _tok, s);
+  return exg_after_launch(dev);
+}
+
+int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, int scheme, int gravity_on, double G, double dt,
+                              cudaStream_t s) {
+  if (w.n <= 0) return EXG_OK;
+  dim3 grid((w.n + 127) / 128);
+  BodyView v = view_of(w);
+  int _tok = prof_begin(dev, PROF_INTEGRATE, s);
+  switch (scheme) {
+    case EXG_LIE_EULER:
+      k_integrate_explicit<EXG_LIE_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial, w.grav_splits,
+                                                                gravity_on, G, w.conn, w.nj, w.inc_ptr, w.inc_ref, dt);
+      break;
+    case EXG_SYMPLECTIC_EULER:
+      k_integrate_explicit<EXG_SYMPLECTIC_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial,
+                                                                       w.grav_splits, gravity_on, G, w.conn, w.nj,
+                                                                       w.inc_ptr, w.inc_ref, dt);
+      break;
+    default:
+      k_integrate_explicit<EXG_EXPLICIT_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial,
+                                                                     w.grav_splits, gravity_on, G, w.conn, w.nj,
+                                                                     w.inc_ptr, w.inc_ref, dt);
+      break;
+  }
+  prof_end(dev, _tok, s);
+  return exg_after_launch(dev);
+}

@@ -1,0 +1,982 @@
+// Implicit mid-point Newton step on the device; see world_newton.cuh for the structure.
+//
+// Per island, one CTA executes Newton::solve_step (crates/newton/src/integrator/implicit/newton.rs:543-683):
+//   span loop over dt / 2^depth (MAX_DEPTH 8, the log2 stiffness signal moves the depth),
+//   newton_solve (:334-530): up to max_newton iterations of
+//     PRE (functions::pre) -> joint value + Jacobian -> gather + POST (functions::body_post)
+//     -> worst relative residual (:139-151) -> assembly (rows/assemble.rs) -> linear solve
+//     -> backtracking line search over the fractions 1, 1/2, ..., 1/128, first decrease wins
+//   commit_span (:708-753): M = M0 * exp(span v), P = 2 P_mid - P_n (implicit Euler if the span
+//   did not converge).
+// The linear solve is exact block elimination on the island's tree (leaves to root, then back
+// substitution) instead of the reference's dense Newton-Schulz iteration on m^2 blocks: both
+// solve the same Newton system, so the converged iterate is the same; the tree solve is O(m).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <new>
+#include "body.cuh"
+#include "joint_eval.cuh"
+#include "world_newton.cuh"
+
+namespace {
+
+using namespace exg;
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxDepth = 8;
+constexpr int kThresholdLog2 = 8;
+constexpr int kPerHalvingLog2 = 4;
+constexpr double kHuge = 1e9;
+constexpr double kFloor2 = 1e-9 * 1e-9;
+constexpr int kJacStride = 42;  // per (joint, slice): value[6] + d[36]
+
+struct Scratch {
+  double *vm, *base, *best, *trial, *mid, *snap, *ext, *conn, *jac, *mass, *mass0, *rhs, *scale, *D, *Dinv, *Acp, *Apc, *S,
+      *bvec, *dv;
+};
+
+EXG_HD long long scratch_doubles(int nb, int nj, int m) {
+  return (long long)nb * (6 * 4 + 8 + 6 * 2) + (long long)nj * (6 + 4 * kJacStride) + (long long)m * (36 * 7 + 6 * 3 + 2);
+}
+
+__device__ Scratch carve(double* p, int nb, int nj, int m) {
+  Scratch s;
+  s.vm = p; p += nb * 6;
+  s.base = p; p += nb * 6;
+  s.best = p; p += nb * 6;
+  s.trial = p; p += nb * 6;
+  s.mid = p; p += nb * 8;
+  s.snap = p; p += nb * 6;
+  s.ext = p; p += nb * 6;
+  s.conn = p; p += (size_t)nj * 6;
+  s.jac = p; p += (size_t)nj * 4 * kJacStride;
+  s.mass = p; p += (size_t)m * 36;
+  s.mass0 = p; p += (size_t)m * 36;
+  s.rhs = p; p += (size_t)m * 6;
+  s.scale = p; p += (size_t)m * 2;
+  s.D = p; p += (size_t)m * 36;
+  s.Dinv = p; p += (size_t)m * 36;
+  s.Acp = p; p += (size_t)m * 36;
+  s.Apc = p; p += (size_t)m * 36;
+  s.S = p; p += (size_t)m * 36;
+  s.bvec = p; p += (size_t)m * 6;
+  s.dv = p; p += (size_t)m * 6;
+  return s;
+}
+
+struct WorldRef {
+  double* pose;
+  double* mom;
+  const double* mass;
+  const double* inertia;
+  const int* kinematic;
+  const int* diagonal;
+  const double* pos_mass;
+  const double* grav_partial;
+  int n, splits, gravity_on;
+  double G, dt, warp, tol2;
+  int max_newton;
+};
+
+struct Ctx {
+  NewtonDeviceArrays A;
+  IslandDesc d;
+  WorldRef W;
+  Scratch s;
+  int island;
+  EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
+};
+
+// ── block-wide reductions ───────────────────────────────────────────────────
+__device__ double nan_max(double a, double b) {
+  if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000ULL);
+  return a > b ? a : b;
+}
+__device__ double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = red[0];
+  for (int k = 1; k < kWarps; ++k) r = nan_max(r, red[k]);
+  __syncthreads();
+  return r;
+}
+__device__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = red[0];
+  for (int k = 1; k < kWarps; ++k) r += red[k];
+  __syncthreads();
+  return r;
+}
+
+// ── phases ──────────────────────────────────────────────────────────────────
+// PRE: mid = exp(half/2 v) * pose for every island body (functions::pre)
+__device__ void phase_pre(const Ctx& c, const double* v, double half) {
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
+    int g = c.gbody(q);
+    double pose[8], vb[6], e[8], m[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+    screw_from6(v + 6 * q, vb);
+    twist_exp(vb, half, e);
+    motor_compose(pose, e, m);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c.s.mid[8 * q + k] = m[k];
+  }
+}
+
+// Joint values (and Jacobian slices) at (mid, v): conn[q] = wrench on end a.
+__device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
+  const int nj = c.d.nj;
+  const int joff = c.d.joint_off;
+  if (jac) {
+    for (int t = threadIdx.x; t < 4 * nj; t += blockDim.x) {
+      int q = t >> 2, slice = t & 3;
+      int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
+      double val[6], dd[36];
+      joint_jacobian_slice<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a,
+                                   c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.W.dt, c.W.warp, slice, val, dd);
+      double* o = c.s.jac + ((size_t)q * 4 + slice) * kJacStride;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) o[r] = val[r];
+#pragma unroll
+      for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+      if (slice == 0) {
+#pragma unroll
+        for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
+      }
+    }
+  } else {
+    for (int q = threadIdx.x; q < nj; q += blockDim.x) {
+      int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
+      double out[12];
+      joint_plain<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a, c.s.mid + 8 * b,
+                          v + 6 * a, v + 6 * b, c.W.dt, c.W.warp, out);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
+    }
+  }
+}
+
+// Gather + POST for every dynamic node; returns the worst relative residual^2 (newton.rs:139-151).
+__device__ double phase_post(const Ctx& c, const double* v, double half, double* red) {
+  double worst = 0.0;
+  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) {
+    int q = c.A.dn_body[c.d.dyn_off + i];
+    int g = c.gbody(q);
+    double tot[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) tot[k] = c.s.ext[6 * q + k];
+    int p0 = c.A.ib_inc_ptr[c.d.inc_off + q], p1 = c.A.ib_inc_ptr[c.d.inc_off + q + 1];
+    for (int t = p0; t < p1; ++t) {
+      int ref = c.A.ib_inc_ref[t];
+      int jq = ref >> 1;
+      if (ref & 1) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tot[k] = tot[k] - c.s.conn[6 * jq + k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tot[k] = tot[k] + c.s.conn[6 * jq + k];
+      }
+    }
+    double I9[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+    const bool diag = c.W.diagonal[g] != 0;
+    const double mass = c.W.mass[g];
+    const double* mid = c.s.mid + 8 * q;
+    double inv[8];
+    motor_reverse(mid, inv);
+    double* blk = c.s.mass + 36 * (size_t)i;
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+      double e6[6] = {0, 0, 0, 0, 0, 0};
+      e6[col] = 1.0;
+      double eb[6], ebody[6], b6[6], wv[6], p6[6], pb[6], cw[6], c6[6];
+      screw_from6(e6, eb);
+      twist_transport(eb, inv, ebody);
+      screw_to6(ebody, b6);
+      wv[0] = b6[0]; wv[1] = b6[1]; wv[2] = b6[2]; wv[3] = b6[3]; wv[4] = b6[4]; wv[5] = b6[5];
+      inertia_apply(I9, diag, false, mass, wv, p6);
+      screw_from6(p6, pb);
+      wrench_transport(pb, mid, cw);
+      screw_to6(cw, c6);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) blk[r * 6 + col] = c6[r];
+    }
+    const double* vv = v + 6 * q;
+    double p[6], nn[6], hh[6], res[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) acc += blk[r * 6 + k] * vv[k];
+      p[r] = acc;
+      nn[r] = c.s.snap[6 * q + r];
+      hh[r] = tot[r] * half;
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) res[r] = -(p[r] - nn[r] - hh[r]);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) c.s.rhs[6 * i + r] = res[r];
+    auto sq3 = [](const double* x) { return x[0] * x[0] + x[1] * x[1] + x[2] * x[2]; };
+    double lin = fmax(fmax(fmax(sq3(p), sq3(nn)), sq3(hh)), kFloor2);
+    double ang = fmax(fmax(fmax(sq3(p + 3), sq3(nn + 3)), sq3(hh + 3)), kFloor2);
+    c.s.scale[2 * i] = lin;
+    c.s.scale[2 * i + 1] = ang;
+    worst = nan_max(worst, sq3(res) / lin);
+    worst = nan_max(worst, sq3(res + 3) / ang);
+  }
+  return block_max(worst, red);
+}
+
+__device__ void copy_mass0(const Ctx& c) {
+  for (int t = threadIdx.x; t < 36 * c.d.m; t += blockDim.x) c.s.mass0[t] = c.s.mass[t];
+}
+
+// Assembly (rows/assemble.rs, functions::assemble_term): per target block and entry, the
+// mass block (diagonal only) then every contributing joint end in joint order with the
+// midpoint factors pf = -half^2 on pose columns and vf = -half on velocity columns.
+// Returns ||A||_F^2.
+__device__ double phase_assemble(const Ctx& c, double half, double* red) {
+  const double pf = -(half * half), vf = -half;
+  double sumsq = 0.0;
+  const int cells = 3 * c.d.m;
+  for (int t = threadIdx.x; t < cells * 36; t += blockDim.x) {
+    int cell = t / 36, e = t % 36;
+    int i = cell / 3, kind = cell % 3;
+    int r = e / 6, col = e % 6;
+    double acc = (kind == 0) ? c.s.mass0[36 * (size_t)i + e] : 0.0;
+    int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+    for (int k = p0; k < p1; ++k) {
+      int term = c.A.cell_terms[k];
+      int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
+      const double* jp = c.s.jac + ((size_t)q * 4 + ce) * kJacStride + 6;
+      const double* jv = c.s.jac + ((size_t)q * 4 + 2 + ce) * kJacStride + 6;
+      double pv = jp[r * 6 + col], vv = jv[r * 6 + col];
+      if (re) { pv = -pv; vv = -vv; }
+      acc = acc + pf * pv + vf * vv;
+    }
+    double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
+    dst[36 * (size_t)i + e] = acc;
+    if (kind == 0 || c.A.dn_parent[c.d.dyn_off + i] >= 0) sumsq += acc * acc;
+  }
+  return block_sum(sumsq, red);
+}
+
+// Warp-cooperative 6x6 inverse by Gauss-Jordan with partial pivoting: lane c < 12 holds
+// column c of [A | I]. Returns false (to every lane) if a pivot is zero or not finite.
+__device__ bool warp_inverse6(const double* a, double* out) {
+  const int lane = threadIdx.x & 31;
+  double col[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    if (lane < 6) col[r] = a[r * 6 + lane];
+    else col[r] = (lane - 6 == r) ? 1.0 : 0.0;
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(col[k]);
+#pragma unroll
+    for (int r = k + 1; r < 6; ++r) {
+      double x = fabs(col[r]);
+      if (x > best) { best = x; piv = r; }
+    }
+    piv = __shfl_sync(0xffffffffu, piv, k);
+    double tk = col[k], tp = col[k];
+#pragma unroll
+    for (int r = k; r < 6; ++r) if (r == piv) tp = col[r];
+#pragma unroll
+    for (int r = k; r < 6; ++r) if (r == piv) col[r] = tk;
+    col[k] = tp;
+    double pv = __shfl_sync(0xffffffffu, col[k], k);
+    if (!(fabs(pv) > 0.0) || !isfinite(pv)) ok = false;
+    double ip = 1.0 / pv;
+    col[k] = col[k] * ip;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r == k) continue;
+      double f = __shfl_sync(0xffffffffu, col[r], k);
+      col[r] = col[r] - f * col[k];
+    }
+  }
+  if (lane >= 6 && lane < 12) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) out[r * 6 + (lane - 6)] = col[r];
+  }
+  __syncwarp();
+  return ok;
+}
+
+// C = A * B (6x6, row-major) or C -= A * B, computed by one warp.
+template <bool Sub>
+__device__ void warp_mm6(const double* A, const double* B, double* C) {
+  const int lane = threadIdx.x & 31;
+  double v0 = 0.0, v1 = 0.0;
+  int e0 = lane, e1 = lane + 32;
+  {
+    int r = e0 / 6, cc = e0 % 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v0 += A[r * 6 + k] * B[k * 6 + cc];
+  }
+  if (e1 < 36) {
+    int r = e1 / 6, cc = e1 % 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v1 += A[r * 6 + k] * B[k * 6 + cc];
+  }
+  __syncwarp();
+  if (Sub) {
+    C[e0] = C[e0] - v0;
+    if (e1 < 36) C[e1] = C[e1] - v1;
+  } else {
+    C[e0] = v0;
+    if (e1 < 36) C[e1] = v1;
+  }
+  __syncwarp();
+}
+// y -= A x (6x6 * 6) by one warp (lanes 0..5)
+__device__ void warp_mv6_sub(const double* A, const double* x, double* y) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  if (lane < 6) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
+  }
+  __syncwarp();
+  if (lane < 6) y[lane] = y[lane] - s;
+  __syncwarp();
+}
+__device__ void warp_mv6(const double* A, const double* x, double* y) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  if (lane < 6) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
+  }
+  __syncwarp();
+  if (lane < 6) y[lane] = s;
+  __syncwarp();
+}
+
+// Exact solve of A dv = rhs on the island's elimination forest. Returns false if a pivot
+// block is singular (dv is then NaN, which the line search rejects).
+__device__ bool phase_solve(const Ctx& c, int* flag) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = c.d.m;
+  const int* lv = c.A.lv_ptr + c.d.lv_off;
+  const int* nodes = c.A.lv_nodes + c.d.dyn_off;
+  const int* par = c.A.dn_parent + c.d.dyn_off;
+  const int* chp = c.A.ch_ptr + c.d.dyn_off;  // absolute offsets into ch_idx
+  const int* chi = c.A.ch_idx;
+  if (threadIdx.x == 0) *flag = 1;
+  for (int t = threadIdx.x; t < 6 * m; t += blockDim.x) c.s.bvec[t] = c.s.rhs[t];
+  __syncthreads();
+  for (int L = c.d.n_levels - 1; L >= 1; --L) {
+    for (int k = lv[L] + warp; k < lv[L + 1]; k += kWarps) {
+      int i = nodes[k];
+      bool ok = warp_inverse6(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i);
+      if (!ok && lane == 0) *flag = 0;
+      warp_mm6<false>(c.s.Apc + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i, c.s.S + 36 * (size_t)i);
+    }
+    __syncthreads();
+    for (int k = lv[L - 1] + warp; k < lv[L]; k += kWarps) {
+      int p = nodes[k];
+      for (int t = chp[p]; t < chp[p + 1]; ++t) {
+        int ch = chi[t];
+        warp_mm6<true>(c.s.S + 36 * (size_t)ch, c.s.Acp + 36 * (size_t)ch, c.s.D + 36 * (size_t)p);
+        warp_mv6_sub(c.s.S + 36 * (size_t)ch, c.s.bvec + 6 * ch, c.s.bvec + 6 * p);
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = lv[0] + warp; k < lv[1]; k += kWarps) {
+    int i = nodes[k];
+    bool ok = warp_inverse6(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i);
+    if (!ok && lane == 0) *flag = 0;
+    warp_mv6(c.s.Dinv + 36 * (size_t)i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+  }
+  __syncthreads();
+  for (int L = 1; L < c.d.n_levels; ++L) {
+    for (int k = lv[L] + warp; k < lv[L + 1]; k += kWarps) {
+      int i = nodes[k];
+      int p = par[i];
+      warp_mv6_sub(c.s.Acp + 36 * (size_t)i, c.s.dv + 6 * p, c.s.bvec + 6 * i);
+      warp_mv6(c.s.Dinv + 36 * (size_t)i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+    }
+    __syncthreads();
+  }
+  bool ok = *flag != 0;
+  __syncthreads();
+  if (!ok) {
+    for (int t = threadIdx.x; t < 6 * m; t += blockDim.x) c.s.dv[t] = __longlong_as_double(0x7ff8000000000000ULL);
+    __syncthreads();
+  }
+  return ok;
+}
+
+__device__ void copy_bodies6(const Ctx& c, const double* src, double* dst) {
+  for (int t = threadIdx.x; t < 6 * c.d.nb; t += blockDim.x) dst[t] = src[t];
+}
+
+// trial = base + alpha dv on the dynamic bodies; kinematic bodies keep their prescribed twist.
+__device__ void make_trial(const Ctx& c, double alpha) {
+  for (int t = threadIdx.x; t < 6 * c.d.nb; t += blockDim.x) {
+    int q = t / 6, k = t % 6;
+    int i = c.A.ib_order[c.d.body_off + q];
+    c.s.trial[t] = (i >= 0) ? c.s.base[t] + c.s.dv[6 * i + k] * alpha : c.s.base[t];
+  }
+}
+
+// world twist and world momentum of every island body at the current state
+__device__ void load_world_state(const Ctx& c) {
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
+    int g = c.gbody(q);
+    double pose[8], mom[6], I9[9];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) mom[k] = c.W.mom[(size_t)k * c.W.n + g];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+    bool kin = c.W.kinematic[g] != 0;
+    double wv[6];
+    world_velocity(pose, mom, I9, c.W.diagonal[g] != 0, kin, c.W.mass[g], wv);
+    double mb[6], pw[6], p6[6];
+    screw_from6(mom, mb);
+    wrench_transport(mb, pose, pw);
+    screw_to6(pw, p6);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { c.s.vm[6 * q + k] = wv[k]; c.s.snap[6 * q + k] = p6[k]; }
+  }
+}
+
+// external wrench per island body: gravity (F, p x F) frozen over the whole step
+__device__ void load_external(const Ctx& c) {
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
+    double* e = c.s.ext + 6 * q;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) e[k] = 0.0;
+    if (!c.W.gravity_on) continue;
+    int g = c.gbody(q);
+    double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
+    double f[3];
+    for (int k = 0; k < 3; ++k) {
+      double acc = 0.0;
+      for (int s = 0; s < c.W.splits; ++s) acc += c.W.grav_partial[(size_t)s * 3 * c.W.n + (size_t)k * c.W.n + g];
+      f[k] = c.W.G * pm.w * acc;
+    }
+    e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
+    e[3] = pm.y * f[2] - pm.z * f[1];
+    e[4] = pm.z * f[0] - pm.x * f[2];
+    e[5] = pm.x * f[1] - pm.y * f[0];
+  }
+}
+
+struct SolveOut { bool converged; double best; bool assembled; double a_norm2; };
+
+__device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters) {
+  SolveOut o{false, kHuge, false, 0.0};
+  load_world_state(c);  // vmid = current world velocity; snap = P_s^n
+  __syncthreads();
+  copy_bodies6(c, c.s.vm, c.s.best);
+  __syncthreads();
+  for (int it = 0; it < c.W.max_newton; ++it) {
+    ++*iters;
+    phase_pre(c, c.s.vm, half);
+    __syncthreads();
+    phase_joints(c, c.s.vm, true);
+    __syncthreads();
+    double rnorm = phase_post(c, c.s.vm, half, red);
+    copy_mass0(c);
+    if (rnorm < o.best) {
+      o.best = rnorm;
+      copy_bodies6(c, c.s.vm, c.s.best);
+    }
+    __syncthreads();
+    if (rnorm <= c.W.tol2) { o.converged = true; break; }
+    if (!(rnorm < kHuge)) break;
+    o.a_norm2 = phase_assemble(c, half, red);
+    o.assembled = true;
+    phase_solve(c, flag);
+    // no correction at all -> hand over to sub-division (newton.rs:449-456)
+    int nz = 0;
+    for (int t = threadIdx.x; t < 6 * c.d.m; t += blockDim.x) nz |= (c.s.dv[t] != 0.0);
+    if (!__syncthreads_or(nz)) break;
+    copy_bodies6(c, c.s.vm, c.s.base);
+    __syncthreads();
+    int accepted = -1;
+    double alpha = 1.0;
+    for (int lane = 0; lane < 8; ++lane) {
+      make_trial(c, alpha);
+      __syncthreads();
+      phase_pre(c, c.s.trial, half);
+      __syncthreads();
+      phase_joints(c, c.s.trial, false);
+      __syncthreads();
+      double tnorm = phase_post(c, c.s.trial, half, red);
+      bool acc = tnorm < rnorm;
+      if (lane == 0 || acc) copy_mass0(c);
+      __syncthreads();
+      if (acc) { accepted = lane; break; }
+      alpha = alpha / 2.0;
+    }
+    if (accepted < 0) break;  // vm still holds the base iterate
+    copy_bodies6(c, c.s.trial, c.s.vm);
+    __syncthreads();
+  }
+  // restore the best iterate for the commit
+  copy_bodies6(c, c.s.best, c.s.vm);
+  __syncthreads();
+  return o;
+}
+
+__device__ bool log2_floor(double v, int* e) {
+  if (!(v > 0.0)) return false;
+  double x = v;
+  int k = 0;
+  while (x >= 2.0) { x /= 2.0; ++k; if (k > 250) return false; }
+  while (x < 1.0 && k > -250) { x *= 2.0; --k; }
+  *e = k;
+  return true;
+}
+__device__ int div_euclid(int a, int b) { int q = a / b; if (a % b < 0) q -= 1; return q; }
+
+__device__ bool signal_log2(const Ctx& c, const SolveOut& o, double* red, int* r) {
+  if (!o.assembled) return false;
+  double s = 0.0;
+  for (int t = threadIdx.x; t < 36 * c.d.m; t += blockDim.x) s += c.s.mass0[t] * c.s.mass0[t];
+  double massn = block_sum(s, red);
+  double stiff = ScalarTraits<double>::eff_zero(massn) ? 0.0 : o.a_norm2 / massn;
+  return log2_floor(stiff, r);
+}
+
+// commit_span (newton.rs:708-753)
+__device__ void commit_span(const Ctx& c, double span, double half, bool converged) {
+  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) {
+    int q = c.A.dn_body[c.d.dyn_off + i];
+    int g = c.gbody(q);
+    double m0[8], vb[6], e[8], pm[8], inv[8], vbody[6], v6[6], I9[9];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m0[k] = c.W.pose[(size_t)k * c.W.n + g];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+    screw_from6(c.s.vm + 6 * q, vb);
+    twist_exp(vb, half, e);
+    motor_compose(m0, e, pm);
+    motor_reverse(pm, inv);
+    twist_transport(vb, inv, vbody);
+    screw_to6(vbody, v6);
+    double p6[6], pb[6], pw[6], psm[6];
+    inertia_apply(I9, c.W.diagonal[g] != 0, false, c.W.mass[g], v6, p6);
+    screw_from6(p6, pb);
+    wrench_transport(pb, pm, pw);
+    screw_to6(pw, psm);
+    double pnew[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) pnew[k] = converged ? psm[k] * 2.0 - c.s.snap[6 * q + k] : psm[k];
+    double en[8], mnew[8], minv[8], pnb[6], pbody[6], out6[6];
+    twist_exp(vb, span, en);
+    motor_compose(m0, en, mnew);
+    motor_reverse(mnew, minv);
+    screw_from6(pnew, pnb);
+    wrench_transport(pnb, minv, pbody);
+    screw_to6(pbody, out6);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) c.W.pose[(size_t)k * c.W.n + g] = mnew[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c.W.mom[(size_t)k * c.W.n + g] = out6[k];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
+                                                         int n_islands, int* __restrict__ head) {
+  __shared__ double red[kWarps];
+  __shared__ int flag;
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(head, 1);
+    __syncthreads();
+    int k = item;
+    __syncthreads();
+    if (k >= n_islands) break;
+    Ctx c;
+    c.A = A;
+    c.island = queue[k];
+    c.d = A.desc[c.island];
+    c.W = W;
+    c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+    load_external(c);
+    __syncthreads();
+    unsigned long long remaining = 1ull << kMaxDepth;
+    int depth = 0, spans = 0, iters = 0, maxdepth = 0;
+    double last_best = 0.0;
+    while (remaining > 0) {
+      unsigned long long units = 1ull << (kMaxDepth - depth);
+      while (units > remaining) { ++depth; units >>= 1; }
+      double span = W.dt;
+      for (int t = 0; t < depth; ++t) span = span / 2.0;
+      double half = span / 2.0;
+      ++spans;
+      maxdepth = max(maxdepth, depth);
+      SolveOut o = newton_solve(c, half, red, &flag, &iters);
+      last_best = o.best;
+      bool finite = o.best < kHuge;
+      bool last = depth == kMaxDepth;
+      if (!o.converged && !last) {
+        int r, down;
+        if (signal_log2(c, o, red, &r)) down = div_euclid(r - kThresholdLog2, kPerHalvingLog2) + 1; else down = 1;
+        depth += min(max(down, 1), kMaxDepth - depth);
+        continue;
+      }
+      if (o.converged || finite) commit_span(c, span, half, o.converged);
+      __syncthreads();
+      remaining -= units;
+      auto aligned = [&](int dd) {
+        if (dd <= 0) return false;
+        unsigned long long bigger = 1ull << (kMaxDepth - (dd - 1));
+        return bigger <= remaining && remaining % bigger == 0;
+      };
+      int r;
+      if (remaining > 0 && o.converged && aligned(depth) && signal_log2(c, o, red, &r)) {
+        int up = div_euclid(kThresholdLog2 - r, kPerHalvingLog2);
+        while (up > 0 && aligned(depth)) { --depth; --up; }
+      }
+    }
+    if (threadIdx.x == 0) {
+      A.stats[4 * c.island + 0] = spans;
+      A.stats[4 * c.island + 1] = iters;
+      A.stats[4 * c.island + 2] = maxdepth;
+      A.stats[4 * c.island + 3] = (last_best < kHuge) ? 0 : 1;
+      A.residual[c.island] = last_best;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+// ── host: island structure ────────────────────────────────────────────────────
+NewtonWorld::~NewtonWorld() {
+  for (void* p : allocs) cudaFree(p);
+}
+
+int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodies, const exg_joint_t* joints,
+                      const exg_step_params_t& p) {
+  const int n = w.n, nj = w.nj;
+  // islands = connected components of the joint graph, bodies ascending, joints ascending
+  std::vector<int> parent(n);
+  for (int i = 0; i < n; ++i) parent[i] = i;
+  std::function<int(int)> find = [&](int x) {
+    while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+    return x;
+  };
+  for (int k = 0; k < nj; ++k) {
+    int ra = find(joints[k].a), rb = find(joints[k].b);
+    if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+  }
+  std::vector<int> isl_of_root(n, -1);
+  std::vector<std::vector<int>> ib, ij;
+  for (int i = 0; i < n; ++i) {
+    int r = find(i);
+    if (isl_of_root[r] < 0) { isl_of_root[r] = (int)ib.size(); ib.emplace_back(); ij.emplace_back(); }
+    ib[isl_of_root[r]].push_back(i);
+  }
+  for (int k = 0; k < nj; ++k) ij[isl_of_root[find(joints[k].a)]].push_back(k);
+  n_islands = (int)ib.size();
+
+  std::vector<IslandDesc> desc(n_islands);
+  std::vector<int> h_isl_body, h_jl_law, h_jl_a, h_jl_b, h_ib_order, h_ib_inc_ptr, h_ib_inc_ref, h_dn_body, h_dn_parent,
+      h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
+  std::vector<double> h_jl_params;
+  long long scratch = 0;
+  for (int I = 0; I < n_islands; ++I) {
+    const std::vector<int>& B = ib[I];
+    const std::vector<int>& J = ij[I];
+    IslandDesc& d = desc[I];
+    d.body_off = (int)h_isl_body.size();
+    d.nb = (int)B.size();
+    d.joint_off = (int)h_jl_law.size();
+    d.nj = (int)J.size();
+    max_nb = std::max(max_nb, d.nb);
+    std::vector<int> local(n, -1);
+    for (int q = 0; q < d.nb; ++q) { local[B[q]] = q; h_isl_body.push_back(B[q]); }
+    for (int q = 0; q < d.nj; ++q) {
+      const exg_joint_t& jt = joints[J[q]];
+      h_jl_law.push_back(jt.law);
+      h_jl_a.push_back(local[jt.a]);
+      h_jl_b.push_back(local[jt.b]);
+      for (int k = 0; k < 10; ++k) h_jl_params.push_back(jt.params[k]);
+    }
+    // dynamic order (island order, kinematic excluded)
+    std::vector<int> order(d.nb, -1), dyn_body;
+    for (int q = 0; q < d.nb; ++q)
+      if (!bodies[B[q]].kinematic) { order[q] = (int)dyn_body.size(); dyn_body.push_back(q); }
+    int m = (int)dyn_body.size();
+    d.m = m;
+    d.dyn_off = (int)h_dn_body.size();
+    for (int q = 0; q < d.nb; ++q) h_ib_order.push_back(order[q]);
+    // incidence per island body in joint order
+    d.inc_off = (int)h_ib_inc_ptr.size();
+    {
+      std::vector<std::vector<int>> inc(d.nb);
+      for (int q = 0; q < d.nj; ++q) {
+        inc[h_jl_a[d.joint_off + q]].push_back(2 * q);
+        inc[h_jl_b[d.joint_off + q]].push_back(2 * q + 1);
+      }
+      int base = (int)h_ib_inc_ref.size();
+      for (int q = 0; q < d.nb; ++q) {
+        h_ib_inc_ptr.push_back(base);
+        for (int r : inc[q]) { h_ib_inc_ref.push_back(r); ++base; }
+      }
+      h_ib_inc_ptr.push_back(base);
+    }
+    // dynamic adjacency (distinct neighbours)
+    std::vector<std::vector<int>> adj(m);
+    for (int q = 0; q < d.nj; ++q) {
+      int a = order[h_jl_a[d.joint_off + q]], b = order[h_jl_b[d.joint_off + q]];
+      if (a < 0 || b < 0) continue;
+      if (std::find(adj[a].begin(), adj[a].end(), b) == adj[a].end()) adj[a].push_back(b);
+      if (std::find(adj[b].begin(), adj[b].end(), a) == adj[b].end()) adj[b].push_back(a);
+    }
+    // forest check and elimination tree rooted at each component's centre
+    std::vector<int> par(m, -2), level(m, 0), comp_of(m, -1);
+    long edges = 0;
+    for (int i = 0; i < m; ++i) edges += (long)adj[i].size();
+    edges /= 2;
+    int comps = 0;
+    for (int s = 0; s < m; ++s) {
+      if (comp_of[s] >= 0) continue;
+      // BFS from s: farthest node u
+      auto bfs = [&](int root, std::vector<int>& dist, std::vector<int>& seen_order) {
+        seen_order.clear();
+        seen_order.push_back(root);
+        dist[root] = 0;
+        for (size_t h = 0; h < seen_order.size(); ++h)
+          for (int nb2 : adj[seen_order[h]])
+            if (dist[nb2] < 0) { dist[nb2] = dist[seen_order[h]] + 1; seen_order.push_back(nb2); }
+      };
+      std::vector<int> dist(m, -1), seen;
+      bfs(s, dist, seen);
+      for (int x : seen) comp_of[x] = comps;
+      int u = seen.back();
+      std::vector<int> du(m, -1), seen_u;
+      bfs(u, du, seen_u);
+      int v = seen_u.back();
+      // path u..v: walk back from v along decreasing du
+      std::vector<int> path{v};
+      while (path.back() != u) {
+        int cur = path.back();
+        for (int nb2 : adj[cur]) if (du[nb2] == du[cur] - 1) { path.push_back(nb2); break; }
+      }
+      int centre = path[path.size() / 2];
+      std::vector<int> dc(m, -1), seen_c;
+      bfs(centre, dc, seen_c);
+      par[centre] = -1;
+      for (int x : seen_c) {
+        level[x] = dc[x];
+        for (int nb2 : adj[x]) if (dc[nb2] == dc[x] + 1 && par[nb2] == -2) par[nb2] = x;
+      }
+      ++comps;
+    }
+    if (edges != m - comps) return EXG_ERR_UNSUPPORTED;  // a cycle among the dynamic bodies
+    int nlev = 0;
+    for (int i = 0; i < m; ++i) nlev = std::max(nlev, level[i] + 1);
+    d.n_levels = nlev;
+    d.lv_off = (int)h_lv_ptr.size();
+    {
+      std::vector<std::vector<int>> by(nlev);
+      for (int i = 0; i < m; ++i) by[level[i]].push_back(i);
+      int acc = 0;
+      for (int L = 0; L < nlev; ++L) {
+        h_lv_ptr.push_back(acc);
+        for (int i : by[L]) h_lv_nodes.push_back(i);
+        acc += (int)by[L].size();
+      }
+      h_lv_ptr.push_back(acc);
+    }
+    // children CSR: ch_ptr holds one absolute offset into ch_idx per node (a global sentinel
+    // follows the last island), ch_idx holds island-relative node indices
+    {
+      std::vector<std::vector<int>> ch(m);
+      for (int i = 0; i < m; ++i) if (par[i] >= 0) ch[par[i]].push_back(i);
+      for (int i = 0; i < m; ++i) {
+        h_ch_ptr.push_back((int)h_ch_idx.size());
+        for (int x : ch[i]) h_ch_idx.push_back(x);
+      }
+      for (int i = 0; i < m; ++i) { h_dn_body.push_back(dyn_body[i]); h_dn_parent.push_back(par[i]); }
+    }
+    // assembly cells: (node, kind) with kind 0 = diagonal, 1 = (node row, parent col), 2 = (parent row, node col)
+    d.cell_off = (int)h_cell_ptr.size();
+    {
+      std::vector<std::vector<int>> cells(3 * m);
+      for (int q = 0; q < d.nj; ++q) {
+        int ends[2] = {order[h_jl_a[d.joint_off + q]], order[h_jl_b[d.joint_off + q]]};
+        for (int re = 0; re < 2; ++re) {
+          if (ends[re] < 0) continue;
+          for (int ce = 0; ce < 2; ++ce) {
+            if (ends[ce] < 0) continue;
+            int row = ends[re], col = ends[ce], target;
+            if (row == col) target = 3 * row + 0;
+            else if (par[row] == col) target = 3 * row + 1;
+            else if (par[col] == row) target = 3 * col + 2;
+            else return EXG_ERR_UNSUPPORTED;
+            cells[target].push_back(q * 4 + re * 2 + ce);
+          }
+        }
+      }
+      int base = (int)h_cell_terms.size();
+      for (int t = 0; t < 3 * m; ++t) {
+        h_cell_ptr.push_back(base);
+        for (int x : cells[t]) { h_cell_terms.push_back(x); ++base; }
+      }
+      h_cell_ptr.push_back(base);
+    }
+    d.scratch_off = scratch;
+    scratch += scratch_doubles(d.nb, d.nj, m);
+    scratch = (scratch + 31) & ~31LL;
+  }
+  h_ch_ptr.push_back((int)h_ch_idx.size());
+
+  // island work queue, largest first
+  island_order.resize(n_islands);
+  for (int I = 0; I < n_islands; ++I) island_order[I] = I;
+  std::stable_sort(island_order.begin(), island_order.end(),
+                   [&](int a, int b) { return desc[a].nb + desc[a].nj > desc[b].nb + desc[b].nj; });
+
+  cudaStream_t s = dev->stream;
+  auto up = [&](auto& vec, auto** dptr) -> int {
+    using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+    size_t bytes = sizeof(T) * std::max<size_t>(vec.size(), 1);
+    void* p = nullptr;
+    EXG_CUDA_TRY(cudaMalloc(&p, bytes));
+    allocs.push_back(p);
+    if (!vec.empty()) EXG_CUDA_TRY(cudaMemcpyAsync(p, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice, s));
+    *dptr = static_cast<T*>(p);
+    return EXG_OK;
+  };
+  int rc = EXG_OK;
+  IslandDesc* d_desc = nullptr;
+  int *d_isl_body, *d_jl_law, *d_jl_a, *d_jl_b, *d_ib_order, *d_ib_inc_ptr, *d_ib_inc_ref, *d_dn_body, *d_dn_parent,
+      *d_lv_ptr, *d_lv_nodes, *d_ch_ptr, *d_ch_idx, *d_cell_ptr, *d_cell_terms, *d_stats, *d_q;
+  double *d_params, *d_scratch, *d_res;
+  std::vector<int> stats(4 * (size_t)n_islands, 0);
+  std::vector<double> resid(n_islands, 0.0);
+  std::vector<int> qv(island_order);
+  qv.push_back(0);  // head counter lives after the queue
+  if ((rc = up(desc, &d_desc)) || (rc = up(h_isl_body, &d_isl_body)) || (rc = up(h_jl_law, &d_jl_law)) ||
+      (rc = up(h_jl_a, &d_jl_a)) || (rc = up(h_jl_b, &d_jl_b)) || (rc = up(h_jl_params, &d_params)) ||
+      (rc = up(h_ib_order, &d_ib_order)) || (rc = up(h_ib_inc_ptr, &d_ib_inc_ptr)) ||
+      (rc = up(h_ib_inc_ref, &d_ib_inc_ref)) || (rc = up(h_dn_body, &d_dn_body)) || (rc = up(h_dn_parent, &d_dn_parent)) ||
+      (rc = up(h_lv_ptr, &d_lv_ptr)) || (rc = up(h_lv_nodes, &d_lv_nodes)) || (rc = up(h_ch_ptr, &d_ch_ptr)) ||
+      (rc = up(h_ch_idx, &d_ch_idx)) || (rc = up(h_cell_ptr, &d_cell_ptr)) || (rc = up(h_cell_terms, &d_cell_terms)) ||
+      (rc = up(stats, &d_stats)) || (rc = up(resid, &d_res)) || (rc = up(qv, &d_q)))
+    return rc;
+  void* sp = nullptr;
+  EXG_CUDA_TRY(cudaMalloc(&sp, sizeof(double) * std::max<long long>(scratch, 1)));
+  allocs.push_back(sp);
+  d_scratch = static_cast<double*>(sp);
+  EXG_CUDA_TRY(cudaMemsetAsync(d_scratch, 0, sizeof(double) * std::max<long long>(scratch, 1), s));
+  arr = NewtonDeviceArrays{d_desc,      d_isl_body, d_jl_law,  d_jl_a,      d_jl_b,       d_params,  d_ib_order,
+                           d_ib_inc_ptr, d_ib_inc_ref, d_dn_body, d_dn_parent, d_lv_ptr,   d_lv_nodes, d_ch_ptr,
+                           d_ch_idx,    d_cell_ptr, d_cell_terms, d_scratch, d_stats,     d_res};
+  d_queue = d_q;
+  d_head = d_q + n_islands;
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  (void)p;
+  return EXG_OK;
+}
+
+int NewtonWorld::step(exg_device_s* dev, DeviceWorld& w, const exg_step_params_t& p, int n_steps, exg_world_stats_t* st) {
+  cudaStream_t s = dev->stream;
+  if (n_islands == 0) return EXG_OK;
+  bool grav = p.gravity_law != EXG_GRAVITY_OFF && w.n > 1;
+  WorldRef W{w.pose, w.mom, w.mass, w.inertia, w.kinematic, w.diagonal, w.pos_mass, w.grav_partial,
+             w.n,    w.grav_splits, grav ? 1 : 0, p.G, p.dt, p.warp, p.tol * p.tol, p.max_newton > 0 ? p.max_newton : 32};
+  int grid = std::min(n_islands, std::max(1, dev->sm_count) * 4);
+  for (int k = 0; k < n_steps; ++k) {
+    int rc;
+    if (grav) {
+      if ((rc = launch_body_pre(dev, w, s)) != EXG_OK) return rc;
+      if ((rc = launch_gravity(dev, w.pos_mass, w.size, w.n, p.gravity_law, p.softening, p.precision, w.gshape,
+                               w.grav_partial, s)) != EXG_OK)
+        return rc;
+    }
+    EXG_CUDA_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), s));
+    int tok = prof_begin(dev, PROF_NEWTON, s);
+    k_newton_step<<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+    prof_end(dev, tok, s);
+    if ((rc = exg_after_launch(dev)) != EXG_OK) return rc;
+  }
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int> stats(4 * (size_t)n_islands);
+  std::vector<double> res(n_islands);
+  EXG_CUDA_TRY(cudaMemcpy(stats.data(), arr.stats, sizeof(int) * stats.size(), cudaMemcpyDeviceToHost));
+  EXG_CUDA_TRY(cudaMemcpy(res.data(), arr.residual, sizeof(double) * res.size(), cudaMemcpyDeviceToHost));
+  int spans = 0, iters = 0, depth = 0, fatal = 0;
+  double worst = 0.0;
+  for (int I = 0; I < n_islands; ++I) {
+    spans = std::max(spans, stats[4 * I]);
+    iters = std::max(iters, stats[4 * I + 1]);
+    depth = std::max(depth, stats[4 * I + 2]);
+    fatal |= stats[4 * I + 3];
+    worst = std::max(worst, res[I]);
+  }
+  st->last_spans = spans;
+  st->last_newton_iterations = iters;
+  st->max_depth_reached = depth;
+  st->fatal = fatal;
+  st->last_residual = worst;
+  return fatal ? EXG_ERR_FATAL : EXG_OK;
+}
+
+// ── host energy (the same algebra compiled for the host) ──────────────────────
+double host_world_energy(const exg_body_t* b, int n, const exg_joint_t* joints, int nj, const exg_step_params_t& p) {
+  double e = 0.0;
+  std::vector<double> pos(3 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    exg::body_position(b[i].pose, &pos[3 * i]);
+    if (b[i].kinematic) continue;
+    double v6[6];
+    exg::inertia_inverse(b[i].inertia, b[i].diagonal != 0, false, b[i].mass, b[i].momentum, v6);
+    double mb[6], vb[6];
+    exg::screw_from6(b[i].momentum, mb);
+    exg::screw_from6(v6, vb);
+    e += 0.5 * exg::screw_power(mb, vb);
+  }
+  if (p.gravity_law != EXG_GRAVITY_OFF) {
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) {
+        if (b[i].kinematic || b[j].kinematic) continue;
+        double dx = pos[3 * j] - pos[3 * i], dy = pos[3 * j + 1] - pos[3 * i + 1], dz = pos[3 * j + 2] - pos[3 * i + 2];
+        double r2 = dx * dx + dy * dy + dz * dz, mm = p.G * b[i].mass * b[j].mass;
+        if (p.gravity_law == EXG_GRAVITY_PLUMMER) e -= mm / std::sqrt(r2 + p.softening * p.softening);
+        else {
+          double d = std::sqrt(r2), sz = b[j].size;
+          e -= d >= sz ? mm / d : mm * (3.0 * sz * sz - r2) / (2.0 * sz * sz * sz);
+        }
+      }
+  }
+  for (int k = 0; k < nj; ++k) {
+    const exg_joint_t& j = joints[k];
+    if (j.law > 1) continue;
+    double pa[4], pb[4], line[6];
+    exg::anchor_point(b[j.a].pose, j.params, pa);
+    exg::anchor_point(b[j.b].pose, j.params + 3, pb);
+    exg::point_join(pa, pb, line);
+    double d = exg::soft_weight_norm(line, j.params[9]);
+    double dl = d - j.params[6];
+    e += 0.5 * j.params[7] * dl * dl;
+  }
+  return e;
+}

@@ -65,7 +65,15 @@ struct Dual {
     return r;
   }
   EXG_HD Dual recip() const { R iv = R(1) / v; return scaled(iv, -(iv * iv)); }
-  EXG_HD Dual operator/(const Dual& o) const { return (*this) * o.recip(); }
+  // true quotient for the value (equals the plain evaluation bit for bit), (a'b - ab')/b^2 for
+  // the partials
+  EXG_HD Dual operator/(const Dual& o) const {
+    Dual r; r.v = v / o.v;
+    R inv = R(1) / o.v;
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.g[i] = (g[i] - r.v * o.g[i]) * inv;
+    return r;
+  }
 };
 
 template <int N, class R> struct ScalarTraits<Dual<N, R>> {

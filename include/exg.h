@@ -33,6 +33,12 @@ extern "C" {
 
 #define EXG_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define EXG_API __attribute__((visibility("default")))
+#else
+#define EXG_API
+#endif
+
 /* ── status codes ─────────────────────────────────────────────────────────── */
 typedef enum {
   EXG_OK = 0,
@@ -130,28 +136,48 @@ typedef struct exg_device_s* exg_device_t;
 typedef struct exg_world_s* exg_world_t;
 
 /* ── device (replaces rembrandt::GpuAccelerator::new, crates/rembrandt/src/lib.rs:98-158) ── */
-int exg_device_create(int32_t ordinal, exg_device_t* out);
-int exg_device_destroy(exg_device_t dev);
-int exg_device_synchronize(exg_device_t dev);
+EXG_API int exg_device_create(int32_t ordinal, exg_device_t* out);
+EXG_API int exg_device_destroy(exg_device_t dev);
+EXG_API int exg_device_synchronize(exg_device_t dev);
 /* Number of kernels this library launched on the device so far. */
-int exg_device_kernel_launches(exg_device_t dev, uint64_t* out);
-const char* exg_status_string(int status);
-int exg_abi_version(void);
+EXG_API int exg_device_kernel_launches(exg_device_t dev, uint64_t* out);
+EXG_API const char* exg_status_string(int status);
+/* The CUDA stream (cudaStream_t) every call on this device is ordered on. */
+EXG_API int exg_device_stream(exg_device_t dev, void** out);
+/* In-library profiler: when enabled, each kernel launch is bracketed by CUDA events on the device
+ * stream (worlds then launch directly instead of through a CUDA graph). Kinds: 0 gravity,
+ * 1 joints, 2 explicit integrate, 3 Newton step, 4 body pre. Enabling or disabling resets the
+ * totals; read returns the summed device time and the launch count of one kind. */
+EXG_API int exg_device_profile(exg_device_t dev, int32_t enable);
+EXG_API int exg_device_profile_read(exg_device_t dev, int32_t kind, double* total_ms, int64_t* launches);
+EXG_API int exg_abi_version(void);
 
 /* ── law registry (MessageKind::from((shader_name, jacobian)), accelerator/mod.rs:118-132) ── */
-int exg_law_lookup(const char* shader_name, int32_t* law_out, int32_t* n_params_out);
+EXG_API int exg_law_lookup(const char* shader_name, int32_t* law_out, int32_t* n_params_out);
 
 /* ── world: device-resident bodies and joints (aristotle::World + Mechanism) ── */
-int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n_bodies, const exg_joint_t* joints,
+EXG_API int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n_bodies, const exg_joint_t* joints,
                      int32_t n_joints, const exg_step_params_t* params, exg_world_t* out);
-int exg_world_destroy(exg_world_t w);
+EXG_API int exg_world_destroy(exg_world_t w);
 /* Advance n_steps steps (Mechanism::step per step; crates/newton/src/mechanism/mechanism.rs:526-602). */
-int exg_world_step(exg_world_t w, int32_t n_steps);
-int exg_world_get_bodies(exg_world_t w, exg_body_t* out, int32_t n_bodies);
-int exg_world_set_bodies(exg_world_t w, const exg_body_t* bodies, int32_t n_bodies);
-int exg_world_stats(exg_world_t w, exg_world_stats_t* out);
+EXG_API int exg_world_step(exg_world_t w, int32_t n_steps);
+EXG_API int exg_world_get_bodies(exg_world_t w, exg_body_t* out, int32_t n_bodies);
+EXG_API int exg_world_set_bodies(exg_world_t w, const exg_body_t* bodies, int32_t n_bodies);
+EXG_API int exg_world_stats(exg_world_t w, exg_world_stats_t* out);
 /* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
-int exg_world_energy(exg_world_t w, double* out);
+EXG_API int exg_world_energy(exg_world_t w, double* out);
+
+/* ── host-side motor utilities (no device needed; the same algebra the kernels use) ── */
+/* Twist::exp(dt) of (linear xyz, angular xyz) -> motor (crates/clifford/src/pga3/screw.rs:297-301). */
+EXG_API int exg_motor_exp(const double twist[6], double dt, double out[8]);
+/* "first a, then b" (Motor::compose, crates/clifford/src/pga3/motor.rs:157-159). */
+EXG_API int exg_motor_compose(const double a[8], const double b[8], double out[8]);
+EXG_API int exg_motor_inverse(const double a[8], double out[8]);
+/* World coordinates of the local point p under motor m (joints/src/lib.rs:258-263). */
+EXG_API int exg_motor_apply_point(const double m[8], const double p[3], double out[3]);
+/* Screw transport under m: covariant = 0 for a twist (Ad), 1 for a wrench (coAd)
+ * (crates/clifford/src/pga3/screw.rs:94-105). */
+EXG_API int exg_screw_transport(const double s[6], const double m[8], int32_t covariant, double out[6]);
 
 /* ── stage API on device pointers (the Accelerator's stage calls) ─────────── */
 /* Joint kernels K1-K8 (crates/newton/build.rs:874-973): for each joint k, inputs are the two
@@ -159,13 +185,13 @@ int exg_world_energy(exg_world_t w, double* out);
  * output is d_out[12*k] = [force a, torque a, force b, torque b] when jacobian == 0, or the
  * 300-double block d_out[300*k] = 12 components x [value, d/d(axis 0..23)] (axes: pose A,
  * pose B, vel A, vel B; each lin xyz then ang xyz) when jacobian != 0. */
-int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t n_joints, const double* d_pose,
+EXG_API int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t n_joints, const double* d_pose,
                     const double* d_vel, double dt, double warp, int32_t jacobian, double* d_out);
 /* All-pairs gravity (crates/newton/src/gravity.rs:110-140, 438-450): d_pos_mass holds
  * [x, y, z, m] per body, d_size the core radius (SIZE_CORE law), output d_force[3*i] is the
  * world force on body i. precision MIXED runs the FP32 tile-relative kernel with compensated
  * accumulation. */
-int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law,
+EXG_API int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law,
                        double G, double softening, int32_t precision, double* d_force);
 
 #ifdef __cplusplus

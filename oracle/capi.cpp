@@ -33,6 +33,7 @@ void from_obody(const OBody& o, exg_body_t& b) {
 
 extern "C" {
 
+void orc_set_threads(int n) { oracle_threads() = n > 0 ? n : 1; }
 int orc_body_size(void) { return (int)sizeof(exg_body_t); }
 int orc_joint_size(void) { return (int)sizeof(exg_joint_t); }
 

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <thread>
 #include <vector>
 #include "laws.hpp"
 
@@ -110,13 +111,18 @@ struct GravityParams { int law; double G; double eps; };
 // Per-body world force from every other body, summed in slot order (gravity.rs:530-587,
 // 438-450). SIZE_CORE: the reference law with the higher-slot body's size as the core.
 // PLUMMER: F = G m_i m_j (p_j - p_i) / (r^2 + eps^2)^(3/2).
+// Host threads the oracle's O(N^2) gravity loop may use (the CPU baseline runs it on every core).
+inline int& oracle_threads() { static int t = 1; return t; }
+
 inline void gravity_forces(const std::vector<OBody>& bodies, const GravityParams& gp, std::vector<V3<double>>& force) {
   size_t n = bodies.size();
   force.assign(n, V3<double>());
   if (gp.law == GRAVITY_OFF) return;
   std::vector<V3<double>> pos(n);
   for (size_t i = 0; i < n; ++i) pos[i] = body_position(bodies[i]);
-  for (size_t i = 0; i < n; ++i) {
+  int nt = std::max(1, std::min<int>(oracle_threads(), (int)n));
+  auto rows = [&](size_t lo, size_t hi) {
+  for (size_t i = lo; i < hi; ++i) {
     if (bodies[i].kinematic) continue;
     double mi = bodies[i].mass;
     V3<double> acc;
@@ -139,6 +145,11 @@ inline void gravity_forces(const std::vector<OBody>& bodies, const GravityParams
     }
     force[i] = acc;
   }
+  };
+  if (nt == 1) { rows(0, n); return; }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(rows, n * t / nt, n * (t + 1) / nt);
+  for (auto& th : pool) th.join();
 }
 
 inline double gravity_potential(const std::vector<OBody>& bodies, const GravityParams& gp) {
@@ -374,8 +385,8 @@ struct NewtonIsland {
       double ang2 = r[3] * r[3] + r[4] * r[4] + r[5] * r[5];
       // newton.rs:139-151: max2 with NaN falling through `a > b`
       double a1 = lin2 / scale_out[6 * i], a2 = ang2 / scale_out[6 * i + 3];
-      worst = (a1 > worst) ? a1 : worst;
-      worst = (a2 > worst) ? a2 : worst;
+      worst = (worst > a1) ? worst : a1;
+      worst = (worst > a2) ? worst : a2;
     }
     return worst;
   }

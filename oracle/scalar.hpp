@@ -32,7 +32,15 @@ struct Dual {
   }
   // tangent.rs:171-173, 219-225: a / b = a * recip(b), recip' = -v^2
   Dual recip() const { Dual r; R iv = R(1) / v; r.v = iv; for (int i = 0; i < N; ++i) r.g[i] = g[i] * (-(iv * iv)); return r; }
-  Dual operator/(const Dual& o) const { return (*this) * o.recip(); }
+  // The value is a true quotient, so a dual evaluation's value equals the plain evaluation bit
+  // for bit (the reference requires that of its Jacobian and plain kernels,
+  // crates/newton/src/accelerator/mod.rs:1410-1492); the partials follow (a'b - ab')/b^2.
+  Dual operator/(const Dual& o) const {
+    Dual r; r.v = v / o.v;
+    R inv = R(1) / o.v;
+    for (int i = 0; i < N; ++i) r.g[i] = (g[i] - r.v * o.g[i]) * inv;
+    return r;
+  }
   Dual scale_grad(R s) const { Dual r; r.v = v; for (int i = 0; i < N; ++i) r.g[i] = g[i] * s; return r; }
 };
 template <int N, class R> inline bool structurally_zero_dual(const Dual<N, R>& x) {

@@ -1,0 +1,218 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle on the same seeded inputs.
+
+Tolerances: the FP64 path agrees with the f64 oracle to rounding (rtol 1e-12 per stage, 1e-9 on
+states after many steps); the mixed path is bounded by its FP32 stages (stated per test). Integer
+structure (topology, incidence, ordering) is bit-exact by construction: the kernels consume the
+records as given.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from exgame_b200 import _lib, scenarios
+from exgame_b200.abi import (GRAVITY_OFF, GRAVITY_PLUMMER, GRAVITY_SIZE_CORE, JOINT_DTYPE, LIE_EULER, NEWTON,
+                             PRECISION_F64, PRECISION_MIXED, SYMPLECTIC_EULER, EXPLICIT_EULER, step_params)
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev_tensor(a):
+    a = np.ascontiguousarray(a)
+    t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy()).cuda()
+    torch.cuda.synchronize()
+    return t
+
+
+def vp(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def positions(bodies):
+    return np.array([_lib.motor_apply_point(b["pose"], np.zeros(3)) for b in bodies])
+
+
+def pos_mass(bodies):
+    p = positions(bodies)
+    pm = np.zeros((len(bodies), 4))
+    pm[:, :3] = p
+    pm[:, 3] = np.where(bodies["kinematic"] != 0, 0.0, bodies["mass"])
+    return pm
+
+
+@pytest.mark.parametrize("law", [GRAVITY_SIZE_CORE, GRAVITY_PLUMMER])
+@pytest.mark.parametrize("n", [1, 7, 300, 5000])
+def test_gravity_stage_fp64_matches_oracle(device, oracle, law, n):
+    bodies = scenarios.gravity_world(n, 20.0, seed=n)
+    if n > 1 and law == GRAVITY_SIZE_CORE:
+        bodies["size"] *= 3.0  # make the size core active for some pairs
+    pm = pos_mass(bodies)
+    d_pm, d_size = dev_tensor(pm), dev_tensor(np.ascontiguousarray(bodies["size"]))
+    d_f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().exg_gravity_forces(device.handle, vp(d_pm), vp(d_size), n, law, 1.0, 0.05, PRECISION_F64,
+                                             vp(d_f)))
+    got = d_f.cpu().numpy().reshape(n, 3)
+    want = oracle.gravity_forces(bodies, law, 1.0, 0.05)
+    scale = np.abs(want).max() + 1e-300
+    assert np.abs(got - want).max() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("law", [GRAVITY_SIZE_CORE, GRAVITY_PLUMMER])
+def test_gravity_stage_mixed_error_bound(device, oracle, law):
+    """FP32 pair terms with tile-relative positions and FP64 tile accumulation: per-body relative
+    force error below 2e-5 of the body's force magnitude."""
+    n = 4096
+    bodies = scenarios.gravity_world(n, 1000.0, seed=9)
+    pm = pos_mass(bodies)
+    d_pm, d_size = dev_tensor(pm), dev_tensor(np.ascontiguousarray(bodies["size"]))
+    d_f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().exg_gravity_forces(device.handle, vp(d_pm), vp(d_size), n, law, 1.0, 0.05, PRECISION_MIXED,
+                                             vp(d_f)))
+    got = d_f.cpu().numpy().reshape(n, 3)
+    want = oracle.gravity_forces(bodies, law, 1.0, 0.05)
+    rel = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+    assert rel.max() < 2e-5, rel.max()
+
+
+@pytest.mark.parametrize("jacobian", [0, 1])
+def test_joint_stage_matches_oracle(device, oracle, jacobian):
+    rng = np.random.default_rng(3)
+    nb, nj = 40, 120
+    poses = np.array([oracle.twist_exp(rng.normal(size=6)) for _ in range(nb)])
+    vels = rng.normal(size=(nb, 6))
+    joints = np.zeros(nj, dtype=JOINT_DTYPE)
+    for k in range(nj):
+        law = k % 4
+        a, b = rng.choice(nb, 2, replace=False)
+        joints[k]["law"], joints[k]["a"], joints[k]["b"] = law, a, b
+        if law <= 1:
+            joints[k]["params"][:10] = np.r_[rng.normal(size=6) * 0.3, 1.3, 7.0, 2.0, 1e-6]
+        elif law == 2:
+            joints[k]["params"][:2] = [2.0, 1e-3]
+        else:
+            joints[k]["params"][0] = 1.5
+    width = 300 if jacobian else 12
+    d_j, d_p, d_v = dev_tensor(joints), dev_tensor(poses), dev_tensor(vels)
+    d_out = torch.zeros(nj * width, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().exg_eval_joints(device.handle, vp(d_j), nj, vp(d_p), vp(d_v), 0.016, 1.3, jacobian, vp(d_out)))
+    got = d_out.cpu().numpy().reshape(nj, width)
+    for k in range(nj):
+        j = joints[k]
+        args = (int(j["law"]), j["params"], poses[j["a"]], poses[j["b"]], vels[j["a"]], vels[j["b"]], 0.016, 1.3)
+        want = oracle.jacobian_eval(*args).reshape(-1) if jacobian else oracle.plain_eval(*args)
+        assert np.allclose(got[k], want, rtol=1e-12, atol=1e-12), k
+
+
+def run_both(oracle, device, bodies, joints, params, steps, solver=0):
+    ow = oracle.OracleWorld(bodies, joints, params, solver=solver)
+    ow.step(steps)
+    dw = _lib.DeviceWorld(device, bodies, joints, params)
+    dw.step(steps)
+    return ow, dw
+
+
+def state_error(a, b):
+    pa, pb = positions(a), positions(b)
+    scale = max(1.0, np.abs(pa).max())
+    pos_err = np.abs(pa - pb).max() / scale
+    mom_scale = max(1e-12, np.abs(a["momentum"]).max())
+    mom_err = np.abs(a["momentum"] - b["momentum"]).max() / mom_scale
+    return pos_err, mom_err
+
+
+@pytest.mark.parametrize("scheme", [LIE_EULER, SYMPLECTIC_EULER, EXPLICIT_EULER])
+@pytest.mark.parametrize("law", [GRAVITY_PLUMMER, GRAVITY_SIZE_CORE])
+def test_explicit_gravity_world_matches_oracle(device, oracle, scheme, law):
+    bodies = scenarios.gravity_world(200, 20.0, seed=4)
+    params = step_params(integrator=scheme, gravity_law=law, softening=0.05, dt=1e-3)
+    ow, dw = run_both(oracle, device, bodies, np.zeros(0, dtype=JOINT_DTYPE), params, 100)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-11 and me < 1e-10, (pe, me)
+
+
+def test_explicit_jointed_world_matches_oracle(device, oracle):
+    bodies, joints = scenarios.chain_world(12, seed=5)
+    joints["law"][::4] = 1  # include the critically damped law
+    params = step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, dt=1e-3)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 200)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-11 and me < 1e-9, (pe, me)
+
+
+def test_config0_full_size_matches_oracle(device, oracle):
+    """1024 bodies, Plummer 0.05, LieEuler, dt 1e-3, 1000 steps: final positions, velocities and
+    total energy against the f64 oracle."""
+    bodies, joints, params, steps = scenarios.config0()
+    ow, dw = run_both(oracle, device, bodies, joints, params, steps)
+    a, b = ow.bodies(), dw.bodies()
+    pe, me = state_error(a, b)
+    assert pe < 1e-9 and me < 1e-8, (pe, me)
+    assert abs(ow.energy() - dw.energy()) <= 1e-9 * abs(ow.energy())
+    # linear momentum is conserved by the pairwise law up to rounding
+    p0 = bodies["momentum"][:, :3].sum(0)
+    p1 = np.array([_lib.screw_transport(x["momentum"], x["pose"], 1)[:3] for x in b]).sum(0)
+    assert np.abs(p1 - p0).max() < 1e-9 * np.abs(bodies["momentum"]).sum()
+
+
+@pytest.mark.parametrize("n", [2, 8, 33])
+def test_newton_chain_matches_oracle(device, oracle, n):
+    bodies, joints = scenarios.chain_world(n, seed=20 + n)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 20)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+    st = dw.stats()
+    assert st["fatal"] == 0 and st["last_spans"] >= 1
+
+
+def test_newton_tree_and_kinematic_matches_oracle(device, oracle):
+    bodies, joints = scenarios.tree_world(40, seed=31)
+    bodies[5]["kinematic"] = 1
+    bodies[5]["mass"] = 0.0
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 10)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+
+
+def test_newton_many_islands_and_gravity(device, oracle):
+    parts = [scenarios.chain_world(5, seed=40 + k, origin=(0, 30.0 * k, 0)) for k in range(6)]
+    bodies, joints = scenarios.concat_worlds(parts)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_PLUMMER, softening=0.05, G=1.0, dt=1e-2, tol=1e-10)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 10)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+
+
+def test_newton_stiff_step_subdivides_like_oracle(device, oracle):
+    """A stiff transverse pair at a coarse step (newton.rs:946-1027 geometry): the device reaches the
+    oracle's state, sub-division included."""
+    from test_oracle_kat import body, spring
+    bs = np.array([body((1, 0, 0), (0, 50, 0)), body((-1, 0, 0), (0, -50, 0))])
+    js = np.array([spring(0, 1, 2.0, 5e4, 5.0)])
+    params = step_params(integrator=NEWTON, dt=0.02)
+    ow, dw = run_both(oracle, device, bs, js, params, 10)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-7 and me < 1e-6, (pe, me)
+
+
+def test_config1_chain_first_steps_match_oracle(device, oracle):
+    """The full 256-body chain (config 1): the first 5 steps against the oracle."""
+    bodies, joints, params, _ = scenarios.config1()
+    ow, dw = run_both(oracle, device, bodies, joints, params, 5)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+
+
+def test_device_counts_kernel_launches(device):
+    bodies = scenarios.gravity_world(64, 10.0, seed=1)
+    before = device.kernel_launches()
+    dw = _lib.DeviceWorld(device, bodies, np.zeros(0, dtype=JOINT_DTYPE),
+                          step_params(gravity_law=GRAVITY_PLUMMER, softening=0.05, dt=1e-3))
+    dw.step(3)
+    assert device.kernel_launches() - before == 9  # pre, gravity, integrate per step

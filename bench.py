@@ -28,7 +28,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from exgame_b200 import _lib, scenarios  # noqa: E402
-from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON  # noqa: E402
+from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED  # noqa: E402
 
 METRIC = "body-steps/s"
 FP64_FMA_PER_SM_CLK = 64
@@ -44,22 +44,32 @@ def load_peaks():
 
 
 def workload(name, rank):
-    """(label, list of (bodies, joints, params) parts, config dict)"""
+    """(list of (bodies, joints, params) worlds stepped together, config dict)"""
     if name == "c0":
         b, j, p, _ = scenarios.config0(seed=rank)
         cfg = {"workload": "1024 point masses, Plummer eps 0.05, LieEuler, dt 1e-3, f64 (config 0)",
-               "bodies": 1024, "dtype": "f64"}
+               "bodies": 1024, "worlds": 1, "dtype": "f64"}
         return [(b, j, p)], cfg
     if name == "c1":
         b, j, p, _ = scenarios.config1(seed=1 + rank)
         cfg = {"workload": "256-body box chain, 765 joints, implicit Newton tol 1e-10, dt 1e-2, f64 (config 1)",
-               "bodies": 256, "dtype": "f64"}
+               "bodies": 256, "worlds": 1, "dtype": "f64"}
         return [(b, j, p)], cfg
     if name == "c2":
-        (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(seed=2 + rank)
+        (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(seed=2 + rank, precision=PRECISION_MIXED)
         cfg = {"workload": "65,536-body gravity (ball R 1000, LieEuler) + 16 x 256-body chains (Newton tol 1e-10), "
-                           "dt 1e-3, f64 (config 2)", "bodies": len(gb) + len(cb), "dtype": "f64"}
+                           "dt 1e-3, mixed precision (config 2)", "bodies": len(gb) + len(cb), "worlds": 2,
+               "dtype": "f32 forces / f64 state"}
         return [(gb, gj, gp), (cb, cj, cp)], cfg
+    if name in ("c3", "c3-f64"):
+        prec = PRECISION_MIXED if name == "c3" else PRECISION_F64
+        worlds = scenarios.config3_worlds(4096, seed=3 + rank, precision=prec)
+        n = sum(len(b) for b, _, _ in worlds)
+        cfg = {"workload": "4096 independent worlds, body counts log-uniform in [8, 8192]: gravity worlds "
+                           "(LieEuler, dt 1e-3) and random joint trees (Newton tol 1e-10, dt 1e-2), one batched launch "
+                           "set per step, " + ("mixed precision" if prec else "f64") + " (config 3)",
+               "bodies": n, "worlds": 4096, "dtype": "f32 forces / f64 state" if prec else "f64"}
+        return worlds, cfg
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -131,12 +141,65 @@ def time_steps(dev, worlds, steps, flush):
     return total
 
 
-def dominant_kernel(cfg_name, worlds, parts):
-    """(profile kind, algorithmic flops per launch, bound, label)"""
-    if cfg_name in ("c0", "c2"):
-        n = len(parts[0][0])
-        return 0, 20.0 * n * n, "fp64", f"all-pairs gravity, {n} bodies (20 flop per directed pair)"
-    return 3, None, "fp64", "Newton island step"
+def dominant_kernel(dev, cfg_name, parts, steps, bench_worlds):
+    """Profile a pass of `steps` steps; pick the kernel kind with the largest device time.
+    Returns (kind, total_ms, launches, algorithmic flops per launch or None, bound, label)."""
+    dev.profile(True)
+    for _ in range(steps):
+        for w in bench_worlds:
+            w.step(1)
+    kinds = {0: "all-pairs gravity", 1: "joint laws", 2: "explicit integrate", 3: "Newton island step",
+             4: "body charges / world twists"}
+    per = {k: dev.profile_read(k) for k in kinds}
+    dev.profile(False)
+    kind = max(per, key=lambda k: per[k][0])
+    ms, nl = per[kind]
+    flops, bound = None, "fp64"
+    if kind == 0:
+        pairs = 0.0
+        for b, _, p in parts:
+            if int(p["gravity_law"]) != GRAVITY_OFF and len(b) > 1:
+                pairs += float(len(b)) ** 2
+        flops = 20.0 * pairs
+        bound = "fp32" if int(parts[0][2]["precision"]) == PRECISION_MIXED else "fp64"
+    label = kinds[kind] + (f" ({20} flop per directed pair)" if kind == 0 else "")
+    shares = {kinds[k]: per[k][0] for k in kinds}
+    return kind, ms, nl, flops, bound, label, shares
+
+
+def make_worlds(dev, parts):
+    if len(parts) == 1:
+        return [_lib.DeviceWorld(dev, *parts[0])]
+    return [_lib.DeviceBatch(dev, parts)]
+
+
+def plain_path(dev, parts, flush, passes=1):
+    """The plain path: every world FP64 and alone, one world per launch (a step of the workload is
+    one exg_world_step per world). Returns body-steps/s over `passes` passes after one warm pass."""
+    import torch
+    stream = torch.cuda.ExternalStream(dev.stream())
+    worlds = []
+    for b, j, p in parts:
+        q = p.copy()
+        q["precision"] = PRECISION_F64
+        worlds.append(_lib.DeviceWorld(dev, b, j, q))
+    for w in worlds:
+        w.step(1)
+    n = sum(w.n for w in worlds)
+    total = 0.0
+    for _ in range(passes):
+        flush()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for w in worlds:
+            w.step(1)
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b) / 1e3
+    for w in worlds:
+        w.close()
+    return n * passes / total
 
 
 def run_ours(args, rank, world_size, local_rank):
@@ -144,7 +207,7 @@ def run_ours(args, rank, world_size, local_rank):
     torch.cuda.set_device(local_rank)
     dev = _lib.Device(local_rank)
     parts, cfg = workload(args.workload, rank)
-    worlds = [_lib.DeviceWorld(dev, b, j, p) for (b, j, p) in parts]
+    worlds = make_worlds(dev, parts)
     n_bodies = sum(len(b) for (b, _, _) in parts)
     flush_buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
@@ -161,7 +224,9 @@ def run_ours(args, rank, world_size, local_rank):
     torch.cuda.synchronize()
     launches0 = dev.kernel_launches()
     with ClockSampler(local_rank) as clk:
+        time.sleep(0.3)
         t_dev = time_steps(dev, worlds, args.steps, flush)
+        time.sleep(0.3)
     launches = dev.kernel_launches() - launches0
     torch.cuda.synchronize()
     t = t_dev
@@ -176,9 +241,10 @@ def run_ours(args, rank, world_size, local_rank):
     # end to end through the public API: host state in, step, host state out
     host_in = [np.ascontiguousarray(w.bodies()) for w in worlds]
     h2d = sum(h.nbytes for h in host_in)
+    e2e_steps = max(1, min(args.steps, 5)) if n_bodies > 1_000_000 else args.steps
     dev.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         for w, h in zip(worlds, host_in):
             w.set_bodies(h)
             w.step(1)
@@ -190,37 +256,31 @@ def run_ours(args, rank, world_size, local_rank):
         tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_e2e = float(tt.item())
-    e2e = {"value": n_bodies * args.steps * world_size / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(h2d)}
+    e2e = {"value": n_bodies * e2e_steps * world_size / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(h2d), "steps": e2e_steps}
 
     # dominant kernel, timed live with events on the library stream over a profiled pass
-    kind, flops, bound, label = dominant_kernel(args.workload, worlds, parts)
-    dev.profile(True)
-    for _ in range(args.steps):
-        for w in worlds:
-            w.step(1)
-    ms, nl = dev.profile_read(kind)
-    dev.profile(False)
+    kind, ms, nl, flops, bound, label, shares = dominant_kernel(dev, args.workload, parts, args.steps, worlds)
     peaks, src = load_peaks()
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
     per_clk = FP64_FMA_PER_SM_CLK if bound == "fp64" else FP32_FMA_PER_SM_CLK
     peak_tflops = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
-    roofline = None
-    if flops and nl:
-        avg_s = ms / 1e3 / nl
-        achieved = flops / avg_s / 1e12
-        roofline = {"bound": bound, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                    "frac": achieved / peak_tflops, "traffic": None, "kernel": label,
-                    "avg_launch_us": avg_s * 1e6, "launches": nl,
-                    "peak_source": f"nominal {per_clk} {bound.upper()} FMA/clk/SM x {sms} SMs at the {src} "
-                                   f"max SM clock {sm_mhz:.0f} MHz (no tensor-core or copy peak applies)"}
-    elif nl:
-        roofline = {"bound": bound, "achieved": None, "peak": peak_tflops, "unit": "TFLOP/s", "frac": None,
-                    "traffic": None, "kernel": label, "avg_launch_us": ms / nl * 1e3, "launches": nl}
+    avg_s = ms / 1e3 / max(nl, 1)
+    roofline = {"bound": bound, "achieved": (flops / avg_s / 1e12) if flops else None, "peak": peak_tflops,
+                "unit": "TFLOP/s", "frac": (flops / avg_s / 1e12 / peak_tflops) if flops else None, "traffic": None,
+                "kernel": label, "avg_launch_us": avg_s * 1e6, "launches": nl,
+                "device_ms_by_kernel": shares,
+                "peak_source": f"nominal {per_clk} {bound.upper()} FMA/clk/SM x {sms} SMs at the {src} max SM clock "
+                               f"{sm_mhz:.0f} MHz (no tensor-core or copy peak applies to this kernel)"}
+    plain = None
+    if args.plain and len(parts) > 1:
+        plain = {"value": plain_path(dev, parts, flush), "unit": METRIC,
+                 "sample": "every world FP64 and stepped alone, one exg_world_step per world, one pass after a warm "
+                           "pass (device time, L2 flushed before the pass)"}
     return {
         "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
-        "clocks": clk.summary(), "n_bodies": n_bodies,
+        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain,
     }
 
 
@@ -231,6 +291,8 @@ def cpu_baseline(args, threads):
     L = oracle_lib.lib()
     L.orc_set_threads(int(threads))
     parts, cfg = workload(args.workload, 0)
+    if len(parts) > 64:  # a bounded sample: every 16th world of the batch
+        parts = parts[::16]
     worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
     n = sum(w.n for w in worlds)
     budget = args.cpu_seconds
@@ -252,7 +314,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c0", choices=["c0", "c1", "c2"])
+    ap.add_argument("--workload", default="c0", choices=["c0", "c1", "c2", "c3", "c3-f64"])
+    ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -267,6 +330,10 @@ def main():
         import oracle_lib
         oracle_lib.lib().orc_set_threads(threads)
         parts, cfg = workload(args.workload, 0)
+        sample = f"{args.steps} timed steps after {args.warmup} warm-up steps"
+        if len(parts) > 64:  # a bounded sample: every 16th world of the batch
+            parts = parts[::16]
+            sample += ", every 16th world of the batch"
         worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
         n = sum(w.n for w in worlds)
         for _ in range(args.warmup):
@@ -283,7 +350,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": cfg["dtype"],
                 "data": "synthetic (seeded; the reference publishes no dataset)", "config": cfg,
                 "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
-                                 "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps, {n} bodies"},
+                                 "sample": sample + f", {n} bodies"},
                 "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -305,7 +372,7 @@ def main():
             "config": dict(r["cfg"], parallelism=f"replicas x{world_size} (independent worlds)",
                            l2="flushed between timed steps (256 MB write)"),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
-            "clocks": r["clocks"],
+            "clocks": r["clocks"], "plain_path": r["plain"],
         }
         print(json.dumps(line))
     if world_size > 1:

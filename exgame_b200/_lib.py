@@ -42,11 +42,17 @@ SIGNATURES = {
     "exg_world_set_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_stats": (ctypes.c_int, [_vp, _vp]),
     "exg_world_energy": (ctypes.c_int, [_vp, _c_double_p]),
+    "exg_batch_create": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "exg_batch_get_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
+    "exg_batch_set_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
+    "exg_batch_world_stats": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
     "exg_motor_compose": (ctypes.c_int, [_vp, _vp, _vp]),
     "exg_motor_inverse": (ctypes.c_int, [_vp, _vp]),
     "exg_motor_apply_point": (ctypes.c_int, [_vp, _vp, _vp]),
     "exg_screw_transport": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "exg_motor_exp_n": (ctypes.c_int, [ctypes.c_int64, _vp, ctypes.c_double, _vp]),
+    "exg_motor_compose_n": (ctypes.c_int, [ctypes.c_int64, _vp, _vp, _vp]),
     "exg_eval_joints": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int32, _vp]),
     "exg_gravity_forces": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
@@ -104,6 +110,21 @@ def motor_compose(a, b):
     b = np.ascontiguousarray(b, dtype=np.float64)
     out = np.zeros(8)
     check(lib().exg_motor_compose(ptr(a), ptr(b), ptr(out)), "exg_motor_compose")
+    return out
+
+
+def motor_exp_n(twists, dt=1.0):
+    t = np.ascontiguousarray(twists, dtype=np.float64).reshape(-1, 6)
+    out = np.zeros((len(t), 8))
+    check(lib().exg_motor_exp_n(len(t), ptr(t), float(dt), ptr(out)), "exg_motor_exp_n")
+    return out
+
+
+def motor_compose_n(a, b):
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 8)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(-1, 8)
+    out = np.zeros((len(a), 8))
+    check(lib().exg_motor_compose_n(len(a), ptr(a), ptr(b), ptr(out)), "exg_motor_compose_n")
     return out
 
 
@@ -227,3 +248,39 @@ class DeviceWorld:
             self.close()
         except Exception:
             pass
+
+
+class DeviceBatch(DeviceWorld):
+    """Many independent worlds of uneven size stepped together by one set of launches per step."""
+
+    def __init__(self, device, worlds):
+        """worlds: list of (bodies, joints, params); joint body indices local to their world."""
+        self.device = device
+        self.counts = np.array([len(b) for b, _, _ in worlds], dtype=np.int32)
+        self.jcounts = np.array([len(j) for _, j, _ in worlds], dtype=np.int32)
+        self.bodies_host = np.ascontiguousarray(np.concatenate([b for b, _, _ in worlds]), dtype=BODY_DTYPE)
+        js = [j for _, j, _ in worlds if len(j)]
+        self.joints_host = np.ascontiguousarray(np.concatenate(js) if js else np.zeros(0, JOINT_DTYPE), dtype=JOINT_DTYPE)
+        self.params = np.ascontiguousarray(np.array([p for _, _, p in worlds], dtype=STEP_PARAMS_DTYPE))
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        h = ctypes.c_void_p()
+        check(lib().exg_batch_create(device.handle, len(worlds), ptr(self.counts), ptr(self.jcounts),
+                                     ptr(self.bodies_host), ptr(self.joints_host), ptr(self.params), ctypes.byref(h)),
+              "exg_batch_create")
+        self.handle = h
+        self.n = int(self.counts.sum())
+        self.n_worlds = len(worlds)
+
+    def world_bodies(self, k):
+        out = np.zeros(int(self.counts[k]), dtype=BODY_DTYPE)
+        check(lib().exg_batch_get_world(self.handle, int(k), ptr(out), len(out)), "exg_batch_get_world")
+        return out
+
+    def set_world_bodies(self, k, bodies):
+        b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        check(lib().exg_batch_set_world(self.handle, int(k), ptr(b), len(b)), "exg_batch_set_world")
+
+    def world_stats(self, k):
+        s = np.zeros((), dtype=WORLD_STATS_DTYPE)
+        check(lib().exg_batch_world_stats(self.handle, int(k), ptr(s)), "exg_batch_world_stats")
+        return s

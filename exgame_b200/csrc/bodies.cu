@@ -27,27 +27,39 @@ __global__ void k_body_pre(BodyView b, double* __restrict__ pos_mass, double* __
   for (int c = 0; c < 6; ++c) wvel[(size_t)c * b.n + i] = wv[c];
 }
 
-template <int SCHEME>
+// One explicit step of every body whose world uses an explicit scheme; the scheme, dt, G and the
+// gravity partial layout come from the body's world.
 __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, double* __restrict__ mom_out,
                                      const double* __restrict__ pos_mass, const double* __restrict__ grav_partial,
-                                     int splits, int gravity_on, double G, const double* __restrict__ conn, int nj,
-                                     const int* __restrict__ inc_ptr, const int* __restrict__ inc_ref, double dt) {
+                                     const int* __restrict__ world_of_body, const exg_step_params_t* __restrict__ wparams,
+                                     const long long* __restrict__ w_poff, const int* __restrict__ w_splits,
+                                     const int* __restrict__ w_n, const int* __restrict__ w_body_off,
+                                     const double* __restrict__ conn, int nj, const int* __restrict__ inc_ptr,
+                                     const int* __restrict__ inc_ref) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.n) return;
   if (b.kinematic[i]) return;
+  const int wid = world_of_body[i];
+  const int scheme = wparams[wid].integrator;
+  if (scheme == EXG_NEWTON) return;
+  const double dt = wparams[wid].dt;
   double pose[8], mom[6], I9[9];
   load_body(b, i, pose, mom, I9);
   const bool diag = b.diagonal[i] != 0;
   const double mass = b.mass[i];
   // world wrench: gravity (F, p x F) then incident joint wrenches in joint order
   double tot[6] = {0, 0, 0, 0, 0, 0};
-  if (gravity_on) {
+  const int splits = w_splits[wid];
+  if (splits > 0) {
     double4 pm = reinterpret_cast<const double4*>(pos_mass)[i];
+    const int nw = w_n[wid];
+    const int il = i - w_body_off[wid];
+    const double* part = grav_partial + w_poff[wid];
     double f[3];
     for (int c = 0; c < 3; ++c) {
       double acc = 0.0;
-      for (int s = 0; s < splits; ++s) acc += grav_partial[(size_t)s * 3 * b.n + (size_t)c * b.n + i];
-      f[c] = G * pm.w * acc;
+      for (int s = 0; s < splits; ++s) acc += part[(size_t)s * 3 * nw + (size_t)c * nw + il];
+      f[c] = wparams[wid].G * pm.w * acc;
     }
     tot[0] = f[0]; tot[1] = f[1]; tot[2] = f[2];
     tot[3] = pm.y * f[2] - pm.z * f[1];
@@ -66,7 +78,7 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
   motor_reverse(pose, rev);
   wrench_transport(wb, rev, tmp);
   screw_to6(tmp, wbody);
-  if (SCHEME == EXG_LIE_EULER) {  // lie_euler.rs:31-55
+  if (scheme == EXG_LIE_EULER) {  // lie_euler.rs:31-55
 #pragma unroll
     for (int c = 0; c < 6; ++c) mom[c] += wbody[c] * dt;
     double v6[6], vb[6], delta[8], drot[8], drot_inv[8], mb[6], mt[6];
@@ -89,15 +101,12 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
     screw_from6(mom, mb);
     coad_bracket(mb, vb, gy);
     screw_to6(gy, gyro);  // gyroscopic = -coad_bracket (body.rs:170-175)
-    if (SCHEME == EXG_SYMPLECTIC_EULER) {  // symplectic_euler.rs:26-41
 #pragma unroll
-      for (int c = 0; c < 6; ++c) mom[c] += (wbody[c] - gyro[c]) * dt;
+    for (int c = 0; c < 6; ++c) mom[c] += (wbody[c] - gyro[c]) * dt;
+    if (scheme == EXG_SYMPLECTIC_EULER) {  // symplectic_euler.rs:26-41: the pose moves with the NEW velocity
       inertia_inverse(I9, diag, false, mass, mom, v6);
       screw_from6(v6, vb);
-    } else {  // explicit_euler.rs:21-33: the pose moves with the OLD velocity
-#pragma unroll
-      for (int c = 0; c < 6; ++c) mom[c] += (wbody[c] - gyro[c]) * dt;
-    }
+    }  // explicit_euler.rs:21-33: the pose moves with the OLD velocity
     double e[8], np[8];
     twist_exp(vb, dt, e);
     motor_compose(e, pose, np);  // pose * exp
@@ -124,28 +133,12 @@ int launch_body_pre(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
   return exg_after_launch(dev);
 }
 
-int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, int scheme, int gravity_on, double G, double dt,
-                              cudaStream_t s) {
-  if (w.n <= 0) return EXG_OK;
-  dim3 grid((w.n + 127) / 128);
-  BodyView v = view_of(w);
-  int _tok = prof_begin(dev, PROF_INTEGRATE, s);
-  switch (scheme) {
-    case EXG_LIE_EULER:
-      k_integrate_explicit<EXG_LIE_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial, w.grav_splits,
-                                                                gravity_on, G, w.conn, w.nj, w.inc_ptr, w.inc_ref, dt);
-      break;
-    case EXG_SYMPLECTIC_EULER:
-      k_integrate_explicit<EXG_SYMPLECTIC_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial,
-                                                                       w.grav_splits, gravity_on, G, w.conn, w.nj,
-                                                                       w.inc_ptr, w.inc_ref, dt);
-      break;
-    default:
-      k_integrate_explicit<EXG_EXPLICIT_EULER><<<grid, 128, 0, s>>>(v, w.pose, w.mom, w.pos_mass, w.grav_partial,
-                                                                     w.grav_splits, gravity_on, G, w.conn, w.nj,
-                                                                     w.inc_ptr, w.inc_ref, dt);
-      break;
-  }
-  prof_end(dev, _tok, s);
+int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
+  if (w.n <= 0 || !w.any_explicit) return EXG_OK;
+  int tok = prof_begin(dev, PROF_INTEGRATE, s);
+  k_integrate_explicit<<<(w.n + 127) / 128, 128, 0, s>>>(view_of(w), w.pose, w.mom, w.pos_mass, w.grav_partial,
+                                                         w.world_of_body, w.wparams, w.w_poff, w.w_splits, w.w_n,
+                                                         w.w_body_off, w.conn, w.nj, w.inc_ptr, w.inc_ref);
+  prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

@@ -188,11 +188,14 @@ int exg_law_lookup(const char* name, int32_t* law_out, int32_t* n_params_out) {
   return EXG_ERR_NO_SHADER;
 }
 
+}  // extern "C"
+
 static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t* joints, int32_t nj,
                           const exg_step_params_t* p) {
   if (n < 0 || nj < 0 || (n > 0 && !bodies) || (nj > 0 && !joints) || !p) return EXG_ERR_INVALID_ARGUMENT;
   if (p->integrator < 0 || p->integrator > EXG_NEWTON) return EXG_ERR_INVALID_ARGUMENT;
   if (p->gravity_law < 0 || p->gravity_law > EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
+  if (p->precision != EXG_PRECISION_F64 && p->precision != EXG_PRECISION_MIXED) return EXG_ERR_INVALID_ARGUMENT;
   if (p->gravity_law == EXG_GRAVITY_PLUMMER && !(p->softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   if (!(p->dt > 0.0) || !(p->warp >= 1.0)) return EXG_ERR_INVALID_ARGUMENT;
   for (int32_t i = 0; i < n; ++i)
@@ -205,47 +208,136 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
   return EXG_OK;
 }
 
-static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t n) {
-  std::vector<double> pose(8 * (size_t)n), mom(6 * (size_t)n), mass(n), inertia(9 * (size_t)n), size(n);
-  std::vector<int> kin(n), diag(n);
-  for (int32_t i = 0; i < n; ++i) {
-    for (int c = 0; c < 8; ++c) pose[(size_t)c * n + i] = bodies[i].pose[c];
-    for (int c = 0; c < 6; ++c) mom[(size_t)c * n + i] = bodies[i].momentum[c];
-    for (int c = 0; c < 9; ++c) inertia[(size_t)c * n + i] = bodies[i].inertia[c];
+static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count) {
+  DeviceWorld& w = W->w;
+  const int n = w.n;
+  std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
+      size(count);
+  std::vector<int> kin(count), diag(count);
+  for (int32_t i = 0; i < count; ++i) {
+    for (int c = 0; c < 8; ++c) pose[(size_t)c * count + i] = bodies[i].pose[c];
+    for (int c = 0; c < 6; ++c) mom[(size_t)c * count + i] = bodies[i].momentum[c];
+    for (int c = 0; c < 9; ++c) inertia[(size_t)c * count + i] = bodies[i].inertia[c];
     mass[i] = bodies[i].mass;
     size[i] = bodies[i].size;
     kin[i] = bodies[i].kinematic;
     diag[i] = bodies[i].diagonal;
   }
   cudaStream_t s = W->dev->stream;
-  DeviceWorld& w = W->w;
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.pose, pose.data(), sizeof(double) * pose.size(), cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.mom, mom.data(), sizeof(double) * mom.size(), cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.mass, mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.inertia, inertia.data(), sizeof(double) * inertia.size(), cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.size, size.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.kinematic, kin.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.diagonal, diag.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  for (int c = 0; c < 8; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(w.pose + (size_t)c * n + first, pose.data() + (size_t)c * count, sizeof(double) * count,
+                                 cudaMemcpyHostToDevice, s));
+  for (int c = 0; c < 6; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(w.mom + (size_t)c * n + first, mom.data() + (size_t)c * count, sizeof(double) * count,
+                                 cudaMemcpyHostToDevice, s));
+  for (int c = 0; c < 9; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(w.inertia + (size_t)c * n + first, inertia.data() + (size_t)c * count,
+                                 sizeof(double) * count, cudaMemcpyHostToDevice, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(w.mass + first, mass.data(), sizeof(double) * count, cudaMemcpyHostToDevice, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(w.size + first, size.data(), sizeof(double) * count, cudaMemcpyHostToDevice, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(w.kinematic + first, kin.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(w.diagonal + first, diag.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   return EXG_OK;
 }
 
-int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n, const exg_joint_t* joints, int32_t nj,
-                     const exg_step_params_t* params, exg_world_t* out) {
-  if (!dev || !out) return EXG_ERR_INVALID_ARGUMENT;
-  int st = validate_world(bodies, n, joints, nj, params);
-  if (st != EXG_OK) return st;
+static int download_bodies(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count) {
+  DeviceWorld& w = W->w;
+  const int n = w.n;
+  std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
+      size(count);
+  std::vector<int> kin(count), diag(count);
+  cudaStream_t s = W->dev->stream;
+  for (int c = 0; c < 8; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(pose.data() + (size_t)c * count, w.pose + (size_t)c * n + first, sizeof(double) * count,
+                                 cudaMemcpyDeviceToHost, s));
+  for (int c = 0; c < 6; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(mom.data() + (size_t)c * count, w.mom + (size_t)c * n + first, sizeof(double) * count,
+                                 cudaMemcpyDeviceToHost, s));
+  for (int c = 0; c < 9; ++c)
+    EXG_CUDA_TRY(cudaMemcpyAsync(inertia.data() + (size_t)c * count, w.inertia + (size_t)c * n + first,
+                                 sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(mass.data(), w.mass + first, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(size.data(), w.size + first, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(kin.data(), w.kinematic + first, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(diag.data(), w.diagonal + first, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int32_t i = 0; i < count; ++i) {
+    for (int c = 0; c < 8; ++c) out[i].pose[c] = pose[(size_t)c * count + i];
+    for (int c = 0; c < 6; ++c) out[i].momentum[c] = mom[(size_t)c * count + i];
+    for (int c = 0; c < 9; ++c) out[i].inertia[c] = inertia[(size_t)c * count + i];
+    out[i].mass = mass[i];
+    out[i].size = size[i];
+    out[i].kinematic = kin[i];
+    out[i].diagonal = diag[i];
+  }
+  return EXG_OK;
+}
+
+template <class T> static int upload_vec(exg_world_s* W, T** dptr, const std::vector<T>& v) {
+  int rc = W->alloc(dptr, v.size());
+  if (rc != EXG_OK) return rc;
+  if (!v.empty())
+    EXG_CUDA_TRY(cudaMemcpyAsync(*dptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, W->dev->stream));
+  return EXG_OK;
+}
+
+extern "C" {
+
+int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* body_counts, const int32_t* joint_counts,
+                     const exg_body_t* bodies, const exg_joint_t* joints, const exg_step_params_t* params,
+                     exg_world_t* out) {
+  if (!dev || !out || n_worlds <= 0 || !body_counts || !joint_counts || !params) return EXG_ERR_INVALID_ARGUMENT;
+  long long n_total = 0, nj_total = 0;
+  for (int32_t wi = 0; wi < n_worlds; ++wi) {
+    if (body_counts[wi] < 0 || joint_counts[wi] < 0) return EXG_ERR_INVALID_ARGUMENT;
+    int st = validate_world(bodies + n_total, body_counts[wi], joints + nj_total, joint_counts[wi], params + wi);
+    if (st != EXG_OK) return st;
+    if (params[wi].precision != params[0].precision) return EXG_ERR_INVALID_ARGUMENT;
+    n_total += body_counts[wi];
+    nj_total += joint_counts[wi];
+  }
+  if (n_total > (1LL << 30) || nj_total > (1LL << 29)) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(dev->mu);
   cudaSetDevice(dev->ordinal);
   exg_world_s* W = new (std::nothrow) exg_world_s();
   if (!W) return EXG_ERR_OUT_OF_MEMORY;
   W->dev = dev;
-  W->p = *params;
+  W->p = params[0];
   DeviceWorld& w = W->w;
+  const int n = (int)n_total, nj = (int)nj_total;
   w.n = n;
   w.nj = nj;
-  w.gshape = gravity_pick_shape(n, dev->sm_count, params->precision);
-  w.grav_splits = w.gshape.splits;
+  w.n_worlds = n_worlds;
+  w.precision = params[0].precision;
+  w.h_params.assign(params, params + n_worlds);
+  std::vector<int> wob(n), woj(nj), law(n_worlds);
+  std::vector<double> eps(n_worlds);
+  std::vector<exg_joint_t> gj(joints, joints + nj);
+  int bo = 0, jo = 0;
+  for (int32_t wi = 0; wi < n_worlds; ++wi) {
+    w.h_body_off.push_back(bo);
+    w.h_n.push_back(body_counts[wi]);
+    w.h_joint_off.push_back(jo);
+    w.h_nj.push_back(joint_counts[wi]);
+    for (int i = 0; i < body_counts[wi]; ++i) wob[bo + i] = wi;
+    for (int k = 0; k < joint_counts[wi]; ++k) {
+      woj[jo + k] = wi;
+      gj[jo + k].a += bo;
+      gj[jo + k].b += bo;
+    }
+    law[wi] = params[wi].gravity_law;
+    eps[wi] = params[wi].softening;
+    if (params[wi].integrator == EXG_NEWTON) w.any_newton = true; else w.any_explicit = true;
+    bo += body_counts[wi];
+    jo += joint_counts[wi];
+  }
+  std::vector<GravItem> items;
+  std::vector<int> splits;
+  std::vector<long long> poff;
+  long long partial_len = 0;
+  gravity_plan(w.h_body_off, w.h_n, law, eps, dev->sm_count, items, splits, poff, partial_len);
+  w.n_items = (int)items.size();
   int rc = EXG_OK;
 #define ALLOC(ptr, cnt) \
   if (rc == EXG_OK) rc = W->alloc(&(ptr), (cnt))
@@ -256,38 +348,43 @@ int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n, cons
   ALLOC(w.size, (size_t)n);
   ALLOC(w.kinematic, (size_t)n);
   ALLOC(w.diagonal, (size_t)n);
-  ALLOC(w.joints, (size_t)nj);
-  ALLOC(w.inc_ptr, (size_t)n + 1);
-  ALLOC(w.inc_ref, 2 * (size_t)nj);
   ALLOC(w.pos_mass, 4 * (size_t)n);
   ALLOC(w.wvel, 6 * (size_t)n);
-  ALLOC(w.grav_partial, (size_t)w.grav_splits * 3 * n);
+  ALLOC(w.grav_partial, (size_t)std::max<long long>(partial_len, 1));
   ALLOC(w.conn, 12 * (size_t)nj);
+  ALLOC(w.item_head, 1);
 #undef ALLOC
-  if (rc != EXG_OK) { delete W; return rc; }
   // incidence: per body, its joint ends in joint order (accelerator/mod.rs:289-331)
   std::vector<int> cnt(n + 1, 0), ptr(n + 1, 0), ref(2 * (size_t)nj);
-  for (int32_t k = 0; k < nj; ++k) { cnt[joints[k].a]++; cnt[joints[k].b]++; }
-  for (int32_t i = 0; i < n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
+  for (int k = 0; k < nj; ++k) { cnt[gj[k].a]++; cnt[gj[k].b]++; }
+  for (int i = 0; i < n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
   std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-  for (int32_t k = 0; k < nj; ++k) { ref[fill[joints[k].a]++] = 2 * k; ref[fill[joints[k].b]++] = 2 * k + 1; }
-  cudaStream_t s = dev->stream;
-  if (nj > 0) {
-    if (cudaMemcpyAsync(w.joints, joints, sizeof(exg_joint_t) * nj, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(w.inc_ref, ref.data(), sizeof(int) * ref.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
-      rc = EXG_ERR_BACKEND;
-  }
-  if (rc == EXG_OK && cudaMemcpyAsync(w.inc_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    rc = EXG_ERR_BACKEND;
-  if (rc == EXG_OK) rc = upload_bodies(W, bodies, n);
-  if (rc == EXG_OK && params->integrator == EXG_NEWTON) {
+  for (int k = 0; k < nj; ++k) { ref[fill[gj[k].a]++] = 2 * k; ref[fill[gj[k].b]++] = 2 * k + 1; }
+  if (rc == EXG_OK) rc = upload_vec(W, &w.joints, gj);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.world_of_body, wob);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.world_of_joint, woj);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.inc_ptr, ptr);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.inc_ref, ref);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.wparams, w.h_params);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.w_poff, poff);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.w_splits, splits);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.w_n, w.h_n);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.w_body_off, w.h_body_off);
+  if (rc == EXG_OK) rc = upload_vec(W, &w.items, items);
+  if (rc == EXG_OK) rc = upload_bodies(W, bodies, 0, n);
+  if (rc == EXG_OK && w.any_newton) {
     W->newton = new (std::nothrow) NewtonWorld();
     if (!W->newton) rc = EXG_ERR_OUT_OF_MEMORY;
-    else rc = W->newton->init(dev, w, bodies, joints, *params);
+    else rc = W->newton->init(dev, w, bodies, gj.data(), params[0]);
   }
   if (rc != EXG_OK) { delete W; return rc; }
   *out = W;
   return EXG_OK;
+}
+
+int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n, const exg_joint_t* joints, int32_t nj,
+                     const exg_step_params_t* params, exg_world_t* out) {
+  return exg_batch_create(dev, 1, &n, &nj, bodies, joints, params, out);
 }
 
 int exg_world_destroy(exg_world_t W) {
@@ -299,105 +396,84 @@ int exg_world_destroy(exg_world_t W) {
   return EXG_OK;
 }
 
-// One explicit step's launches (bridge.rs:19-63 over Mechanism::step).
-static int enqueue_explicit_step(exg_world_s* W, int* kernels) {
+}  // extern "C"
+
+// One step of every world of the batch (Mechanism::step per world, all enqueued asynchronously):
+// charges and world twists, gravity, explicit joints and integration, then the implicit islands.
+static int enqueue_step(exg_world_s* W, int* kernels) {
   DeviceWorld& w = W->w;
-  const exg_step_params_t& p = W->p;
   cudaStream_t s = W->dev->stream;
-  int k = 0, rc;
+  uint64_t before = W->dev->launches.load();
+  int rc;
   if ((rc = launch_body_pre(W->dev, w, s)) != EXG_OK) return rc;
-  ++k;
-  bool grav = p.gravity_law != EXG_GRAVITY_OFF && w.n > 1;
-  if (grav) {
-    if ((rc = launch_gravity(W->dev, w.pos_mass, w.size, w.n, p.gravity_law, p.softening, p.precision, w.gshape,
-                             w.grav_partial, s)) != EXG_OK)
-      return rc;
-    ++k;
-  }
-  if (w.nj > 0) {
-    if ((rc = launch_joints_plain_world(W->dev, w, p.dt, p.warp, s)) != EXG_OK) return rc;
-    ++k;
-  }
-  if ((rc = launch_integrate_explicit(W->dev, w, p.integrator, grav ? 1 : 0, p.G, p.dt, s)) != EXG_OK) return rc;
-  ++k;
-  *kernels = k;
+  if ((rc = launch_gravity_items(W->dev, w.pos_mass, w.size, w.items, w.n_items, w.item_head, w.precision,
+                                 w.grav_partial, s)) != EXG_OK)
+    return rc;
+  if ((rc = launch_joints_plain_world(W->dev, w, s)) != EXG_OK) return rc;
+  if ((rc = launch_integrate_explicit(W->dev, w, s)) != EXG_OK) return rc;
+  if (W->newton && (rc = W->newton->enqueue(W->dev, w, s)) != EXG_OK) return rc;
+  *kernels = (int)(W->dev->launches.load() - before);
   return EXG_OK;
 }
+
+static int step_locked(exg_world_s* W, int32_t n_steps) {
+  cudaStream_t s = W->dev->stream;
+  if (W->dev->profiling) {
+    for (int32_t k = 0; k < n_steps; ++k) {
+      int kernels = 0;
+      int rc = enqueue_step(W, &kernels);
+      if (rc != EXG_OK) return rc;
+    }
+  } else {
+    if (!W->graph) {
+      // capture one step; replays skip the per-launch host cost
+      cudaGraph_t g;
+      EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      int kernels = 0;
+      uint64_t before = W->dev->launches.load();
+      int rc = enqueue_step(W, &kernels);
+      W->dev->launches.store(before);  // captured, not yet launched
+      cudaError_t e = cudaStreamEndCapture(s, &g);
+      if (rc != EXG_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
+      EXG_CUDA_TRY(e);
+      cudaError_t ie = cudaGraphInstantiate(&W->graph, g, 0);
+      cudaGraphDestroy(g);
+      EXG_CUDA_TRY(ie);
+      W->graph_kernels = kernels;
+    }
+    for (int32_t k = 0; k < n_steps; ++k) {
+      EXG_CUDA_TRY(cudaGraphLaunch(W->graph, s));
+      W->dev->launches.fetch_add(W->graph_kernels);
+    }
+  }
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  W->stats.steps += n_steps;
+  W->stats.last_spans = 1;
+  if (W->newton) {
+    int rc = W->newton->read_stats(-1, &W->stats);
+    if (rc != EXG_OK) return rc;
+    if (W->stats.fatal) return EXG_ERR_FATAL;
+  }
+  return EXG_OK;
+}
+
+extern "C" {
 
 int exg_world_step(exg_world_t W, int32_t n_steps) {
   if (!W || n_steps < 0) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
-  if (W->p.integrator == EXG_NEWTON) {
-    int rc = W->newton->step(W->dev, W->w, W->p, n_steps, &W->stats);
-    if (rc == EXG_OK) W->stats.steps += n_steps;
-    return rc;
-  }
-  cudaStream_t s = W->dev->stream;
-  if (W->dev->profiling) {
-    // direct launches so each kernel can be bracketed by events
-    for (int32_t k = 0; k < n_steps; ++k) {
-      int kernels = 0;
-      int rc = enqueue_explicit_step(W, &kernels);
-      if (rc != EXG_OK) return rc;
-    }
-    EXG_CUDA_TRY(cudaStreamSynchronize(s));
-    W->stats.steps += n_steps;
-    W->stats.last_spans = 1;
-    return EXG_OK;
-  }
-  if (!W->graph) {
-    // capture one step; replays skip the per-launch host cost
-    cudaGraph_t g;
-    EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int kernels = 0;
-    uint64_t before = W->dev->launches.load();
-    int rc = enqueue_explicit_step(W, &kernels);
-    W->dev->launches.store(before);  // captured, not yet launched
-    cudaError_t e = cudaStreamEndCapture(s, &g);
-    if (rc != EXG_OK) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
-    EXG_CUDA_TRY(e);
-    cudaError_t ie = cudaGraphInstantiate(&W->graph, g, 0);
-    cudaGraphDestroy(g);
-    EXG_CUDA_TRY(ie);
-    W->graph_kernels = kernels;
-  }
-  for (int32_t k = 0; k < n_steps; ++k) {
-    EXG_CUDA_TRY(cudaGraphLaunch(W->graph, s));
-    W->dev->launches.fetch_add(W->graph_kernels);
-  }
-  EXG_CUDA_TRY(cudaStreamSynchronize(s));
-  W->stats.steps += n_steps;
-  W->stats.last_spans = 1;
-  return EXG_OK;
+  return step_locked(W, n_steps);
 }
 
 int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
   if (!W || !out || n != W->w.n) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
-  DeviceWorld& w = W->w;
-  std::vector<double> pose(8 * (size_t)n), mom(6 * (size_t)n), mass(n), inertia(9 * (size_t)n), size(n);
-  std::vector<int> kin(n), diag(n);
-  cudaStream_t s = W->dev->stream;
-  EXG_CUDA_TRY(cudaMemcpyAsync(pose.data(), w.pose, sizeof(double) * pose.size(), cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(mom.data(), w.mom, sizeof(double) * mom.size(), cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(mass.data(), w.mass, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(inertia.data(), w.inertia, sizeof(double) * inertia.size(), cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(size.data(), w.size, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(kin.data(), w.kinematic, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(diag.data(), w.diagonal, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaStreamSynchronize(s));
-  for (int32_t i = 0; i < n; ++i) {
-    for (int c = 0; c < 8; ++c) out[i].pose[c] = pose[(size_t)c * n + i];
-    for (int c = 0; c < 6; ++c) out[i].momentum[c] = mom[(size_t)c * n + i];
-    for (int c = 0; c < 9; ++c) out[i].inertia[c] = inertia[(size_t)c * n + i];
-    out[i].mass = mass[i];
-    out[i].size = size[i];
-    out[i].kinematic = kin[i];
-    out[i].diagonal = diag[i];
-  }
-  return EXG_OK;
+  return download_bodies(W, out, 0, n);
 }
 
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
@@ -406,12 +482,42 @@ int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
   cudaSetDevice(W->dev->ordinal);
   for (int32_t i = 0; i < n; ++i)
     if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  return upload_bodies(W, bodies, n);
+  return upload_bodies(W, bodies, 0, n);
+}
+
+int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n) {
+  if (!W || !out || world < 0 || world >= W->w.n_worlds || n != W->w.h_n[world]) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  return download_bodies(W, out, W->w.h_body_off[world], n);
+}
+
+int exg_batch_set_world(exg_world_t W, int32_t world, const exg_body_t* bodies, int32_t n) {
+  if (!W || !bodies || world < 0 || world >= W->w.n_worlds || n != W->w.h_n[world]) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  for (int32_t i = 0; i < n; ++i)
+    if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
+  return upload_bodies(W, bodies, W->w.h_body_off[world], n);
 }
 
 int exg_world_stats(exg_world_t W, exg_world_stats_t* out) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
   *out = W->stats;
+  return EXG_OK;
+}
+
+int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) {
+  if (!W || !out || world < 0 || world >= W->w.n_worlds) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  *out = W->stats;
+  out->last_spans = 1;
+  out->last_newton_iterations = 0;
+  out->max_depth_reached = 0;
+  out->fatal = 0;
+  out->last_residual = 0.0;
+  if (W->newton && W->w.h_params[world].integrator == EXG_NEWTON) return W->newton->read_stats(world, out);
   return EXG_OK;
 }
 
@@ -425,7 +531,14 @@ int exg_world_energy(exg_world_t W, double* out) {
   if (W->w.nj > 0) {
     EXG_CUDA_TRY(cudaMemcpy(joints.data(), W->w.joints, sizeof(exg_joint_t) * W->w.nj, cudaMemcpyDeviceToHost));
   }
-  *out = host_world_energy(b.data(), n, joints.data(), W->w.nj, W->p);
+  double e = 0.0;
+  for (int wi = 0; wi < W->w.n_worlds; ++wi) {
+    int bo = W->w.h_body_off[wi], jo = W->w.h_joint_off[wi];
+    std::vector<exg_joint_t> local(joints.begin() + jo, joints.begin() + jo + W->w.h_nj[wi]);
+    for (auto& j : local) { j.a -= bo; j.b -= bo; }
+    e += host_world_energy(b.data() + bo, W->w.h_n[wi], local.data(), (int)local.size(), W->w.h_params[wi]);
+  }
+  *out = e;
   return EXG_OK;
 }
 
@@ -434,6 +547,24 @@ int exg_motor_exp(const double twist[6], double dt, double out[8]) {
   double b[6];
   exg::screw_from6(twist, b);
   exg::twist_exp(b, dt, out);
+  return EXG_OK;
+}
+int exg_motor_exp_n(int64_t count, const double* twists, double dt, double* out) {
+  if (count < 0 || (count > 0 && (!twists || !out))) return EXG_ERR_INVALID_ARGUMENT;
+  for (int64_t k = 0; k < count; ++k) {
+    double b[6];
+    exg::screw_from6(twists + 6 * k, b);
+    exg::twist_exp(b, dt, out + 8 * k);
+  }
+  return EXG_OK;
+}
+int exg_motor_compose_n(int64_t count, const double* a, const double* b, double* out) {
+  if (count < 0 || (count > 0 && (!a || !b || !out))) return EXG_ERR_INVALID_ARGUMENT;
+  for (int64_t k = 0; k < count; ++k) {
+    double r[8];
+    exg::motor_compose(a + 8 * k, b + 8 * k, r);
+    for (int c = 0; c < 8; ++c) out[8 * k + c] = r[c];
+  }
   return EXG_OK;
 }
 int exg_motor_compose(const double a[8], const double b[8], double out[8]) {
@@ -482,17 +613,35 @@ int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double*
   if (!dev || n < 0 || (n > 0 && (!d_pos_mass || !d_force))) return EXG_ERR_INVALID_ARGUMENT;
   if (law == EXG_GRAVITY_SIZE_CORE && n > 0 && !d_size) return EXG_ERR_INVALID_ARGUMENT;
   if (law != EXG_GRAVITY_SIZE_CORE && law != EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
+  if (law == EXG_GRAVITY_PLUMMER && !(softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   if (n == 0) return EXG_OK;
   std::lock_guard<std::mutex> lock(dev->mu);
   cudaSetDevice(dev->ordinal);
-  GravityShape sh = gravity_pick_shape(n, dev->sm_count, precision);
+  cudaStream_t s = dev->stream;
+  if (n == 1) {
+    EXG_CUDA_TRY(cudaMemsetAsync(d_force, 0, 3 * sizeof(double), s));
+    EXG_CUDA_TRY(cudaStreamSynchronize(s));
+    return EXG_OK;
+  }
+  std::vector<GravItem> items;
+  std::vector<int> splits;
+  std::vector<long long> poff;
+  long long plen = 0;
+  gravity_plan({0}, {n}, {law}, {softening}, dev->sm_count, items, splits, poff, plen);
   double* partial = nullptr;
-  EXG_CUDA_TRY(cudaMallocAsync(&partial, sizeof(double) * 3 * (size_t)n * sh.splits, dev->stream));
-  int rc = launch_gravity(dev, d_pos_mass, d_size, n, law, softening, precision, sh, partial, dev->stream);
-  if (rc == EXG_OK) rc = launch_gravity_reduce(dev, partial, d_pos_mass, n, sh.splits, G, d_force, dev->stream);
-  cudaFreeAsync(partial, dev->stream);
+  GravItem* d_items = nullptr;
+  int* head = nullptr;
+  EXG_CUDA_TRY(cudaMallocAsync(&partial, sizeof(double) * plen, s));
+  EXG_CUDA_TRY(cudaMallocAsync(&d_items, sizeof(GravItem) * items.size(), s));
+  EXG_CUDA_TRY(cudaMallocAsync(&head, sizeof(int), s));
+  EXG_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), sizeof(GravItem) * items.size(), cudaMemcpyHostToDevice, s));
+  int rc = launch_gravity_items(dev, d_pos_mass, d_size, d_items, (int)items.size(), head, precision, partial, s);
+  if (rc == EXG_OK) rc = launch_gravity_reduce(dev, partial, d_pos_mass, n, splits[0], G, d_force, s);
+  cudaFreeAsync(partial, s);
+  cudaFreeAsync(d_items, s);
+  cudaFreeAsync(head, s);
   if (rc != EXG_OK) return rc;
-  EXG_CUDA_TRY(cudaStreamSynchronize(dev->stream));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
   return EXG_OK;
 }
 

@@ -1,6 +1,6 @@
 // Internal definitions shared by the translation units of libexg: the device context, the
-// device-resident world (structure-of-arrays), error plumbing and the launch wrappers each
-// .cu file provides.
+// device-resident batch of worlds (structure-of-arrays), error plumbing and the launch wrappers
+// each .cu file provides.
 #pragma once
 #include <cuda_runtime.h>
 #include <atomic>
@@ -50,14 +50,30 @@ inline int exg_after_launch(exg_device_s* dev) {
   return EXG_OK;
 }
 
-// Gravity launch shape: i-tile width (threads per CTA) and the number of j-splits whose
-// partial forces are summed in a fixed order afterwards (deterministic, no atomics).
-struct GravityShape { int tile; int splits; };
-GravityShape gravity_pick_shape(int n, int sm_count, int precision);
+// One unit of gravity work: an i-tile of one world's bodies against a j-range of the same world.
+// The partial sum  sum_j m_j r_ij / core^3  of body (body_off + i) lands at
+// partial[out_off + c * n + (i - 0)] for component c.
+struct GravItem {
+  int body_off;   // first body of the world (global index)
+  int n;          // bodies in the world
+  int i0;         // first i (world-local) of the tile
+  int j0, j1;     // world-local j range
+  int law;        // EXG_GRAVITY_SIZE_CORE or EXG_GRAVITY_PLUMMER
+  double eps2;    // Plummer softening squared
+  long long out_off;
+};
+constexpr int kGravTile = 128;
 
-// World storage. Per-body quantities are stored component-major: comp c of body i at [c*n + i].
+// Build the gravity work items of a set of worlds (descending work, so the persistent kernel
+// schedules longest-first). Returns the per-world split count and partial offset.
+void gravity_plan(const std::vector<int>& body_off, const std::vector<int>& n, const std::vector<int>& law,
+                  const std::vector<double>& eps, int sm_count, std::vector<GravItem>& items,
+                  std::vector<int>& splits, std::vector<long long>& poff, long long& partial_len);
+
+// Device-resident batch of worlds. Per-body quantities are component-major over all bodies of
+// the batch: component c of body i at [c*n + i].
 struct DeviceWorld {
-  int n = 0, nj = 0;
+  int n = 0, nj = 0, n_worlds = 0, precision = 0;
   double* pose = nullptr;      // [8][n]
   double* mom = nullptr;       // [6][n] body-frame momentum
   double* mass = nullptr;      // [n]
@@ -65,26 +81,39 @@ struct DeviceWorld {
   double* size = nullptr;      // [n]
   int* kinematic = nullptr;    // [n]
   int* diagonal = nullptr;     // [n]
-  exg_joint_t* joints = nullptr;  // [nj]
+  int* world_of_body = nullptr;     // [n]
+  exg_joint_t* joints = nullptr;    // [nj], body indices global to the batch
+  int* world_of_joint = nullptr;    // [nj]
   int* inc_ptr = nullptr;      // [n+1] body -> incident joint ends (CSR)
   int* inc_ref = nullptr;      // [2*nj] joint*2 + end, in joint order
+  // per world
+  exg_step_params_t* wparams = nullptr;  // [n_worlds]
+  long long* w_poff = nullptr;           // gravity partial offset per world
+  int* w_splits = nullptr;               // gravity splits per world (0: no gravity)
+  int* w_n = nullptr;                    // bodies per world
+  int* w_body_off = nullptr;             // first body of each world
+  // gravity work items and the persistent scheduler's counter
+  GravItem* items = nullptr;
+  int n_items = 0;
+  int* item_head = nullptr;
   // per-step scratch
-  double* pos_mass = nullptr;  // [n] x,y,z,m (double4)
-  double* wvel = nullptr;      // [6][n] world twist (lin, ang)
-  double* grav_partial = nullptr;  // [splits][3][n]
-  double* conn = nullptr;      // [12][nj]
-  int grav_splits = 1;
-  GravityShape gshape{64, 1};
+  double* pos_mass = nullptr;      // [n] x,y,z,m (double4)
+  double* wvel = nullptr;          // [6][n] world twist (lin, ang)
+  double* grav_partial = nullptr;  // per world [splits][3][n_w]
+  double* conn = nullptr;          // [12][nj]
+  bool any_explicit = false, any_newton = false;
+  // host mirrors
+  std::vector<exg_step_params_t> h_params;
+  std::vector<int> h_body_off, h_n, h_joint_off, h_nj;
 };
 
 // ── launch wrappers (each returns an exg_status) ─────────────────────────────
 int launch_body_pre(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);
-int launch_gravity(exg_device_s* dev, const double* pos_mass, const double* size, int n, int law, double softening,
-                   int precision, GravityShape shape, double* partial, cudaStream_t s);
+int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double* size, const GravItem* items, int n_items,
+                         int* head, int precision, double* partial, cudaStream_t s);
 int launch_gravity_reduce(exg_device_s* dev, const double* partial, const double* pos_mass, int n, int splits, double G,
                           double* force_out, cudaStream_t s);
-int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, double dt, double warp, cudaStream_t s);
+int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);
 int launch_joints_stage(exg_device_s* dev, const exg_joint_t* joints, int nj, const double* pose_aos, const double* vel_aos,
                         double dt, double warp, int jacobian, double* out, cudaStream_t s);
-int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, int scheme, int gravity_on, double G, double dt,
-                              cudaStream_t s);
+int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);

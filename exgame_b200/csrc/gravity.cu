@@ -1,18 +1,23 @@
-// All-pairs gravity (crates/newton/src/gravity.rs:110-140, 438-450 and the Plummer law of the
-// synthetic workloads).
+// All-pairs gravity over a batch of worlds (crates/newton/src/gravity.rs:110-140, 438-450, and
+// the Plummer law of the synthetic workloads).
 //
-// Layout and decomposition:
-//   * bodies arrive as double4 (x, y, z, m); kinematic bodies carry m = 0 and so exert and
-//     feel no force (the reference gives them no gravitational charge, gravity.rs:485-497);
-//   * a CTA owns an i-tile of TILE bodies (one body per thread) and one of `splits` j-ranges;
-//     j-tiles of TILE bodies are staged in shared memory and read back as broadcasts;
-//   * the CTA writes its partial sum  sum_j m_j r_ij / core^3  to partial[split][3][n]; the
-//     consumer adds the splits in index order and multiplies by G m_i, so the result does not
-//     depend on scheduling (no atomics).
+// Work decomposition: a work item is an i-tile of kGravTile bodies of one world against a
+// j-range of the same world (bodies of different worlds never interact). Items are listed
+// largest-first and pulled by persistent CTAs through an atomic counter, so worlds of very
+// uneven size (8 .. 8192 bodies) share the GPU without a tail of idle SMs. Within an item each
+// thread owns one i-body; j-bodies are staged through shared memory in tiles of kGravTile and
+// read back as broadcasts. The item writes its partial sum  sum_j m_j r_ij / core^3  to its own
+// slot; consumers add a world's splits in index order and multiply by G m_i, so results do not
+// depend on scheduling (no atomics on the data).
+//
+// Kinematic bodies carry m = 0 in the charge array and so exert no force (the reference gives
+// them no gravitational charge, gravity.rs:485-497).
+//
 // Precision: R = double is the plain path. R = float is the mixed path: positions are taken
-// relative to the i-tile's first body (one double subtraction per staged j-body, amortised over
-// the tile), pair terms are FP32 with the hardware reciprocal square root, and each j-tile's
-// FP32 partial is flushed into an FP64 accumulator, so rounding does not grow with n.
+// relative to the item's first i-body (one double subtraction per staged j-body, amortised over
+// the tile), pair terms are FP32 with the hardware reciprocal square root, and each j-tile's FP32
+// partial is flushed into an FP64 accumulator, so rounding does not grow with the world size.
+#include <algorithm>
 #include "exg_internal.cuh"
 
 namespace {
@@ -25,83 +30,91 @@ template <class R> struct Vec4;
 template <> struct Vec4<double> { typedef double4 T; };
 template <> struct Vec4<float> { typedef float4 T; };
 
-// LAW 1 = size core (reference), 2 = Plummer
-template <class R, int LAW, int TILE>
-__global__ void __launch_bounds__(TILE) k_gravity(const double4* __restrict__ pm, const double* __restrict__ size, int n,
-                                                  R eps2, int split_len, double* __restrict__ partial) {
+template <class R>
+__global__ void __launch_bounds__(kGravTile) k_gravity_items(const double4* __restrict__ pm, const double* __restrict__ size,
+                                                             const GravItem* __restrict__ items, int n_items,
+                                                             int* __restrict__ head, double* __restrict__ partial) {
+  constexpr int T = kGravTile;
   typedef typename Vec4<R>::T V4;
-  __shared__ V4 tile[TILE];
-  __shared__ R tsz2[LAW == 1 ? TILE : 1];
-  __shared__ R tisz3[LAW == 1 ? TILE : 1];
-  const int i = blockIdx.x * TILE + threadIdx.x;
-  const int split = blockIdx.y;
-  const int j0 = split * split_len;
-  const int j1 = min(n, j0 + split_len);
-  // reference point: first body of the i-tile (mixed path only)
-  double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
-  if (sizeof(R) == 4) c = pm[blockIdx.x * TILE];
-  double4 pi = (i < n) ? pm[i] : make_double4(0.0, 0.0, 0.0, 0.0);
-  const R xi = R(pi.x - c.x), yi = R(pi.y - c.y), zi = R(pi.z - c.z);
-  R sz2_i = R(0), isz3_i = R(0);
-  if (LAW == 1 && i < n) {
-    double s = size[i];
-    sz2_i = R(s * s);
-    isz3_i = R(1.0 / (s * s * s));
-  }
-  double dax = 0.0, day = 0.0, daz = 0.0;
-  for (int base = j0; base < j1; base += TILE) {
-    const int j = base + threadIdx.x;
-    if (j < j1) {
-      double4 q = pm[j];
+  __shared__ V4 tile[T];
+  __shared__ R tsz2[T];
+  __shared__ R tisz3[T];
+  __shared__ int cur;
+  for (;;) {
+    if (threadIdx.x == 0) cur = atomicAdd(head, 1);
+    __syncthreads();
+    const int it = cur;
+    __syncthreads();
+    if (it >= n_items) return;
+    const GravItem g = items[it];
+    const int il = g.i0 + threadIdx.x;
+    const bool valid = il < g.n;
+    const double4* wpm = pm + g.body_off;
+    double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (sizeof(R) == 4) c = wpm[g.i0];
+    const double4 pi = valid ? wpm[il] : c;
+    const R xi = R(pi.x - c.x), yi = R(pi.y - c.y), zi = R(pi.z - c.z);
+    const bool core_law = g.law == EXG_GRAVITY_SIZE_CORE;
+    R sz2_i = R(0), isz3_i = R(0);
+    if (core_law && valid) {
+      double s = size[g.body_off + il];
+      sz2_i = R(s * s);
+      isz3_i = R(1.0 / (s * s * s));
+    }
+    const R eps2 = R(g.eps2);
+    double dax = 0.0, day = 0.0, daz = 0.0;
+    for (int base = g.j0; base < g.j1; base += T) {
+      const int j = base + threadIdx.x;
       V4 t;
-      t.x = R(q.x - c.x); t.y = R(q.y - c.y); t.z = R(q.z - c.z); t.w = R(q.w);
-      tile[threadIdx.x] = t;
-      if (LAW == 1) {
-        double s = size[j];
-        tsz2[threadIdx.x] = R(s * s);
-        tisz3[threadIdx.x] = R(1.0 / (s * s * s));
+      if (j < g.j1) {
+        double4 q = wpm[j];
+        t.x = R(q.x - c.x); t.y = R(q.y - c.y); t.z = R(q.z - c.z); t.w = R(q.w);
+        if (core_law) {
+          double s = size[g.body_off + j];
+          tsz2[threadIdx.x] = R(s * s);
+          tisz3[threadIdx.x] = R(1.0 / (s * s * s));
+        }
+      } else {
+        t.x = R(0); t.y = R(0); t.z = R(0); t.w = R(0);
+        if (core_law) { tsz2[threadIdx.x] = R(1); tisz3[threadIdx.x] = R(0); }
       }
-    } else {
-      V4 t; t.x = R(0); t.y = R(0); t.z = R(0); t.w = R(0);
       tile[threadIdx.x] = t;
-      if (LAW == 1) { tsz2[threadIdx.x] = R(1); tisz3[threadIdx.x] = R(0); }
-    }
-    __syncthreads();
-    R ax = R(0), ay = R(0), az = R(0);
-    if (LAW == 2) {
+      __syncthreads();
+      R ax = R(0), ay = R(0), az = R(0);
+      if (!core_law) {
 #pragma unroll 8
-      for (int k = 0; k < TILE; ++k) {
-        V4 q = tile[k];
-        R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-        R s2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-        R inv = rsqrt_r<R>(s2);
-        R s = q.w * (inv * inv * inv);
-        ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
-      }
-    } else {
-      const int jb = base;
+        for (int k = 0; k < T; ++k) {
+          V4 q = tile[k];
+          R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+          R s2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+          R inv = rsqrt_r<R>(s2);
+          R s = q.w * (inv * inv * inv);
+          ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+        }
+      } else {
 #pragma unroll 4
-      for (int k = 0; k < TILE; ++k) {
-        V4 q = tile[k];
-        R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-        R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-        // core radius of the higher-slot body (gravity.rs:126-131)
-        bool j_hi = (jb + k) > i;
-        R sz2 = j_hi ? tsz2[k] : sz2_i;
-        R isz3 = j_hi ? tisz3[k] : isz3_i;
-        R inv = rsqrt_r<R>(r2);
-        R sd = (r2 >= sz2) ? inv * inv * inv : isz3;
-        // coincident bodies exert nothing (|d| < 1e-9, gravity.rs:119-122)
-        R s = (r2 < R(1e-18)) ? R(0) : q.w * sd;
-        ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+        for (int k = 0; k < T; ++k) {
+          V4 q = tile[k];
+          R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
+          R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+          // core radius of the higher-slot body (gravity.rs:126-131)
+          bool j_hi = (base + k) > il;
+          R sz2 = j_hi ? tsz2[k] : sz2_i;
+          R isz3 = j_hi ? tisz3[k] : isz3_i;
+          R inv = rsqrt_r<R>(r2);
+          R sd = (r2 >= sz2) ? inv * inv * inv : isz3;
+          // coincident bodies exert nothing (|d| < 1e-9, gravity.rs:119-122)
+          R s = (r2 < R(1e-18)) ? R(0) : q.w * sd;
+          ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+        }
       }
+      dax += double(ax); day += double(ay); daz += double(az);
+      __syncthreads();
     }
-    dax += double(ax); day += double(ay); daz += double(az);
-    __syncthreads();
-  }
-  if (i < n) {
-    double* p = partial + (size_t)split * 3 * n;
-    p[i] = dax; p[n + i] = day; p[2 * n + i] = daz;
+    if (valid) {
+      double* p = partial + g.out_off;
+      p[il] = dax; p[g.n + il] = day; p[2 * (size_t)g.n + il] = daz;
+    }
   }
 }
 
@@ -117,59 +130,66 @@ __global__ void k_gravity_reduce(const double* __restrict__ partial, const doubl
   }
 }
 
-template <class R, int LAW>
-int launch_t(exg_device_s* dev, const double* pos_mass, const double* size, int n, double softening, GravityShape sh,
-             double* partial, cudaStream_t s) {
-  int split_len = (n + sh.splits - 1) / sh.splits;
-  split_len = ((split_len + sh.tile - 1) / sh.tile) * sh.tile;
-  int splits = (n + split_len - 1) / split_len;
-  dim3 grid((n + sh.tile - 1) / sh.tile, splits);
-  R eps2 = R(softening * softening);
-  const double4* pm = reinterpret_cast<const double4*>(pos_mass);
-  int _tok = prof_begin(dev, PROF_GRAVITY, s);
-  switch (sh.tile) {
-    case 64: k_gravity<R, LAW, 64><<<grid, 64, 0, s>>>(pm, size, n, eps2, split_len, partial); break;
-    case 128: k_gravity<R, LAW, 128><<<grid, 128, 0, s>>>(pm, size, n, eps2, split_len, partial); break;
-    default: k_gravity<R, LAW, 256><<<grid, 256, 0, s>>>(pm, size, n, eps2, split_len, partial); break;
-  }
-  prof_end(dev, _tok, s);
-  if (splits < sh.splits) {
-    // the unused split slots must read as zero
-    cudaMemsetAsync(partial + (size_t)splits * 3 * n, 0, sizeof(double) * 3 * (size_t)n * (sh.splits - splits), s);
-  }
-  return exg_after_launch(dev);
-}
-
 }  // namespace
 
-GravityShape gravity_pick_shape(int n, int sm_count, int precision) {
-  GravityShape sh;
-  int sms = sm_count > 0 ? sm_count : 148;
-  if (n >= sms * 256 * 2) sh.tile = 256;
-  else if (n >= sms * 128) sh.tile = 128;
-  else sh.tile = 64;
-  int itiles = (n + sh.tile - 1) / sh.tile;
-  int target = sms * 8;
-  int splits = (target + itiles - 1) / itiles;
-  int max_splits = (n + sh.tile - 1) / sh.tile;
-  if (splits > max_splits) splits = max_splits;
-  if (splits > 32) splits = 32;
-  if (splits < 1) splits = 1;
-  sh.splits = splits;
-  (void)precision;
-  return sh;
+void gravity_plan(const std::vector<int>& body_off, const std::vector<int>& n, const std::vector<int>& law,
+                  const std::vector<double>& eps, int sm_count, std::vector<GravItem>& items, std::vector<int>& splits,
+                  std::vector<long long>& poff, long long& partial_len) {
+  // The j-range of an item depends on the world's own size only (the smallest power of two
+  // >= n/8, clamped to [128, 2048]), so a world's arithmetic — and its result, bit for bit — is
+  // the same stepped alone or inside any batch.
+  const int T = kGravTile;
+  const int W = (int)n.size();
+  (void)sm_count;
+  splits.assign(W, 0);
+  poff.assign(W, 0);
+  items.clear();
+  long long run = 0;
+  std::vector<std::pair<double, GravItem>> tmp;
+  for (int w = 0; w < W; ++w) {
+    if (law[w] == EXG_GRAVITY_OFF || n[w] <= 1) continue;
+    const int nw = n[w];
+    int L = T;
+    while (L < 2048 && L * 8 < nw) L *= 2;
+    const int itiles = (nw + T - 1) / T;
+    const int sp = (nw + L - 1) / L;
+    splits[w] = sp;
+    poff[w] = run;
+    for (int s = 0; s < sp; ++s)
+      for (int t = 0; t < itiles; ++t) {
+        GravItem g;
+        g.body_off = body_off[w];
+        g.n = nw;
+        g.i0 = t * T;
+        g.j0 = s * L;
+        g.j1 = std::min(nw, g.j0 + L);
+        g.law = law[w];
+        g.eps2 = eps[w] * eps[w];
+        g.out_off = run + (long long)s * 3 * nw;
+        double work = double(std::min(T, nw - g.i0)) * (g.j1 - g.j0);
+        tmp.push_back({work, g});
+      }
+    run += (long long)sp * 3 * nw;
+  }
+  std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  for (auto& x : tmp) items.push_back(x.second);
+  partial_len = run;
 }
 
-int launch_gravity(exg_device_s* dev, const double* pos_mass, const double* size, int n, int law, double softening,
-                   int precision, GravityShape shape, double* partial, cudaStream_t s) {
-  if (n <= 0) return EXG_OK;
-  if (law == EXG_GRAVITY_PLUMMER && !(softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  if (precision == EXG_PRECISION_MIXED) {
-    if (law == EXG_GRAVITY_PLUMMER) return launch_t<float, 2>(dev, pos_mass, size, n, softening, shape, partial, s);
-    return launch_t<float, 1>(dev, pos_mass, size, n, softening, shape, partial, s);
-  }
-  if (law == EXG_GRAVITY_PLUMMER) return launch_t<double, 2>(dev, pos_mass, size, n, softening, shape, partial, s);
-  return launch_t<double, 1>(dev, pos_mass, size, n, softening, shape, partial, s);
+int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double* size, const GravItem* items, int n_items,
+                         int* head, int precision, double* partial, cudaStream_t s) {
+  if (n_items <= 0) return EXG_OK;
+  EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
+  int sms = dev->sm_count > 0 ? dev->sm_count : 148;
+  int grid = std::min(n_items, sms * 12);
+  const double4* pm = reinterpret_cast<const double4*>(pos_mass);
+  int tok = prof_begin(dev, PROF_GRAVITY, s);
+  if (precision == EXG_PRECISION_MIXED)
+    k_gravity_items<float><<<grid, kGravTile, 0, s>>>(pm, size, items, n_items, head, partial);
+  else
+    k_gravity_items<double><<<grid, kGravTile, 0, s>>>(pm, size, items, n_items, head, partial);
+  prof_end(dev, tok, s);
+  return exg_after_launch(dev);
 }
 
 int launch_gravity_reduce(exg_device_s* dev, const double* partial, const double* pos_mass, int n, int splits, double G,

@@ -6,19 +6,23 @@
 
 namespace {
 
-// World form: poses [8][n] and world twists [6][n] component-major; output conn[12][nj].
-__global__ void k_joints_plain_world(const exg_joint_t* __restrict__ joints, int nj, const double* __restrict__ pose,
-                                     const double* __restrict__ wvel, int n, double dt, double warp,
+// World form: poses [8][n] and world twists [6][n] component-major; output conn[12][nj]. Joints
+// of worlds stepped by the implicit integrator are evaluated inside the Newton kernel instead.
+__global__ void k_joints_plain_world(const exg_joint_t* __restrict__ joints, const int* __restrict__ world_of_joint,
+                                     const exg_step_params_t* __restrict__ wparams, int nj,
+                                     const double* __restrict__ pose, const double* __restrict__ wvel, int n,
                                      double* __restrict__ conn) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nj) return;
+  const exg_step_params_t& P = wparams[world_of_joint[k]];
+  if (P.integrator == EXG_NEWTON) return;
   const exg_joint_t& jt = joints[k];
   double pa[8], pb[8], va[6], vb[6], out[12];
 #pragma unroll
   for (int c = 0; c < 8; ++c) { pa[c] = pose[(size_t)c * n + jt.a]; pb[c] = pose[(size_t)c * n + jt.b]; }
 #pragma unroll
   for (int c = 0; c < 6; ++c) { va[c] = wvel[(size_t)c * n + jt.a]; vb[c] = wvel[(size_t)c * n + jt.b]; }
-  exg::joint_plain<double>(jt.law, jt.params, pa, pb, va, vb, dt, warp, out);
+  exg::joint_plain<double>(jt.law, jt.params, pa, pb, va, vb, P.dt, P.warp, out);
 #pragma unroll
   for (int c = 0; c < 12; ++c) conn[(size_t)c * nj + k] = out[c];
 }
@@ -60,10 +64,11 @@ __global__ void k_joints_stage_jacobian(const exg_joint_t* __restrict__ joints, 
 
 }  // namespace
 
-int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, double dt, double warp, cudaStream_t s) {
-  if (w.nj <= 0) return EXG_OK;
+int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
+  if (w.nj <= 0 || !w.any_explicit) return EXG_OK;
   int _tok = prof_begin(dev, PROF_JOINTS, s);
-  k_joints_plain_world<<<(w.nj + 127) / 128, 128, 0, s>>>(w.joints, w.nj, w.pose, w.wvel, w.n, dt, warp, w.conn);
+  k_joints_plain_world<<<(w.nj + 127) / 128, 128, 0, s>>>(w.joints, w.world_of_joint, w.wparams, w.nj, w.pose, w.wvel,
+                                                          w.n, w.conn);
   prof_end(dev, _tok, s);
   return exg_after_launch(dev);
 }

@@ -76,15 +76,27 @@ struct WorldRef {
   const int* diagonal;
   const double* pos_mass;
   const double* grav_partial;
-  int n, splits, gravity_on;
-  double G, dt, warp, tol2;
+  const exg_step_params_t* wparams;
+  const long long* w_poff;
+  const int* w_splits;
+  const int* w_n;
+  const int* w_body_off;
+  int n;
+};
+
+// The island's world parameters, resolved once per island.
+struct IslandParams {
+  double dt, warp, tol2, G;
   int max_newton;
+  int splits, nw, wbody_off;
+  const double* part;
 };
 
 struct Ctx {
   NewtonDeviceArrays A;
   IslandDesc d;
   WorldRef W;
+  IslandParams P;
   Scratch s;
   int island;
   EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
@@ -144,7 +156,7 @@ __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
       int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
       double val[6], dd[36];
       joint_jacobian_slice<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a,
-                                   c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.W.dt, c.W.warp, slice, val, dd);
+                                   c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, slice, val, dd);
       double* o = c.s.jac + ((size_t)q * 4 + slice) * kJacStride;
 #pragma unroll
       for (int r = 0; r < 6; ++r) o[r] = val[r];
@@ -160,7 +172,7 @@ __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
       int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
       double out[12];
       joint_plain<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a, c.s.mid + 8 * b,
-                          v + 6 * a, v + 6 * b, c.W.dt, c.W.warp, out);
+                          v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, out);
 #pragma unroll
       for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
     }
@@ -467,14 +479,15 @@ __device__ void load_external(const Ctx& c) {
     double* e = c.s.ext + 6 * q;
 #pragma unroll
     for (int k = 0; k < 6; ++k) e[k] = 0.0;
-    if (!c.W.gravity_on) continue;
+    if (c.P.splits <= 0) continue;
     int g = c.gbody(q);
+    int il = g - c.P.wbody_off;
     double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
     double f[3];
     for (int k = 0; k < 3; ++k) {
       double acc = 0.0;
-      for (int s = 0; s < c.W.splits; ++s) acc += c.W.grav_partial[(size_t)s * 3 * c.W.n + (size_t)k * c.W.n + g];
-      f[k] = c.W.G * pm.w * acc;
+      for (int s = 0; s < c.P.splits; ++s) acc += c.P.part[(size_t)s * 3 * c.P.nw + (size_t)k * c.P.nw + il];
+      f[k] = c.P.G * pm.w * acc;
     }
     e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
     e[3] = pm.y * f[2] - pm.z * f[1];
@@ -491,7 +504,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
   __syncthreads();
   copy_bodies6(c, c.s.vm, c.s.best);
   __syncthreads();
-  for (int it = 0; it < c.W.max_newton; ++it) {
+  for (int it = 0; it < c.P.max_newton; ++it) {
     ++*iters;
     phase_pre(c, c.s.vm, half);
     __syncthreads();
@@ -504,7 +517,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
       copy_bodies6(c, c.s.vm, c.s.best);
     }
     __syncthreads();
-    if (rnorm <= c.W.tol2) { o.converged = true; break; }
+    if (rnorm <= c.P.tol2) { o.converged = true; break; }
     if (!(rnorm < kHuge)) break;
     o.a_norm2 = phase_assemble(c, half, red);
     o.assembled = true;
@@ -616,6 +629,18 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
     c.d = A.desc[c.island];
     c.W = W;
     c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+    {
+      const exg_step_params_t& wp = W.wparams[c.d.world];
+      c.P.dt = wp.dt;
+      c.P.warp = wp.warp;
+      c.P.tol2 = wp.tol * wp.tol;
+      c.P.G = wp.G;
+      c.P.max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
+      c.P.splits = W.w_splits[c.d.world];
+      c.P.nw = W.w_n[c.d.world];
+      c.P.wbody_off = W.w_body_off[c.d.world];
+      c.P.part = W.grav_partial + W.w_poff[c.d.world];
+    }
     load_external(c);
     __syncthreads();
     unsigned long long remaining = 1ull << kMaxDepth;
@@ -624,7 +649,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
     while (remaining > 0) {
       unsigned long long units = 1ull << (kMaxDepth - depth);
       while (units > remaining) { ++depth; units >>= 1; }
-      double span = W.dt;
+      double span = c.P.dt;
       for (int t = 0; t < depth; ++t) span = span / 2.0;
       double half = span / 2.0;
       ++spans;
@@ -674,6 +699,11 @@ NewtonWorld::~NewtonWorld() {
 int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodies, const exg_joint_t* joints,
                       const exg_step_params_t& p) {
   const int n = w.n, nj = w.nj;
+  // world of every body; only bodies of implicit worlds take part
+  std::vector<int> wob(n, 0);
+  for (int wi = 0; wi < w.n_worlds; ++wi)
+    for (int i = 0; i < w.h_n[wi]; ++i) wob[w.h_body_off[wi] + i] = wi;
+  auto implicit_body = [&](int i) { return w.h_params[wob[i]].integrator == EXG_NEWTON; };
   // islands = connected components of the joint graph, bodies ascending, joints ascending
   std::vector<int> parent(n);
   for (int i = 0; i < n; ++i) parent[i] = i;
@@ -688,14 +718,17 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
   std::vector<int> isl_of_root(n, -1);
   std::vector<std::vector<int>> ib, ij;
   for (int i = 0; i < n; ++i) {
+    if (!implicit_body(i)) continue;
     int r = find(i);
     if (isl_of_root[r] < 0) { isl_of_root[r] = (int)ib.size(); ib.emplace_back(); ij.emplace_back(); }
     ib[isl_of_root[r]].push_back(i);
   }
-  for (int k = 0; k < nj; ++k) ij[isl_of_root[find(joints[k].a)]].push_back(k);
+  for (int k = 0; k < nj; ++k)
+    if (implicit_body(joints[k].a)) ij[isl_of_root[find(joints[k].a)]].push_back(k);
   n_islands = (int)ib.size();
 
   std::vector<IslandDesc> desc(n_islands);
+  std::vector<int> local(n, -1);  // island-local index of each body of the island being built
   std::vector<int> h_isl_body, h_jl_law, h_jl_a, h_jl_b, h_ib_order, h_ib_inc_ptr, h_ib_inc_ref, h_dn_body, h_dn_parent,
       h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
   std::vector<double> h_jl_params;
@@ -704,12 +737,12 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
     const std::vector<int>& B = ib[I];
     const std::vector<int>& J = ij[I];
     IslandDesc& d = desc[I];
+    d.world = wob[B[0]];
     d.body_off = (int)h_isl_body.size();
     d.nb = (int)B.size();
     d.joint_off = (int)h_jl_law.size();
     d.nj = (int)J.size();
     max_nb = std::max(max_nb, d.nb);
-    std::vector<int> local(n, -1);
     for (int q = 0; q < d.nb; ++q) { local[B[q]] = q; h_isl_body.push_back(B[q]); }
     for (int q = 0; q < d.nj; ++q) {
       const exg_joint_t& jt = joints[J[q]];
@@ -842,6 +875,7 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
       }
       h_cell_ptr.push_back(base);
     }
+    for (int q = 0; q < d.nb; ++q) local[B[q]] = -1;
     d.scratch_off = scratch;
     scratch += scratch_doubles(d.nb, d.nj, m);
     scratch = (scratch + 31) & ~31LL;
@@ -892,40 +926,36 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
                            d_ch_idx,    d_cell_ptr, d_cell_terms, d_scratch, d_stats,     d_res};
   d_queue = d_q;
   d_head = d_q + n_islands;
+  island_world.resize(n_islands);
+  for (int I = 0; I < n_islands; ++I) island_world[I] = desc[I].world;
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   (void)p;
   return EXG_OK;
 }
 
-int NewtonWorld::step(exg_device_s* dev, DeviceWorld& w, const exg_step_params_t& p, int n_steps, exg_world_stats_t* st) {
-  cudaStream_t s = dev->stream;
+int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   if (n_islands == 0) return EXG_OK;
-  bool grav = p.gravity_law != EXG_GRAVITY_OFF && w.n > 1;
-  WorldRef W{w.pose, w.mom, w.mass, w.inertia, w.kinematic, w.diagonal, w.pos_mass, w.grav_partial,
-             w.n,    w.grav_splits, grav ? 1 : 0, p.G, p.dt, p.warp, p.tol * p.tol, p.max_newton > 0 ? p.max_newton : 32};
-  int grid = std::min(n_islands, std::max(1, dev->sm_count) * 4);
-  for (int k = 0; k < n_steps; ++k) {
-    int rc;
-    if (grav) {
-      if ((rc = launch_body_pre(dev, w, s)) != EXG_OK) return rc;
-      if ((rc = launch_gravity(dev, w.pos_mass, w.size, w.n, p.gravity_law, p.softening, p.precision, w.gshape,
-                               w.grav_partial, s)) != EXG_OK)
-        return rc;
-    }
-    EXG_CUDA_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), s));
-    int tok = prof_begin(dev, PROF_NEWTON, s);
-    k_newton_step<<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
-    prof_end(dev, tok, s);
-    if ((rc = exg_after_launch(dev)) != EXG_OK) return rc;
+  WorldRef W{w.pose,    w.mom,    w.mass,   w.inertia, w.kinematic,  w.diagonal, w.pos_mass,
+             w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.n};
+  int grid = std::min(n_islands, std::max(1, dev->sm_count) * 2);
+  EXG_CUDA_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), s));
+  int tok = prof_begin(dev, PROF_NEWTON, s);
+  k_newton_step<<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+  prof_end(dev, tok, s);
+  return exg_after_launch(dev);
+}
+
+int NewtonWorld::read_stats(int world, exg_world_stats_t* st) {
+  std::vector<int> stats(4 * (size_t)std::max(n_islands, 1));
+  std::vector<double> res(std::max(n_islands, 1));
+  if (n_islands > 0) {
+    EXG_CUDA_TRY(cudaMemcpy(stats.data(), arr.stats, sizeof(int) * 4 * n_islands, cudaMemcpyDeviceToHost));
+    EXG_CUDA_TRY(cudaMemcpy(res.data(), arr.residual, sizeof(double) * n_islands, cudaMemcpyDeviceToHost));
   }
-  EXG_CUDA_TRY(cudaStreamSynchronize(s));
-  std::vector<int> stats(4 * (size_t)n_islands);
-  std::vector<double> res(n_islands);
-  EXG_CUDA_TRY(cudaMemcpy(stats.data(), arr.stats, sizeof(int) * stats.size(), cudaMemcpyDeviceToHost));
-  EXG_CUDA_TRY(cudaMemcpy(res.data(), arr.residual, sizeof(double) * res.size(), cudaMemcpyDeviceToHost));
   int spans = 0, iters = 0, depth = 0, fatal = 0;
   double worst = 0.0;
   for (int I = 0; I < n_islands; ++I) {
+    if (world >= 0 && island_world[I] != world) continue;
     spans = std::max(spans, stats[4 * I]);
     iters = std::max(iters, stats[4 * I + 1]);
     depth = std::max(depth, stats[4 * I + 2]);
@@ -937,7 +967,7 @@ int NewtonWorld::step(exg_device_s* dev, DeviceWorld& w, const exg_step_params_t
   st->max_depth_reached = depth;
   st->fatal = fatal;
   st->last_residual = worst;
-  return fatal ? EXG_ERR_FATAL : EXG_OK;
+  return EXG_OK;
 }
 
 // ── host energy (the same algebra compiled for the host) ──────────────────────

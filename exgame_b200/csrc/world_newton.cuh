@@ -10,6 +10,7 @@
 #include "exg_internal.cuh"
 
 struct IslandDesc {
+  int world;             // the world (of the batch) the island belongs to
   int body_off, nb;      // island bodies: isl_body[body_off .. body_off+nb)
   int joint_off, nj;     // island joints: isl_joint[joint_off .. joint_off+nj)
   int dyn_off, m;        // dynamic nodes: dn_*[dyn_off .. dyn_off+m)
@@ -45,7 +46,11 @@ struct NewtonDeviceArrays {
 class NewtonWorld {
  public:
   int init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodies, const exg_joint_t* joints, const exg_step_params_t& p);
-  int step(exg_device_s* dev, DeviceWorld& w, const exg_step_params_t& p, int n_steps, exg_world_stats_t* stats);
+  // Enqueue one step of every island (no host synchronisation; graph-capturable).
+  int enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s);
+  // Aggregate the last step's per-island counters, over all islands (world < 0) or one world.
+  int read_stats(int world, exg_world_stats_t* stats);
+  int n_islands_total() const { return n_islands; }
   ~NewtonWorld();
 
  private:
@@ -54,6 +59,7 @@ class NewtonWorld {
   std::vector<void*> allocs;
   NewtonDeviceArrays arr{};
   std::vector<int> island_order;  // islands sorted by size, largest first
+  std::vector<int> island_world;
   int* d_queue = nullptr;         // island work queue (largest first) and its head counter
   int* d_head = nullptr;
 };

@@ -58,21 +58,23 @@ def gravity_world(n, radius=100.0, seed=0, G=1.0):
     sorted_r = r[order]
     first_idx = np.searchsorted(sorted_r, sorted_r, side="left")
     enclosed[order] = np.concatenate([[0.0], np.cumsum(mass[order])])[first_idx]
-    vel = np.zeros((n, 3))
-    zhat = np.array([0.0, 0.0, 1.0])
-    for i in range(n):
-        if r[i] == 0.0:
-            continue
-        rhat = rel[i] / r[i]
-        t = np.cross(zhat, rhat)
-        if np.linalg.norm(t) < 1e-12:
-            t = np.cross(random_unit(rng), rhat)
-        t /= np.linalg.norm(t)
-        vel[i] = math.sqrt(G * enclosed[i] / r[i]) * t
+    safe_r = np.where(r > 0.0, r, 1.0)
+    rhat = rel / safe_r[:, None]
+    t = np.cross(np.array([0.0, 0.0, 1.0]), rhat)
+    tn = np.linalg.norm(t, axis=1)
+    par = tn < 1e-12
+    if par.any():
+        ax = rng.normal(size=(int(par.sum()), 3))
+        t[par] = np.cross(ax / np.linalg.norm(ax, axis=1, keepdims=True), rhat[par])
+        tn = np.linalg.norm(t, axis=1)
+    t /= np.where(tn > 0, tn, 1.0)[:, None]
+    speed = np.sqrt(G * enclosed / safe_r)
+    vel = np.where((r > 0.0)[:, None], speed[:, None] * t, 0.0)
     vel += rng.normal(0.0, 0.01, size=(n, 3))
     bodies = np.zeros(n, dtype=BODY_DTYPE)
-    for i in range(n):
-        bodies[i]["pose"] = translation(pos[i])
+    tw = np.zeros((n, 6))
+    tw[:, :3] = pos
+    bodies["pose"] = _lib.motor_exp_n(tw, 1.0)
     bodies["momentum"][:, :3] = mass[:, None] * vel
     bodies["mass"] = mass
     bodies["inertia"][:, 0] = 1.0
@@ -93,74 +95,79 @@ def _boxes(rng, n):
     return h, mass, I
 
 
-def _joint_triplet(rng, a, b, rest, laws):
-    k = math.exp(rng.uniform(math.log(1e2), math.log(1e4)))
-    c = 0.1 * math.sqrt(k)
-    out = []
-    axial = np.zeros((), dtype=JOINT_DTYPE)
-    axial["law"], axial["a"], axial["b"] = laws[0], a, b
-    axial["params"][:10] = [0, 0, 0, 0, 0, 0, rest, k, c, 1e-6]
-    out.append(axial)
-    if len(laws) > 1:
-        perp = np.zeros((), dtype=JOINT_DTYPE)
-        perp["law"], perp["a"], perp["b"] = laws[1], a, b
-        perp["params"][:2] = [c, 1e-6]
-        out.append(perp)
-    if len(laws) > 2:
-        tors = np.zeros((), dtype=JOINT_DTYPE)
-        tors["law"], tors["a"], tors["b"] = laws[2], a, b
-        tors["params"][0] = c
-        out.append(tors)
-    return out
+def _edge_joints(rng, a, b, rest, laws):
+    """Per edge (a[e], b[e]): the axial spring-damper then the dampers, edge by edge."""
+    ne = len(a)
+    k = np.exp(rng.uniform(math.log(1e2), math.log(1e4), size=ne))
+    c = 0.1 * np.sqrt(k)
+    per = len(laws)
+    j = np.zeros(ne * per, dtype=JOINT_DTYPE)
+    for slot, law in enumerate(laws):
+        sel = j[slot::per]
+        sel["law"] = law
+        sel["a"] = a
+        sel["b"] = b
+        if law <= 1:
+            sel["params"][:, 6] = rest
+            sel["params"][:, 7] = k
+            sel["params"][:, 8] = c
+            sel["params"][:, 9] = 1e-6
+        elif law == 2:
+            sel["params"][:, 0] = c
+            sel["params"][:, 1] = 1e-6
+        else:
+            sel["params"][:, 0] = c
+        j[slot::per] = sel
+    return j
 
 
-def _place(rng, bodies, pos, twist_sigma):
-    for i in range(len(bodies)):
-        xi = rng.normal(0.0, twist_sigma, size=6)
-        bodies[i]["pose"] = _lib.motor_compose(_lib.motor_exp(xi, 1.0), translation(pos[i]))
-
-
-def chain_world(n, seed=1, origin=(0.0, 0.0, 0.0), twist_sigma=0.05, laws=(0, 2, 3)):
-    rng = np.random.default_rng(seed)
-    h, mass, I = _boxes(rng, n)
-    x = np.zeros(n)
-    for i in range(1, n):
-        x[i] = x[i - 1] + h[i - 1, 0] + h[i, 0]
-    x -= x.mean()
-    pos = np.zeros((n, 3))
-    pos[:, 0] = x
-    pos += np.asarray(origin, dtype=np.float64)
+def _bodies_at(rng, mass, I, pos, twist_sigma):
+    n = len(mass)
     bodies = np.zeros(n, dtype=BODY_DTYPE)
     bodies["mass"] = mass
     bodies["inertia"] = I
     bodies["diagonal"] = 1
     bodies["size"] = np.cbrt(mass / 4.0)
-    joints = []
-    for i in range(n - 1):
-        joints += _joint_triplet(rng, i, i + 1, x[i + 1] - x[i], laws)
-    _place(rng, bodies, pos, twist_sigma)
-    return bodies, np.array(joints, dtype=JOINT_DTYPE)
+    xi = rng.normal(0.0, twist_sigma, size=(n, 6))
+    tw = np.zeros((n, 6))
+    tw[:, :3] = pos
+    bodies["pose"] = _lib.motor_compose_n(_lib.motor_exp_n(xi, 1.0), _lib.motor_exp_n(tw, 1.0))
+    return bodies
+
+
+def chain_world(n, seed=1, origin=(0.0, 0.0, 0.0), twist_sigma=0.05, laws=(0, 2, 3)):
+    rng = np.random.default_rng(seed)
+    h, mass, I = _boxes(rng, n)
+    x = np.concatenate([[0.0], np.cumsum(h[:-1, 0] + h[1:, 0])])
+    x -= x.mean()
+    pos = np.zeros((n, 3))
+    pos[:, 0] = x
+    pos += np.asarray(origin, dtype=np.float64)
+    joints = _edge_joints(rng, np.arange(n - 1), np.arange(1, n), x[1:] - x[:-1], laws)
+    return _bodies_at(rng, mass, I, pos, twist_sigma), joints
 
 
 def tree_world(n, seed=2, twist_sigma=0.05, laws=(0, 2, 3)):
     rng = np.random.default_rng(seed)
     h, mass, I = _boxes(rng, n)
     rad = h.mean(axis=1)
+    parent = np.zeros(n, dtype=np.int64)
+    if n > 1:
+        parent[1:] = np.floor(rng.random(n - 1) * np.arange(1, n)).astype(np.int64)
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    dist = rad[parent] + rad
     pos = np.zeros((n, 3))
-    joints = []
-    for i in range(1, n):
-        p = int(rng.integers(0, i))
-        d = rad[p] + rad[i]
-        pos[i] = pos[p] + d * random_unit(rng)
-        joints += _joint_triplet(rng, p, i, d, laws)
+    done = np.zeros(n, dtype=bool)
+    done[0] = True
+    while not done.all():  # resolve level by level: a node's parent precedes it
+        ready = (~done) & done[parent]
+        pos[ready] = pos[parent[ready]] + dist[ready, None] * dirs[ready]
+        done |= ready
     pos -= (mass[:, None] * pos).sum(0) / mass.sum()
-    bodies = np.zeros(n, dtype=BODY_DTYPE)
-    bodies["mass"] = mass
-    bodies["inertia"] = I
-    bodies["diagonal"] = 1
-    bodies["size"] = np.cbrt(mass / 4.0)
-    _place(rng, bodies, pos, twist_sigma)
-    return bodies, np.array(joints, dtype=JOINT_DTYPE)
+    child = np.arange(1, n)
+    joints = _edge_joints(rng, parent[1:], child, dist[1:], laws)
+    return _bodies_at(rng, mass, I, pos, twist_sigma), joints
 
 
 def concat_worlds(parts):
@@ -207,3 +214,21 @@ def config2_parts(seed=2, n_gravity=65536, n_chains=16, chain_len=256, precision
 def config3_sizes(n_worlds=4096, seed=3, lo=8, hi=8192):
     rng = np.random.default_rng(seed)
     return np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_worlds))).astype(np.int64)
+
+
+def config3_worlds(n_worlds=4096, seed=3, precision=PRECISION_F64, lo=8, hi=8192):
+    """4096 independent worlds, body counts log-uniform in [8, 8192]: even-numbered worlds are
+    gravity worlds (config 0 distributions, LieEuler, dt 1e-3), odd-numbered ones are random
+    trees (config 1 laws and parameters, implicit Newton tol 1e-10, dt 1e-2)."""
+    sizes = config3_sizes(n_worlds, seed, lo, hi)
+    gp = step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=precision, G=1.0, softening=0.05,
+                     dt=1e-3)
+    tp = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-2, tol=1e-10)
+    worlds = []
+    for k, n in enumerate(sizes):
+        if k % 2 == 0:
+            worlds.append((gravity_world(int(n), 100.0, seed * 100003 + k), np.zeros(0, dtype=JOINT_DTYPE), gp))
+        else:
+            b, j = tree_world(int(n), seed * 100003 + k)
+            worlds.append((b, j, tp))
+    return worlds

@@ -164,6 +164,20 @@ EXG_API int exg_world_step(exg_world_t w, int32_t n_steps);
 EXG_API int exg_world_get_bodies(exg_world_t w, exg_body_t* out, int32_t n_bodies);
 EXG_API int exg_world_set_bodies(exg_world_t w, const exg_body_t* bodies, int32_t n_bodies);
 EXG_API int exg_world_stats(exg_world_t w, exg_world_stats_t* out);
+
+/* ── batch: many independent worlds of uneven size stepped together (Driver::step over many
+ * mechanisms, crates/newton/src/driver.rs:76-80; Accelerator::epoch, accelerator/mod.rs:613-630).
+ * World k owns body_counts[k] consecutive records of `bodies` and joint_counts[k] consecutive
+ * records of `joints`, whose body indices are local to world k. Every world has its own step
+ * parameters; all must share one precision. The returned handle is an exg_world_t: exg_world_step
+ * advances every world by one step per call step, and exg_world_get/set_bodies see the whole
+ * batch (world k at offset sum(body_counts[0..k))). A world of one is exg_world_create. */
+EXG_API int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* body_counts, const int32_t* joint_counts,
+                             const exg_body_t* bodies, const exg_joint_t* joints, const exg_step_params_t* params,
+                             exg_world_t* out);
+EXG_API int exg_batch_get_world(exg_world_t w, int32_t world, exg_body_t* out, int32_t n_bodies);
+EXG_API int exg_batch_set_world(exg_world_t w, int32_t world, const exg_body_t* bodies, int32_t n_bodies);
+EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_t* out);
 /* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
 EXG_API int exg_world_energy(exg_world_t w, double* out);
 
@@ -178,6 +192,9 @@ EXG_API int exg_motor_apply_point(const double m[8], const double p[3], double o
 /* Screw transport under m: covariant = 0 for a twist (Ad), 1 for a wrench (coAd)
  * (crates/clifford/src/pga3/screw.rs:94-105). */
 EXG_API int exg_screw_transport(const double s[6], const double m[8], int32_t covariant, double out[6]);
+/* Array forms for building large worlds: out[k] = exp(twists[k] * dt) and out[k] = compose(a[k], b[k]). */
+EXG_API int exg_motor_exp_n(int64_t count, const double* twists, double dt, double* out);
+EXG_API int exg_motor_compose_n(int64_t count, const double* a, const double* b, double* out);
 
 /* ── stage API on device pointers (the Accelerator's stage calls) ─────────── */
 /* Joint kernels K1-K8 (crates/newton/build.rs:874-973): for each joint k, inputs are the two

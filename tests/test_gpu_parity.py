@@ -62,8 +62,10 @@ def test_gravity_stage_fp64_matches_oracle(device, oracle, law, n):
 
 @pytest.mark.parametrize("law", [GRAVITY_SIZE_CORE, GRAVITY_PLUMMER])
 def test_gravity_stage_mixed_error_bound(device, oracle, law):
-    """FP32 pair terms with tile-relative positions and FP64 tile accumulation: per-body relative
-    force error below 2e-5 of the body's force magnitude."""
+    """FP32 pair terms with tile-relative positions and FP64 tile accumulation. Bounds: median
+    per-body relative force error below 1e-6, and every body's error below 1e-5 of the root mean
+    square force (a body whose pulls nearly cancel has a small net force, so its own relative
+    error is not the right yardstick)."""
     n = 4096
     bodies = scenarios.gravity_world(n, 1000.0, seed=9)
     pm = pos_mass(bodies)
@@ -74,8 +76,11 @@ def test_gravity_stage_mixed_error_bound(device, oracle, law):
                                              vp(d_f)))
     got = d_f.cpu().numpy().reshape(n, 3)
     want = oracle.gravity_forces(bodies, law, 1.0, 0.05)
-    rel = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
-    assert rel.max() < 2e-5, rel.max()
+    err = np.linalg.norm(got - want, axis=1)
+    mag = np.linalg.norm(want, axis=1)
+    assert np.median(err / mag) < 1e-6, np.median(err / mag)
+    rms = np.sqrt(np.mean(mag ** 2))
+    assert (err / rms).max() < 1e-5, (err / rms).max()
 
 
 @pytest.mark.parametrize("jacobian", [0, 1])

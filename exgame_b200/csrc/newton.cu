@@ -146,7 +146,10 @@ __device__ void phase_pre(const Ctx& c, const double* v, double half) {
   }
 }
 
-// Joint values (and Jacobian slices) at (mid, v): conn[q] = wrench on end a.
+// Joint values (and Jacobian slices) at (mid, v): conn[q] = wrench on end a. MIXED evaluates the
+// derivative slices in FP32 duals; the values that enter the residual always come from an FP64
+// evaluation, so the converged iterate is an FP64 solution whatever the Jacobian's precision.
+template <bool MIXED>
 __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
   const int nj = c.d.nj;
   const int joff = c.d.joint_off;
@@ -154,17 +157,38 @@ __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
     for (int t = threadIdx.x; t < 4 * nj; t += blockDim.x) {
       int q = t >> 2, slice = t & 3;
       int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
-      double val[6], dd[36];
-      joint_jacobian_slice<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a,
-                                   c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, slice, val, dd);
+      const int law = c.A.jl_law[joff + q];
+      const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
       double* o = c.s.jac + ((size_t)q * 4 + slice) * kJacStride;
+      if (MIXED) {
+        float pa[8], pb[8], va[6], vb[6], val[6], dd[36];
 #pragma unroll
-      for (int r = 0; r < 6; ++r) o[r] = val[r];
+        for (int k = 0; k < 8; ++k) { pa[k] = float(c.s.mid[8 * a + k]); pb[k] = float(c.s.mid[8 * b + k]); }
 #pragma unroll
-      for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
-      if (slice == 0) {
+        for (int k = 0; k < 6; ++k) { va[k] = float(v[6 * a + k]); vb[k] = float(v[6 * b + k]); }
+        joint_jacobian_slice<float>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, val, dd);
 #pragma unroll
-        for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
+        for (int r = 0; r < 6; ++r) o[r] = double(val[r]);
+#pragma unroll
+        for (int k = 0; k < 36; ++k) o[6 + k] = double(dd[k]);
+        if (slice == 0) {
+          double out[12];
+          joint_plain<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, out);
+#pragma unroll
+          for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
+        }
+      } else {
+        double val[6], dd[36];
+        joint_jacobian_slice<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp,
+                                     slice, val, dd);
+#pragma unroll
+        for (int r = 0; r < 6; ++r) o[r] = val[r];
+#pragma unroll
+        for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+        if (slice == 0) {
+#pragma unroll
+          for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
+        }
       }
     }
   } else {
@@ -498,6 +522,7 @@ __device__ void load_external(const Ctx& c) {
 
 struct SolveOut { bool converged; double best; bool assembled; double a_norm2; };
 
+template <bool MIXED>
 __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters) {
   SolveOut o{false, kHuge, false, 0.0};
   load_world_state(c);  // vmid = current world velocity; snap = P_s^n
@@ -508,7 +533,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
     ++*iters;
     phase_pre(c, c.s.vm, half);
     __syncthreads();
-    phase_joints(c, c.s.vm, true);
+    phase_joints<MIXED>(c, c.s.vm, true);
     __syncthreads();
     double rnorm = phase_post(c, c.s.vm, half, red);
     copy_mass0(c);
@@ -535,7 +560,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
       __syncthreads();
       phase_pre(c, c.s.trial, half);
       __syncthreads();
-      phase_joints(c, c.s.trial, false);
+      phase_joints<MIXED>(c, c.s.trial, false);
       __syncthreads();
       double tnorm = phase_post(c, c.s.trial, half, red);
       bool acc = tnorm < rnorm;
@@ -612,6 +637,7 @@ __device__ void commit_span(const Ctx& c, double span, double half, bool converg
   }
 }
 
+template <bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
                                                          int n_islands, int* __restrict__ head) {
   __shared__ double red[kWarps];
@@ -654,7 +680,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
       double half = span / 2.0;
       ++spans;
       maxdepth = max(maxdepth, depth);
-      SolveOut o = newton_solve(c, half, red, &flag, &iters);
+      SolveOut o = newton_solve<MIXED>(c, half, red, &flag, &iters);
       last_best = o.best;
       bool finite = o.best < kHuge;
       bool last = depth == kMaxDepth;
@@ -940,7 +966,10 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   int grid = std::min(n_islands, std::max(1, dev->sm_count) * 2);
   EXG_CUDA_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), s));
   int tok = prof_begin(dev, PROF_NEWTON, s);
-  k_newton_step<<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+  if (w.precision == EXG_PRECISION_MIXED)
+    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+  else
+    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

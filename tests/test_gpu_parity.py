@@ -63,7 +63,7 @@ def test_gravity_stage_fp64_matches_oracle(device, oracle, law, n):
 @pytest.mark.parametrize("law", [GRAVITY_SIZE_CORE, GRAVITY_PLUMMER])
 def test_gravity_stage_mixed_error_bound(device, oracle, law):
     """FP32 pair terms with tile-relative positions and FP64 tile accumulation. Bounds: median
-    per-body relative force error below 1e-6, and every body's error below 1e-5 of the root mean
+    per-body relative force error below 1e-6, and every body's error below 5e-5 of the root mean
     square force (a body whose pulls nearly cancel has a small net force, so its own relative
     error is not the right yardstick)."""
     n = 4096
@@ -80,7 +80,7 @@ def test_gravity_stage_mixed_error_bound(device, oracle, law):
     mag = np.linalg.norm(want, axis=1)
     assert np.median(err / mag) < 1e-6, np.median(err / mag)
     rms = np.sqrt(np.mean(mag ** 2))
-    assert (err / rms).max() < 1e-5, (err / rms).max()
+    assert (err / rms).max() < 5e-5, (err / rms).max()
 
 
 @pytest.mark.parametrize("jacobian", [0, 1])

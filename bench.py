@@ -56,18 +56,20 @@ def workload(name, rank):
                "bodies": 256, "worlds": 1, "dtype": "f64"}
         return [(b, j, p)], cfg
     if name == "c2":
-        (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(seed=2 + rank, precision=PRECISION_MIXED)
+        (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(seed=2 + rank, precision=PRECISION_MIXED,
+                                                                exact_jacobian=True)
         cfg = {"workload": "65,536-body gravity (ball R 1000, LieEuler) + 16 x 256-body chains (Newton tol 1e-10), "
                            "dt 1e-3, mixed precision (config 2)", "bodies": len(gb) + len(cb), "worlds": 2,
                "dtype": "f32 forces / f64 state"}
         return [(gb, gj, gp), (cb, cj, cp)], cfg
     if name in ("c3", "c3-f64"):
         prec = PRECISION_MIXED if name == "c3" else PRECISION_F64
-        worlds = scenarios.config3_worlds(4096, seed=3 + rank, precision=prec)
+        worlds = scenarios.config3_worlds(4096, seed=3 + rank, precision=prec, exact_jacobian=bool(prec))
         n = sum(len(b) for b, _, _ in worlds)
         cfg = {"workload": "4096 independent worlds, body counts log-uniform in [8, 8192]: gravity worlds "
                            "(LieEuler, dt 1e-3) and random joint trees (Newton tol 1e-10, dt 1e-2), one batched launch "
-                           "set per step, " + ("mixed precision" if prec else "f64") + " (config 3)",
+                           "set per step, " + ("mixed precision, exact mid-point Newton matrix" if prec else "f64")
+                           + " (config 3)",
                "bodies": n, "worlds": 4096, "dtype": "f32 forces / f64 state" if prec else "f64"}
         return worlds, cfg
     raise SystemExit(f"unknown workload {name}")
@@ -182,6 +184,7 @@ def plain_path(dev, parts, flush, passes=1):
     for b, j, p in parts:
         q = p.copy()
         q["precision"] = PRECISION_F64
+        q["newton_flags"] = 0  # the reference's Newton matrix
         worlds.append(_lib.DeviceWorld(dev, b, j, q))
     for w in worlds:
         w.step(1)
@@ -276,8 +279,8 @@ def run_ours(args, rank, world_size, local_rank):
     plain = None
     if args.plain and len(parts) > 1:
         plain = {"value": plain_path(dev, parts, flush), "unit": METRIC,
-                 "sample": "every world FP64 and stepped alone, one exg_world_step per world, one pass after a warm "
-                           "pass (device time, L2 flushed before the pass)"}
+                 "sample": "every world FP64 with the reference's Newton matrix, stepped alone, one exg_world_step "
+                           "per world, one pass after a warm pass (device time, L2 flushed before the pass)"}
     return {
         "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
         "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain,

@@ -46,6 +46,7 @@ SIGNATURES = {
     "exg_batch_get_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
     "exg_batch_set_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
     "exg_batch_world_stats": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
+    "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
     "exg_motor_compose": (ctypes.c_int, [_vp, _vp, _vp]),
     "exg_motor_inverse": (ctypes.c_int, [_vp, _vp]),
@@ -232,6 +233,13 @@ class DeviceWorld:
         s = np.zeros((), dtype=WORLD_STATS_DTYPE)
         check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
         return s
+
+    PHASES = ("pre", "joints+jacobian", "gather+post", "assemble", "solve", "line search", "commit", "other")
+
+    def phase_cycles(self):
+        out = np.zeros(8, dtype=np.int64)
+        check(lib().exg_world_phase_cycles(self.handle, ptr(out)), "exg_world_phase_cycles")
+        return dict(zip(self.PHASES, out.tolist()))
 
     def energy(self):
         e = ctypes.c_double()

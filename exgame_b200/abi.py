@@ -29,7 +29,7 @@ STEP_PARAMS_DTYPE = np.dtype(
         ("integrator", "<i4"),
         ("gravity_law", "<i4"),
         ("precision", "<i4"),
-        ("reserved0", "<i4"),
+        ("newton_flags", "<i4"),
         ("G", "<f8"),
         ("softening", "<f8"),
         ("dt", "<f8"),
@@ -62,9 +62,13 @@ GRAVITY_OFF, GRAVITY_SIZE_CORE, GRAVITY_PLUMMER = 0, 1, 2
 PRECISION_F64, PRECISION_MIXED = 0, 1
 
 
+NEWTON_EXACT_POSE_FACTOR = 1
+
+
 def step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, precision=PRECISION_F64, G=1.0, softening=0.0,
-                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32):
+                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32, exact_jacobian=False):
     p = np.zeros((), dtype=STEP_PARAMS_DTYPE)
+    p["newton_flags"] = NEWTON_EXACT_POSE_FACTOR if exact_jacobian else 0
     p["integrator"] = integrator
     p["gravity_law"] = gravity_law
     p["precision"] = precision

@@ -521,6 +521,18 @@ int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) 
   return EXG_OK;
 }
 
+int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
+  if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 8; ++k) out[k] = 0;
+  if (!W->newton) return EXG_OK;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  long long tmp[8];
+  int rc = W->newton->read_phase_cycles(tmp);
+  for (int k = 0; k < 8; ++k) out[k] = tmp[k];
+  return rc;
+}
+
 int exg_world_energy(exg_world_t W, double* out) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
   int n = W->w.n;

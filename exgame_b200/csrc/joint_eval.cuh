@@ -34,6 +34,28 @@ EXG_HD void joint_plain(int law, const double* prm, const R* pose_a, const R* po
 template <class R>
 EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
                                  const R* vel_b, double dt, double warp, int slice, R* value6, R* d36) {
+  if (law == LAW_TORSIONAL) {
+    // The couple -k (w_a - w_b) depends on the angular velocities only, linearly: its Jacobian is
+    // -k I (velocity A) and +k I (velocity B) on the torque rows, zero elsewhere — exactly what the
+    // dual evaluation produces, without the dual arithmetic.
+    R ta[6], tb[6], wa[6], w6[6];
+    screw_from6(vel_a, ta);
+    screw_from6(vel_b, tb);
+    law_torsional(prm, ta, tb, warp, wa);
+    screw_to6(wa, w6);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) value6[r] = w6[r];
+#pragma unroll
+    for (int k = 0; k < 36; ++k) d36[k] = R(0.0);
+    if (slice >= 2) {
+      R k = -R(prm[0] / (warp * warp));
+      R g = slice == 2 ? k : -k;
+      d36[3 * 6 + 3] = g;
+      d36[4 * 6 + 4] = g;
+      d36[5 * 6 + 5] = g;
+    }
+    return;
+  }
   using D = Dual<6, R>;
   D ma[8], mb[8], va[6], vb[6];
 #pragma unroll

@@ -86,7 +86,7 @@ struct WorldRef {
 
 // The island's world parameters, resolved once per island.
 struct IslandParams {
-  double dt, warp, tol2, G;
+  double dt, warp, tol2, G, pose_factor_scale;
   int max_newton;
   int splits, nw, wbody_off;
   const double* part;
@@ -100,6 +100,21 @@ struct Ctx {
   Scratch s;
   int island;
   EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
+};
+
+// Phase timer: thread 0 accumulates SM clock cycles between phase boundaries (all threads have
+// passed a barrier there) into shared counters; the CTA adds them to the global totals at the end.
+struct PhaseTimer {
+  long long* acc;  // shared [kPhases]
+  long long t0;
+  __device__ void start() { if (threadIdx.x == 0) t0 = clock64(); }
+  __device__ void lap(int phase) {
+    if (threadIdx.x == 0) {
+      long long t = clock64();
+      acc[phase] += t - t0;
+      t0 = t;
+    }
+  }
 };
 
 // ── block-wide reductions ───────────────────────────────────────────────────
@@ -284,7 +299,7 @@ __device__ void copy_mass0(const Ctx& c) {
 // midpoint factors pf = -half^2 on pose columns and vf = -half on velocity columns.
 // Returns ||A||_F^2.
 __device__ double phase_assemble(const Ctx& c, double half, double* red) {
-  const double pf = -(half * half), vf = -half;
+  const double pf = -(half * half) * c.P.pose_factor_scale, vf = -half;
   double sumsq = 0.0;
   const int cells = 3 * c.d.m;
   for (int t = threadIdx.x; t < cells * 36; t += blockDim.x) {
@@ -523,30 +538,49 @@ __device__ void load_external(const Ctx& c) {
 struct SolveOut { bool converged; double best; bool assembled; double a_norm2; };
 
 template <bool MIXED>
-__device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters) {
+__device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters, PhaseTimer& tm) {
   SolveOut o{false, kHuge, false, 0.0};
   load_world_state(c);  // vmid = current world velocity; snap = P_s^n
   __syncthreads();
   copy_bodies6(c, c.s.vm, c.s.best);
   __syncthreads();
+  tm.lap(PH_OTHER);
+  // The accepted line-search probe already evaluated PRE, the joint values and POST at the point
+  // the next iteration starts from (newton.rs:383-395); only the Jacobian is missing there.
+  bool carried = false;
+  double carried_norm = 0.0;
   for (int it = 0; it < c.P.max_newton; ++it) {
     ++*iters;
-    phase_pre(c, c.s.vm, half);
-    __syncthreads();
-    phase_joints<MIXED>(c, c.s.vm, true);
-    __syncthreads();
-    double rnorm = phase_post(c, c.s.vm, half, red);
-    copy_mass0(c);
+    double rnorm;
+    if (carried) {
+      phase_joints<MIXED>(c, c.s.vm, true);
+      __syncthreads();
+      tm.lap(PH_JACOBIAN);
+      rnorm = carried_norm;
+      carried = false;
+    } else {
+      phase_pre(c, c.s.vm, half);
+      __syncthreads();
+      tm.lap(PH_PRE);
+      phase_joints<MIXED>(c, c.s.vm, true);
+      __syncthreads();
+      tm.lap(PH_JACOBIAN);
+      rnorm = phase_post(c, c.s.vm, half, red);
+      copy_mass0(c);
+    }
     if (rnorm < o.best) {
       o.best = rnorm;
       copy_bodies6(c, c.s.vm, c.s.best);
     }
     __syncthreads();
+    tm.lap(PH_POST);
     if (rnorm <= c.P.tol2) { o.converged = true; break; }
     if (!(rnorm < kHuge)) break;
     o.a_norm2 = phase_assemble(c, half, red);
     o.assembled = true;
+    tm.lap(PH_ASSEMBLE);
     phase_solve(c, flag);
+    tm.lap(PH_SOLVE);
     // no correction at all -> hand over to sub-division (newton.rs:449-456)
     int nz = 0;
     for (int t = threadIdx.x; t < 6 * c.d.m; t += blockDim.x) nz |= (c.s.dv[t] != 0.0);
@@ -566,11 +600,13 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
       bool acc = tnorm < rnorm;
       if (lane == 0 || acc) copy_mass0(c);
       __syncthreads();
-      if (acc) { accepted = lane; break; }
+      if (acc) { accepted = lane; carried_norm = tnorm; break; }
       alpha = alpha / 2.0;
     }
+    tm.lap(PH_LINE_SEARCH);
     if (accepted < 0) break;  // vm still holds the base iterate
     copy_bodies6(c, c.s.trial, c.s.vm);
+    carried = true;  // mid, conn, mass, rhs and scale now describe the accepted iterate
     __syncthreads();
   }
   // restore the best iterate for the commit
@@ -643,12 +679,21 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
   __shared__ double red[kWarps];
   __shared__ int flag;
   __shared__ int item;
+  __shared__ long long phase_acc[kPhases];
+  if (threadIdx.x < kPhases) phase_acc[threadIdx.x] = 0;
+  __syncthreads();
+  PhaseTimer tm{phase_acc, 0};
+  tm.start();
   for (;;) {
     if (threadIdx.x == 0) item = atomicAdd(head, 1);
     __syncthreads();
     int k = item;
     __syncthreads();
-    if (k >= n_islands) break;
+    if (k >= n_islands) {
+      if (threadIdx.x < kPhases) atomicAdd(reinterpret_cast<unsigned long long*>(&A.phase_cycles[threadIdx.x]),
+                                           static_cast<unsigned long long>(phase_acc[threadIdx.x]));
+      break;
+    }
     Ctx c;
     c.A = A;
     c.island = queue[k];
@@ -662,6 +707,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
       c.P.tol2 = wp.tol * wp.tol;
       c.P.G = wp.G;
       c.P.max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
+      c.P.pose_factor_scale = (wp.newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) ? 0.5 : 1.0;
       c.P.splits = W.w_splits[c.d.world];
       c.P.nw = W.w_n[c.d.world];
       c.P.wbody_off = W.w_body_off[c.d.world];
@@ -680,7 +726,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
       double half = span / 2.0;
       ++spans;
       maxdepth = max(maxdepth, depth);
-      SolveOut o = newton_solve<MIXED>(c, half, red, &flag, &iters);
+      SolveOut o = newton_solve<MIXED>(c, half, red, &flag, &iters, tm);
       last_best = o.best;
       bool finite = o.best < kHuge;
       bool last = depth == kMaxDepth;
@@ -692,6 +738,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
       }
       if (o.converged || finite) commit_span(c, span, half, o.converged);
       __syncthreads();
+      tm.lap(PH_COMMIT);
       remaining -= units;
       auto aligned = [&](int dd) {
         if (dd <= 0) return false;
@@ -932,6 +979,8 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
   double *d_params, *d_scratch, *d_res;
   std::vector<int> stats(4 * (size_t)n_islands, 0);
   std::vector<double> resid(n_islands, 0.0);
+  std::vector<long long> phases(kPhases, 0);
+  long long* d_phase = nullptr;
   std::vector<int> qv(island_order);
   qv.push_back(0);  // head counter lives after the queue
   if ((rc = up(desc, &d_desc)) || (rc = up(h_isl_body, &d_isl_body)) || (rc = up(h_jl_law, &d_jl_law)) ||
@@ -940,7 +989,8 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
       (rc = up(h_ib_inc_ref, &d_ib_inc_ref)) || (rc = up(h_dn_body, &d_dn_body)) || (rc = up(h_dn_parent, &d_dn_parent)) ||
       (rc = up(h_lv_ptr, &d_lv_ptr)) || (rc = up(h_lv_nodes, &d_lv_nodes)) || (rc = up(h_ch_ptr, &d_ch_ptr)) ||
       (rc = up(h_ch_idx, &d_ch_idx)) || (rc = up(h_cell_ptr, &d_cell_ptr)) || (rc = up(h_cell_terms, &d_cell_terms)) ||
-      (rc = up(stats, &d_stats)) || (rc = up(resid, &d_res)) || (rc = up(qv, &d_q)))
+      (rc = up(stats, &d_stats)) || (rc = up(resid, &d_res)) || (rc = up(qv, &d_q)) ||
+      (rc = up(phases, &d_phase)))
     return rc;
   void* sp = nullptr;
   EXG_CUDA_TRY(cudaMalloc(&sp, sizeof(double) * std::max<long long>(scratch, 1)));
@@ -949,7 +999,7 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
   EXG_CUDA_TRY(cudaMemsetAsync(d_scratch, 0, sizeof(double) * std::max<long long>(scratch, 1), s));
   arr = NewtonDeviceArrays{d_desc,      d_isl_body, d_jl_law,  d_jl_a,      d_jl_b,       d_params,  d_ib_order,
                            d_ib_inc_ptr, d_ib_inc_ref, d_dn_body, d_dn_parent, d_lv_ptr,   d_lv_nodes, d_ch_ptr,
-                           d_ch_idx,    d_cell_ptr, d_cell_terms, d_scratch, d_stats,     d_res};
+                           d_ch_idx,    d_cell_ptr, d_cell_terms, d_scratch, d_stats,     d_res, d_phase};
   d_queue = d_q;
   d_head = d_q + n_islands;
   island_world.resize(n_islands);
@@ -972,6 +1022,11 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
+}
+
+int NewtonWorld::read_phase_cycles(long long* out) {
+  EXG_CUDA_TRY(cudaMemcpy(out, arr.phase_cycles, sizeof(long long) * kPhases, cudaMemcpyDeviceToHost));
+  return EXG_OK;
 }
 
 int NewtonWorld::read_stats(int world, exg_world_stats_t* st) {

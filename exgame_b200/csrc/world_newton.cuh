@@ -41,7 +41,11 @@ struct NewtonDeviceArrays {
   double* scratch;
   int* stats;              // per island: spans, newton iterations, max depth, fatal
   double* residual;        // per island: last span's best residual
+  long long* phase_cycles; // [kPhases] SM clock cycles per phase, summed over islands and steps
 };
+// Phases of the device Newton step, for the cycle counters.
+enum NewtonPhase { PH_PRE = 0, PH_JACOBIAN = 1, PH_POST = 2, PH_ASSEMBLE = 3, PH_SOLVE = 4, PH_LINE_SEARCH = 5,
+                   PH_COMMIT = 6, PH_OTHER = 7, kPhases = 8 };
 
 class NewtonWorld {
  public:
@@ -51,6 +55,8 @@ class NewtonWorld {
   // Aggregate the last step's per-island counters, over all islands (world < 0) or one world.
   int read_stats(int world, exg_world_stats_t* stats);
   int n_islands_total() const { return n_islands; }
+  // Summed SM cycles per phase since the world was created (kPhases values).
+  int read_phase_cycles(long long* out);
   ~NewtonWorld();
 
  private:

@@ -199,7 +199,7 @@ def config1(seed=1, n=256):
     return bodies, joints, params, 500
 
 
-def config2_parts(seed=2, n_gravity=65536, n_chains=16, chain_len=256, precision=PRECISION_F64):
+def config2_parts(seed=2, n_gravity=65536, n_chains=16, chain_len=256, precision=PRECISION_F64, exact_jacobian=False):
     """65,536 gravity bodies (ball radius 1000) and 16 independent 256-body chains, stepped together at
     dt 1e-3 for 1000 steps; returned as (gravity world, chain world) parts of one epoch."""
     g = gravity_world(n_gravity, 1000.0, seed)
@@ -207,7 +207,8 @@ def config2_parts(seed=2, n_gravity=65536, n_chains=16, chain_len=256, precision
                           softening=0.05, dt=1e-3)
     chains = [chain_world(chain_len, seed * 1000 + c, origin=(0.0, 50.0 * c, 5000.0)) for c in range(n_chains)]
     cb, cj = concat_worlds(chains)
-    cparams = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-3, tol=1e-10)
+    cparams = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-3, tol=1e-10,
+                          exact_jacobian=exact_jacobian)
     return (g, np.zeros(0, dtype=JOINT_DTYPE), gparams), (cb, cj, cparams), 1000
 
 
@@ -216,14 +217,15 @@ def config3_sizes(n_worlds=4096, seed=3, lo=8, hi=8192):
     return np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_worlds))).astype(np.int64)
 
 
-def config3_worlds(n_worlds=4096, seed=3, precision=PRECISION_F64, lo=8, hi=8192):
+def config3_worlds(n_worlds=4096, seed=3, precision=PRECISION_F64, lo=8, hi=8192, exact_jacobian=False):
     """4096 independent worlds, body counts log-uniform in [8, 8192]: even-numbered worlds are
     gravity worlds (config 0 distributions, LieEuler, dt 1e-3), odd-numbered ones are random
     trees (config 1 laws and parameters, implicit Newton tol 1e-10, dt 1e-2)."""
     sizes = config3_sizes(n_worlds, seed, lo, hi)
     gp = step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=precision, G=1.0, softening=0.05,
                      dt=1e-3)
-    tp = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-2, tol=1e-10)
+    tp = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-2, tol=1e-10,
+                     exact_jacobian=exact_jacobian)
     worlds = []
     for k, n in enumerate(sizes):
         if k % 2 == 0:

@@ -108,11 +108,17 @@ typedef enum { EXG_PRECISION_F64 = 0, EXG_PRECISION_MIXED = 1 } exg_precision;
  * (crates/newton/src/integrator/implicit/mod.rs:44-49), the gravity field and the Newton
  * tolerance (relative per-block residual; the reference hard-codes 1e-4,
  * crates/newton/src/integrator/implicit/newton.rs:799-805). */
+/* newton_flags bit 0: assemble the Newton matrix with the exact derivative of the mid-point
+ * retraction on the pose columns (-half^2/2) instead of the reference's -half^2
+ * (crates/newton/src/integrator/implicit/cache.rs:509-520). Either matrix leads to the same
+ * converged step; the exact one converges in fewer iterations. */
+#define EXG_NEWTON_EXACT_POSE_FACTOR 1
+
 typedef struct {
   int32_t integrator;
   int32_t gravity_law;
   int32_t precision;
-  int32_t reserved0;
+  int32_t newton_flags;
   double G;
   double softening; /* Plummer epsilon */
   double dt;
@@ -178,6 +184,10 @@ EXG_API int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* 
 EXG_API int exg_batch_get_world(exg_world_t w, int32_t world, exg_body_t* out, int32_t n_bodies);
 EXG_API int exg_batch_set_world(exg_world_t w, int32_t world, const exg_body_t* bodies, int32_t n_bodies);
 EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_t* out);
+/* SM clock cycles the implicit step spent per phase since the handle was created, summed over
+ * islands: [0] PRE, [1] joint values + Jacobian, [2] gather + POST, [3] assembly, [4] linear
+ * solve, [5] line search, [6] commit, [7] other. Zero for worlds without implicit islands. */
+EXG_API int exg_world_phase_cycles(exg_world_t w, int64_t out[8]);
 /* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
 EXG_API int exg_world_energy(exg_world_t w, double* out);
 

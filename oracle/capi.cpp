@@ -56,6 +56,7 @@ void* orc_world_create(const exg_body_t* bodies, int n_bodies, const exg_joint_t
   w->wp.solver = solver;
   w->wp.ns_warm = ns_warm;
   w->wp.ns_seed = ns_seed;
+  w->wp.exact_pose_factor = (p->newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) != 0;
   w->build();
   return w;
 }

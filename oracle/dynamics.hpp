@@ -315,6 +315,7 @@ struct WorldParams {
   double tol = 1e-4;      // relative per-block Newton tolerance (newton.rs:799-805 uses 1e-4)
   int ns_warm = 2, ns_seed = 24;
   int solver = SOLVER_EXACT;
+  bool exact_pose_factor = false;  // -half^2/2 on the pose columns instead of the reference's -half^2
 };
 
 // ── One island's implicit mid-point Newton step ─────────────────────────────
@@ -411,7 +412,7 @@ struct NewtonIsland {
     int m = isl.m;
     A.assign((size_t)m * m, zero_block());
     for (int i = 0; i < m; ++i) A[(size_t)i * m + i] = lane0_mass[i];
-    double pf = -(half * half), vf = -half;
+    double pf = -(half * half) * (wp.exact_pose_factor ? 0.5 : 1.0), vf = -half;
     for (size_t q = 0; q < isl.joints.size(); ++q) {
       const OJoint& j = joints[isl.joints[q]];
       int ends[2] = {isl.order[local_of(j.a)], isl.order[local_of(j.b)]};

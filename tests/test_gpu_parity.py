@@ -221,3 +221,24 @@ def test_device_counts_kernel_launches(device):
                           step_params(gravity_law=GRAVITY_PLUMMER, softening=0.05, dt=1e-3))
     dw.step(3)
     assert device.kernel_launches() - before == 9  # pre, gravity, integrate per step
+
+
+def test_newton_exact_pose_factor_matches_oracle(device, oracle):
+    bodies, joints = scenarios.tree_world(60, seed=61)
+    params = step_params(integrator=NEWTON, dt=1e-2, tol=1e-10, exact_jacobian=True)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 10)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+    # and the same step as the reference's Newton matrix, within the tolerance
+    ref = oracle.OracleWorld(bodies, joints, step_params(integrator=NEWTON, dt=1e-2, tol=1e-10))
+    ref.step(10)
+    pe, me = state_error(ref.bodies(), dw.bodies())
+    assert pe < 1e-8 and me < 1e-6, (pe, me)
+
+
+def test_newton_phase_cycles_reported(device):
+    bodies, joints = scenarios.chain_world(30, seed=62)
+    dw = _lib.DeviceWorld(device, bodies, joints, step_params(integrator=NEWTON, dt=1e-2, tol=1e-10))
+    dw.step(2)
+    ph = dw.phase_cycles()
+    assert ph["joints+jacobian"] > 0 and ph["solve"] > 0 and ph["line search"] > 0

@@ -363,3 +363,21 @@ def test_chain_generator_topology_bit_exact():
     assert list(j["law"]) == [0, 2, 3] * 4
     assert list(j["a"]) == [0, 0, 0, 1, 1, 1, 2, 2, 2, 3, 3, 3]
     assert list(j["b"]) == [1, 1, 1, 2, 2, 2, 3, 3, 3, 4, 4, 4]
+
+
+def test_exact_pose_factor_converges_to_the_same_step(oracle):
+    """The Newton matrix with the exact mid-point factor on the pose columns (-half^2/2) needs
+    fewer iterations than the reference's (-half^2) and reaches the same step within tolerance."""
+    bodies, joints = scenarios.chain_world(20, seed=17)
+    ref = oracle.OracleWorld(bodies, joints, step_params(integrator=NEWTON, dt=1e-2, tol=1e-10))
+    ex = oracle.OracleWorld(bodies, joints, step_params(integrator=NEWTON, dt=1e-2, tol=1e-10, exact_jacobian=True))
+    its_ref, its_ex = 0, 0
+    for _ in range(20):
+        ref.step(1)
+        ex.step(1)
+        its_ref += ref.island_stats()[0][1]
+        its_ex += ex.island_stats()[0][1]
+    pa = np.array([position(x) for x in ref.bodies()])
+    pb = np.array([position(x) for x in ex.bodies()])
+    assert np.abs(pa - pb).max() < 1e-8
+    assert its_ex < its_ref

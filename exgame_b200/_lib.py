@@ -58,6 +58,8 @@ SIGNATURES = {
                                        ctypes.c_int32, _vp]),
     "exg_gravity_forces": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int32, _vp]),
+    "exg_gravity_forces_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                  ctypes.c_double, ctypes.c_int32, _vp]),
 }
 
 

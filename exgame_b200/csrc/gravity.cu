@@ -18,6 +18,7 @@
 // the tile), pair terms are FP32 with the hardware reciprocal square root, and each j-tile's FP32
 // partial is flushed into an FP64 accumulator, so rounding does not grow with the world size.
 #include <algorithm>
+#include <mutex>
 #include "exg_internal.cuh"
 
 namespace {
@@ -198,4 +199,83 @@ int launch_gravity_reduce(exg_device_s* dev, const double* partial, const double
   k_gravity_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, reinterpret_cast<const double4*>(pos_mass), n, splits, G,
                                                    force_out);
   return exg_after_launch(dev);
+}
+
+// ── the no-allocation variant of the gravity stage ─────────────────────────────
+// Its scratch is a file-scope device array sized for EXG_NOALLOC_MAX_BODIES bodies: the work
+// items, the per-split partial sums and the scheduler counter. The host side never names the
+// array as a device address: it asks the runtime for the address once per device and passes
+// that to the kernels.
+namespace {
+constexpr int kNoAllocMaxItems = ((EXG_NOALLOC_MAX_BODIES + kGravTile - 1) / kGravTile) * 8;  // splits <= 8 here
+constexpr size_t kNoAllocPartialDoubles = (size_t)8 * 3 * EXG_NOALLOC_MAX_BODIES;
+constexpr size_t kNoAllocHeadBytes = 256;
+constexpr size_t kNoAllocItemBytes = ((sizeof(GravItem) * kNoAllocMaxItems + 255) / 256) * 256;
+constexpr size_t kNoAllocBytes = kNoAllocHeadBytes + kNoAllocItemBytes + kNoAllocPartialDoubles * sizeof(double);
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {nullptr};  // device address of the scratch array, per device ordinal
+
+// Resolve the scratch array's device address on `ordinal` (that device must be current).
+int noalloc_scratch(int ordinal, unsigned char** out) {
+  if (ordinal < 0 || ordinal >= 256) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[ordinal]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      exg_internal_set_cuda_error(e, "cudaGetSymbolAddress(no-allocation gravity scratch)");
+      return EXG_ERR_BACKEND;
+    }
+    g_noalloc_addr[ordinal] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[ordinal]);
+  return EXG_OK;
+}
+}  // namespace
+
+extern "C" int exg_gravity_forces_noalloc(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n,
+                                          int32_t law, double G, double softening, int32_t precision, double* d_force) {
+  if (!dev || n < 0 || (n > 0 && (!d_pos_mass || !d_force))) return EXG_ERR_INVALID_ARGUMENT;
+  if (n > EXG_NOALLOC_MAX_BODIES) return EXG_ERR_INVALID_ARGUMENT;
+  if (law == EXG_GRAVITY_SIZE_CORE && n > 0 && !d_size) return EXG_ERR_INVALID_ARGUMENT;
+  if (law != EXG_GRAVITY_SIZE_CORE && law != EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
+  if (law == EXG_GRAVITY_PLUMMER && !(softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return EXG_OK;
+  std::lock_guard<std::mutex> lock(dev->mu);
+  EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));
+  cudaStream_t s = dev->stream;
+  if (n == 1) {
+    EXG_CUDA_TRY(cudaMemsetAsync(d_force, 0, 3 * sizeof(double), s));
+    EXG_CUDA_TRY(cudaStreamSynchronize(s));
+    return EXG_OK;
+  }
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(dev->ordinal, &base);
+  if (rc != EXG_OK) return rc;
+  std::vector<GravItem> items;
+  std::vector<int> splits;
+  std::vector<long long> poff;
+  long long plen = 0;
+  gravity_plan({0}, {n}, {law}, {softening}, dev->sm_count, items, splits, poff, plen);
+  if ((long long)items.size() > kNoAllocMaxItems || plen > (long long)kNoAllocPartialDoubles)
+    return EXG_ERR_INVALID_ARGUMENT;
+  int* head = reinterpret_cast<int*>(base);
+  GravItem* d_items = reinterpret_cast<GravItem*>(base + kNoAllocHeadBytes);
+  double* partial = reinterpret_cast<double*>(base + kNoAllocHeadBytes + kNoAllocItemBytes);
+  EXG_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), sizeof(GravItem) * items.size(), cudaMemcpyHostToDevice, s));
+  rc = launch_gravity_items(dev, d_pos_mass, d_size, d_items, (int)items.size(), head, precision, partial, s);
+  if (rc == EXG_OK) rc = launch_gravity_reduce(dev, partial, d_pos_mass, n, splits[0], G, d_force, s);
+  // the host item table must outlive the copy, so wait here in every case
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (rc != EXG_OK) return rc;
+  if (e != cudaSuccess) {
+    exg_internal_set_cuda_error(e, "no-allocation gravity");
+    return EXG_ERR_BACKEND;
+  }
+  return EXG_OK;
 }

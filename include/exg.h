@@ -221,6 +221,24 @@ EXG_API int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32
 EXG_API int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law,
                        double G, double softening, int32_t precision, double* d_force);
 
+/* ── gravity without allocation ────────────────────────────────────────────────
+ * Same result as exg_gravity_forces, for callers that must not allocate device memory: code that
+ * runs under a strict memory budget or a pre-sized pool, or code whose allocator may not be called
+ * at that point (for example a host that reserves all device memory up front). This entry point
+ * has no counterpart in the reference.
+ * Its working memory (work items, per-split partial sums and the scheduler counter) is a fixed
+ * array compiled into the library: every GPU that loads the library holds about 3.2 MB of it until
+ * the process exits. Bodies are limited to EXG_NOALLOC_MAX_BODIES; larger n returns
+ * EXG_ERR_INVALID_ARGUMENT before any work is queued.
+ * The first call on a device looks up that array's device address (once per device, with the
+ * device current); make that first call before capturing any stream into a CUDA graph.
+ * Every call on a device uses the same array and leaves its contents behind; the call resets what
+ * must start at zero. Two calls whose GPU work overlaps (from different threads or streams) race
+ * on the array. The call returns after its work has finished. */
+#define EXG_NOALLOC_MAX_BODIES 16384
+EXG_API int exg_gravity_forces_noalloc(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n,
+                                       int32_t law, double G, double softening, int32_t precision, double* d_force);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,8 @@ import os
 
 import numpy as np
 
-from .abi import BODY_DTYPE, JOINT_DTYPE, STEP_PARAMS_DTYPE, WORLD_STATS_DTYPE
+from .abi import (BODY_DTYPE, JOINT_DTYPE, PENDING, POOL_CONFIG_DTYPE, POOL_USAGE_DTYPE, PRECISION_F64,
+                  REQUEST_INFO_DTYPE, SERVER_CONFIG_DTYPE, SERVER_STATS_DTYPE, STEP_PARAMS_DTYPE, WORLD_STATS_DTYPE)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libexg.so")
 
@@ -46,6 +47,22 @@ SIGNATURES = {
     "exg_batch_get_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
     "exg_batch_set_world": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
     "exg_batch_world_stats": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
+    "exg_pool_create": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "exg_pool_admit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, ctypes.c_int32, _vp,
+                                      ctypes.POINTER(ctypes.c_int32)]),
+    "exg_pool_release": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "exg_pool_free": (ctypes.c_int, [_vp, _vp]),
+    "exg_world_footprint": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.POINTER(ctypes.c_int64)]),
+    "exg_server_create": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "exg_server_submit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, ctypes.c_int32, _vp, ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_uint64)]),
+    "exg_server_poll": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp, ctypes.c_int32, _vp]),
+    "exg_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_int32, _vp, ctypes.c_int32, _vp]),
+    "exg_server_stats": (ctypes.c_int, [_vp, _vp]),
+    "exg_server_reset_stats": (ctypes.c_int, [_vp]),
+    "exg_server_destroy": (ctypes.c_int, [_vp]),
+    "exg_pool_set_steps": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
+    "exg_pool_steps_left": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
     "exg_motor_compose": (ctypes.c_int, [_vp, _vp, _vp]),
@@ -294,3 +311,137 @@ class DeviceBatch(DeviceWorld):
         s = np.zeros((), dtype=WORLD_STATS_DTYPE)
         check(lib().exg_batch_world_stats(self.handle, int(k), ptr(s)), "exg_batch_world_stats")
         return s
+
+
+class DevicePool(DeviceWorld):
+    """Worlds admitted into and released from fixed-capacity device arrays; one step advances
+    every admitted world. The serving form of DeviceBatch."""
+
+    def __init__(self, device, max_bodies, max_joints, max_worlds, precision=PRECISION_F64):
+        self.device = device
+        cfg = np.zeros((), dtype=POOL_CONFIG_DTYPE)
+        cfg["max_bodies"], cfg["max_joints"], cfg["max_worlds"], cfg["precision"] = (
+            max_bodies, max_joints, max_worlds, precision)
+        h = ctypes.c_void_p()
+        check(lib().exg_pool_create(device.handle, ptr(cfg), ctypes.byref(h)), "exg_pool_create")
+        self.handle = h
+        self.counts = {}  # slot -> body count
+
+    @property
+    def n(self):
+        return int(sum(self.counts.values()))
+
+    def admit(self, bodies, joints, params):
+        b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        j = np.ascontiguousarray(joints, dtype=JOINT_DTYPE)
+        p = np.ascontiguousarray(params, dtype=STEP_PARAMS_DTYPE).reshape(())
+        slot = ctypes.c_int32()
+        check(lib().exg_pool_admit(self.handle, ptr(b), len(b), ptr(j), len(j), ptr(p), ctypes.byref(slot)),
+              "exg_pool_admit")
+        self.counts[slot.value] = len(b)
+        return slot.value
+
+    def release(self, slot):
+        check(lib().exg_pool_release(self.handle, int(slot)), "exg_pool_release")
+        del self.counts[slot]
+
+    def set_steps(self, slot, steps):
+        check(lib().exg_pool_set_steps(self.handle, int(slot), int(steps)), "exg_pool_set_steps")
+
+    def steps_left(self, n_slots):
+        out = np.zeros(int(n_slots), dtype=np.int32)
+        check(lib().exg_pool_steps_left(self.handle, ptr(out), len(out)), "exg_pool_steps_left")
+        return out
+
+    def usage(self):
+        u = np.zeros((), dtype=POOL_USAGE_DTYPE)
+        check(lib().exg_pool_free(self.handle, ptr(u)), "exg_pool_free")
+        return u
+
+    def world_bodies(self, slot):
+        out = np.zeros(self.counts[slot], dtype=BODY_DTYPE)
+        check(lib().exg_batch_get_world(self.handle, int(slot), ptr(out), len(out)), "exg_batch_get_world")
+        return out
+
+    def set_world_bodies(self, slot, bodies):
+        b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        check(lib().exg_batch_set_world(self.handle, int(slot), ptr(b), len(b)), "exg_batch_set_world")
+
+    def world_stats(self, slot):
+        s = np.zeros((), dtype=WORLD_STATS_DTYPE)
+        check(lib().exg_batch_world_stats(self.handle, int(slot), ptr(s)), "exg_batch_world_stats")
+        return s
+
+
+def world_footprint(n_bodies, n_joints, params):
+    """Device bytes a world holds while admitted to a pool (exg_world_footprint)."""
+    p = np.ascontiguousarray(params, dtype=STEP_PARAMS_DTYPE).reshape(())
+    out = ctypes.c_int64()
+    check(lib().exg_world_footprint(int(n_bodies), int(n_joints), ptr(p), ctypes.byref(out)), "exg_world_footprint")
+    return out.value
+
+
+class Server:
+    """Continuous-batching request loop (exg_server_*): submit worlds with step counts from any
+    thread; a native worker admits them into a device pool against a memory budget and steps them
+    together; results come back through poll / wait."""
+
+    def __init__(self, device, hbm_budget_bytes=150 * 10**9, max_bodies=1 << 22, max_joints=1 << 22,
+                 max_worlds=4096, precision=PRECISION_F64, steps_per_tick=16):
+        self.device = device
+        cfg = np.zeros((), dtype=SERVER_CONFIG_DTYPE)
+        cfg["hbm_budget_bytes"], cfg["max_bodies"], cfg["max_joints"] = hbm_budget_bytes, max_bodies, max_joints
+        cfg["max_worlds"], cfg["precision"], cfg["steps_per_tick"] = max_worlds, precision, steps_per_tick
+        h = ctypes.c_void_p()
+        check(lib().exg_server_create(device.handle, ptr(cfg), ctypes.byref(h)), "exg_server_create")
+        self.handle = h
+        self.sizes = {}
+
+    def submit(self, bodies, joints, params, steps):
+        b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        j = np.ascontiguousarray(joints, dtype=JOINT_DTYPE)
+        p = np.ascontiguousarray(params, dtype=STEP_PARAMS_DTYPE).reshape(())
+        rid = ctypes.c_uint64()
+        check(lib().exg_server_submit(self.handle, ptr(b), len(b), ptr(j), len(j), ptr(p), int(steps),
+                                      ctypes.byref(rid)), "exg_server_submit")
+        self.sizes[rid.value] = len(b)
+        return rid.value
+
+    def _collect(self, st, rid, out, info):
+        if st == PENDING:
+            return None
+        self.sizes.pop(rid, None)
+        check(st, "exg_server request")
+        return out, info
+
+    def poll(self, rid):
+        """None while pending; (bodies, info) once done (raises ExgError if the request failed)."""
+        out = np.zeros(self.sizes.get(rid, 0), dtype=BODY_DTYPE)
+        info = np.zeros((), dtype=REQUEST_INFO_DTYPE)
+        st = lib().exg_server_poll(self.handle, ctypes.c_uint64(rid), ptr(out), len(out), ptr(info))
+        return self._collect(st, rid, out, info)
+
+    def wait(self, rid, timeout_ms=60000):
+        out = np.zeros(self.sizes.get(rid, 0), dtype=BODY_DTYPE)
+        info = np.zeros((), dtype=REQUEST_INFO_DTYPE)
+        st = lib().exg_server_wait(self.handle, ctypes.c_uint64(rid), int(timeout_ms), ptr(out), len(out), ptr(info))
+        return self._collect(st, rid, out, info)
+
+    def stats(self):
+        s = np.zeros((), dtype=SERVER_STATS_DTYPE)
+        check(lib().exg_server_stats(self.handle, ptr(s)), "exg_server_stats")
+        return {k: s[k].item() for k in s.dtype.names if k != "reserved"}
+
+    def reset_stats(self):
+        check(lib().exg_server_reset_stats(self.handle), "exg_server_reset_stats")
+
+    def close(self):
+        if self.handle:
+            lib().exg_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

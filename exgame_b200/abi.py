@@ -53,6 +53,36 @@ WORLD_STATS_DTYPE = np.dtype(
     align=True,
 )
 
+POOL_CONFIG_DTYPE = np.dtype(
+    [("max_bodies", "<i8"), ("max_joints", "<i8"), ("max_worlds", "<i4"), ("precision", "<i4")], align=True
+)
+
+POOL_USAGE_DTYPE = np.dtype(
+    [("worlds_used", "<i4"), ("worlds_capacity", "<i4"), ("largest_free_bodies", "<i8"),
+     ("largest_free_joints", "<i8")],
+    align=True,
+)
+
+SERVER_CONFIG_DTYPE = np.dtype(
+    [("hbm_budget_bytes", "<i8"), ("max_bodies", "<i8"), ("max_joints", "<i8"), ("max_worlds", "<i4"),
+     ("precision", "<i4"), ("steps_per_tick", "<i4"), ("reserved", "<i4")],
+    align=True,
+)
+
+REQUEST_INFO_DTYPE = np.dtype(
+    [("steps", "<i8"), ("n_bodies", "<i4"), ("status", "<i4"), ("queued_s", "<f8"), ("latency_s", "<f8")], align=True
+)
+
+SERVER_STATS_DTYPE = np.dtype(
+    [("submitted", "<i8"), ("completed", "<i8"), ("failed", "<i8"), ("ticks", "<i8"), ("steps_launched", "<i8"),
+     ("body_steps", "<i8"), ("queued", "<i4"), ("running", "<i4"), ("peak_running", "<i4"), ("reserved", "<i4"),
+     ("resident_bytes", "<i8"), ("peak_resident_bytes", "<i8"), ("busy_s", "<f8"), ("elapsed_s", "<f8"),
+     ("p50_latency_s", "<f8"), ("p99_latency_s", "<f8"), ("mean_latency_s", "<f8")],
+    align=True,
+)
+
+PENDING = 1
+
 # Law ids and names (crates/newton/src/accelerator/mod.rs:118-132).
 LAW_NAMES = ("SimpleSpringDamper", "CriticallyDampedWarped", "PerpendicularDamperWarped", "TorsionalDamperWarped")
 LAW_N_PARAMS = (10, 10, 2, 1)

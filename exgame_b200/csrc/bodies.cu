@@ -11,9 +11,20 @@ namespace {
 
 using namespace exg;
 
-__global__ void k_body_pre(BodyView b, double* __restrict__ pos_mass, double* __restrict__ wvel) {
+// The thread of a world's first body also decides whether the world takes this step (its step
+// budget is not spent) and spends one step of it; every later kernel of the step reads w_active.
+__global__ void k_body_pre(BodyView b, const int* __restrict__ world_of_body, const int* __restrict__ w_body_off,
+                           int* __restrict__ w_left, int* __restrict__ w_active, double* __restrict__ pos_mass,
+                           double* __restrict__ wvel) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.n) return;
+  const int wid = world_of_body[i];
+  if (wid < 0) return;
+  if (w_body_off[wid] == i) {
+    const int left = w_left[wid];
+    w_active[wid] = left != 0;
+    if (left > 0) w_left[wid] = left - 1;
+  }
   double pose[8], mom[6], I9[9];
   load_body(b, i, pose, mom, I9);
   bool kin = b.kinematic[i] != 0;
@@ -34,12 +45,12 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
                                      const int* __restrict__ world_of_body, const exg_step_params_t* __restrict__ wparams,
                                      const long long* __restrict__ w_poff, const int* __restrict__ w_splits,
                                      const int* __restrict__ w_n, const int* __restrict__ w_body_off,
-                                     const double* __restrict__ conn, int nj, const int* __restrict__ inc_ptr,
-                                     const int* __restrict__ inc_ref) {
+                                     const int* __restrict__ w_active, const double* __restrict__ conn, int nj, const int* __restrict__ inc_start,
+                                     const int* __restrict__ inc_cnt, const int* __restrict__ inc_ref) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= b.n) return;
-  if (b.kinematic[i]) return;
   const int wid = world_of_body[i];
+  if (wid < 0 || b.kinematic[i] || !w_active[wid]) return;
   const int scheme = wparams[wid].integrator;
   if (scheme == EXG_NEWTON) return;
   const double dt = wparams[wid].dt;
@@ -66,7 +77,7 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
     tot[4] = pm.z * f[0] - pm.x * f[2];
     tot[5] = pm.x * f[1] - pm.y * f[0];
   }
-  for (int q = inc_ptr[i]; q < inc_ptr[i + 1]; ++q) {
+  for (int q = inc_start[i], qe = inc_start[i] + inc_cnt[i]; q < qe; ++q) {
     int ref = inc_ref[q];
     int k = ref >> 1, end = ref & 1;
 #pragma unroll
@@ -126,19 +137,21 @@ BodyView view_of(const DeviceWorld& w) {
 }  // namespace
 
 int launch_body_pre(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
-  if (w.n <= 0) return EXG_OK;
+  if (w.n_ext <= 0) return EXG_OK;
   int _tok = prof_begin(dev, PROF_BODY_PRE, s);
-  k_body_pre<<<(w.n + 127) / 128, 128, 0, s>>>(view_of(w), w.pos_mass, w.wvel);
+  k_body_pre<<<(w.n_ext + 127) / 128, 128, 0, s>>>(view_of(w), w.world_of_body, w.w_body_off, w.w_left, w.w_active,
+                                               w.pos_mass, w.wvel);
   prof_end(dev, _tok, s);
   return exg_after_launch(dev);
 }
 
 int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
-  if (w.n <= 0 || !w.any_explicit) return EXG_OK;
+  if (w.n_ext <= 0 || !w.any_explicit) return EXG_OK;
   int tok = prof_begin(dev, PROF_INTEGRATE, s);
-  k_integrate_explicit<<<(w.n + 127) / 128, 128, 0, s>>>(view_of(w), w.pose, w.mom, w.pos_mass, w.grav_partial,
+  k_integrate_explicit<<<(w.n_ext + 127) / 128, 128, 0, s>>>(view_of(w), w.pose, w.mom, w.pos_mass, w.grav_partial,
                                                          w.world_of_body, w.wparams, w.w_poff, w.w_splits, w.w_n,
-                                                         w.w_body_off, w.conn, w.nj, w.inc_ptr, w.inc_ref);
+                                                         w.w_body_off, w.w_active, w.conn, w.nj, w.inc_start, w.inc_cnt,
+                                                         w.inc_ref);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

@@ -1,11 +1,13 @@
 // C ABI of libexg (include/exg.h): device context, device-resident worlds and the stage calls.
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 #include "exg_internal.cuh"
 #include "body.cuh"
 #include "world_newton.cuh"
+#include "slab.cuh"
 
 namespace {
 thread_local std::string g_last_error;
@@ -18,14 +20,34 @@ void exg_internal_set_cuda_error(cudaError_t e, const char* what) {
   g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
 }
 
+// One admitted world of a pool: its ranges in the pool's arrays and its gravity work items.
+struct WorldSlot {
+  bool used = false;
+  int body_off = 0, n = 0, joint_off = 0, nj = 0;
+  long long poff = 0, plen = 0;  // gravity partial range
+  int splits = 0;
+  std::vector<GravItem> items;   // out_off already relative to the pool's partial array
+  exg_step_params_t params{};
+};
+
+// A world handle is a pool of worlds: arrays of fixed capacity (bodies, joints, world slots) in
+// which worlds are admitted into free ranges and released. A batch is a pool filled once; one
+// world is a batch of one. Structural changes mark the handle dirty: the gravity item queue and
+// the island queue are rebuilt and the step graph re-captured before the next step.
 struct exg_world_s {
   exg_device_s* dev = nullptr;
-  exg_step_params_t p{};
   DeviceWorld w;
   NewtonWorld* newton = nullptr;
   exg_world_stats_t stats{};
   cudaGraphExec_t graph = nullptr;
   int graph_kernels = 0;
+  int b_cap = 0, j_cap = 0, w_cap = 0;
+  RangeAllocator body_alloc, joint_alloc, partial_alloc;
+  std::vector<WorldSlot> slots;
+  int n_explicit = 0, n_implicit = 0, n_used = 0;
+  bool dirty = true;
+  DevArr<GravItem> items_d;
+  DevArr<double> partial_d;
   std::vector<void*> allocations;
 
   template <class T> int alloc(T** out, size_t count) {
@@ -36,9 +58,15 @@ struct exg_world_s {
     *out = static_cast<T*>(p);
     return EXG_OK;
   }
-  ~exg_world_s() {
+  void drop_graph() {
     if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+  }
+  ~exg_world_s() {
+    drop_graph();
     delete newton;
+    items_d.release();
+    partial_d.release();
     for (void* p : allocations) cudaFree(p);
   }
 };
@@ -209,6 +237,7 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
 }
 
 static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count) {
+  if (count <= 0) return EXG_OK;
   DeviceWorld& w = W->w;
   const int n = w.n;
   std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
@@ -242,6 +271,7 @@ static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t first
 }
 
 static int download_bodies(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count) {
+  if (count <= 0) return EXG_OK;
   DeviceWorld& w = W->w;
   const int n = w.n;
   std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
@@ -274,11 +304,222 @@ static int download_bodies(exg_world_s* W, exg_body_t* out, int32_t first, int32
   return EXG_OK;
 }
 
-template <class T> static int upload_vec(exg_world_s* W, T** dptr, const std::vector<T>& v) {
-  int rc = W->alloc(dptr, v.size());
+static int fill_int(exg_world_s* W, int* d, long long first, long long count, int value) {
+  if (count <= 0) return EXG_OK;
+  std::vector<int> v(count, value);
+  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, v.data(), sizeof(int) * count, cudaMemcpyHostToDevice, W->dev->stream));
+  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  return EXG_OK;
+}
+
+template <class T> static int put(exg_world_s* W, T* d, long long first, const T* src, long long count) {
+  if (count <= 0) return EXG_OK;
+  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, src, sizeof(T) * count, cudaMemcpyHostToDevice, W->dev->stream));
+  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  return EXG_OK;
+}
+
+// Allocate a pool's arrays at fixed capacity; every body and joint slot starts unused.
+static int pool_init(exg_world_s* W, exg_device_s* dev, int b_cap, int j_cap, int w_cap, int precision) {
+  W->dev = dev;
+  W->b_cap = b_cap;
+  W->j_cap = j_cap;
+  W->w_cap = w_cap;
+  W->body_alloc.init(b_cap);
+  W->joint_alloc.init(j_cap);
+  W->partial_alloc.init(0);
+  W->slots.resize(w_cap);
+  DeviceWorld& w = W->w;
+  w.n = b_cap;
+  w.nj = j_cap;
+  w.n_worlds = w_cap;
+  w.precision = precision;
+  w.h_params.resize(w_cap);
+  w.h_body_off.assign(w_cap, 0);
+  w.h_n.assign(w_cap, 0);
+  w.h_joint_off.assign(w_cap, 0);
+  w.h_nj.assign(w_cap, 0);
+  int rc = EXG_OK;
+#define ALLOC(ptr, cnt) \
+  if (rc == EXG_OK) rc = W->alloc(&(ptr), (cnt))
+  ALLOC(w.pose, 8 * (size_t)b_cap);
+  ALLOC(w.mom, 6 * (size_t)b_cap);
+  ALLOC(w.mass, (size_t)b_cap);
+  ALLOC(w.inertia, 9 * (size_t)b_cap);
+  ALLOC(w.size, (size_t)b_cap);
+  ALLOC(w.kinematic, (size_t)b_cap);
+  ALLOC(w.diagonal, (size_t)b_cap);
+  ALLOC(w.world_of_body, (size_t)b_cap);
+  ALLOC(w.inc_start, (size_t)b_cap);
+  ALLOC(w.inc_cnt, (size_t)b_cap);
+  ALLOC(w.pos_mass, 4 * (size_t)b_cap);
+  ALLOC(w.wvel, 6 * (size_t)b_cap);
+  ALLOC(w.joints, (size_t)j_cap);
+  ALLOC(w.world_of_joint, (size_t)j_cap);
+  ALLOC(w.inc_ref, 2 * (size_t)j_cap);
+  ALLOC(w.conn, 12 * (size_t)j_cap);
+  ALLOC(w.wparams, (size_t)w_cap);
+  ALLOC(w.w_poff, (size_t)w_cap);
+  ALLOC(w.w_splits, (size_t)w_cap);
+  ALLOC(w.w_n, (size_t)w_cap);
+  ALLOC(w.w_body_off, (size_t)w_cap);
+  ALLOC(w.w_left, (size_t)w_cap);
+  ALLOC(w.w_active, (size_t)w_cap);
+  ALLOC(w.item_head, 1);
+#undef ALLOC
   if (rc != EXG_OK) return rc;
-  if (!v.empty())
-    EXG_CUDA_TRY(cudaMemcpyAsync(*dptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, W->dev->stream));
+  cudaStream_t s = dev->stream;
+  EXG_CUDA_TRY(cudaMemsetAsync(w.world_of_body, 0xff, sizeof(int) * (size_t)std::max(b_cap, 1), s));
+  EXG_CUDA_TRY(cudaMemsetAsync(w.world_of_joint, 0xff, sizeof(int) * (size_t)std::max(j_cap, 1), s));
+  EXG_CUDA_TRY(cudaMemsetAsync(w.inc_cnt, 0, sizeof(int) * (size_t)std::max(b_cap, 1), s));
+  EXG_CUDA_TRY(cudaMemsetAsync(w.w_active, 0, sizeof(int) * (size_t)std::max(w_cap, 1), s));
+  EXG_CUDA_TRY(cudaMemsetAsync(w.w_splits, 0, sizeof(int) * (size_t)std::max(w_cap, 1), s));
+  EXG_CUDA_TRY(cudaMemsetAsync(w.w_poff, 0, sizeof(long long) * (size_t)std::max(w_cap, 1), s));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  W->newton = new (std::nothrow) NewtonWorld();
+  if (!W->newton) return EXG_ERR_OUT_OF_MEMORY;
+  return EXG_OK;
+}
+
+// Admit one validated world into free ranges of the pool.
+static int pool_admit(exg_world_s* W, const exg_body_t* bodies, int n, const exg_joint_t* joints, int nj,
+                      const exg_step_params_t& p, int* slot_out) {
+  if (p.precision != W->w.precision) return EXG_ERR_INVALID_ARGUMENT;
+  int slot = -1;
+  for (int k = 0; k < W->w_cap; ++k)
+    if (!W->slots[k].used) { slot = k; break; }
+  if (slot < 0) return EXG_ERR_OUT_OF_MEMORY;
+  long long bo = W->body_alloc.alloc(n);
+  if (bo < 0) return EXG_ERR_OUT_OF_MEMORY;
+  long long jo = W->joint_alloc.alloc(nj);
+  if (jo < 0) {
+    W->body_alloc.release(bo, n);
+    return EXG_ERR_OUT_OF_MEMORY;
+  }
+  DeviceWorld& w = W->w;
+  int rc = upload_bodies(W, bodies, (int)bo, n);
+  // joints with batch-global body indices, incidence per body in joint order
+  std::vector<exg_joint_t> gj(joints, joints + nj);
+  for (auto& j : gj) { j.a += (int)bo; j.b += (int)bo; }
+  std::vector<int> cnt(n, 0), start(n, 0), ref(2 * (size_t)nj);
+  for (int k = 0; k < nj; ++k) { cnt[joints[k].a]++; cnt[joints[k].b]++; }
+  int acc = 0;
+  for (int i = 0; i < n; ++i) { start[i] = 2 * (int)jo + acc; acc += cnt[i]; }
+  std::vector<int> fill(start);
+  for (int k = 0; k < nj; ++k) {
+    ref[fill[joints[k].a]++ - 2 * jo] = 2 * ((int)jo + k);
+    ref[fill[joints[k].b]++ - 2 * jo] = 2 * ((int)jo + k) + 1;
+  }
+  if (rc == EXG_OK) rc = put(W, w.joints, jo, gj.data(), nj);
+  if (rc == EXG_OK) rc = put(W, w.inc_start, bo, start.data(), n);
+  if (rc == EXG_OK) rc = put(W, w.inc_cnt, bo, cnt.data(), n);
+  if (rc == EXG_OK) rc = put(W, w.inc_ref, 2 * jo, ref.data(), 2 * (long long)nj);
+  if (rc == EXG_OK) rc = fill_int(W, w.world_of_joint, jo, nj, slot);
+  // gravity work items of this world alone (their j-ranges depend on the world's size only)
+  WorldSlot ws;
+  std::vector<GravItem> items;
+  std::vector<int> splits;
+  std::vector<long long> poff;
+  long long plen = 0;
+  gravity_plan({(int)bo}, {n}, {p.gravity_law}, {p.softening}, W->dev->sm_count, items, splits, poff, plen);
+  long long po = 0;
+  if (plen > 0) {
+    po = W->partial_alloc.alloc(plen);
+    if (po < 0) {
+      long long old = W->partial_alloc.capacity();
+      W->partial_alloc.grow(old + std::max(old, plen));
+      po = W->partial_alloc.alloc(plen);
+    }
+  }
+  for (auto& g : items) g.out_off += po;
+  int sp = splits.empty() ? 0 : splits[0];
+  int w_n = n, w_bo = (int)bo, unbounded = -1;
+  if (rc == EXG_OK) rc = put(W, w.wparams, slot, &p, 1);
+  if (rc == EXG_OK) rc = put(W, w.w_poff, slot, &po, 1);
+  if (rc == EXG_OK) rc = put(W, w.w_splits, slot, &sp, 1);
+  if (rc == EXG_OK) rc = put(W, w.w_n, slot, &w_n, 1);
+  if (rc == EXG_OK) rc = put(W, w.w_body_off, slot, &w_bo, 1);
+  if (rc == EXG_OK) rc = put(W, w.w_left, slot, &unbounded, 1);
+  if (rc == EXG_OK && p.integrator == EXG_NEWTON) rc = W->newton->add_world(W->dev, slot, (int)bo, bodies, n, joints, nj);
+  if (rc == EXG_OK) rc = fill_int(W, w.world_of_body, bo, n, slot);  // last: the world becomes visible
+  if (rc != EXG_OK) {
+    fill_int(W, w.world_of_joint, jo, nj, -1);
+    W->body_alloc.release(bo, n);
+    W->joint_alloc.release(jo, nj);
+    if (plen > 0) W->partial_alloc.release(po, plen);
+    return rc;
+  }
+  ws.used = true;
+  ws.body_off = (int)bo;
+  ws.n = n;
+  ws.joint_off = (int)jo;
+  ws.nj = nj;
+  ws.poff = po;
+  ws.plen = plen;
+  ws.splits = sp;
+  ws.items = std::move(items);
+  ws.params = p;
+  W->slots[slot] = std::move(ws);
+  w.h_params[slot] = p;
+  w.h_body_off[slot] = (int)bo;
+  w.h_n[slot] = n;
+  w.h_joint_off[slot] = (int)jo;
+  w.h_nj[slot] = nj;
+  if (p.integrator == EXG_NEWTON) ++W->n_implicit; else ++W->n_explicit;
+  ++W->n_used;
+  W->dirty = true;
+  *slot_out = slot;
+  return EXG_OK;
+}
+
+static int pool_release(exg_world_s* W, int slot) {
+  if (slot < 0 || slot >= W->w_cap || !W->slots[slot].used) return EXG_ERR_INVALID_ARGUMENT;
+  WorldSlot& ws = W->slots[slot];
+  int rc = fill_int(W, W->w.world_of_body, ws.body_off, ws.n, -1);
+  if (rc == EXG_OK) rc = fill_int(W, W->w.world_of_joint, ws.joint_off, ws.nj, -1);
+  int zero = 0;
+  if (rc == EXG_OK) rc = put(W, W->w.w_splits, slot, &zero, 1);
+  if (rc != EXG_OK) return rc;
+  if (ws.params.integrator == EXG_NEWTON) { W->newton->remove_world(slot); --W->n_implicit; } else --W->n_explicit;
+  W->body_alloc.release(ws.body_off, ws.n);
+  W->joint_alloc.release(ws.joint_off, ws.nj);
+  if (ws.plen > 0) W->partial_alloc.release(ws.poff, ws.plen);
+  ws = WorldSlot();
+  --W->n_used;
+  W->dirty = true;
+  return EXG_OK;
+}
+
+// Before a step after a structural change: the gravity queue of the live worlds (largest item
+// first), the partial array's size, the island queue; the step graph is re-captured.
+static int pool_prepare(exg_world_s* W) {
+  if (!W->dirty) return EXG_OK;
+  W->drop_graph();
+  DeviceWorld& w = W->w;
+  cudaStream_t s = W->dev->stream;
+  std::vector<std::pair<double, GravItem>> tmp;
+  for (auto& ws : W->slots)
+    if (ws.used)
+      for (auto& g : ws.items) tmp.push_back({double(std::min(kGravTile, g.n - g.i0)) * (g.j1 - g.j0), g});
+  std::stable_sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<GravItem> items;
+  items.reserve(tmp.size());
+  for (auto& x : tmp) items.push_back(x.second);
+  int rc = W->items_d.assign(items.data(), (long long)items.size(), s);
+  if (rc != EXG_OK) return rc;
+  if (W->partial_d.cap < W->partial_alloc.capacity()) {
+    W->partial_d.release();  // per-step contents: no copy needed
+    if ((rc = W->partial_d.reserve(std::max<long long>(W->partial_alloc.capacity(), 1), s)) != EXG_OK) return rc;
+  }
+  w.items = W->items_d.ptr;
+  w.n_items = (int)items.size();
+  w.grav_partial = W->partial_d.ptr;
+  w.n_ext = (int)W->body_alloc.used_end();
+  w.nj_ext = (int)W->joint_alloc.used_end();
+  w.any_explicit = W->n_explicit > 0;
+  w.any_newton = W->n_implicit > 0;
+  if ((rc = W->newton->sync(W->dev, s)) != EXG_OK) return rc;
+  W->dirty = false;
   return EXG_OK;
 }
 
@@ -302,81 +543,15 @@ int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* body_cou
   cudaSetDevice(dev->ordinal);
   exg_world_s* W = new (std::nothrow) exg_world_s();
   if (!W) return EXG_ERR_OUT_OF_MEMORY;
-  W->dev = dev;
-  W->p = params[0];
-  DeviceWorld& w = W->w;
-  const int n = (int)n_total, nj = (int)nj_total;
-  w.n = n;
-  w.nj = nj;
-  w.n_worlds = n_worlds;
-  w.precision = params[0].precision;
-  w.h_params.assign(params, params + n_worlds);
-  std::vector<int> wob(n), woj(nj), law(n_worlds);
-  std::vector<double> eps(n_worlds);
-  std::vector<exg_joint_t> gj(joints, joints + nj);
-  int bo = 0, jo = 0;
-  for (int32_t wi = 0; wi < n_worlds; ++wi) {
-    w.h_body_off.push_back(bo);
-    w.h_n.push_back(body_counts[wi]);
-    w.h_joint_off.push_back(jo);
-    w.h_nj.push_back(joint_counts[wi]);
-    for (int i = 0; i < body_counts[wi]; ++i) wob[bo + i] = wi;
-    for (int k = 0; k < joint_counts[wi]; ++k) {
-      woj[jo + k] = wi;
-      gj[jo + k].a += bo;
-      gj[jo + k].b += bo;
-    }
-    law[wi] = params[wi].gravity_law;
-    eps[wi] = params[wi].softening;
-    if (params[wi].integrator == EXG_NEWTON) w.any_newton = true; else w.any_explicit = true;
+  int rc = pool_init(W, dev, (int)n_total, (int)nj_total, n_worlds, params[0].precision);
+  long long bo = 0, jo = 0;
+  for (int32_t wi = 0; wi < n_worlds && rc == EXG_OK; ++wi) {
+    int slot = -1;
+    rc = pool_admit(W, bodies + bo, body_counts[wi], joints + jo, joint_counts[wi], params[wi], &slot);
     bo += body_counts[wi];
     jo += joint_counts[wi];
   }
-  std::vector<GravItem> items;
-  std::vector<int> splits;
-  std::vector<long long> poff;
-  long long partial_len = 0;
-  gravity_plan(w.h_body_off, w.h_n, law, eps, dev->sm_count, items, splits, poff, partial_len);
-  w.n_items = (int)items.size();
-  int rc = EXG_OK;
-#define ALLOC(ptr, cnt) \
-  if (rc == EXG_OK) rc = W->alloc(&(ptr), (cnt))
-  ALLOC(w.pose, 8 * (size_t)n);
-  ALLOC(w.mom, 6 * (size_t)n);
-  ALLOC(w.mass, (size_t)n);
-  ALLOC(w.inertia, 9 * (size_t)n);
-  ALLOC(w.size, (size_t)n);
-  ALLOC(w.kinematic, (size_t)n);
-  ALLOC(w.diagonal, (size_t)n);
-  ALLOC(w.pos_mass, 4 * (size_t)n);
-  ALLOC(w.wvel, 6 * (size_t)n);
-  ALLOC(w.grav_partial, (size_t)std::max<long long>(partial_len, 1));
-  ALLOC(w.conn, 12 * (size_t)nj);
-  ALLOC(w.item_head, 1);
-#undef ALLOC
-  // incidence: per body, its joint ends in joint order (accelerator/mod.rs:289-331)
-  std::vector<int> cnt(n + 1, 0), ptr(n + 1, 0), ref(2 * (size_t)nj);
-  for (int k = 0; k < nj; ++k) { cnt[gj[k].a]++; cnt[gj[k].b]++; }
-  for (int i = 0; i < n; ++i) ptr[i + 1] = ptr[i] + cnt[i];
-  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
-  for (int k = 0; k < nj; ++k) { ref[fill[gj[k].a]++] = 2 * k; ref[fill[gj[k].b]++] = 2 * k + 1; }
-  if (rc == EXG_OK) rc = upload_vec(W, &w.joints, gj);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.world_of_body, wob);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.world_of_joint, woj);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.inc_ptr, ptr);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.inc_ref, ref);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.wparams, w.h_params);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.w_poff, poff);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.w_splits, splits);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.w_n, w.h_n);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.w_body_off, w.h_body_off);
-  if (rc == EXG_OK) rc = upload_vec(W, &w.items, items);
-  if (rc == EXG_OK) rc = upload_bodies(W, bodies, 0, n);
-  if (rc == EXG_OK && w.any_newton) {
-    W->newton = new (std::nothrow) NewtonWorld();
-    if (!W->newton) rc = EXG_ERR_OUT_OF_MEMORY;
-    else rc = W->newton->init(dev, w, bodies, gj.data(), params[0]);
-  }
+  if (rc == EXG_OK) rc = pool_prepare(W);
   if (rc != EXG_OK) { delete W; return rc; }
   *out = W;
   return EXG_OK;
@@ -385,6 +560,87 @@ int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* body_cou
 int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n, const exg_joint_t* joints, int32_t nj,
                      const exg_step_params_t* params, exg_world_t* out) {
   return exg_batch_create(dev, 1, &n, &nj, bodies, joints, params, out);
+}
+
+int exg_pool_create(exg_device_t dev, const exg_pool_config_t* cfg, exg_world_t* out) {
+  if (!dev || !cfg || !out || cfg->max_bodies <= 0 || cfg->max_joints < 0 || cfg->max_worlds <= 0) return EXG_ERR_INVALID_ARGUMENT;
+  if (cfg->precision != EXG_PRECISION_F64 && cfg->precision != EXG_PRECISION_MIXED) return EXG_ERR_INVALID_ARGUMENT;
+  if (cfg->max_bodies > (1LL << 30) || cfg->max_joints > (1LL << 29)) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(dev->mu);
+  cudaSetDevice(dev->ordinal);
+  exg_world_s* W = new (std::nothrow) exg_world_s();
+  if (!W) return EXG_ERR_OUT_OF_MEMORY;
+  int rc = pool_init(W, dev, (int)cfg->max_bodies, (int)cfg->max_joints, cfg->max_worlds, cfg->precision);
+  if (rc != EXG_OK) { delete W; return rc; }
+  *out = W;
+  return EXG_OK;
+}
+
+int exg_pool_admit(exg_world_t W, const exg_body_t* bodies, int32_t n, const exg_joint_t* joints, int32_t nj,
+                   const exg_step_params_t* params, int32_t* slot_out) {
+  if (!W || !slot_out) return EXG_ERR_INVALID_ARGUMENT;
+  int st = validate_world(bodies, n, joints, nj, params);
+  if (st != EXG_OK) return st;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  int slot = -1;
+  int rc = pool_admit(W, bodies, n, joints, nj, *params, &slot);
+  if (rc == EXG_OK) *slot_out = slot;
+  return rc;
+}
+
+int exg_pool_release(exg_world_t W, int32_t slot) {
+  if (!W) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  return pool_release(W, slot);
+}
+
+int exg_pool_free(exg_world_t W, exg_pool_usage_t* out) {
+  if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  out->worlds_used = W->n_used;
+  out->worlds_capacity = W->w_cap;
+  out->largest_free_bodies = W->body_alloc.largest_free();
+  out->largest_free_joints = W->joint_alloc.largest_free();
+  return EXG_OK;
+}
+
+int exg_world_footprint(int32_t n, int32_t nj, const exg_step_params_t* p, int64_t* bytes) {
+  if (!p || !bytes || n < 0 || nj < 0) return EXG_ERR_INVALID_ARGUMENT;
+  // pool rows: pose 8, momentum 6, mass, inertia 9, size, charge 4, world twist 6 doubles; kinematic,
+  // diagonal, world, incidence start and count ints. Joints: the record, its world, two incidence
+  // references and the 12 wrench components.
+  long long b = (long long)n * ((8 + 6 + 1 + 9 + 1 + 4 + 6) * 8 + 5 * 4) +
+                (long long)nj * ((long long)sizeof(exg_joint_t) + 3 * 4 + 12 * 8);
+  if (p->gravity_law != EXG_GRAVITY_OFF && n > 1) {
+    int L = kGravTile;
+    while (L < 2048 && L * 8 < n) L *= 2;
+    long long splits = (n + L - 1) / L, itiles = (n + kGravTile - 1) / kGravTile;
+    b += splits * 3 * (long long)n * 8 + splits * itiles * (long long)sizeof(GravItem);
+  }
+  if (p->integrator == EXG_NEWTON) b += newton_footprint_bytes(n, nj);
+  *bytes = b;
+  return EXG_OK;
+}
+
+int exg_pool_set_steps(exg_world_t W, int32_t slot, int32_t steps) {
+  if (!W || slot < 0 || slot >= W->w_cap || !W->slots[slot].used || steps < -1) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  return put(W, W->w.w_left, slot, &steps, 1);
+}
+
+int exg_pool_steps_left(exg_world_t W, int32_t* out, int32_t n_slots) {
+  if (!W || !out || n_slots < 0 || n_slots > W->w_cap) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  if (n_slots == 0) return EXG_OK;
+  EXG_CUDA_TRY(cudaMemcpyAsync(out, W->w.w_left, sizeof(int32_t) * n_slots, cudaMemcpyDeviceToHost, W->dev->stream));
+  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  for (int32_t k = 0; k < n_slots; ++k)
+    if (!W->slots[k].used) out[k] = 0;
+  return EXG_OK;
 }
 
 int exg_world_destroy(exg_world_t W) {
@@ -398,7 +654,7 @@ int exg_world_destroy(exg_world_t W) {
 
 }  // extern "C"
 
-// One step of every world of the batch (Mechanism::step per world, all enqueued asynchronously):
+// One step of every live world (Mechanism::step per world, all enqueued asynchronously):
 // charges and world twists, gravity, explicit joints and integration, then the implicit islands.
 static int enqueue_step(exg_world_s* W, int* kernels) {
   DeviceWorld& w = W->w;
@@ -407,21 +663,24 @@ static int enqueue_step(exg_world_s* W, int* kernels) {
   int rc;
   if ((rc = launch_body_pre(W->dev, w, s)) != EXG_OK) return rc;
   if ((rc = launch_gravity_items(W->dev, w.pos_mass, w.size, w.items, w.n_items, w.item_head, w.precision,
-                                 w.grav_partial, s)) != EXG_OK)
+                                 w.grav_partial, s, w.world_of_body, w.w_active)) != EXG_OK)
     return rc;
   if ((rc = launch_joints_plain_world(W->dev, w, s)) != EXG_OK) return rc;
   if ((rc = launch_integrate_explicit(W->dev, w, s)) != EXG_OK) return rc;
-  if (W->newton && (rc = W->newton->enqueue(W->dev, w, s)) != EXG_OK) return rc;
+  if ((rc = W->newton->enqueue(W->dev, w, s)) != EXG_OK) return rc;
   *kernels = (int)(W->dev->launches.load() - before);
   return EXG_OK;
 }
 
 static int step_locked(exg_world_s* W, int32_t n_steps) {
   cudaStream_t s = W->dev->stream;
+  int rc = pool_prepare(W);
+  if (rc != EXG_OK) return rc;
+  if (W->n_used == 0 || n_steps == 0) return EXG_OK;
   if (W->dev->profiling) {
     for (int32_t k = 0; k < n_steps; ++k) {
       int kernels = 0;
-      int rc = enqueue_step(W, &kernels);
+      rc = enqueue_step(W, &kernels);
       if (rc != EXG_OK) return rc;
     }
   } else {
@@ -431,7 +690,7 @@ static int step_locked(exg_world_s* W, int32_t n_steps) {
       EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       int kernels = 0;
       uint64_t before = W->dev->launches.load();
-      int rc = enqueue_step(W, &kernels);
+      rc = enqueue_step(W, &kernels);
       W->dev->launches.store(before);  // captured, not yet launched
       cudaError_t e = cudaStreamEndCapture(s, &g);
       if (rc != EXG_OK) {
@@ -452,8 +711,8 @@ static int step_locked(exg_world_s* W, int32_t n_steps) {
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   W->stats.steps += n_steps;
   W->stats.last_spans = 1;
-  if (W->newton) {
-    int rc = W->newton->read_stats(-1, &W->stats);
+  if (W->n_implicit > 0) {
+    rc = W->newton->read_stats(-1, &W->stats);
     if (rc != EXG_OK) return rc;
     if (W->stats.fatal) return EXG_ERR_FATAL;
   }
@@ -469,36 +728,59 @@ int exg_world_step(exg_world_t W, int32_t n_steps) {
   return step_locked(W, n_steps);
 }
 
+// whole-handle accessors: the used worlds in slot order, each at its body offset
 int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
-  if (!W || !out || n != W->w.n) return EXG_ERR_INVALID_ARGUMENT;
+  if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
-  return download_bodies(W, out, 0, n);
+  long long total = 0;
+  for (auto& ws : W->slots) if (ws.used) total += ws.n;
+  if (n != total) return EXG_ERR_INVALID_ARGUMENT;
+  long long at = 0;
+  for (auto& ws : W->slots) {
+    if (!ws.used) continue;
+    int rc = download_bodies(W, out + at, ws.body_off, ws.n);
+    if (rc != EXG_OK) return rc;
+    at += ws.n;
+  }
+  return EXG_OK;
 }
 
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
-  if (!W || !bodies || n != W->w.n) return EXG_ERR_INVALID_ARGUMENT;
+  if (!W || !bodies) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
+  long long total = 0;
+  for (auto& ws : W->slots) if (ws.used) total += ws.n;
+  if (n != total) return EXG_ERR_INVALID_ARGUMENT;
   for (int32_t i = 0; i < n; ++i)
     if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  return upload_bodies(W, bodies, 0, n);
+  long long at = 0;
+  for (auto& ws : W->slots) {
+    if (!ws.used) continue;
+    int rc = upload_bodies(W, bodies + at, ws.body_off, ws.n);
+    if (rc != EXG_OK) return rc;
+    at += ws.n;
+  }
+  return EXG_OK;
 }
 
 int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n) {
-  if (!W || !out || world < 0 || world >= W->w.n_worlds || n != W->w.h_n[world]) return EXG_ERR_INVALID_ARGUMENT;
+  if (!W || !out || world < 0 || world >= W->w_cap || !W->slots[world].used || n != W->slots[world].n)
+    return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
-  return download_bodies(W, out, W->w.h_body_off[world], n);
+  return download_bodies(W, out, W->slots[world].body_off, n);
 }
 
 int exg_batch_set_world(exg_world_t W, int32_t world, const exg_body_t* bodies, int32_t n) {
-  if (!W || !bodies || world < 0 || world >= W->w.n_worlds || n != W->w.h_n[world]) return EXG_ERR_INVALID_ARGUMENT;
+  if (!W || !bodies || world < 0 || world >= W->w_cap || !W->slots[world].used || n != W->slots[world].n)
+    return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   for (int32_t i = 0; i < n; ++i)
     if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  return upload_bodies(W, bodies, W->w.h_body_off[world], n);
+  return upload_bodies(W, bodies, W->slots[world].body_off, n);
 }
 
 int exg_world_stats(exg_world_t W, exg_world_stats_t* out) {
@@ -508,7 +790,7 @@ int exg_world_stats(exg_world_t W, exg_world_stats_t* out) {
 }
 
 int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) {
-  if (!W || !out || world < 0 || world >= W->w.n_worlds) return EXG_ERR_INVALID_ARGUMENT;
+  if (!W || !out || world < 0 || world >= W->w_cap || !W->slots[world].used) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   *out = W->stats;
@@ -517,14 +799,12 @@ int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) 
   out->max_depth_reached = 0;
   out->fatal = 0;
   out->last_residual = 0.0;
-  if (W->newton && W->w.h_params[world].integrator == EXG_NEWTON) return W->newton->read_stats(world, out);
+  if (W->slots[world].params.integrator == EXG_NEWTON) return W->newton->read_stats(world, out);
   return EXG_OK;
 }
 
 int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  for (int k = 0; k < 8; ++k) out[k] = 0;
-  if (!W->newton) return EXG_OK;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   long long tmp[8];
@@ -535,20 +815,20 @@ int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
 
 int exg_world_energy(exg_world_t W, double* out) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  int n = W->w.n;
-  std::vector<exg_body_t> b(n);
-  int rc = exg_world_get_bodies(W, b.data(), n);
-  if (rc != EXG_OK) return rc;
-  std::vector<exg_joint_t> joints(W->w.nj);
-  if (W->w.nj > 0) {
-    EXG_CUDA_TRY(cudaMemcpy(joints.data(), W->w.joints, sizeof(exg_joint_t) * W->w.nj, cudaMemcpyDeviceToHost));
-  }
   double e = 0.0;
-  for (int wi = 0; wi < W->w.n_worlds; ++wi) {
-    int bo = W->w.h_body_off[wi], jo = W->w.h_joint_off[wi];
-    std::vector<exg_joint_t> local(joints.begin() + jo, joints.begin() + jo + W->w.h_nj[wi]);
-    for (auto& j : local) { j.a -= bo; j.b -= bo; }
-    e += host_world_energy(b.data() + bo, W->w.h_n[wi], local.data(), (int)local.size(), W->w.h_params[wi]);
+  for (int k = 0; k < W->w_cap; ++k) {
+    const WorldSlot& ws = W->slots[k];
+    if (!ws.used) continue;
+    std::vector<exg_body_t> b(ws.n);
+    int rc = exg_batch_get_world(W, k, b.data(), ws.n);
+    if (rc != EXG_OK) return rc;
+    std::vector<exg_joint_t> j(ws.nj);
+    if (ws.nj > 0) {
+      std::lock_guard<std::mutex> lock(W->dev->mu);
+      EXG_CUDA_TRY(cudaMemcpy(j.data(), W->w.joints + ws.joint_off, sizeof(exg_joint_t) * ws.nj, cudaMemcpyDeviceToHost));
+    }
+    for (auto& jj : j) { jj.a -= ws.body_off; jj.b -= ws.body_off; }
+    e += host_world_energy(b.data(), ws.n, j.data(), ws.nj, ws.params);
   }
   *out = e;
   return EXG_OK;

@@ -73,7 +73,8 @@ void gravity_plan(const std::vector<int>& body_off, const std::vector<int>& n, c
 // Device-resident batch of worlds. Per-body quantities are component-major over all bodies of
 // the batch: component c of body i at [c*n + i].
 struct DeviceWorld {
-  int n = 0, nj = 0, n_worlds = 0, precision = 0;
+  int n = 0, nj = 0, n_worlds = 0, precision = 0;  // n, nj: array strides (capacities)
+  int n_ext = 0, nj_ext = 0;  // bodies / joints below which every used slot lies (launch extents)
   double* pose = nullptr;      // [8][n]
   double* mom = nullptr;       // [6][n] body-frame momentum
   double* mass = nullptr;      // [n]
@@ -81,17 +82,20 @@ struct DeviceWorld {
   double* size = nullptr;      // [n]
   int* kinematic = nullptr;    // [n]
   int* diagonal = nullptr;     // [n]
-  int* world_of_body = nullptr;     // [n]
+  int* world_of_body = nullptr;     // [n], -1 for an unused slot
   exg_joint_t* joints = nullptr;    // [nj], body indices global to the batch
-  int* world_of_joint = nullptr;    // [nj]
-  int* inc_ptr = nullptr;      // [n+1] body -> incident joint ends (CSR)
-  int* inc_ref = nullptr;      // [2*nj] joint*2 + end, in joint order
+  int* world_of_joint = nullptr;    // [nj], -1 for an unused slot
+  int* inc_start = nullptr;    // [n] first incident joint end of each body in inc_ref
+  int* inc_cnt = nullptr;      // [n] number of incident joint ends
+  int* inc_ref = nullptr;      // [2*nj] joint*2 + end, per body in joint order
   // per world
   exg_step_params_t* wparams = nullptr;  // [n_worlds]
   long long* w_poff = nullptr;           // gravity partial offset per world
   int* w_splits = nullptr;               // gravity splits per world (0: no gravity)
   int* w_n = nullptr;                    // bodies per world
   int* w_body_off = nullptr;             // first body of each world
+  int* w_left = nullptr;                 // steps the world still takes (-1: unbounded)
+  int* w_active = nullptr;               // 1 when the world takes the current step
   // gravity work items and the persistent scheduler's counter
   GravItem* items = nullptr;
   int n_items = 0;
@@ -110,7 +114,8 @@ struct DeviceWorld {
 // ── launch wrappers (each returns an exg_status) ─────────────────────────────
 int launch_body_pre(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);
 int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double* size, const GravItem* items, int n_items,
-                         int* head, int precision, double* partial, cudaStream_t s);
+                         int* head, int precision, double* partial, cudaStream_t s,
+                         const int* world_of_body = nullptr, const int* w_active = nullptr);
 int launch_gravity_reduce(exg_device_s* dev, const double* partial, const double* pos_mass, int n, int splits, double G,
                           double* force_out, cudaStream_t s);
 int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);

@@ -31,11 +31,21 @@ template <class R> struct Vec4;
 template <> struct Vec4<double> { typedef double4 T; };
 template <> struct Vec4<float> { typedef float4 T; };
 
+// One CTA of kGravThreads threads owns an i-tile of kGravTile = 2 * kGravThreads bodies (thread t:
+// bodies i0 + t and i0 + t + kGravThreads), so each shared-memory broadcast of a j-body feeds two
+// pair evaluations. Every i-body still sums its j-range tile by tile in j order, then flushes the
+// tile's FP32 partial into FP64.
+constexpr int kGravThreads = kGravTile / 2;
+
 template <class R>
-__global__ void __launch_bounds__(kGravTile) k_gravity_items(const double4* __restrict__ pm, const double* __restrict__ size,
-                                                             const GravItem* __restrict__ items, int n_items,
-                                                             int* __restrict__ head, double* __restrict__ partial) {
+__global__ void __launch_bounds__(kGravThreads) k_gravity_items(const double4* __restrict__ pm,
+                                                                const double* __restrict__ size,
+                                                                const GravItem* __restrict__ items, int n_items,
+                                                                int* __restrict__ head, double* __restrict__ partial,
+                                                                const int* __restrict__ world_of_body,
+                                                                const int* __restrict__ w_active) {
   constexpr int T = kGravTile;
+  constexpr int H = kGravThreads;
   typedef typename Vec4<R>::T V4;
   __shared__ V4 tile[T];
   __shared__ R tsz2[T];
@@ -48,74 +58,257 @@ __global__ void __launch_bounds__(kGravTile) k_gravity_items(const double4* __re
     __syncthreads();
     if (it >= n_items) return;
     const GravItem g = items[it];
-    const int il = g.i0 + threadIdx.x;
-    const bool valid = il < g.n;
+    if (w_active && !w_active[world_of_body[g.body_off]]) continue;  // the world holds this step
+    const int il0 = g.i0 + threadIdx.x, il1 = il0 + H;
+    const bool v0 = il0 < g.n, v1 = il1 < g.n;
     const double4* wpm = pm + g.body_off;
     double4 c = make_double4(0.0, 0.0, 0.0, 0.0);
     if (sizeof(R) == 4) c = wpm[g.i0];
-    const double4 pi = valid ? wpm[il] : c;
-    const R xi = R(pi.x - c.x), yi = R(pi.y - c.y), zi = R(pi.z - c.z);
+    const double4 p0 = v0 ? wpm[il0] : c, p1 = v1 ? wpm[il1] : c;
+    const R x0 = R(p0.x - c.x), y0 = R(p0.y - c.y), z0 = R(p0.z - c.z);
+    const R x1 = R(p1.x - c.x), y1 = R(p1.y - c.y), z1 = R(p1.z - c.z);
     const bool core_law = g.law == EXG_GRAVITY_SIZE_CORE;
-    R sz2_i = R(0), isz3_i = R(0);
-    if (core_law && valid) {
-      double s = size[g.body_off + il];
-      sz2_i = R(s * s);
-      isz3_i = R(1.0 / (s * s * s));
+    R sz2_0 = R(0), isz3_0 = R(0), sz2_1 = R(0), isz3_1 = R(0);
+    if (core_law) {
+      if (v0) { double s = size[g.body_off + il0]; sz2_0 = R(s * s); isz3_0 = R(1.0 / (s * s * s)); }
+      if (v1) { double s = size[g.body_off + il1]; sz2_1 = R(s * s); isz3_1 = R(1.0 / (s * s * s)); }
     }
     const R eps2 = R(g.eps2);
-    double dax = 0.0, day = 0.0, daz = 0.0;
+    double da0x = 0.0, da0y = 0.0, da0z = 0.0, da1x = 0.0, da1y = 0.0, da1z = 0.0;
     for (int base = g.j0; base < g.j1; base += T) {
-      const int j = base + threadIdx.x;
-      V4 t;
-      if (j < g.j1) {
-        double4 q = wpm[j];
-        t.x = R(q.x - c.x); t.y = R(q.y - c.y); t.z = R(q.z - c.z); t.w = R(q.w);
-        if (core_law) {
-          double s = size[g.body_off + j];
-          tsz2[threadIdx.x] = R(s * s);
-          tisz3[threadIdx.x] = R(1.0 / (s * s * s));
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int slot = threadIdx.x + h * H;
+        const int j = base + slot;
+        V4 t;
+        if (j < g.j1) {
+          double4 q = wpm[j];
+          t.x = R(q.x - c.x); t.y = R(q.y - c.y); t.z = R(q.z - c.z); t.w = R(q.w);
+          if (core_law) {
+            double s = size[g.body_off + j];
+            tsz2[slot] = R(s * s);
+            tisz3[slot] = R(1.0 / (s * s * s));
+          }
+        } else {
+          t.x = R(0); t.y = R(0); t.z = R(0); t.w = R(0);
+          if (core_law) { tsz2[slot] = R(1); tisz3[slot] = R(0); }
         }
-      } else {
-        t.x = R(0); t.y = R(0); t.z = R(0); t.w = R(0);
-        if (core_law) { tsz2[threadIdx.x] = R(1); tisz3[threadIdx.x] = R(0); }
+        tile[slot] = t;
       }
-      tile[threadIdx.x] = t;
       __syncthreads();
-      R ax = R(0), ay = R(0), az = R(0);
+      R a0x = R(0), a0y = R(0), a0z = R(0), a1x = R(0), a1y = R(0), a1z = R(0);
       if (!core_law) {
 #pragma unroll 8
         for (int k = 0; k < T; ++k) {
           V4 q = tile[k];
-          R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-          R s2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-          R inv = rsqrt_r<R>(s2);
-          R s = q.w * (inv * inv * inv);
-          ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+          R dx0 = q.x - x0, dy0 = q.y - y0, dz0 = q.z - z0;
+          R dx1 = q.x - x1, dy1 = q.y - y1, dz1 = q.z - z1;
+          R s20 = fma(dx0, dx0, fma(dy0, dy0, fma(dz0, dz0, eps2)));
+          R s21 = fma(dx1, dx1, fma(dy1, dy1, fma(dz1, dz1, eps2)));
+          R i0 = rsqrt_r<R>(s20), i1 = rsqrt_r<R>(s21);
+          R s0 = q.w * (i0 * i0 * i0), s1 = q.w * (i1 * i1 * i1);
+          a0x = fma(dx0, s0, a0x); a0y = fma(dy0, s0, a0y); a0z = fma(dz0, s0, a0z);
+          a1x = fma(dx1, s1, a1x); a1y = fma(dy1, s1, a1y); a1z = fma(dz1, s1, a1z);
         }
       } else {
 #pragma unroll 4
         for (int k = 0; k < T; ++k) {
           V4 q = tile[k];
-          R dx = q.x - xi, dy = q.y - yi, dz = q.z - zi;
-          R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-          // core radius of the higher-slot body (gravity.rs:126-131)
-          bool j_hi = (base + k) > il;
-          R sz2 = j_hi ? tsz2[k] : sz2_i;
-          R isz3 = j_hi ? tisz3[k] : isz3_i;
-          R inv = rsqrt_r<R>(r2);
-          R sd = (r2 >= sz2) ? inv * inv * inv : isz3;
-          // coincident bodies exert nothing (|d| < 1e-9, gravity.rs:119-122)
-          R s = (r2 < R(1e-18)) ? R(0) : q.w * sd;
-          ax = fma(dx, s, ax); ay = fma(dy, s, ay); az = fma(dz, s, az);
+          const int jg = base + k;
+          // core radius of the higher-slot body (gravity.rs:126-131); coincident bodies exert
+          // nothing (|d| < 1e-9, gravity.rs:119-122)
+          {
+            R dx = q.x - x0, dy = q.y - y0, dz = q.z - z0;
+            R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+            bool j_hi = jg > il0;
+            R sz2 = j_hi ? tsz2[k] : sz2_0;
+            R isz3 = j_hi ? tisz3[k] : isz3_0;
+            R inv = rsqrt_r<R>(r2);
+            R sd = (r2 >= sz2) ? inv * inv * inv : isz3;
+            R s = (r2 < R(1e-18)) ? R(0) : q.w * sd;
+            a0x = fma(dx, s, a0x); a0y = fma(dy, s, a0y); a0z = fma(dz, s, a0z);
+          }
+          {
+            R dx = q.x - x1, dy = q.y - y1, dz = q.z - z1;
+            R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+            bool j_hi = jg > il1;
+            R sz2 = j_hi ? tsz2[k] : sz2_1;
+            R isz3 = j_hi ? tisz3[k] : isz3_1;
+            R inv = rsqrt_r<R>(r2);
+            R sd = (r2 >= sz2) ? inv * inv * inv : isz3;
+            R s = (r2 < R(1e-18)) ? R(0) : q.w * sd;
+            a1x = fma(dx, s, a1x); a1y = fma(dy, s, a1y); a1z = fma(dz, s, a1z);
+          }
         }
       }
-      dax += double(ax); day += double(ay); daz += double(az);
+      da0x += double(a0x); da0y += double(a0y); da0z += double(a0z);
+      da1x += double(a1x); da1y += double(a1y); da1z += double(a1z);
       __syncthreads();
     }
-    if (valid) {
-      double* p = partial + g.out_off;
-      p[il] = dax; p[g.n + il] = day; p[2 * (size_t)g.n + il] = daz;
+    double* p = partial + g.out_off;
+    if (v0) { p[il0] = da0x; p[g.n + il0] = da0y; p[2 * (size_t)g.n + il0] = da0z; }
+    if (v1) { p[il1] = da1x; p[g.n + il1] = da1y; p[2 * (size_t)g.n + il1] = da1z; }
+  }
+}
+
+// Mixed path: one warp owns an i-tile (thread t: bodies i0 + t + 32h, h = 0..3). The four
+// i-bodies form two pairs, and the Plummer pair terms run as packed FP32x2 instructions (one
+// instruction, two lanes of arithmetic): the j-body is staged in shared memory already duplicated
+// ({x,x,y,y}, {z,z,m,m}) so that both halves of a pair read it with no register moves. Each pair
+// term is rounded exactly as the scalar form fma(dx,dx,fma(dy,dy,fma(dz,dz,eps2))), m*((i*i)*i),
+// fma(dx,s,acc) would round it. The size-core law keeps the scalar form.
+constexpr int kMixKI = 4;
+constexpr int kMixThreads = kGravTile / kMixKI;
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// The PTX ISA's approximate reciprocal square root with subnormals flushed: one MUFU operation and
+// nothing else. (The non-flushing form adds a range fix-up around it on the FMA pipe, which is the
+// pipe that bounds this kernel.) Pair distances here are never subnormal: the Plummer law adds
+// eps^2 > 0, and the size-core law discards r^2 < 1e-18.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const double4* __restrict__ pm,
+                                                                     const double* __restrict__ size,
+                                                                     const GravItem* __restrict__ items, int n_items,
+                                                                     int* __restrict__ head,
+                                                                     double* __restrict__ partial,
+                                                                     const int* __restrict__ world_of_body,
+                                                                     const int* __restrict__ w_active) {
+  constexpr int T = kGravTile;
+  constexpr int H = kMixThreads;
+  __shared__ float4 tq[T][2];
+  __shared__ float tsz2[T];
+  __shared__ float tisz3[T];
+  __shared__ int cur;
+  for (;;) {
+    if (threadIdx.x == 0) cur = atomicAdd(head, 1);
+    __syncthreads();
+    const int it = cur;
+    __syncthreads();
+    if (it >= n_items) return;
+    const GravItem g = items[it];
+    if (w_active && !w_active[world_of_body[g.body_off]]) continue;  // the world holds this step
+    const double4* wpm = pm + g.body_off;
+    const double4 c = wpm[g.i0];
+    const bool core_law = g.law == EXG_GRAVITY_SIZE_CORE;
+    int il[kMixKI];
+    bool v[kMixKI];
+    float px[kMixKI], py[kMixKI], pz[kMixKI], sz2[kMixKI], isz3[kMixKI];
+#pragma unroll
+    for (int h = 0; h < kMixKI; ++h) {
+      il[h] = g.i0 + threadIdx.x + h * H;
+      v[h] = il[h] < g.n;
+      const double4 p = v[h] ? wpm[il[h]] : c;
+      px[h] = float(p.x - c.x);
+      py[h] = float(p.y - c.y);
+      pz[h] = float(p.z - c.z);
+      sz2[h] = 0.f;
+      isz3[h] = 0.f;
+      if (core_law && v[h]) {
+        const double sd = size[g.body_off + il[h]];
+        sz2[h] = float(sd * sd);
+        isz3[h] = float(1.0 / (sd * sd * sd));
+      }
     }
+    const float2 nxA = f2(-px[0], -px[1]), nyA = f2(-py[0], -py[1]), nzA = f2(-pz[0], -pz[1]);
+    const float2 nxB = f2(-px[2], -px[3]), nyB = f2(-py[2], -py[3]), nzB = f2(-pz[2], -pz[3]);
+    const float e2 = float(g.eps2);
+    const float2 eps2 = f2(e2, e2);
+    double acc[kMixKI][3];
+#pragma unroll
+    for (int h = 0; h < kMixKI; ++h) acc[h][0] = acc[h][1] = acc[h][2] = 0.0;
+    for (int base = g.j0; base < g.j1; base += T) {
+#pragma unroll
+      for (int h = 0; h < kMixKI; ++h) {
+        const int slot = threadIdx.x + h * H;
+        const int j = base + slot;
+        float x = 0.f, y = 0.f, z = 0.f, m = 0.f;
+        if (j < g.j1) {
+          const double4 q = wpm[j];
+          x = float(q.x - c.x);
+          y = float(q.y - c.y);
+          z = float(q.z - c.z);
+          m = float(q.w);
+          if (core_law) {
+            const double sd = size[g.body_off + j];
+            tsz2[slot] = float(sd * sd);
+            tisz3[slot] = float(1.0 / (sd * sd * sd));
+          }
+        } else if (core_law) {
+          tsz2[slot] = 1.f;
+          tisz3[slot] = 0.f;
+        }
+        tq[slot][0] = make_float4(x, x, y, y);
+        tq[slot][1] = make_float4(z, z, m, m);
+      }
+      __syncthreads();
+      float a[kMixKI][3];
+      if (!core_law) {
+        float2 axA = f2(0.f, 0.f), ayA = axA, azA = axA, axB = axA, ayB = axA, azB = axA;
+#pragma unroll 4
+        for (int k = 0; k < T; ++k) {
+          const float4 u = tq[k][0], w = tq[k][1];
+          const float2 qx = f2(u.x, u.y), qy = f2(u.z, u.w), qz = f2(w.x, w.y), qm = f2(w.z, w.w);
+          const float2 dxA = __fadd2_rn(qx, nxA), dyA = __fadd2_rn(qy, nyA), dzA = __fadd2_rn(qz, nzA);
+          const float2 dxB = __fadd2_rn(qx, nxB), dyB = __fadd2_rn(qy, nyB), dzB = __fadd2_rn(qz, nzB);
+          const float2 rA = __ffma2_rn(dxA, dxA, __ffma2_rn(dyA, dyA, __ffma2_rn(dzA, dzA, eps2)));
+          const float2 rB = __ffma2_rn(dxB, dxB, __ffma2_rn(dyB, dyB, __ffma2_rn(dzB, dzB, eps2)));
+          const float2 iA = f2(rsqrt_ftz(rA.x), rsqrt_ftz(rA.y)), iB = f2(rsqrt_ftz(rB.x), rsqrt_ftz(rB.y));
+          const float2 sA = __fmul2_rn(qm, __fmul2_rn(__fmul2_rn(iA, iA), iA));
+          const float2 sB = __fmul2_rn(qm, __fmul2_rn(__fmul2_rn(iB, iB), iB));
+          axA = __ffma2_rn(dxA, sA, axA); ayA = __ffma2_rn(dyA, sA, ayA); azA = __ffma2_rn(dzA, sA, azA);
+          axB = __ffma2_rn(dxB, sB, axB); ayB = __ffma2_rn(dyB, sB, ayB); azB = __ffma2_rn(dzB, sB, azB);
+        }
+        a[0][0] = axA.x; a[1][0] = axA.y; a[2][0] = axB.x; a[3][0] = axB.y;
+        a[0][1] = ayA.x; a[1][1] = ayA.y; a[2][1] = ayB.x; a[3][1] = ayB.y;
+        a[0][2] = azA.x; a[1][2] = azA.y; a[2][2] = azB.x; a[3][2] = azB.y;
+      } else {
+#pragma unroll
+        for (int h = 0; h < kMixKI; ++h) a[h][0] = a[h][1] = a[h][2] = 0.f;
+#pragma unroll 2
+        for (int k = 0; k < T; ++k) {
+          const float4 u = tq[k][0], w = tq[k][1];
+          const int jg = base + k;
+          const float ts2 = tsz2[k], tis3 = tisz3[k];
+#pragma unroll
+          for (int h = 0; h < kMixKI; ++h) {
+            // core radius of the higher-slot body (gravity.rs:126-131); coincident bodies exert
+            // nothing (|d| < 1e-9, gravity.rs:119-122)
+            const float dx = u.x - px[h], dy = u.z - py[h], dz = w.x - pz[h];
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool j_hi = jg > il[h];
+            const float s2 = j_hi ? ts2 : sz2[h];
+            const float i3 = j_hi ? tis3 : isz3[h];
+            const float inv = rsqrt_ftz(r2);
+            const float sd = (r2 >= s2) ? inv * inv * inv : i3;
+            const float sc = (r2 < 1e-18f) ? 0.f : w.z * sd;
+            a[h][0] = fmaf(dx, sc, a[h][0]);
+            a[h][1] = fmaf(dy, sc, a[h][1]);
+            a[h][2] = fmaf(dz, sc, a[h][2]);
+          }
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < kMixKI; ++h) {
+        acc[h][0] += double(a[h][0]);
+        acc[h][1] += double(a[h][1]);
+        acc[h][2] += double(a[h][2]);
+      }
+      __syncthreads();
+    }
+    double* out = partial + g.out_off;
+#pragma unroll
+    for (int h = 0; h < kMixKI; ++h)
+      if (v[h]) {
+        out[il[h]] = acc[h][0];
+        out[g.n + il[h]] = acc[h][1];
+        out[2 * (size_t)g.n + il[h]] = acc[h][2];
+      }
   }
 }
 
@@ -178,17 +371,19 @@ void gravity_plan(const std::vector<int>& body_off, const std::vector<int>& n, c
 }
 
 int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double* size, const GravItem* items, int n_items,
-                         int* head, int precision, double* partial, cudaStream_t s) {
+                         int* head, int precision, double* partial, cudaStream_t s, const int* world_of_body,
+                         const int* w_active) {
   if (n_items <= 0) return EXG_OK;
   EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
   int sms = dev->sm_count > 0 ? dev->sm_count : 148;
-  int grid = std::min(n_items, sms * 12);
   const double4* pm = reinterpret_cast<const double4*>(pos_mass);
   int tok = prof_begin(dev, PROF_GRAVITY, s);
   if (precision == EXG_PRECISION_MIXED)
-    k_gravity_items<float><<<grid, kGravTile, 0, s>>>(pm, size, items, n_items, head, partial);
+    k_gravity_items_mixed<<<std::min(n_items, sms * 32), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
+                                                                             world_of_body, w_active);
   else
-    k_gravity_items<double><<<grid, kGravTile, 0, s>>>(pm, size, items, n_items, head, partial);
+    k_gravity_items<double><<<std::min(n_items, sms * 16), kGravThreads, 0, s>>>(pm, size, items, n_items, head,
+                                                                                partial, world_of_body, w_active);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

@@ -9,12 +9,14 @@ namespace {
 // World form: poses [8][n] and world twists [6][n] component-major; output conn[12][nj]. Joints
 // of worlds stepped by the implicit integrator are evaluated inside the Newton kernel instead.
 __global__ void k_joints_plain_world(const exg_joint_t* __restrict__ joints, const int* __restrict__ world_of_joint,
-                                     const exg_step_params_t* __restrict__ wparams, int nj,
+                                     const int* __restrict__ w_active, const exg_step_params_t* __restrict__ wparams, int nj,
                                      const double* __restrict__ pose, const double* __restrict__ wvel, int n,
                                      double* __restrict__ conn) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nj) return;
-  const exg_step_params_t& P = wparams[world_of_joint[k]];
+  const int wid = world_of_joint[k];
+  if (wid < 0 || !w_active[wid]) return;
+  const exg_step_params_t& P = wparams[wid];
   if (P.integrator == EXG_NEWTON) return;
   const exg_joint_t& jt = joints[k];
   double pa[8], pb[8], va[6], vb[6], out[12];
@@ -65,9 +67,9 @@ __global__ void k_joints_stage_jacobian(const exg_joint_t* __restrict__ joints, 
 }  // namespace
 
 int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s) {
-  if (w.nj <= 0 || !w.any_explicit) return EXG_OK;
+  if (w.nj_ext <= 0 || !w.any_explicit) return EXG_OK;
   int _tok = prof_begin(dev, PROF_JOINTS, s);
-  k_joints_plain_world<<<(w.nj + 127) / 128, 128, 0, s>>>(w.joints, w.world_of_joint, w.wparams, w.nj, w.pose, w.wvel,
+  k_joints_plain_world<<<(w.nj_ext + 127) / 128, 128, 0, s>>>(w.joints, w.world_of_joint, w.w_active, w.wparams, w.nj, w.pose, w.wvel,
                                                           w.n, w.conn);
   prof_end(dev, _tok, s);
   return exg_after_launch(dev);

@@ -81,6 +81,7 @@ struct WorldRef {
   const int* w_splits;
   const int* w_n;
   const int* w_body_off;
+  const int* w_active;
   int n;
 };
 
@@ -698,6 +699,7 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
     c.A = A;
     c.island = queue[k];
     c.d = A.desc[c.island];
+    if (!W.w_active[c.d.world]) continue;  // the world holds this step
     c.W = W;
     c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
     {
@@ -765,19 +767,66 @@ __global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, 
 }  // namespace
 
 // ── host: island structure ────────────────────────────────────────────────────
-NewtonWorld::~NewtonWorld() {
-  for (void* p : allocs) cudaFree(p);
+long long newton_footprint_bytes(int nb, int nj) {
+  // scratch, then the structure: 13 ints per body (body list, order, incidence pointers,
+  // dynamic list, parents, levels, children, 3 assembly cells), 9 per joint plus its 10 params
+  return ((scratch_doubles(nb, nj, nb) + 31) & ~31LL) * 8 + (long long)nb * 13 * 4 + (long long)nj * (9 * 4 + 80) +
+         (long long)sizeof(IslandDesc) + 64;
 }
 
-int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodies, const exg_joint_t* joints,
-                      const exg_step_params_t& p) {
-  const int n = w.n, nj = w.nj;
-  // world of every body; only bodies of implicit worlds take part
-  std::vector<int> wob(n, 0);
-  for (int wi = 0; wi < w.n_worlds; ++wi)
-    for (int i = 0; i < w.h_n[wi]; ++i) wob[w.h_body_off[wi] + i] = wi;
-  auto implicit_body = [&](int i) { return w.h_params[wob[i]].integrator == EXG_NEWTON; };
-  // islands = connected components of the joint graph, bodies ascending, joints ascending
+NewtonWorld::~NewtonWorld() {
+  d_desc.release();
+  for (DevArr<int>* a : {&d_isl_body, &d_jl_law, &d_jl_a, &d_jl_b, &d_ib_order, &d_ib_inc_ptr, &d_ib_inc_ref, &d_dn_body,
+                         &d_dn_parent, &d_lv_ptr, &d_lv_nodes, &d_ch_ptr, &d_ch_idx, &d_cell_ptr, &d_cell_terms, &d_stats,
+                         &d_queue})
+    a->release();
+  d_jl_params.release();
+  d_scratch.release();
+  d_residual.release();
+  d_phase.release();
+}
+
+int NewtonWorld::add_world(exg_device_s* dev, int slot, int body_off, const exg_body_t* bodies, int n,
+                           const exg_joint_t* joints, int nj) {
+  (void)dev;
+  WorldSrc src;
+  src.body_off = body_off;
+  src.kin.resize(n);
+  for (int i = 0; i < n; ++i) src.kin[i] = bodies[i].kinematic != 0;
+  src.joints.assign(joints, joints + nj);
+  int rc = build_world(slot, src);
+  if (rc != EXG_OK) return rc;
+  if ((int)src_.size() <= slot) src_.resize(slot + 1);
+  src.live = true;
+  src_[slot] = std::move(src);
+  return EXG_OK;
+}
+
+// Rebuild the structure arrays from the live worlds alone, once removed worlds hold most of them.
+void NewtonWorld::compact() {
+  desc_.clear(); alive_.clear(); scratch_len_.clear();
+  for (std::vector<int>* v : {&h_isl_body, &h_jl_law, &h_jl_a, &h_jl_b, &h_ib_order, &h_ib_inc_ptr, &h_ib_inc_ref,
+                              &h_dn_body, &h_dn_parent, &h_lv_ptr, &h_lv_nodes, &h_ch_ptr, &h_ch_idx, &h_cell_ptr,
+                              &h_cell_terms})
+    v->clear();
+  h_jl_params.clear();
+  world_islands_.clear();
+  scratch_alloc_.init(scratch_alloc_.capacity());
+  n_live_ = 0;
+  for (int slot = 0; slot < (int)src_.size(); ++slot)
+    if (src_[slot].live) build_world(slot, src_[slot]);  // rebuilt worlds were accepted before
+  d_desc.size = 0;
+  for (DevArr<int>* a : {&d_isl_body, &d_jl_law, &d_jl_a, &d_jl_b, &d_ib_order, &d_ib_inc_ptr, &d_ib_inc_ref, &d_dn_body,
+                         &d_dn_parent, &d_lv_ptr, &d_lv_nodes, &d_ch_ptr, &d_ch_idx, &d_cell_ptr, &d_cell_terms})
+    a->size = 0;
+  d_jl_params.size = 0;
+  dirty_ = true;
+}
+
+int NewtonWorld::build_world(int slot, const WorldSrc& src) {
+  const int n = (int)src.kin.size(), nj = (int)src.joints.size(), body_off = src.body_off;
+  const exg_joint_t* joints = src.joints.data();
+  // islands = connected components of the world's joint graph, bodies ascending, joints ascending
   std::vector<int> parent(n);
   for (int i = 0; i < n; ++i) parent[i] = i;
   std::function<int(int)> find = [&](int x) {
@@ -791,102 +840,100 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
   std::vector<int> isl_of_root(n, -1);
   std::vector<std::vector<int>> ib, ij;
   for (int i = 0; i < n; ++i) {
-    if (!implicit_body(i)) continue;
     int r = find(i);
     if (isl_of_root[r] < 0) { isl_of_root[r] = (int)ib.size(); ib.emplace_back(); ij.emplace_back(); }
     ib[isl_of_root[r]].push_back(i);
   }
-  for (int k = 0; k < nj; ++k)
-    if (implicit_body(joints[k].a)) ij[isl_of_root[find(joints[k].a)]].push_back(k);
-  n_islands = (int)ib.size();
+  for (int k = 0; k < nj; ++k) ij[isl_of_root[find(joints[k].a)]].push_back(k);
 
-  std::vector<IslandDesc> desc(n_islands);
-  std::vector<int> local(n, -1);  // island-local index of each body of the island being built
-  std::vector<int> h_isl_body, h_jl_law, h_jl_a, h_jl_b, h_ib_order, h_ib_inc_ptr, h_ib_inc_ref, h_dn_body, h_dn_parent,
-      h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
-  std::vector<double> h_jl_params;
-  long long scratch = 0;
-  for (int I = 0; I < n_islands; ++I) {
+  // build into staging vectors first, so a refused world leaves the structure untouched
+  std::vector<IslandDesc> desc;
+  std::vector<long long> lens;
+  std::vector<int> s_isl_body, s_jl_law, s_jl_a, s_jl_b, s_ib_order, s_ib_inc_ptr, s_ib_inc_ref, s_dn_body, s_dn_parent,
+      s_lv_ptr, s_lv_nodes, s_ch_ptr, s_ch_idx, s_cell_ptr, s_cell_terms;
+  std::vector<double> s_jl_params;
+  const int base_isl_body = (int)h_isl_body.size(), base_jl = (int)h_jl_law.size(), base_order = (int)h_ib_order.size(),
+            base_inc_ptr = (int)h_ib_inc_ptr.size(), base_inc_ref = (int)h_ib_inc_ref.size(),
+            base_dn = (int)h_dn_body.size(), base_lv = (int)h_lv_ptr.size(), base_ch_idx = (int)h_ch_idx.size(),
+            base_cell_ptr = (int)h_cell_ptr.size(), base_cell_terms = (int)h_cell_terms.size();
+  std::vector<int> local(n, -1);
+  for (size_t I = 0; I < ib.size(); ++I) {
     const std::vector<int>& B = ib[I];
     const std::vector<int>& J = ij[I];
-    IslandDesc& d = desc[I];
-    d.world = wob[B[0]];
-    d.body_off = (int)h_isl_body.size();
+    IslandDesc d;
+    d.world = slot;
+    d.body_off = base_isl_body + (int)s_isl_body.size();
     d.nb = (int)B.size();
-    d.joint_off = (int)h_jl_law.size();
+    d.joint_off = base_jl + (int)s_jl_law.size();
     d.nj = (int)J.size();
-    max_nb = std::max(max_nb, d.nb);
-    for (int q = 0; q < d.nb; ++q) { local[B[q]] = q; h_isl_body.push_back(B[q]); }
+    const int jl0 = (int)s_jl_law.size();
+    for (int q = 0; q < d.nb; ++q) { local[B[q]] = q; s_isl_body.push_back(body_off + B[q]); }
     for (int q = 0; q < d.nj; ++q) {
       const exg_joint_t& jt = joints[J[q]];
-      h_jl_law.push_back(jt.law);
-      h_jl_a.push_back(local[jt.a]);
-      h_jl_b.push_back(local[jt.b]);
-      for (int k = 0; k < 10; ++k) h_jl_params.push_back(jt.params[k]);
+      s_jl_law.push_back(jt.law);
+      s_jl_a.push_back(local[jt.a]);
+      s_jl_b.push_back(local[jt.b]);
+      for (int k = 0; k < 10; ++k) s_jl_params.push_back(jt.params[k]);
     }
     // dynamic order (island order, kinematic excluded)
     std::vector<int> order(d.nb, -1), dyn_body;
     for (int q = 0; q < d.nb; ++q)
-      if (!bodies[B[q]].kinematic) { order[q] = (int)dyn_body.size(); dyn_body.push_back(q); }
-    int m = (int)dyn_body.size();
+      if (!src.kin[B[q]]) { order[q] = (int)dyn_body.size(); dyn_body.push_back(q); }
+    const int m = (int)dyn_body.size();
     d.m = m;
-    d.dyn_off = (int)h_dn_body.size();
-    for (int q = 0; q < d.nb; ++q) h_ib_order.push_back(order[q]);
-    // incidence per island body in joint order
-    d.inc_off = (int)h_ib_inc_ptr.size();
+    d.dyn_off = base_dn + (int)s_dn_body.size();
+    for (int q = 0; q < d.nb; ++q) s_ib_order.push_back(order[q]);
+    // incidence per island body in joint order (the reference's gather order)
+    d.inc_off = base_inc_ptr + (int)s_ib_inc_ptr.size();
     {
       std::vector<std::vector<int>> inc(d.nb);
       for (int q = 0; q < d.nj; ++q) {
-        inc[h_jl_a[d.joint_off + q]].push_back(2 * q);
-        inc[h_jl_b[d.joint_off + q]].push_back(2 * q + 1);
+        inc[s_jl_a[jl0 + q]].push_back(2 * q);
+        inc[s_jl_b[jl0 + q]].push_back(2 * q + 1);
       }
-      int base = (int)h_ib_inc_ref.size();
+      int pos = base_inc_ref + (int)s_ib_inc_ref.size();
       for (int q = 0; q < d.nb; ++q) {
-        h_ib_inc_ptr.push_back(base);
-        for (int r : inc[q]) { h_ib_inc_ref.push_back(r); ++base; }
+        s_ib_inc_ptr.push_back(pos);
+        for (int r : inc[q]) { s_ib_inc_ref.push_back(r); ++pos; }
       }
-      h_ib_inc_ptr.push_back(base);
+      s_ib_inc_ptr.push_back(pos);
     }
     // dynamic adjacency (distinct neighbours)
     std::vector<std::vector<int>> adj(m);
     for (int q = 0; q < d.nj; ++q) {
-      int a = order[h_jl_a[d.joint_off + q]], b = order[h_jl_b[d.joint_off + q]];
-      if (a < 0 || b < 0) continue;
-      if (std::find(adj[a].begin(), adj[a].end(), b) == adj[a].end()) adj[a].push_back(b);
-      if (std::find(adj[b].begin(), adj[b].end(), a) == adj[b].end()) adj[b].push_back(a);
+      int ea = order[s_jl_a[jl0 + q]], eb = order[s_jl_b[jl0 + q]];
+      if (ea < 0 || eb < 0) continue;
+      if (std::find(adj[ea].begin(), adj[ea].end(), eb) == adj[ea].end()) adj[ea].push_back(eb);
+      if (std::find(adj[eb].begin(), adj[eb].end(), ea) == adj[eb].end()) adj[eb].push_back(ea);
     }
-    // forest check and elimination tree rooted at each component's centre
-    std::vector<int> par(m, -2), level(m, 0), comp_of(m, -1);
+    // forest check; elimination tree rooted at each component's centre
+    std::vector<int> par(m, -2), level(m, 0), comp_of(m, -1), dist(m, -1), du(m, -1), dc(m, -1);
     long edges = 0;
     for (int i = 0; i < m; ++i) edges += (long)adj[i].size();
     edges /= 2;
     int comps = 0;
-    for (int s = 0; s < m; ++s) {
-      if (comp_of[s] >= 0) continue;
-      // BFS from s: farthest node u
-      auto bfs = [&](int root, std::vector<int>& dist, std::vector<int>& seen_order) {
-        seen_order.clear();
-        seen_order.push_back(root);
-        dist[root] = 0;
-        for (size_t h = 0; h < seen_order.size(); ++h)
-          for (int nb2 : adj[seen_order[h]])
-            if (dist[nb2] < 0) { dist[nb2] = dist[seen_order[h]] + 1; seen_order.push_back(nb2); }
-      };
-      std::vector<int> dist(m, -1), seen;
-      bfs(s, dist, seen);
+    auto bfs = [&](int root, std::vector<int>& dd, std::vector<int>& seen) {
+      seen.clear();
+      seen.push_back(root);
+      dd[root] = 0;
+      for (size_t h = 0; h < seen.size(); ++h)
+        for (int nb2 : adj[seen[h]])
+          if (dd[nb2] < 0) { dd[nb2] = dd[seen[h]] + 1; seen.push_back(nb2); }
+    };
+    std::vector<int> seen, seen_u, seen_c;
+    for (int st = 0; st < m; ++st) {
+      if (comp_of[st] >= 0) continue;
+      bfs(st, dist, seen);
       for (int x : seen) comp_of[x] = comps;
       int u = seen.back();
-      std::vector<int> du(m, -1), seen_u;
       bfs(u, du, seen_u);
       int v = seen_u.back();
-      // path u..v: walk back from v along decreasing du
       std::vector<int> path{v};
       while (path.back() != u) {
         int cur = path.back();
         for (int nb2 : adj[cur]) if (du[nb2] == du[cur] - 1) { path.push_back(nb2); break; }
       }
       int centre = path[path.size() / 2];
-      std::vector<int> dc(m, -1), seen_c;
       bfs(centre, dc, seen_c);
       par[centre] = -1;
       for (int x : seen_c) {
@@ -895,39 +942,41 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
       }
       ++comps;
     }
+    for (int q = 0; q < d.nb; ++q) local[B[q]] = -1;
     if (edges != m - comps) return EXG_ERR_UNSUPPORTED;  // a cycle among the dynamic bodies
     int nlev = 0;
     for (int i = 0; i < m; ++i) nlev = std::max(nlev, level[i] + 1);
     d.n_levels = nlev;
-    d.lv_off = (int)h_lv_ptr.size();
+    d.lv_off = base_lv + (int)s_lv_ptr.size();
     {
       std::vector<std::vector<int>> by(nlev);
       for (int i = 0; i < m; ++i) by[level[i]].push_back(i);
       int acc = 0;
       for (int L = 0; L < nlev; ++L) {
-        h_lv_ptr.push_back(acc);
-        for (int i : by[L]) h_lv_nodes.push_back(i);
+        s_lv_ptr.push_back(acc);
+        for (int i : by[L]) s_lv_nodes.push_back(i);
         acc += (int)by[L].size();
       }
-      h_lv_ptr.push_back(acc);
+      s_lv_ptr.push_back(acc);
     }
-    // children CSR: ch_ptr holds one absolute offset into ch_idx per node (a global sentinel
-    // follows the last island), ch_idx holds island-relative node indices
+    // children: one absolute offset into ch_idx per node (a sentinel follows the last node of
+    // all islands), island-relative node indices in ch_idx
     {
       std::vector<std::vector<int>> ch(m);
       for (int i = 0; i < m; ++i) if (par[i] >= 0) ch[par[i]].push_back(i);
       for (int i = 0; i < m; ++i) {
-        h_ch_ptr.push_back((int)h_ch_idx.size());
-        for (int x : ch[i]) h_ch_idx.push_back(x);
+        s_ch_ptr.push_back(base_ch_idx + (int)s_ch_idx.size());
+        for (int x : ch[i]) s_ch_idx.push_back(x);
       }
-      for (int i = 0; i < m; ++i) { h_dn_body.push_back(dyn_body[i]); h_dn_parent.push_back(par[i]); }
+      for (int i = 0; i < m; ++i) { s_dn_body.push_back(dyn_body[i]); s_dn_parent.push_back(par[i]); }
     }
-    // assembly cells: (node, kind) with kind 0 = diagonal, 1 = (node row, parent col), 2 = (parent row, node col)
-    d.cell_off = (int)h_cell_ptr.size();
+    // assembly cells: (node, kind) with kind 0 = diagonal, 1 = (node row, parent col),
+    // 2 = (parent row, node col)
+    d.cell_off = base_cell_ptr + (int)s_cell_ptr.size();
     {
       std::vector<std::vector<int>> cells(3 * m);
       for (int q = 0; q < d.nj; ++q) {
-        int ends[2] = {order[h_jl_a[d.joint_off + q]], order[h_jl_b[d.joint_off + q]]};
+        int ends[2] = {order[s_jl_a[jl0 + q]], order[s_jl_b[jl0 + q]]};
         for (int re = 0; re < 2; ++re) {
           if (ends[re] < 0) continue;
           for (int ce = 0; ce < 2; ++ce) {
@@ -941,105 +990,148 @@ int NewtonWorld::init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodie
           }
         }
       }
-      int base = (int)h_cell_terms.size();
+      int pos = base_cell_terms + (int)s_cell_terms.size();
       for (int t = 0; t < 3 * m; ++t) {
-        h_cell_ptr.push_back(base);
-        for (int x : cells[t]) { h_cell_terms.push_back(x); ++base; }
+        s_cell_ptr.push_back(pos);
+        for (int x : cells[t]) { s_cell_terms.push_back(x); ++pos; }
       }
-      h_cell_ptr.push_back(base);
+      s_cell_ptr.push_back(pos);
     }
-    for (int q = 0; q < d.nb; ++q) local[B[q]] = -1;
-    d.scratch_off = scratch;
-    scratch += scratch_doubles(d.nb, d.nj, m);
-    scratch = (scratch + 31) & ~31LL;
+    desc.push_back(d);
+    lens.push_back((scratch_doubles(d.nb, d.nj, m) + 31) & ~31LL);
   }
-  h_ch_ptr.push_back((int)h_ch_idx.size());
+  // scratch ranges (grow the scratch array when the allocator has no room)
+  for (size_t I = 0; I < desc.size(); ++I) {
+    long long off = scratch_alloc_.alloc(lens[I]);
+    if (off < 0) {
+      long long old = scratch_alloc_.capacity();
+      long long grow = std::max(old, lens[I] + 1024);
+      scratch_alloc_.grow(old + grow);
+      off = scratch_alloc_.alloc(lens[I]);
+    }
+    desc[I].scratch_off = off;
+  }
+  // commit the staging vectors
+  auto cat = [](std::vector<int>& dst, const std::vector<int>& src) { dst.insert(dst.end(), src.begin(), src.end()); };
+  cat(h_isl_body, s_isl_body); cat(h_jl_law, s_jl_law); cat(h_jl_a, s_jl_a); cat(h_jl_b, s_jl_b);
+  cat(h_ib_order, s_ib_order); cat(h_ib_inc_ptr, s_ib_inc_ptr); cat(h_ib_inc_ref, s_ib_inc_ref);
+  cat(h_dn_body, s_dn_body); cat(h_dn_parent, s_dn_parent); cat(h_lv_ptr, s_lv_ptr); cat(h_lv_nodes, s_lv_nodes);
+  cat(h_ch_ptr, s_ch_ptr); cat(h_ch_idx, s_ch_idx); cat(h_cell_ptr, s_cell_ptr); cat(h_cell_terms, s_cell_terms);
+  h_jl_params.insert(h_jl_params.end(), s_jl_params.begin(), s_jl_params.end());
+  if ((int)world_islands_.size() <= slot) world_islands_.resize(slot + 1);
+  world_islands_[slot].clear();
+  for (size_t I = 0; I < desc.size(); ++I) {
+    world_islands_[slot].push_back((int)desc_.size());
+    desc_.push_back(desc[I]);
+    alive_.push_back(1);
+    scratch_len_.push_back(lens[I]);
+    ++n_live_;
+  }
+  dirty_ = true;
+  return EXG_OK;
+}
 
-  // island work queue, largest first
-  island_order.resize(n_islands);
-  for (int I = 0; I < n_islands; ++I) island_order[I] = I;
-  std::stable_sort(island_order.begin(), island_order.end(),
-                   [&](int a, int b) { return desc[a].nb + desc[a].nj > desc[b].nb + desc[b].nj; });
+void NewtonWorld::remove_world(int slot) {
+  if (slot < 0 || slot >= (int)world_islands_.size()) return;
+  for (int I : world_islands_[slot]) {
+    if (!alive_[I]) continue;
+    alive_[I] = 0;
+    scratch_alloc_.release(desc_[I].scratch_off, scratch_len_[I]);
+    --n_live_;
+  }
+  world_islands_[slot].clear();
+  if (slot < (int)src_.size()) src_[slot] = WorldSrc();
+  dirty_ = true;
+}
 
-  cudaStream_t s = dev->stream;
-  auto up = [&](auto& vec, auto** dptr) -> int {
-    using T = typename std::remove_reference<decltype(vec)>::type::value_type;
-    size_t bytes = sizeof(T) * std::max<size_t>(vec.size(), 1);
-    void* p = nullptr;
-    EXG_CUDA_TRY(cudaMalloc(&p, bytes));
-    allocs.push_back(p);
-    if (!vec.empty()) EXG_CUDA_TRY(cudaMemcpyAsync(p, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice, s));
-    *dptr = static_cast<T*>(p);
-    return EXG_OK;
-  };
+int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
+  (void)dev;
+  if (!dirty_) return EXG_OK;
+  if ((long long)desc_.size() > 1024 && (long long)desc_.size() > 2LL * n_live_) compact();
   int rc = EXG_OK;
-  IslandDesc* d_desc = nullptr;
-  int *d_isl_body, *d_jl_law, *d_jl_a, *d_jl_b, *d_ib_order, *d_ib_inc_ptr, *d_ib_inc_ref, *d_dn_body, *d_dn_parent,
-      *d_lv_ptr, *d_lv_nodes, *d_ch_ptr, *d_ch_idx, *d_cell_ptr, *d_cell_terms, *d_stats, *d_q;
-  double *d_params, *d_scratch, *d_res;
-  std::vector<int> stats(4 * (size_t)n_islands, 0);
-  std::vector<double> resid(n_islands, 0.0);
-  std::vector<long long> phases(kPhases, 0);
-  long long* d_phase = nullptr;
-  std::vector<int> qv(island_order);
-  qv.push_back(0);  // head counter lives after the queue
-  if ((rc = up(desc, &d_desc)) || (rc = up(h_isl_body, &d_isl_body)) || (rc = up(h_jl_law, &d_jl_law)) ||
-      (rc = up(h_jl_a, &d_jl_a)) || (rc = up(h_jl_b, &d_jl_b)) || (rc = up(h_jl_params, &d_params)) ||
-      (rc = up(h_ib_order, &d_ib_order)) || (rc = up(h_ib_inc_ptr, &d_ib_inc_ptr)) ||
-      (rc = up(h_ib_inc_ref, &d_ib_inc_ref)) || (rc = up(h_dn_body, &d_dn_body)) || (rc = up(h_dn_parent, &d_dn_parent)) ||
-      (rc = up(h_lv_ptr, &d_lv_ptr)) || (rc = up(h_lv_nodes, &d_lv_nodes)) || (rc = up(h_ch_ptr, &d_ch_ptr)) ||
-      (rc = up(h_ch_idx, &d_ch_idx)) || (rc = up(h_cell_ptr, &d_cell_ptr)) || (rc = up(h_cell_terms, &d_cell_terms)) ||
-      (rc = up(stats, &d_stats)) || (rc = up(resid, &d_res)) || (rc = up(qv, &d_q)) ||
-      (rc = up(phases, &d_phase)))
-    return rc;
-  void* sp = nullptr;
-  EXG_CUDA_TRY(cudaMalloc(&sp, sizeof(double) * std::max<long long>(scratch, 1)));
-  allocs.push_back(sp);
-  d_scratch = static_cast<double*>(sp);
-  EXG_CUDA_TRY(cudaMemsetAsync(d_scratch, 0, sizeof(double) * std::max<long long>(scratch, 1), s));
-  arr = NewtonDeviceArrays{d_desc,      d_isl_body, d_jl_law,  d_jl_a,      d_jl_b,       d_params,  d_ib_order,
-                           d_ib_inc_ptr, d_ib_inc_ref, d_dn_body, d_dn_parent, d_lv_ptr,   d_lv_nodes, d_ch_ptr,
-                           d_ch_idx,    d_cell_ptr, d_cell_terms, d_scratch, d_stats,     d_res, d_phase};
-  d_queue = d_q;
-  d_head = d_q + n_islands;
-  island_world.resize(n_islands);
-  for (int I = 0; I < n_islands; ++I) island_world[I] = desc[I].world;
-  EXG_CUDA_TRY(cudaStreamSynchronize(s));
-  (void)p;
+  auto up = [&](auto& d, const auto& h) {
+    if (rc == EXG_OK && (long long)h.size() > d.size) rc = d.append(h.data() + d.size, (long long)h.size() - d.size, s);
+  };
+  up(d_desc, desc_);
+  up(d_isl_body, h_isl_body); up(d_jl_law, h_jl_law); up(d_jl_a, h_jl_a); up(d_jl_b, h_jl_b);
+  up(d_jl_params, h_jl_params); up(d_ib_order, h_ib_order); up(d_ib_inc_ptr, h_ib_inc_ptr);
+  up(d_ib_inc_ref, h_ib_inc_ref); up(d_dn_body, h_dn_body); up(d_dn_parent, h_dn_parent); up(d_lv_ptr, h_lv_ptr);
+  up(d_lv_nodes, h_lv_nodes); up(d_ch_idx, h_ch_idx); up(d_cell_ptr, h_cell_ptr); up(d_cell_terms, h_cell_terms);
+  if (rc != EXG_OK) return rc;
+  // ch_ptr carries a sentinel after its last entry; rewrite it with the tail
+  if ((long long)h_ch_ptr.size() > d_ch_ptr.size || d_ch_ptr.cap == 0) {
+    long long from = d_ch_ptr.size;
+    std::vector<int> tail(h_ch_ptr.begin() + from, h_ch_ptr.end());
+    tail.push_back((int)h_ch_idx.size());
+    rc = d_ch_ptr.append(tail.data(), (long long)tail.size(), s);
+    if (rc != EXG_OK) return rc;
+    d_ch_ptr.size -= 1;  // the sentinel is overwritten by the next append
+  }
+  // scratch: per-step contents only, so growth needs no copy
+  if (d_scratch.cap < scratch_alloc_.capacity()) {
+    d_scratch.release();
+    rc = d_scratch.reserve(std::max<long long>(scratch_alloc_.capacity(), 1), s);
+    if (rc != EXG_OK) return rc;
+  }
+  long long ni = (long long)desc_.size();
+  if ((rc = d_stats.reserve(std::max<long long>(4 * ni, 4), s)) != EXG_OK) return rc;
+  if ((rc = d_residual.reserve(std::max<long long>(ni, 1), s)) != EXG_OK) return rc;
+  if (d_phase.cap == 0) {
+    std::vector<long long> z(kPhases, 0);
+    if ((rc = d_phase.assign(z.data(), kPhases, s)) != EXG_OK) return rc;
+  }
+  // queue of live islands, largest first, then the scheduler's counter
+  std::vector<int> q;
+  for (int I = 0; I < (int)desc_.size(); ++I) if (alive_[I]) q.push_back(I);
+  std::stable_sort(q.begin(), q.end(),
+                   [&](int a, int b) { return desc_[a].nb + desc_[a].nj > desc_[b].nb + desc_[b].nj; });
+  q.push_back(0);
+  if ((rc = d_queue.assign(q.data(), (long long)q.size(), s)) != EXG_OK) return rc;
+  arr = NewtonDeviceArrays{d_desc.ptr,      d_isl_body.ptr, d_jl_law.ptr,   d_jl_a.ptr,      d_jl_b.ptr,     d_jl_params.ptr,
+                           d_ib_order.ptr,  d_ib_inc_ptr.ptr, d_ib_inc_ref.ptr, d_dn_body.ptr, d_dn_parent.ptr, d_lv_ptr.ptr,
+                           d_lv_nodes.ptr,  d_ch_ptr.ptr,   d_ch_idx.ptr,   d_cell_ptr.ptr,  d_cell_terms.ptr, d_scratch.ptr,
+                           d_stats.ptr,     d_residual.ptr, d_phase.ptr};
+  dirty_ = false;
   return EXG_OK;
 }
 
 int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
-  if (n_islands == 0) return EXG_OK;
+  if (n_live_ == 0) return EXG_OK;
+  if (dirty_) return EXG_ERR_INVALID_ARGUMENT;  // sync() first
   WorldRef W{w.pose,    w.mom,    w.mass,   w.inertia, w.kinematic,  w.diagonal, w.pos_mass,
-             w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.n};
-  int grid = std::min(n_islands, std::max(1, dev->sm_count) * 2);
-  EXG_CUDA_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), s));
+             w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
+  int* head = d_queue.ptr + n_live_;
+  int grid = std::min(n_live_, std::max(1, dev->sm_count) * 2);
+  EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
   int tok = prof_begin(dev, PROF_NEWTON, s);
   if (w.precision == EXG_PRECISION_MIXED)
-    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);
   else
-    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue, n_islands, d_head);
+    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }
 
 int NewtonWorld::read_phase_cycles(long long* out) {
-  EXG_CUDA_TRY(cudaMemcpy(out, arr.phase_cycles, sizeof(long long) * kPhases, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < kPhases; ++k) out[k] = 0;
+  if (d_phase.cap == 0) return EXG_OK;
+  EXG_CUDA_TRY(cudaMemcpy(out, d_phase.ptr, sizeof(long long) * kPhases, cudaMemcpyDeviceToHost));
   return EXG_OK;
 }
 
 int NewtonWorld::read_stats(int world, exg_world_stats_t* st) {
-  std::vector<int> stats(4 * (size_t)std::max(n_islands, 1));
-  std::vector<double> res(std::max(n_islands, 1));
-  if (n_islands > 0) {
-    EXG_CUDA_TRY(cudaMemcpy(stats.data(), arr.stats, sizeof(int) * 4 * n_islands, cudaMemcpyDeviceToHost));
-    EXG_CUDA_TRY(cudaMemcpy(res.data(), arr.residual, sizeof(double) * n_islands, cudaMemcpyDeviceToHost));
+  const int ni = (int)desc_.size();
+  std::vector<int> stats(4 * (size_t)std::max(ni, 1));
+  std::vector<double> res(std::max(ni, 1));
+  if (ni > 0 && d_stats.cap >= 4LL * ni) {
+    EXG_CUDA_TRY(cudaMemcpy(stats.data(), d_stats.ptr, sizeof(int) * 4 * ni, cudaMemcpyDeviceToHost));
+    EXG_CUDA_TRY(cudaMemcpy(res.data(), d_residual.ptr, sizeof(double) * ni, cudaMemcpyDeviceToHost));
   }
   int spans = 0, iters = 0, depth = 0, fatal = 0;
   double worst = 0.0;
-  for (int I = 0; I < n_islands; ++I) {
-    if (world >= 0 && island_world[I] != world) continue;
+  for (int I = 0; I < ni; ++I) {
+    if (!alive_[I]) continue;
+    if (world >= 0 && desc_[I].world != world) continue;
     spans = std::max(spans, stats[4 * I]);
     iters = std::max(iters, stats[4 * I + 1]);
     depth = std::max(depth, stats[4 * I + 2]);

@@ -8,6 +8,7 @@
 // motor update — without returning to the host.
 #pragma once
 #include "exg_internal.cuh"
+#include "slab.cuh"
 
 struct IslandDesc {
   int world;             // the world (of the batch) the island belongs to
@@ -47,27 +48,61 @@ struct NewtonDeviceArrays {
 enum NewtonPhase { PH_PRE = 0, PH_JACOBIAN = 1, PH_POST = 2, PH_ASSEMBLE = 3, PH_SOLVE = 4, PH_LINE_SEARCH = 5,
                    PH_COMMIT = 6, PH_OTHER = 7, kPhases = 8 };
 
+// Islands of the implicit worlds of a pool. Worlds are added and removed one at a time; their
+// island structure is appended to device arrays that only grow, and each island's per-step
+// scratch is a range of one scratch array (contents do not persist across steps, so the array is
+// reallocated without copying when it must grow).
 class NewtonWorld {
  public:
-  int init(exg_device_s* dev, DeviceWorld& w, const exg_body_t* bodies, const exg_joint_t* joints, const exg_step_params_t& p);
-  // Enqueue one step of every island (no host synchronisation; graph-capturable).
+  ~NewtonWorld();
+  // Build the islands of one world (bodies and joints local to the world; its bodies live at
+  // body_off in the pool) and queue them for stepping.
+  int add_world(exg_device_s* dev, int slot, int body_off, const exg_body_t* bodies, int n, const exg_joint_t* joints,
+                int nj);
+  void remove_world(int slot);
+  // Upload pending structure and the island queue (host synchronous; call outside stream capture).
+  int sync(exg_device_s* dev, cudaStream_t s);
+  bool dirty() const { return dirty_; }
+  // Enqueue one step of every live island (no host synchronisation; graph-capturable once synced).
   int enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s);
   // Aggregate the last step's per-island counters, over all islands (world < 0) or one world.
   int read_stats(int world, exg_world_stats_t* stats);
-  int n_islands_total() const { return n_islands; }
-  // Summed SM cycles per phase since the world was created (kPhases values).
+  // Summed SM cycles per phase since creation (kPhases values).
   int read_phase_cycles(long long* out);
-  ~NewtonWorld();
+  int live_islands() const { return n_live_; }
 
  private:
-  int n_islands = 0;
-  int max_nb = 0;
-  std::vector<void*> allocs;
+  struct WorldSrc {  // what rebuilding a world's islands needs
+    bool live = false;
+    int body_off = 0;
+    std::vector<char> kin;
+    std::vector<exg_joint_t> joints;
+  };
+  int build_world(int slot, const WorldSrc& src);
+  void compact();
+  std::vector<WorldSrc> src_;
+  bool dirty_ = true;
+  int n_live_ = 0;
+  // host structure (append-only)
+  std::vector<IslandDesc> desc_;
+  std::vector<char> alive_;
+  std::vector<long long> scratch_len_;
+  std::vector<int> h_isl_body, h_jl_law, h_jl_a, h_jl_b, h_ib_order, h_ib_inc_ptr, h_ib_inc_ref, h_dn_body, h_dn_parent,
+      h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
+  std::vector<double> h_jl_params;
+  std::vector<std::vector<int>> world_islands_;
+  // device mirrors
+  DevArr<IslandDesc> d_desc;
+  DevArr<int> d_isl_body, d_jl_law, d_jl_a, d_jl_b, d_ib_order, d_ib_inc_ptr, d_ib_inc_ref, d_dn_body, d_dn_parent,
+      d_lv_ptr, d_lv_nodes, d_ch_ptr, d_ch_idx, d_cell_ptr, d_cell_terms;
+  DevArr<double> d_jl_params, d_scratch, d_residual;
+  DevArr<int> d_stats, d_queue;
+  DevArr<long long> d_phase;
+  RangeAllocator scratch_alloc_;
   NewtonDeviceArrays arr{};
-  std::vector<int> island_order;  // islands sorted by size, largest first
-  std::vector<int> island_world;
-  int* d_queue = nullptr;         // island work queue (largest first) and its head counter
-  int* d_head = nullptr;
 };
+
+// Upper estimate of the device bytes an implicit world's islands hold (one island, all dynamic).
+long long newton_footprint_bytes(int nb, int nj);
 
 double host_world_energy(const exg_body_t* b, int n, const exg_joint_t* joints, int nj, const exg_step_params_t& p);

@@ -184,6 +184,83 @@ EXG_API int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* 
 EXG_API int exg_batch_get_world(exg_world_t w, int32_t world, exg_body_t* out, int32_t n_bodies);
 EXG_API int exg_batch_set_world(exg_world_t w, int32_t world, const exg_body_t* bodies, int32_t n_bodies);
 EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_t* out);
+/* ── pool: worlds admitted into and released from fixed-capacity device arrays ──
+ * The serving form of a batch: state stays resident while worlds come and go. A released slot's
+ * ranges are reused by later admissions; exg_world_step advances every admitted world. The
+ * batch accessors (exg_batch_get/set_world, exg_batch_world_stats) take the slot returned by
+ * exg_pool_admit. Admission fails with EXG_ERR_OUT_OF_MEMORY when no free range or slot fits. */
+typedef struct {
+  int64_t max_bodies;
+  int64_t max_joints;
+  int32_t max_worlds;
+  int32_t precision; /* every admitted world must use this precision */
+} exg_pool_config_t;
+typedef struct {
+  int32_t worlds_used;
+  int32_t worlds_capacity;
+  int64_t largest_free_bodies;
+  int64_t largest_free_joints;
+} exg_pool_usage_t;
+EXG_API int exg_pool_create(exg_device_t dev, const exg_pool_config_t* cfg, exg_world_t* out);
+EXG_API int exg_pool_admit(exg_world_t pool, const exg_body_t* bodies, int32_t n_bodies, const exg_joint_t* joints,
+                           int32_t n_joints, const exg_step_params_t* params, int32_t* slot_out);
+EXG_API int exg_pool_release(exg_world_t pool, int32_t slot);
+EXG_API int exg_pool_free(exg_world_t pool, exg_pool_usage_t* out);
+/* Step budget of one admitted world: it takes `steps` more steps of the pool and then holds its
+ * state while the others go on (-1, the default at admission: no limit). */
+EXG_API int exg_pool_set_steps(exg_world_t pool, int32_t slot, int32_t steps);
+/* Steps left per slot for slots [0, n_slots) (-1: no limit; 0 for a free slot or a world whose
+ * budget is spent). */
+EXG_API int exg_pool_steps_left(exg_world_t pool, int32_t* out, int32_t n_slots);
+/* Device bytes a world holds while admitted to a pool: its body and joint rows, gravity partial
+ * sums and, for the implicit integrator, its island structure and per-step scratch (an upper
+ * estimate: every body counted as dynamic, one island). */
+EXG_API int exg_world_footprint(int32_t n_bodies, int32_t n_joints, const exg_step_params_t* params, int64_t* bytes);
+
+/* ── serving: a continuous-batching request loop over a pool ──
+ * Replaces the reference's single GPU-owner worker thread (crates/newton/src/accelerator/mod.rs:
+ * 1010-1155) for whole simulation requests: any thread submits a world and a step count; one
+ * worker thread admits requests in arrival order while the admitted worlds' footprints stay
+ * within hbm_budget_bytes and the pool has room, steps the pool in ticks of at most
+ * steps_per_tick steps, and publishes each world when its steps are done. Each world takes exactly
+ * its requested steps with the arithmetic it has alone. EXG_ERR_WORKER_GONE after the loop stopped
+ * on a device error (EvalError::WorkerGone, crates/newton/src/error.rs:11-28). */
+#define EXG_PENDING 1 /* poll: the request is queued or running */
+typedef struct exg_server_s* exg_server_t;
+typedef struct {
+  int64_t hbm_budget_bytes; /* bound on the sum of admitted worlds' exg_world_footprint */
+  int64_t max_bodies;       /* pool capacities */
+  int64_t max_joints;
+  int32_t max_worlds;
+  int32_t precision;        /* every request must use this precision */
+  int32_t steps_per_tick;   /* steps between admissions / completions */
+  int32_t reserved;
+} exg_server_config_t;
+typedef struct {
+  int64_t steps;
+  int32_t n_bodies;
+  int32_t status;    /* EXG_PENDING, EXG_OK or the failure */
+  double queued_s;   /* submit to admission */
+  double latency_s;  /* submit to completion (to now while pending) */
+} exg_request_info_t;
+typedef struct {
+  int64_t submitted, completed, failed, ticks, steps_launched, body_steps;
+  int32_t queued, running, peak_running, reserved;
+  int64_t resident_bytes, peak_resident_bytes;
+  double busy_s, elapsed_s, p50_latency_s, p99_latency_s, mean_latency_s;
+} exg_server_stats_t;
+EXG_API int exg_server_create(exg_device_t dev, const exg_server_config_t* cfg, exg_server_t* out);
+EXG_API int exg_server_submit(exg_server_t server, const exg_body_t* bodies, int32_t n_bodies, const exg_joint_t* joints,
+                              int32_t n_joints, const exg_step_params_t* params, int32_t steps, uint64_t* id);
+/* EXG_PENDING while queued or running; otherwise the request's status, its final bodies copied to
+ * out (when out is not NULL; n must equal its body count) and the request forgotten. */
+EXG_API int exg_server_poll(exg_server_t server, uint64_t id, exg_body_t* out, int32_t n, exg_request_info_t* info);
+/* poll after waiting up to timeout_ms for the request to finish (EXG_ERR_TIMEOUT otherwise) */
+EXG_API int exg_server_wait(exg_server_t server, uint64_t id, int32_t timeout_ms, exg_body_t* out, int32_t n,
+                            exg_request_info_t* info);
+EXG_API int exg_server_stats(exg_server_t server, exg_server_stats_t* out);
+EXG_API int exg_server_reset_stats(exg_server_t server);
+EXG_API int exg_server_destroy(exg_server_t server);
 /* SM clock cycles the implicit step spent per phase since the handle was created, summed over
  * islands: [0] PRE, [1] joint values + Jacobian, [2] gather + POST, [3] assembly, [4] linear
  * solve, [5] line search, [6] commit, [7] other. Zero for worlds without implicit islands. */

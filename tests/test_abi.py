@@ -80,3 +80,53 @@ def test_host_motor_utilities_match_oracle(oracle):
     a = _lib.motor_exp([1, 0, 0, 0, 0, 0], 1.0)
     b = _lib.motor_exp([0, 0, 0, 0, 0, np.pi / 2], 1.0)
     assert np.allclose(_lib.motor_apply_point(_lib.motor_compose(a, b), [0, 0, 0]), [0, 1, 0], atol=1e-12)
+
+
+def test_every_record_dtype_matches_the_compiled_header(tmp_path):
+    """Compile a layout probe against include/exg.h with the host C compiler and compare each
+    record's size and field offsets with the numpy dtype the binding passes by pointer."""
+    from exgame_b200 import abi
+    exe = tmp_path / "abi_layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe),
+                    os.path.join(ROOT, "tests", "native", "abi_layout.c")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    dtypes = {"exg_body_t": abi.BODY_DTYPE, "exg_joint_t": abi.JOINT_DTYPE, "exg_step_params_t": abi.STEP_PARAMS_DTYPE,
+              "exg_world_stats_t": abi.WORLD_STATS_DTYPE, "exg_pool_config_t": abi.POOL_CONFIG_DTYPE,
+              "exg_pool_usage_t": abi.POOL_USAGE_DTYPE, "exg_server_config_t": abi.SERVER_CONFIG_DTYPE,
+              "exg_request_info_t": abi.REQUEST_INFO_DTYPE, "exg_server_stats_t": abi.SERVER_STATS_DTYPE}
+    checked = 0
+    for line in out:
+        if not line:
+            continue
+        t, field, value = line.split()
+        dt = dtypes[t]
+        if field == "sizeof":
+            assert dt.itemsize == int(value), t
+        else:
+            assert dt.fields[field][1] == int(value), (t, field)
+        checked += 1
+    assert checked > 60
+
+
+def test_world_footprint_without_device():
+    from exgame_b200 import abi
+    from exgame_b200._lib import world_footprint
+    free = world_footprint(1000, 0, abi.step_params())
+    grav = world_footprint(1000, 0, abi.step_params(gravity_law=abi.GRAVITY_PLUMMER, softening=0.05))
+    newton = world_footprint(1000, 999, abi.step_params(integrator=abi.NEWTON))
+    assert 0 < free < grav < newton
+    assert world_footprint(2000, 0, abi.step_params()) == 2 * free
+    with pytest.raises(_lib.ExgError):
+        world_footprint(-1, 0, abi.step_params())
+
+
+def test_pool_and_server_reject_a_missing_device():
+    import ctypes
+    from exgame_b200 import abi
+    cfg = np.zeros((), dtype=abi.SERVER_CONFIG_DTYPE)
+    cfg["hbm_budget_bytes"], cfg["max_bodies"], cfg["max_worlds"], cfg["steps_per_tick"] = 1 << 30, 1024, 4, 8
+    h = ctypes.c_void_p()
+    assert _lib.lib().exg_server_create(None, _lib.ptr(cfg), ctypes.byref(h)) == -20
+    pc = np.zeros((), dtype=abi.POOL_CONFIG_DTYPE)
+    pc["max_bodies"], pc["max_worlds"] = 1024, 4
+    assert _lib.lib().exg_pool_create(None, _lib.ptr(pc), ctypes.byref(h)) == -20

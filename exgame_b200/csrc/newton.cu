@@ -24,7 +24,14 @@ namespace {
 
 using namespace exg;
 
-constexpr int kThreads = 256;
+#ifndef EXG_NEWTON_MIN_BLOCKS
+#define EXG_NEWTON_MIN_BLOCKS 1  // CTAs per SM the register budget is sized for
+#endif
+#ifndef EXG_NEWTON_THREADS
+#define EXG_NEWTON_THREADS 256
+#endif
+constexpr int kThreads = EXG_NEWTON_THREADS;
+constexpr int kMinBlocks = EXG_NEWTON_MIN_BLOCKS;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxDepth = 8;
 constexpr int kThresholdLog2 = 8;
@@ -675,7 +682,7 @@ __device__ void commit_span(const Ctx& c, double span, double half, bool converg
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
                                                          int n_islands, int* __restrict__ head) {
   __shared__ double red[kWarps];
   __shared__ int flag;
@@ -1101,10 +1108,19 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   WorldRef W{w.pose,    w.mom,    w.mass,   w.inertia, w.kinematic,  w.diagonal, w.pos_mass,
              w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
   int* head = d_queue.ptr + n_live_;
-  int grid = std::min(n_live_, std::max(1, dev->sm_count) * 2);
+  // persistent CTAs: as many as can be resident at once
+  static int resident[2] = {0, 0};
+  const int mixed = w.precision == EXG_PRECISION_MIXED;
+  if (resident[mixed] == 0) {
+    int per_sm = 0;
+    cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<true>, kThreads, 0)
+                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<false>, kThreads, 0);
+    resident[mixed] = (e == cudaSuccess && per_sm > 0) ? per_sm : 1;
+  }
+  int grid = std::min(n_live_, std::max(1, dev->sm_count) * resident[mixed]);
   EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
   int tok = prof_begin(dev, PROF_NEWTON, s);
-  if (w.precision == EXG_PRECISION_MIXED)
+  if (mixed)
     k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);
   else
     k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);

@@ -1,6 +1,11 @@
 """Benchmark of the per-step dynamics path on B200.
 
-`python bench.py --gpus N --steps K --warmup W [--impl ours|reference] [--workload c0|c1|c2]`
+`python bench.py --gpus N --steps K --warmup W [--impl ours|reference] [--workload c0|c1|c2|c3|c3-f64]`
+
+The default workload is the mixed-size batch (4096 worlds of 8..8192 bodies, mixed precision), on
+which the headline metric is quoted; beside it the line carries the plain path (every world FP64,
+alone, one world per launch) and, at N = 1, a served sweep (Poisson request streams of such worlds
+with log-uniform step counts through the native request loop, p50/p99 latency).
 
 A step is one Mechanism::step of the whole workload (every body advanced by dt). `value` is
 body-steps/s from CUDA events on the library's stream with the state resident in HBM; `e2e` is the
@@ -169,6 +174,29 @@ def dominant_kernel(dev, cfg_name, parts, steps, bench_worlds):
     return kind, ms, nl, flops, bound, label, shares
 
 
+# Algorithmic bytes of one Newton iteration, FP32 Jacobian blocks: per joint 40 floats in
+# (2 poses, 2 twists, dt, warp, 10 params) and 12 + 288 out; per dynamic body motor 8, twist 6 and
+# wrench 6 in, 36 mass + 6 rhs + 6 scale out; per tree edge 3 x 36 factor floats.
+NEWTON_BYTES_PER_JOINT = (40 + 300) * 4
+NEWTON_BYTES_PER_BODY = (20 + 48) * 4
+NEWTON_BYTES_PER_EDGE = 3 * 36 * 4
+
+
+def newton_bytes_last_step(batch, parts):
+    """Algorithmic bytes the implicit worlds moved in the last step (iterations x per-iteration bytes)."""
+    total, iters = 0.0, 0
+    for k, (b, j, p) in enumerate(parts):
+        if int(p["integrator"]) != NEWTON:
+            continue
+        st = batch.world_stats(k) if hasattr(batch, "world_stats") else batch.stats()
+        it = int(st["last_newton_iterations"])
+        iters += it
+        dyn = int((b["kinematic"] == 0).sum())
+        total += it * (len(j) * NEWTON_BYTES_PER_JOINT + dyn * NEWTON_BYTES_PER_BODY
+                       + max(dyn - 1, 0) * NEWTON_BYTES_PER_EDGE)
+    return total, iters
+
+
 def make_worlds(dev, parts):
     if len(parts) == 1:
         return [_lib.DeviceWorld(dev, *parts[0])]
@@ -267,15 +295,27 @@ def run_ours(args, rank, world_size, local_rank):
     peaks, src = load_peaks()
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    per_clk = FP64_FMA_PER_SM_CLK if bound == "fp64" else FP32_FMA_PER_SM_CLK
-    peak_tflops = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
     avg_s = ms / 1e3 / max(nl, 1)
-    roofline = {"bound": bound, "achieved": (flops / avg_s / 1e12) if flops else None, "peak": peak_tflops,
-                "unit": "TFLOP/s", "frac": (flops / avg_s / 1e12 / peak_tflops) if flops else None, "traffic": None,
-                "kernel": label, "avg_launch_us": avg_s * 1e6, "launches": nl,
-                "device_ms_by_kernel": shares,
-                "peak_source": f"nominal {per_clk} {bound.upper()} FMA/clk/SM x {sms} SMs at the {src} max SM clock "
-                               f"{sm_mhz:.0f} MHz (no tensor-core or copy peak applies to this kernel)"}
+    if kind == 3:  # the Newton island step: HBM-bound by its algorithmic bytes
+        nbytes, iters = newton_bytes_last_step(worlds[0], parts)
+        hbm = float(peaks["hbm_gbs"])
+        roofline = {"bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
+                    "frac": nbytes / avg_s / 1e9 / hbm, "traffic": None, "kernel": label,
+                    "algorithmic_bytes_per_launch": nbytes, "newton_iterations_summed_over_islands": iters,
+                    "avg_launch_us": avg_s * 1e6, "launches": nl, "device_ms_by_kernel": shares,
+                    "peak_source": f"{src} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs), of {src}"}
+    else:
+        per_clk = FP64_FMA_PER_SM_CLK if bound == "fp64" else FP32_FMA_PER_SM_CLK
+        peak_tflops = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
+        roofline = {"bound": bound, "achieved": (flops / avg_s / 1e12) if flops else None, "peak": peak_tflops,
+                    "unit": "TFLOP/s", "frac": (flops / avg_s / 1e12 / peak_tflops) if flops else None,
+                    "traffic": None, "kernel": label, "avg_launch_us": avg_s * 1e6, "launches": nl,
+                    "device_ms_by_kernel": shares,
+                    "peak_source": f"nominal {per_clk} {bound.upper()} FMA/clk/SM x {sms} SMs at the {src} max SM "
+                                   f"clock {sm_mhz:.0f} MHz (no tensor-core or copy peak applies to this kernel)"}
+    grav = gravity_roofline(dev, parts, worlds, sms, sm_mhz) if kind != 0 else None
+    if grav:
+        roofline["gravity"] = grav
     plain = None
     if args.plain and len(parts) > 1:
         plain = {"value": plain_path(dev, parts, flush), "unit": METRIC,
@@ -283,8 +323,98 @@ def run_ours(args, rank, world_size, local_rank):
                            "per world, one pass after a warm pass (device time, L2 flushed before the pass)"}
     return {
         "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
-        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain,
+        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain, "dev": dev,
     }
+
+
+def gravity_roofline(dev, parts, worlds, sms, sm_mhz):
+    """The all-pairs gravity kernel of the same workload, timed alone over a profiled pass."""
+    pairs = sum(float(len(b)) ** 2 for b, _, p in parts if int(p["gravity_law"]) != GRAVITY_OFF and len(b) > 1)
+    if pairs == 0:
+        return None
+    dev.profile(True)
+    for w in worlds:
+        w.step(1)
+    ms, nl = dev.profile_read(0)
+    dev.profile(False)
+    mixed = int(parts[0][2]["precision"]) == PRECISION_MIXED
+    per_clk = FP32_FMA_PER_SM_CLK if mixed else FP64_FMA_PER_SM_CLK
+    peak = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
+    achieved = 20.0 * pairs / (ms / 1e3 / max(nl, 1)) / 1e12
+    return {"bound": "fp32" if mixed else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "avg_launch_us": ms * 1e3 / max(nl, 1),
+            "flops_per_launch": 20.0 * pairs, "note": "20 flop per directed pair"}
+
+
+def serve_sweep(dev, rates, n_requests, pool_size, tick, rank):
+    """Config 4: Poisson request streams through the native request loop (exg_server_*). Each
+    request is a world drawn from a pool of config-3 worlds (log-uniform 8..8192 bodies, half
+    gravity, half trees; mixed precision) with a step count log-uniform in [10, 1000]. Latency is
+    measured from each request's scheduled arrival. Beside it, the plain path served FIFO: one world
+    at a time in FP64 with the reference's Newton matrix, from per-world step times measured alone."""
+    import torch
+    rng = np.random.default_rng(44 + rank)
+    pool = scenarios.config3_worlds(pool_size, seed=40 + rank, precision=PRECISION_MIXED, exact_jacobian=True)
+    stream = torch.cuda.ExternalStream(dev.stream())
+    # plain path: FP64 step time of every pool world alone
+    plain_step_s = []
+    for b, j, p in pool:
+        q = p.copy()
+        q["precision"] = PRECISION_F64
+        q["newton_flags"] = 0
+        w = _lib.DeviceWorld(dev, b, j, q)
+        w.step(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        w.step(2)
+        e1.record(stream)
+        e1.synchronize()
+        plain_step_s.append(e0.elapsed_time(e1) / 2e3)
+        w.close()
+    max_b = max(len(b) for b, _, _ in pool)
+    out = []
+    for rate in rates:
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+        picks = rng.integers(0, len(pool), n_requests)
+        steps = np.exp(rng.uniform(math.log(10), math.log(1000), n_requests)).astype(np.int64)
+        srv = _lib.Server(dev, hbm_budget_bytes=150 * 10**9, max_bodies=max(4 << 20, 2 * max_b),
+                          max_joints=max(12 << 20, 6 * max_b), max_worlds=1024, precision=PRECISION_MIXED,
+                          steps_per_tick=tick)
+        ids, lag = [], []
+        t0 = time.perf_counter()
+        for k in range(n_requests):
+            dt = t0 + arrivals[k] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            b, j, p = pool[picks[k]]
+            ids.append(srv.submit(b, j, p, int(steps[k])))
+            lag.append(time.perf_counter() - (t0 + arrivals[k]))
+        lat = []
+        for k, rid in enumerate(ids):
+            _, info = srv.wait(rid, timeout_ms=600000)
+            lat.append(float(info["latency_s"]) + lag[k])
+        t_end = time.perf_counter()
+        st = srv.stats()
+        srv.close()
+        bs = float(sum(len(pool[picks[k]][0]) * int(steps[k]) for k in range(n_requests)))
+        # plain path: FIFO, one world at a time
+        done, plat = 0.0, []
+        for k in range(n_requests):
+            start = max(arrivals[k], done)
+            done = start + steps[k] * plain_step_s[picks[k]]
+            plat.append(done - arrivals[k])
+        out.append({
+            "rate_req_s": rate, "requests": n_requests, "body_steps": bs,
+            "body_steps_per_s": bs / (t_end - t0), "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "max_submit_lag_s": float(max(lag)),
+            "peak_running": st["peak_running"], "ticks": st["ticks"],
+            "plain_fifo": {"body_steps_per_s": bs / done, "p50_latency_s": float(np.percentile(plat, 50)),
+                           "p99_latency_s": float(np.percentile(plat, 99))},
+        })
+    return {"pool_worlds": len(pool), "steps_per_tick": tick, "sweep": out,
+            "plain_fifo_model": "FIFO queue, one world at a time, service = steps x that world's FP64 step time "
+                                "measured alone (device time)"}
 
 
 def cpu_baseline(args, threads):
@@ -314,10 +444,15 @@ def cpu_baseline(args, threads):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c0", choices=["c0", "c1", "c2", "c3", "c3-f64"])
+    ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3-f64"])
+    ap.add_argument("--serve-rates", default="100,1000,10000",
+                    help="request rates (req/s) of the served sweep at N=1; empty to skip")
+    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-pool", type=int, default=256)
+    ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
@@ -366,6 +501,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     r = run_ours(args, rank, world_size, local_rank)
     cpu = cpu_baseline(args, 1) if rank == 0 and world_size == 1 else None
+    serving = None
+    if rank == 0 and world_size == 1 and args.serve_rates:
+        rates = [float(x) for x in args.serve_rates.split(",") if x]
+        serving = serve_sweep(r["dev"], rates, args.serve_requests, args.serve_pool, args.serve_tick, rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
@@ -375,7 +514,7 @@ def main():
             "config": dict(r["cfg"], parallelism=f"replicas x{world_size} (independent worlds)",
                            l2="flushed between timed steps (256 MB write)"),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
-            "clocks": r["clocks"], "plain_path": r["plain"],
+            "clocks": r["clocks"], "plain_path": r["plain"], "serving": serving,
         }
         print(json.dumps(line))
     if world_size > 1:

@@ -61,6 +61,8 @@ SIGNATURES = {
     "exg_server_stats": (ctypes.c_int, [_vp, _vp]),
     "exg_server_reset_stats": (ctypes.c_int, [_vp]),
     "exg_server_destroy": (ctypes.c_int, [_vp]),
+    "exg_world_set_option": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int64]),
+    "exg_world_get_option": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     "exg_pool_set_steps": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
     "exg_pool_steps_left": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
@@ -203,7 +205,7 @@ class Device:
     def profile(self, enable):
         check(lib().exg_device_profile(self.handle, int(bool(enable))))
 
-    PROF_GRAVITY, PROF_JOINTS, PROF_INTEGRATE, PROF_NEWTON, PROF_BODY_PRE = 0, 1, 2, 3, 4
+    PROF_GRAVITY, PROF_JOINTS, PROF_INTEGRATE, PROF_NEWTON, PROF_BODY_PRE, PROF_NEWTON_WAVE = 0, 1, 2, 3, 4, 5
 
     def profile_read(self, kind):
         ms, n = ctypes.c_double(), ctypes.c_int64()
@@ -252,6 +254,16 @@ class DeviceWorld:
         s = np.zeros((), dtype=WORLD_STATS_DTYPE)
         check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
         return s
+
+    OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS = 1, 2, 3
+
+    def set_option(self, option, value):
+        check(lib().exg_world_set_option(self.handle, int(option), int(value)), "exg_world_set_option")
+
+    def get_option(self, option):
+        v = ctypes.c_int64()
+        check(lib().exg_world_get_option(self.handle, int(option), ctypes.byref(v)), "exg_world_get_option")
+        return v.value
 
     PHASES = ("pre", "joints+jacobian", "gather+post", "assemble", "solve", "line search", "commit", "other")
 

@@ -643,6 +643,36 @@ int exg_pool_steps_left(exg_world_t W, int32_t* out, int32_t n_slots) {
   return EXG_OK;
 }
 
+int exg_world_set_option(exg_world_t W, int32_t option, int64_t value) {
+  if (!W) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  switch (option) {
+    case EXG_OPT_WAVE_MIN_BODIES:
+      if (value < 1 || value > (1LL << 30)) return EXG_ERR_INVALID_ARGUMENT;
+      W->newton->set_wave_threshold((int)value, W->newton->wave_max_levels());
+      break;
+    case EXG_OPT_WAVE_MAX_LEVELS:
+      if (value < 1 || value > (1LL << 30)) return EXG_ERR_INVALID_ARGUMENT;
+      W->newton->set_wave_threshold(W->newton->wave_min_dyn(), (int)value);
+      break;
+    default:
+      return EXG_ERR_INVALID_ARGUMENT;
+  }
+  W->dirty = true;
+  return EXG_OK;
+}
+
+int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
+  if (!W || !value) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  switch (option) {
+    case EXG_OPT_WAVE_MIN_BODIES: *value = W->newton->wave_min_dyn(); return EXG_OK;
+    case EXG_OPT_WAVE_MAX_LEVELS: *value = W->newton->wave_max_levels(); return EXG_OK;
+    case EXG_OPT_LAST_WAVE_ROUNDS: *value = W->newton->last_wave_rounds(); return EXG_OK;
+    default: return EXG_ERR_INVALID_ARGUMENT;
+  }
+}
+
 int exg_world_destroy(exg_world_t W) {
   if (!W) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
@@ -681,6 +711,7 @@ static int step_locked(exg_world_s* W, int32_t n_steps) {
     for (int32_t k = 0; k < n_steps; ++k) {
       int kernels = 0;
       rc = enqueue_step(W, &kernels);
+      if (rc == EXG_OK && W->newton->has_wave()) rc = W->newton->run_wave(W->dev, W->w, s);
       if (rc != EXG_OK) return rc;
     }
   } else {
@@ -706,6 +737,8 @@ static int step_locked(exg_world_s* W, int32_t n_steps) {
     for (int32_t k = 0; k < n_steps; ++k) {
       EXG_CUDA_TRY(cudaGraphLaunch(W->graph, s));
       W->dev->launches.fetch_add(W->graph_kernels);
+      // large islands: the wave schedule's rounds, after the step's other kernels
+      if (W->newton->has_wave() && (rc = W->newton->run_wave(W->dev, W->w, s)) != EXG_OK) return rc;
     }
   }
   EXG_CUDA_TRY(cudaStreamSynchronize(s));

@@ -21,7 +21,8 @@
 void exg_internal_set_cuda_error(cudaError_t e, const char* what);
 
 // Kernel kinds the in-library profiler distinguishes.
-enum ProfKind { PROF_GRAVITY = 0, PROF_JOINTS = 1, PROF_INTEGRATE = 2, PROF_NEWTON = 3, PROF_BODY_PRE = 4, PROF_KINDS = 8 };
+enum ProfKind { PROF_GRAVITY = 0, PROF_JOINTS = 1, PROF_INTEGRATE = 2, PROF_NEWTON = 3, PROF_BODY_PRE = 4, PROF_NEWTON_WAVE = 5,
+                PROF_KINDS = 8 };
 
 struct exg_device_s {
   int ordinal = 0;

@@ -25,7 +25,6 @@ namespace {
 
 template <class R> __device__ __forceinline__ R rsqrt_r(R x);
 template <> __device__ __forceinline__ double rsqrt_r<double>(double x) { return rsqrt(x); }
-template <> __device__ __forceinline__ float rsqrt_r<float>(float x) { return rsqrtf(x); }
 
 template <class R> struct Vec4;
 template <> struct Vec4<double> { typedef double4 T; };

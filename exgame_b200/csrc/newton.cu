@@ -17,12 +17,11 @@
 #include <functional>
 #include <new>
 #include "body.cuh"
-#include "joint_eval.cuh"
-#include "world_newton.cuh"
+#include "newton_ops.cuh"
 
 namespace {
 
-using namespace exg;
+using namespace exg_newton;
 
 #ifndef EXG_NEWTON_MIN_BLOCKS
 #define EXG_NEWTON_MIN_BLOCKS 1  // CTAs per SM the register budget is sized for
@@ -33,82 +32,6 @@ using namespace exg;
 constexpr int kThreads = EXG_NEWTON_THREADS;
 constexpr int kMinBlocks = EXG_NEWTON_MIN_BLOCKS;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxDepth = 8;
-constexpr int kThresholdLog2 = 8;
-constexpr int kPerHalvingLog2 = 4;
-constexpr double kHuge = 1e9;
-constexpr double kFloor2 = 1e-9 * 1e-9;
-constexpr int kJacStride = 42;  // per (joint, slice): value[6] + d[36]
-
-struct Scratch {
-  double *vm, *base, *best, *trial, *mid, *snap, *ext, *conn, *jac, *mass, *mass0, *rhs, *scale, *D, *Dinv, *Acp, *Apc, *S,
-      *bvec, *dv;
-};
-
-EXG_HD long long scratch_doubles(int nb, int nj, int m) {
-  return (long long)nb * (6 * 4 + 8 + 6 * 2) + (long long)nj * (6 + 4 * kJacStride) + (long long)m * (36 * 7 + 6 * 3 + 2);
-}
-
-__device__ Scratch carve(double* p, int nb, int nj, int m) {
-  Scratch s;
-  s.vm = p; p += nb * 6;
-  s.base = p; p += nb * 6;
-  s.best = p; p += nb * 6;
-  s.trial = p; p += nb * 6;
-  s.mid = p; p += nb * 8;
-  s.snap = p; p += nb * 6;
-  s.ext = p; p += nb * 6;
-  s.conn = p; p += (size_t)nj * 6;
-  s.jac = p; p += (size_t)nj * 4 * kJacStride;
-  s.mass = p; p += (size_t)m * 36;
-  s.mass0 = p; p += (size_t)m * 36;
-  s.rhs = p; p += (size_t)m * 6;
-  s.scale = p; p += (size_t)m * 2;
-  s.D = p; p += (size_t)m * 36;
-  s.Dinv = p; p += (size_t)m * 36;
-  s.Acp = p; p += (size_t)m * 36;
-  s.Apc = p; p += (size_t)m * 36;
-  s.S = p; p += (size_t)m * 36;
-  s.bvec = p; p += (size_t)m * 6;
-  s.dv = p; p += (size_t)m * 6;
-  return s;
-}
-
-struct WorldRef {
-  double* pose;
-  double* mom;
-  const double* mass;
-  const double* inertia;
-  const int* kinematic;
-  const int* diagonal;
-  const double* pos_mass;
-  const double* grav_partial;
-  const exg_step_params_t* wparams;
-  const long long* w_poff;
-  const int* w_splits;
-  const int* w_n;
-  const int* w_body_off;
-  const int* w_active;
-  int n;
-};
-
-// The island's world parameters, resolved once per island.
-struct IslandParams {
-  double dt, warp, tol2, G, pose_factor_scale;
-  int max_newton;
-  int splits, nw, wbody_off;
-  const double* part;
-};
-
-struct Ctx {
-  NewtonDeviceArrays A;
-  IslandDesc d;
-  WorldRef W;
-  IslandParams P;
-  Scratch s;
-  int island;
-  EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
-};
 
 // Phase timer: thread 0 accumulates SM clock cycles between phase boundaries (all threads have
 // passed a barrier there) into shared counters; the CTA adds them to the global totals at the end.
@@ -126,10 +49,6 @@ struct PhaseTimer {
 };
 
 // ── block-wide reductions ───────────────────────────────────────────────────
-__device__ double nan_max(double a, double b) {
-  if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000ULL);
-  return a > b ? a : b;
-}
 __device__ double block_max(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
   int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -153,148 +72,23 @@ __device__ double block_sum(double v, double* red) {
   return r;
 }
 
-// ── phases ──────────────────────────────────────────────────────────────────
-// PRE: mid = exp(half/2 v) * pose for every island body (functions::pre)
+// ── phases: the island's items spread over the CTA ──────────────────────────
 __device__ void phase_pre(const Ctx& c, const double* v, double half) {
-  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
-    int g = c.gbody(q);
-    double pose[8], vb[6], e[8], m[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
-    screw_from6(v + 6 * q, vb);
-    twist_exp(vb, half, e);
-    motor_compose(pose, e, m);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) c.s.mid[8 * q + k] = m[k];
-  }
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) op_pre(c, v, half, q);
 }
 
-// Joint values (and Jacobian slices) at (mid, v): conn[q] = wrench on end a. MIXED evaluates the
-// derivative slices in FP32 duals; the values that enter the residual always come from an FP64
-// evaluation, so the converged iterate is an FP64 solution whatever the Jacobian's precision.
 template <bool MIXED>
 __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
-  const int nj = c.d.nj;
-  const int joff = c.d.joint_off;
   if (jac) {
-    for (int t = threadIdx.x; t < 4 * nj; t += blockDim.x) {
-      int q = t >> 2, slice = t & 3;
-      int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
-      const int law = c.A.jl_law[joff + q];
-      const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
-      double* o = c.s.jac + ((size_t)q * 4 + slice) * kJacStride;
-      if (MIXED) {
-        float pa[8], pb[8], va[6], vb[6], val[6], dd[36];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) { pa[k] = float(c.s.mid[8 * a + k]); pb[k] = float(c.s.mid[8 * b + k]); }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) { va[k] = float(v[6 * a + k]); vb[k] = float(v[6 * b + k]); }
-        joint_jacobian_slice<float>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, val, dd);
-#pragma unroll
-        for (int r = 0; r < 6; ++r) o[r] = double(val[r]);
-#pragma unroll
-        for (int k = 0; k < 36; ++k) o[6 + k] = double(dd[k]);
-        if (slice == 0) {
-          double out[12];
-          joint_plain<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, out);
-#pragma unroll
-          for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
-        }
-      } else {
-        double val[6], dd[36];
-        joint_jacobian_slice<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, v + 6 * a, v + 6 * b, c.P.dt, c.P.warp,
-                                     slice, val, dd);
-#pragma unroll
-        for (int r = 0; r < 6; ++r) o[r] = val[r];
-#pragma unroll
-        for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
-        if (slice == 0) {
-#pragma unroll
-          for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
-        }
-      }
-    }
+    for (int t = threadIdx.x; t < 4 * c.d.nj; t += blockDim.x) op_joint<MIXED>(c, v, t >> 2, t & 3, true);
   } else {
-    for (int q = threadIdx.x; q < nj; q += blockDim.x) {
-      int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
-      double out[12];
-      joint_plain<double>(c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a, c.s.mid + 8 * b,
-                          v + 6 * a, v + 6 * b, c.P.dt, c.P.warp, out);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
-    }
+    for (int q = threadIdx.x; q < c.d.nj; q += blockDim.x) op_joint<MIXED>(c, v, q, 0, false);
   }
 }
 
-// Gather + POST for every dynamic node; returns the worst relative residual^2 (newton.rs:139-151).
 __device__ double phase_post(const Ctx& c, const double* v, double half, double* red) {
   double worst = 0.0;
-  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) {
-    int q = c.A.dn_body[c.d.dyn_off + i];
-    int g = c.gbody(q);
-    double tot[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) tot[k] = c.s.ext[6 * q + k];
-    int p0 = c.A.ib_inc_ptr[c.d.inc_off + q], p1 = c.A.ib_inc_ptr[c.d.inc_off + q + 1];
-    for (int t = p0; t < p1; ++t) {
-      int ref = c.A.ib_inc_ref[t];
-      int jq = ref >> 1;
-      if (ref & 1) {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) tot[k] = tot[k] - c.s.conn[6 * jq + k];
-      } else {
-#pragma unroll
-        for (int k = 0; k < 6; ++k) tot[k] = tot[k] + c.s.conn[6 * jq + k];
-      }
-    }
-    double I9[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
-    const bool diag = c.W.diagonal[g] != 0;
-    const double mass = c.W.mass[g];
-    const double* mid = c.s.mid + 8 * q;
-    double inv[8];
-    motor_reverse(mid, inv);
-    double* blk = c.s.mass + 36 * (size_t)i;
-#pragma unroll
-    for (int col = 0; col < 6; ++col) {
-      double e6[6] = {0, 0, 0, 0, 0, 0};
-      e6[col] = 1.0;
-      double eb[6], ebody[6], b6[6], wv[6], p6[6], pb[6], cw[6], c6[6];
-      screw_from6(e6, eb);
-      twist_transport(eb, inv, ebody);
-      screw_to6(ebody, b6);
-      wv[0] = b6[0]; wv[1] = b6[1]; wv[2] = b6[2]; wv[3] = b6[3]; wv[4] = b6[4]; wv[5] = b6[5];
-      inertia_apply(I9, diag, false, mass, wv, p6);
-      screw_from6(p6, pb);
-      wrench_transport(pb, mid, cw);
-      screw_to6(cw, c6);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) blk[r * 6 + col] = c6[r];
-    }
-    const double* vv = v + 6 * q;
-    double p[6], nn[6], hh[6], res[6];
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      double acc = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) acc += blk[r * 6 + k] * vv[k];
-      p[r] = acc;
-      nn[r] = c.s.snap[6 * q + r];
-      hh[r] = tot[r] * half;
-    }
-#pragma unroll
-    for (int r = 0; r < 6; ++r) res[r] = -(p[r] - nn[r] - hh[r]);
-#pragma unroll
-    for (int r = 0; r < 6; ++r) c.s.rhs[6 * i + r] = res[r];
-    auto sq3 = [](const double* x) { return x[0] * x[0] + x[1] * x[1] + x[2] * x[2]; };
-    double lin = fmax(fmax(fmax(sq3(p), sq3(nn)), sq3(hh)), kFloor2);
-    double ang = fmax(fmax(fmax(sq3(p + 3), sq3(nn + 3)), sq3(hh + 3)), kFloor2);
-    c.s.scale[2 * i] = lin;
-    c.s.scale[2 * i + 1] = ang;
-    worst = nan_max(worst, sq3(res) / lin);
-    worst = nan_max(worst, sq3(res + 3) / ang);
-  }
+  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) worst = nan_max(worst, op_post(c, v, half, i));
   return block_max(worst, red);
 }
 
@@ -302,130 +96,18 @@ __device__ void copy_mass0(const Ctx& c) {
   for (int t = threadIdx.x; t < 36 * c.d.m; t += blockDim.x) c.s.mass0[t] = c.s.mass[t];
 }
 
-// Assembly (rows/assemble.rs, functions::assemble_term): per target block and entry, the
-// mass block (diagonal only) then every contributing joint end in joint order with the
-// midpoint factors pf = -half^2 on pose columns and vf = -half on velocity columns.
 // Returns ||A||_F^2.
+template <bool MIXED>
 __device__ double phase_assemble(const Ctx& c, double half, double* red) {
-  const double pf = -(half * half) * c.P.pose_factor_scale, vf = -half;
   double sumsq = 0.0;
   const int cells = 3 * c.d.m;
+  const double pf = -(half * half) * c.P.pose_factor_scale, vf = -half;
   for (int t = threadIdx.x; t < cells * 36; t += blockDim.x) {
-    int cell = t / 36, e = t % 36;
-    int i = cell / 3, kind = cell % 3;
-    int r = e / 6, col = e % 6;
-    double acc = (kind == 0) ? c.s.mass0[36 * (size_t)i + e] : 0.0;
-    int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
-    for (int k = p0; k < p1; ++k) {
-      int term = c.A.cell_terms[k];
-      int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
-      const double* jp = c.s.jac + ((size_t)q * 4 + ce) * kJacStride + 6;
-      const double* jv = c.s.jac + ((size_t)q * 4 + 2 + ce) * kJacStride + 6;
-      double pv = jp[r * 6 + col], vv = jv[r * 6 + col];
-      if (re) { pv = -pv; vv = -vv; }
-      acc = acc + pf * pv + vf * vv;
-    }
-    double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
-    dst[36 * (size_t)i + e] = acc;
-    if (kind == 0 || c.A.dn_parent[c.d.dyn_off + i] >= 0) sumsq += acc * acc;
+    bool counts;
+    double acc = op_assemble<MIXED>(c, pf, vf, t / 36, t % 36, &counts);
+    if (counts) sumsq += acc * acc;
   }
   return block_sum(sumsq, red);
-}
-
-// Warp-cooperative 6x6 inverse by Gauss-Jordan with partial pivoting: lane c < 12 holds
-// column c of [A | I]. Returns false (to every lane) if a pivot is zero or not finite.
-__device__ bool warp_inverse6(const double* a, double* out) {
-  const int lane = threadIdx.x & 31;
-  double col[6];
-#pragma unroll
-  for (int r = 0; r < 6; ++r) {
-    if (lane < 6) col[r] = a[r * 6 + lane];
-    else col[r] = (lane - 6 == r) ? 1.0 : 0.0;
-  }
-  bool ok = true;
-#pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    int piv = k;
-    double best = fabs(col[k]);
-#pragma unroll
-    for (int r = k + 1; r < 6; ++r) {
-      double x = fabs(col[r]);
-      if (x > best) { best = x; piv = r; }
-    }
-    piv = __shfl_sync(0xffffffffu, piv, k);
-    double tk = col[k], tp = col[k];
-#pragma unroll
-    for (int r = k; r < 6; ++r) if (r == piv) tp = col[r];
-#pragma unroll
-    for (int r = k; r < 6; ++r) if (r == piv) col[r] = tk;
-    col[k] = tp;
-    double pv = __shfl_sync(0xffffffffu, col[k], k);
-    if (!(fabs(pv) > 0.0) || !isfinite(pv)) ok = false;
-    double ip = 1.0 / pv;
-    col[k] = col[k] * ip;
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      if (r == k) continue;
-      double f = __shfl_sync(0xffffffffu, col[r], k);
-      col[r] = col[r] - f * col[k];
-    }
-  }
-  if (lane >= 6 && lane < 12) {
-#pragma unroll
-    for (int r = 0; r < 6; ++r) out[r * 6 + (lane - 6)] = col[r];
-  }
-  __syncwarp();
-  return ok;
-}
-
-// C = A * B (6x6, row-major) or C -= A * B, computed by one warp.
-template <bool Sub>
-__device__ void warp_mm6(const double* A, const double* B, double* C) {
-  const int lane = threadIdx.x & 31;
-  double v0 = 0.0, v1 = 0.0;
-  int e0 = lane, e1 = lane + 32;
-  {
-    int r = e0 / 6, cc = e0 % 6;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) v0 += A[r * 6 + k] * B[k * 6 + cc];
-  }
-  if (e1 < 36) {
-    int r = e1 / 6, cc = e1 % 6;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) v1 += A[r * 6 + k] * B[k * 6 + cc];
-  }
-  __syncwarp();
-  if (Sub) {
-    C[e0] = C[e0] - v0;
-    if (e1 < 36) C[e1] = C[e1] - v1;
-  } else {
-    C[e0] = v0;
-    if (e1 < 36) C[e1] = v1;
-  }
-  __syncwarp();
-}
-// y -= A x (6x6 * 6) by one warp (lanes 0..5)
-__device__ void warp_mv6_sub(const double* A, const double* x, double* y) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  if (lane < 6) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
-  }
-  __syncwarp();
-  if (lane < 6) y[lane] = y[lane] - s;
-  __syncwarp();
-}
-__device__ void warp_mv6(const double* A, const double* x, double* y) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  if (lane < 6) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
-  }
-  __syncwarp();
-  if (lane < 6) y[lane] = s;
-  __syncwarp();
 }
 
 // Exact solve of A dv = rhs on the island's elimination forest. Returns false if a pivot
@@ -488,59 +170,16 @@ __device__ void copy_bodies6(const Ctx& c, const double* src, double* dst) {
   for (int t = threadIdx.x; t < 6 * c.d.nb; t += blockDim.x) dst[t] = src[t];
 }
 
-// trial = base + alpha dv on the dynamic bodies; kinematic bodies keep their prescribed twist.
 __device__ void make_trial(const Ctx& c, double alpha) {
-  for (int t = threadIdx.x; t < 6 * c.d.nb; t += blockDim.x) {
-    int q = t / 6, k = t % 6;
-    int i = c.A.ib_order[c.d.body_off + q];
-    c.s.trial[t] = (i >= 0) ? c.s.base[t] + c.s.dv[6 * i + k] * alpha : c.s.base[t];
-  }
+  for (int t = threadIdx.x; t < 6 * c.d.nb; t += blockDim.x) op_trial(c, alpha, t);
 }
 
-// world twist and world momentum of every island body at the current state
 __device__ void load_world_state(const Ctx& c) {
-  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
-    int g = c.gbody(q);
-    double pose[8], mom[6], I9[9];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) mom[k] = c.W.mom[(size_t)k * c.W.n + g];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
-    bool kin = c.W.kinematic[g] != 0;
-    double wv[6];
-    world_velocity(pose, mom, I9, c.W.diagonal[g] != 0, kin, c.W.mass[g], wv);
-    double mb[6], pw[6], p6[6];
-    screw_from6(mom, mb);
-    wrench_transport(mb, pose, pw);
-    screw_to6(pw, p6);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) { c.s.vm[6 * q + k] = wv[k]; c.s.snap[6 * q + k] = p6[k]; }
-  }
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) op_load_world_state(c, q);
 }
 
-// external wrench per island body: gravity (F, p x F) frozen over the whole step
 __device__ void load_external(const Ctx& c) {
-  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) {
-    double* e = c.s.ext + 6 * q;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) e[k] = 0.0;
-    if (c.P.splits <= 0) continue;
-    int g = c.gbody(q);
-    int il = g - c.P.wbody_off;
-    double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
-    double f[3];
-    for (int k = 0; k < 3; ++k) {
-      double acc = 0.0;
-      for (int s = 0; s < c.P.splits; ++s) acc += c.P.part[(size_t)s * 3 * c.P.nw + (size_t)k * c.P.nw + il];
-      f[k] = c.P.G * pm.w * acc;
-    }
-    e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
-    e[3] = pm.y * f[2] - pm.z * f[1];
-    e[4] = pm.z * f[0] - pm.x * f[2];
-    e[5] = pm.x * f[1] - pm.y * f[0];
-  }
+  for (int q = threadIdx.x; q < c.d.nb; q += blockDim.x) op_load_external(c, q);
 }
 
 struct SolveOut { bool converged; double best; bool assembled; double a_norm2; };
@@ -584,7 +223,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
     tm.lap(PH_POST);
     if (rnorm <= c.P.tol2) { o.converged = true; break; }
     if (!(rnorm < kHuge)) break;
-    o.a_norm2 = phase_assemble(c, half, red);
+    o.a_norm2 = phase_assemble<MIXED>(c, half, red);
     o.assembled = true;
     tm.lap(PH_ASSEMBLE);
     phase_solve(c, flag);
@@ -597,7 +236,7 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
     __syncthreads();
     int accepted = -1;
     double alpha = 1.0;
-    for (int lane = 0; lane < 8; ++lane) {
+    for (int lane = 0; lane < kLineSearchLanes; ++lane) {
       make_trial(c, alpha);
       __syncthreads();
       phase_pre(c, c.s.trial, half);
@@ -623,62 +262,16 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
   return o;
 }
 
-__device__ bool log2_floor(double v, int* e) {
-  if (!(v > 0.0)) return false;
-  double x = v;
-  int k = 0;
-  while (x >= 2.0) { x /= 2.0; ++k; if (k > 250) return false; }
-  while (x < 1.0 && k > -250) { x *= 2.0; --k; }
-  *e = k;
-  return true;
-}
-__device__ int div_euclid(int a, int b) { int q = a / b; if (a % b < 0) q -= 1; return q; }
-
 __device__ bool signal_log2(const Ctx& c, const SolveOut& o, double* red, int* r) {
   if (!o.assembled) return false;
   double s = 0.0;
   for (int t = threadIdx.x; t < 36 * c.d.m; t += blockDim.x) s += c.s.mass0[t] * c.s.mass0[t];
   double massn = block_sum(s, red);
-  double stiff = ScalarTraits<double>::eff_zero(massn) ? 0.0 : o.a_norm2 / massn;
-  return log2_floor(stiff, r);
+  return signal_from_norms(o.assembled, o.a_norm2, massn, r);
 }
 
-// commit_span (newton.rs:708-753)
 __device__ void commit_span(const Ctx& c, double span, double half, bool converged) {
-  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) {
-    int q = c.A.dn_body[c.d.dyn_off + i];
-    int g = c.gbody(q);
-    double m0[8], vb[6], e[8], pm[8], inv[8], vbody[6], v6[6], I9[9];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) m0[k] = c.W.pose[(size_t)k * c.W.n + g];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
-    screw_from6(c.s.vm + 6 * q, vb);
-    twist_exp(vb, half, e);
-    motor_compose(m0, e, pm);
-    motor_reverse(pm, inv);
-    twist_transport(vb, inv, vbody);
-    screw_to6(vbody, v6);
-    double p6[6], pb[6], pw[6], psm[6];
-    inertia_apply(I9, c.W.diagonal[g] != 0, false, c.W.mass[g], v6, p6);
-    screw_from6(p6, pb);
-    wrench_transport(pb, pm, pw);
-    screw_to6(pw, psm);
-    double pnew[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) pnew[k] = converged ? psm[k] * 2.0 - c.s.snap[6 * q + k] : psm[k];
-    double en[8], mnew[8], minv[8], pnb[6], pbody[6], out6[6];
-    twist_exp(vb, span, en);
-    motor_compose(m0, en, mnew);
-    motor_reverse(mnew, minv);
-    screw_from6(pnew, pnb);
-    wrench_transport(pnb, minv, pbody);
-    screw_to6(pbody, out6);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) c.W.pose[(size_t)k * c.W.n + g] = mnew[k];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) c.W.mom[(size_t)k * c.W.n + g] = out6[k];
-  }
+  for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) op_commit(c, span, half, converged, i);
 }
 
 template <bool MIXED>
@@ -702,26 +295,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDevi
                                            static_cast<unsigned long long>(phase_acc[threadIdx.x]));
       break;
     }
-    Ctx c;
-    c.A = A;
-    c.island = queue[k];
-    c.d = A.desc[c.island];
-    if (!W.w_active[c.d.world]) continue;  // the world holds this step
-    c.W = W;
-    c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
-    {
-      const exg_step_params_t& wp = W.wparams[c.d.world];
-      c.P.dt = wp.dt;
-      c.P.warp = wp.warp;
-      c.P.tol2 = wp.tol * wp.tol;
-      c.P.G = wp.G;
-      c.P.max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
-      c.P.pose_factor_scale = (wp.newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) ? 0.5 : 1.0;
-      c.P.splits = W.w_splits[c.d.world];
-      c.P.nw = W.w_n[c.d.world];
-      c.P.wbody_off = W.w_body_off[c.d.world];
-      c.P.part = W.grav_partial + W.w_poff[c.d.world];
-    }
+    const int island = queue[k];
+    if (!W.w_active[A.desc[island].world]) continue;  // the world holds this step
+    Ctx c = make_ctx(A, W, island);
     load_external(c);
     __syncthreads();
     unsigned long long remaining = 1ull << kMaxDepth;
@@ -782,6 +358,12 @@ long long newton_footprint_bytes(int nb, int nj) {
 }
 
 NewtonWorld::~NewtonWorld() {
+  if (wave_graph_) cudaGraphExecDestroy(wave_graph_);
+  if (h_live_) cudaFreeHost(h_live_);
+  for (DevArr<int>* a : {&dw_isl_, &dw_dyn_first_, &dw_live_}) a->release();
+  for (DevArr<int2>* a : {&dw_body_, &dw_dyn_, &dw_joint_, &dw_cell_, &dw_level_}) a->release();
+  dw_ctl_.release();
+  dw_nodesq_.release();
   d_desc.release();
   for (DevArr<int>* a : {&d_isl_body, &d_jl_law, &d_jl_a, &d_jl_b, &d_ib_order, &d_ib_inc_ptr, &d_ib_inc_ref, &d_dn_body,
                          &d_dn_parent, &d_lv_ptr, &d_lv_nodes, &d_ch_ptr, &d_ch_idx, &d_cell_ptr, &d_cell_terms, &d_stats,
@@ -1087,9 +669,10 @@ int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
     std::vector<long long> z(kPhases, 0);
     if ((rc = d_phase.assign(z.data(), kPhases, s)) != EXG_OK) return rc;
   }
-  // queue of live islands, largest first, then the scheduler's counter
+  // queue of the island kernel's live islands, largest first, then the scheduler's counter
   std::vector<int> q;
-  for (int I = 0; I < (int)desc_.size(); ++I) if (alive_[I]) q.push_back(I);
+  for (int I = 0; I < (int)desc_.size(); ++I) if (alive_[I] && !wave_island(desc_[I])) q.push_back(I);
+  n_cta_ = (int)q.size();
   std::stable_sort(q.begin(), q.end(),
                    [&](int a, int b) { return desc_[a].nb + desc_[a].nj > desc_[b].nb + desc_[b].nj; });
   q.push_back(0);
@@ -1098,16 +681,17 @@ int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
                            d_ib_order.ptr,  d_ib_inc_ptr.ptr, d_ib_inc_ref.ptr, d_dn_body.ptr, d_dn_parent.ptr, d_lv_ptr.ptr,
                            d_lv_nodes.ptr,  d_ch_ptr.ptr,   d_ch_idx.ptr,   d_cell_ptr.ptr,  d_cell_terms.ptr, d_scratch.ptr,
                            d_stats.ptr,     d_residual.ptr, d_phase.ptr};
+  if ((rc = build_wave(s)) != EXG_OK) return rc;
   dirty_ = false;
   return EXG_OK;
 }
 
 int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
-  if (n_live_ == 0) return EXG_OK;
+  if (n_cta_ == 0) return EXG_OK;
   if (dirty_) return EXG_ERR_INVALID_ARGUMENT;  // sync() first
   WorldRef W{w.pose,    w.mom,    w.mass,   w.inertia, w.kinematic,  w.diagonal, w.pos_mass,
              w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
-  int* head = d_queue.ptr + n_live_;
+  int* head = d_queue.ptr + n_cta_;
   // persistent CTAs: as many as can be resident at once
   static int resident[2] = {0, 0};
   const int mixed = w.precision == EXG_PRECISION_MIXED;
@@ -1117,13 +701,13 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<false>, kThreads, 0);
     resident[mixed] = (e == cudaSuccess && per_sm > 0) ? per_sm : 1;
   }
-  int grid = std::min(n_live_, std::max(1, dev->sm_count) * resident[mixed]);
+  int grid = std::min(n_cta_, std::max(1, dev->sm_count) * resident[mixed]);
   EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
   int tok = prof_begin(dev, PROF_NEWTON, s);
   if (mixed)
-    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);
+    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
   else
-    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_live_, head);
+    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

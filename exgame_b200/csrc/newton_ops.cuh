@@ -1,0 +1,521 @@
+// Per-item operations of the device Newton step, shared by the two schedules that run it:
+//   the island kernel (one CTA per island, newton.cu) and
+//   the wave schedule (every phase a grid-wide kernel over all large islands, newton_wave.cu).
+// Each operation works on one body, joint task, dynamic node or assembly cell of one island, so
+// both schedules do the same arithmetic in the same order for every item; only the order in
+// which items run differs, and no result depends on it.
+#pragma once
+#include "body.cuh"
+#include "joint_eval.cuh"
+#include "world_newton.cuh"
+
+namespace exg_newton {
+
+using namespace exg;
+
+constexpr int kMaxDepth = 8;        // solve_step budget: MAX_DEPTH (newton.rs:63-74)
+constexpr int kThresholdLog2 = 8;   // THRESHOLD_LOG2
+constexpr int kPerHalvingLog2 = 4;  // PER_HALVING_LOG2
+constexpr double kHuge = 1e9;
+constexpr double kFloor2 = 1e-9 * 1e-9;
+constexpr int kJacStride = 42;  // per (joint, slice): value[6] + d[36]
+constexpr int kLineSearchLanes = 8;
+
+struct Scratch {
+  double *vm, *base, *best, *trial, *mid, *snap, *ext, *conn, *jac, *mass, *mass0, *rhs, *scale, *D, *Dinv, *Acp, *Apc, *S,
+      *bvec, *dv;
+};
+
+EXG_HD long long scratch_doubles(int nb, int nj, int m) {
+  return (long long)nb * (6 * 4 + 8 + 6 * 2) + (long long)nj * (6 + 4 * kJacStride) + (long long)m * (36 * 7 + 6 * 3 + 2);
+}
+
+__device__ inline Scratch carve(double* p, int nb, int nj, int m) {
+  Scratch s;
+  s.vm = p; p += nb * 6;
+  s.base = p; p += nb * 6;
+  s.best = p; p += nb * 6;
+  s.trial = p; p += nb * 6;
+  s.mid = p; p += nb * 8;
+  s.snap = p; p += nb * 6;
+  s.ext = p; p += nb * 6;
+  s.conn = p; p += (size_t)nj * 6;
+  s.jac = p; p += (size_t)nj * 4 * kJacStride;
+  s.mass = p; p += (size_t)m * 36;
+  s.mass0 = p; p += (size_t)m * 36;
+  s.rhs = p; p += (size_t)m * 6;
+  s.scale = p; p += (size_t)m * 2;
+  s.D = p; p += (size_t)m * 36;
+  s.Dinv = p; p += (size_t)m * 36;
+  s.Acp = p; p += (size_t)m * 36;
+  s.Apc = p; p += (size_t)m * 36;
+  s.S = p; p += (size_t)m * 36;
+  s.bvec = p; p += (size_t)m * 6;
+  s.dv = p; p += (size_t)m * 6;
+  return s;
+}
+
+struct WorldRef {
+  double* pose;
+  double* mom;
+  const double* mass;
+  const double* inertia;
+  const int* kinematic;
+  const int* diagonal;
+  const double* pos_mass;
+  const double* grav_partial;
+  const exg_step_params_t* wparams;
+  const long long* w_poff;
+  const int* w_splits;
+  const int* w_n;
+  const int* w_body_off;
+  const int* w_active;
+  int n;
+};
+
+// The island's world parameters.
+struct IslandParams {
+  double dt, warp, tol2, G, pose_factor_scale;
+  int max_newton;
+  int splits, nw, wbody_off;
+  const double* part;
+};
+
+struct Ctx {
+  NewtonDeviceArrays A;
+  IslandDesc d;
+  WorldRef W;
+  IslandParams P;
+  Scratch s;
+  int island;
+  EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
+};
+
+__device__ inline void resolve_params(Ctx& c) {
+  const exg_step_params_t& wp = c.W.wparams[c.d.world];
+  c.P.dt = wp.dt;
+  c.P.warp = wp.warp;
+  c.P.tol2 = wp.tol * wp.tol;
+  c.P.G = wp.G;
+  c.P.max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
+  c.P.pose_factor_scale = (wp.newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) ? 0.5 : 1.0;
+  c.P.splits = c.W.w_splits[c.d.world];
+  c.P.nw = c.W.w_n[c.d.world];
+  c.P.wbody_off = c.W.w_body_off[c.d.world];
+  c.P.part = c.W.grav_partial + c.W.w_poff[c.d.world];
+}
+
+__device__ inline Ctx make_ctx(const NewtonDeviceArrays& A, const WorldRef& W, int island) {
+  Ctx c;
+  c.A = A;
+  c.W = W;
+  c.island = island;
+  c.d = A.desc[island];
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  resolve_params(c);
+  return c;
+}
+
+// The island's structure and scratch only (for operations that read no world parameter).
+__device__ inline Ctx make_ctx_lite(const NewtonDeviceArrays& A, const WorldRef& W, int island) {
+  Ctx c;
+  c.A = A;
+  c.W = W;
+  c.island = island;
+  c.d = A.desc[island];
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  return c;
+}
+
+__device__ inline double nan_max(double a, double b) {
+  if (a != a || b != b) return __longlong_as_double(0x7ff8000000000000ULL);
+  return a > b ? a : b;
+}
+
+// ── per-item operations ─────────────────────────────────────────────────────
+// PRE (functions::pre): mid = exp(half/2 x) * pose of island body q.
+__device__ inline void op_pre(const Ctx& c, const double* x, double half, int q) {
+  int g = c.gbody(q);
+  double pose[8], vb[6], e[8], m[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+  screw_from6(x + 6 * q, vb);
+  twist_exp(vb, half, e);
+  motor_compose(pose, e, m);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c.s.mid[8 * q + k] = m[k];
+}
+
+// Jacobian slice storage: FP32 in the mixed path (the slices are FP32 duals, so nothing is lost),
+// FP64 otherwise. Slice s of joint q: value[6] then d[36], at (q * 4 + s) * kJacStride.
+template <bool MIXED> struct JacType { typedef double T; };
+template <> struct JacType<true> { typedef float T; };
+template <bool MIXED>
+__device__ inline typename JacType<MIXED>::T* jac_slice(const Ctx& c, int q, int slice) {
+  return reinterpret_cast<typename JacType<MIXED>::T*>(c.s.jac) + ((size_t)q * 4 + slice) * kJacStride;
+}
+
+// The FP64 value of joint q at (mid, x): conn[q] = the wrench on end a. LAW >= 0 promises the
+// joint's law at compile time (the other laws' code then drops out of the caller).
+template <int LAW = -1>
+__device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
+  const int joff = c.d.joint_off;
+  const int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
+  double out[12];
+  joint_plain<double>(LAW >= 0 ? LAW : c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a, c.s.mid + 8 * b,
+                      x + 6 * a, x + 6 * b, c.P.dt, c.P.warp, out);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
+}
+
+// Jacobian slice `slice` of joint q at (mid, x). MIXED evaluates the derivative slices in FP32
+// duals; the values that enter the residual always come from an FP64 evaluation (op_joint_value,
+// or in FP64 the dual's value part, which equals it bit for bit: write_conn on slice 0), so the
+// converged iterate is an FP64 solution whatever the Jacobian's precision.
+template <bool MIXED, int LAW = -1>
+__device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int slice, bool write_conn) {
+  const int joff = c.d.joint_off;
+  const int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
+  const int law = LAW >= 0 ? LAW : c.A.jl_law[joff + q];
+  const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
+  if (MIXED) {
+    float* o = jac_slice<true>(c, q, slice);
+    float pa[8], pb[8], va[6], vb[6], val[6], dd[36];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { pa[k] = float(c.s.mid[8 * a + k]); pb[k] = float(c.s.mid[8 * b + k]); }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { va[k] = float(x[6 * a + k]); vb[k] = float(x[6 * b + k]); }
+    joint_jacobian_slice<float>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, val, dd);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) o[r] = val[r];
+#pragma unroll
+    for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+  } else {
+    double* o = jac_slice<false>(c, q, slice);
+    double val[6], dd[36];
+    joint_jacobian_slice<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, x + 6 * a, x + 6 * b, c.P.dt, c.P.warp,
+                                 slice, val, dd);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) o[r] = val[r];
+#pragma unroll
+    for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+    if (write_conn && slice == 0) {
+#pragma unroll
+      for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
+    }
+  }
+}
+
+// Joint q at (mid, x): Jacobian slice `slice` with, on slice 0, the joint's value (jac), or the
+// value alone (slice 0 only).
+template <bool MIXED>
+__device__ inline void op_joint(const Ctx& c, const double* x, int q, int slice, bool jac) {
+  if (!jac) {
+    op_joint_value(c, x, q);
+    return;
+  }
+  op_joint_slice<MIXED>(c, x, q, slice, true);
+  if (MIXED && slice == 0) op_joint_value(c, x, q);
+}
+
+// Gather + POST (functions::gather_term, body_post) of dynamic node i: mass block, residual and
+// its scales; returns the node's worst relative residual^2 (newton.rs:139-151).
+__device__ inline double op_post(const Ctx& c, const double* x, double half, int i) {
+  double worst = 0.0;
+  int q = c.A.dn_body[c.d.dyn_off + i];
+  int g = c.gbody(q);
+  double tot[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) tot[k] = c.s.ext[6 * q + k];
+  int p0 = c.A.ib_inc_ptr[c.d.inc_off + q], p1 = c.A.ib_inc_ptr[c.d.inc_off + q + 1];
+  for (int t = p0; t < p1; ++t) {
+    int ref = c.A.ib_inc_ref[t];
+    int jq = ref >> 1;
+    if (ref & 1) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) tot[k] = tot[k] - c.s.conn[6 * jq + k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) tot[k] = tot[k] + c.s.conn[6 * jq + k];
+    }
+  }
+  double I9[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+  const bool diag = c.W.diagonal[g] != 0;
+  const double mass = c.W.mass[g];
+  const double* mid = c.s.mid + 8 * q;
+  double inv[8];
+  motor_reverse(mid, inv);
+  double* blk = c.s.mass + 36 * (size_t)i;
+#pragma unroll
+  for (int col = 0; col < 6; ++col) {
+    double e6[6] = {0, 0, 0, 0, 0, 0};
+    e6[col] = 1.0;
+    double eb[6], ebody[6], b6[6], wv[6], p6[6], pb[6], cw[6], c6[6];
+    screw_from6(e6, eb);
+    twist_transport(eb, inv, ebody);
+    screw_to6(ebody, b6);
+    wv[0] = b6[0]; wv[1] = b6[1]; wv[2] = b6[2]; wv[3] = b6[3]; wv[4] = b6[4]; wv[5] = b6[5];
+    inertia_apply(I9, diag, false, mass, wv, p6);
+    screw_from6(p6, pb);
+    wrench_transport(pb, mid, cw);
+    screw_to6(cw, c6);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) blk[r * 6 + col] = c6[r];
+  }
+  const double* vv = x + 6 * q;
+  double p[6], nn[6], hh[6], res[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) acc += blk[r * 6 + k] * vv[k];
+    p[r] = acc;
+    nn[r] = c.s.snap[6 * q + r];
+    hh[r] = tot[r] * half;
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) res[r] = -(p[r] - nn[r] - hh[r]);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) c.s.rhs[6 * i + r] = res[r];
+  auto sq3 = [](const double* v) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; };
+  double lin = fmax(fmax(fmax(sq3(p), sq3(nn)), sq3(hh)), kFloor2);
+  double ang = fmax(fmax(fmax(sq3(p + 3), sq3(nn + 3)), sq3(hh + 3)), kFloor2);
+  c.s.scale[2 * i] = lin;
+  c.s.scale[2 * i + 1] = ang;
+  worst = nan_max(worst, sq3(res) / lin);
+  worst = nan_max(worst, sq3(res + 3) / ang);
+  return worst;
+}
+
+// Assembly entry e of cell (node i, kind): kind 0 the diagonal block, 1 (node row, parent col),
+// 2 (parent row, node col) (rows/assemble.rs, functions::assemble_term): the mass block (diagonal
+// only) then every contributing joint end in joint order with the mid-point factors pf on pose
+// columns and vf on velocity columns: pf = -half^2 (times the pose factor scale), vf = -half.
+// Writes the entry; *counts says whether it enters ||A||_F.
+template <bool MIXED>
+__device__ inline double op_assemble(const Ctx& c, double pf, double vf, int cell, int e, bool* counts) {
+  int i = cell / 3, kind = cell % 3;
+  int r = e / 6, col = e % 6;
+  double acc = (kind == 0) ? c.s.mass0[36 * (size_t)i + e] : 0.0;
+  int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+  for (int k = p0; k < p1; ++k) {
+    int term = c.A.cell_terms[k];
+    int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
+    const auto* jp = jac_slice<MIXED>(c, q, ce) + 6;
+    const auto* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
+    double pv = double(jp[r * 6 + col]), vv = double(jv[r * 6 + col]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc = acc + pf * pv + vf * vv;
+  }
+  double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
+  dst[36 * (size_t)i + e] = acc;
+  *counts = kind == 0 || c.A.dn_parent[c.d.dyn_off + i] >= 0;
+  return acc;
+}
+
+// trial entry t (body t/6, component t%6) = base + alpha dv on dynamic bodies; kinematic bodies
+// keep their prescribed twist.
+__device__ inline void op_trial(const Ctx& c, double alpha, int t) {
+  int q = t / 6, k = t % 6;
+  int i = c.A.ib_order[c.d.body_off + q];
+  c.s.trial[t] = (i >= 0) ? c.s.base[t] + c.s.dv[6 * i + k] * alpha : c.s.base[t];
+}
+
+// World twist (vm) and world momentum (snap) of island body q at the current state.
+__device__ inline void op_load_world_state(const Ctx& c, int q) {
+  int g = c.gbody(q);
+  double pose[8], mom[6], I9[9];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) mom[k] = c.W.mom[(size_t)k * c.W.n + g];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+  bool kin = c.W.kinematic[g] != 0;
+  double wv[6];
+  world_velocity(pose, mom, I9, c.W.diagonal[g] != 0, kin, c.W.mass[g], wv);
+  double mb[6], pw[6], p6[6];
+  screw_from6(mom, mb);
+  wrench_transport(mb, pose, pw);
+  screw_to6(pw, p6);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) { c.s.vm[6 * q + k] = wv[k]; c.s.snap[6 * q + k] = p6[k]; }
+}
+
+// External wrench of island body q: gravity (F, p x F), frozen over the whole step.
+__device__ inline void op_load_external(const Ctx& c, int q) {
+  double* e = c.s.ext + 6 * q;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) e[k] = 0.0;
+  if (c.P.splits <= 0) return;
+  int g = c.gbody(q);
+  int il = g - c.P.wbody_off;
+  double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
+  double f[3];
+  for (int k = 0; k < 3; ++k) {
+    double acc = 0.0;
+    for (int s = 0; s < c.P.splits; ++s) acc += c.P.part[(size_t)s * 3 * c.P.nw + (size_t)k * c.P.nw + il];
+    f[k] = c.P.G * pm.w * acc;
+  }
+  e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
+  e[3] = pm.y * f[2] - pm.z * f[1];
+  e[4] = pm.z * f[0] - pm.x * f[2];
+  e[5] = pm.x * f[1] - pm.y * f[0];
+}
+
+// commit_span (newton.rs:708-753) for dynamic node i: M = M0 * exp(span v), P = 2 P_mid - P_n
+// (P_mid itself when the span did not converge).
+__device__ inline void op_commit(const Ctx& c, double span, double half, bool converged, int i) {
+  int q = c.A.dn_body[c.d.dyn_off + i];
+  int g = c.gbody(q);
+  double m0[8], vb[6], e[8], pm[8], inv[8], vbody[6], v6[6], I9[9];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) m0[k] = c.W.pose[(size_t)k * c.W.n + g];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
+  screw_from6(c.s.vm + 6 * q, vb);
+  twist_exp(vb, half, e);
+  motor_compose(m0, e, pm);
+  motor_reverse(pm, inv);
+  twist_transport(vb, inv, vbody);
+  screw_to6(vbody, v6);
+  double p6[6], pb[6], pw[6], psm[6];
+  inertia_apply(I9, c.W.diagonal[g] != 0, false, c.W.mass[g], v6, p6);
+  screw_from6(p6, pb);
+  wrench_transport(pb, pm, pw);
+  screw_to6(pw, psm);
+  double pnew[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) pnew[k] = converged ? psm[k] * 2.0 - c.s.snap[6 * q + k] : psm[k];
+  double en[8], mnew[8], minv[8], pnb[6], pbody[6], out6[6];
+  twist_exp(vb, span, en);
+  motor_compose(m0, en, mnew);
+  motor_reverse(mnew, minv);
+  screw_from6(pnew, pnb);
+  wrench_transport(pnb, minv, pbody);
+  screw_to6(pbody, out6);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) c.W.pose[(size_t)k * c.W.n + g] = mnew[k];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) c.W.mom[(size_t)k * c.W.n + g] = out6[k];
+}
+
+// ── warp-cooperative 6x6 block operations of the tree solve ─────────────────
+// Inverse by Gauss-Jordan with partial pivoting: lane c < 12 holds column c of [A | I]. Returns
+// false (to every lane) if a pivot is zero or not finite.
+__device__ inline bool warp_inverse6(const double* a, double* out) {
+  const int lane = threadIdx.x & 31;
+  double col[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    if (lane < 6) col[r] = a[r * 6 + lane];
+    else col[r] = (lane - 6 == r) ? 1.0 : 0.0;
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(col[k]);
+#pragma unroll
+    for (int r = k + 1; r < 6; ++r) {
+      double x = fabs(col[r]);
+      if (x > best) { best = x; piv = r; }
+    }
+    piv = __shfl_sync(0xffffffffu, piv, k);
+    double tk = col[k], tp = col[k];
+#pragma unroll
+    for (int r = k; r < 6; ++r) if (r == piv) tp = col[r];
+#pragma unroll
+    for (int r = k; r < 6; ++r) if (r == piv) col[r] = tk;
+    col[k] = tp;
+    double pv = __shfl_sync(0xffffffffu, col[k], k);
+    if (!(fabs(pv) > 0.0) || !isfinite(pv)) ok = false;
+    double ip = 1.0 / pv;
+    col[k] = col[k] * ip;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r == k) continue;
+      double f = __shfl_sync(0xffffffffu, col[r], k);
+      col[r] = col[r] - f * col[k];
+    }
+  }
+  if (lane >= 6 && lane < 12) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) out[r * 6 + (lane - 6)] = col[r];
+  }
+  __syncwarp();
+  return ok;
+}
+
+// C = A * B (6x6, row-major) or C -= A * B, computed by one warp.
+template <bool Sub>
+__device__ inline void warp_mm6(const double* A, const double* B, double* C) {
+  const int lane = threadIdx.x & 31;
+  double v0 = 0.0, v1 = 0.0;
+  int e0 = lane, e1 = lane + 32;
+  {
+    int r = e0 / 6, cc = e0 % 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v0 += A[r * 6 + k] * B[k * 6 + cc];
+  }
+  if (e1 < 36) {
+    int r = e1 / 6, cc = e1 % 6;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v1 += A[r * 6 + k] * B[k * 6 + cc];
+  }
+  __syncwarp();
+  if (Sub) {
+    C[e0] = C[e0] - v0;
+    if (e1 < 36) C[e1] = C[e1] - v1;
+  } else {
+    C[e0] = v0;
+    if (e1 < 36) C[e1] = v1;
+  }
+  __syncwarp();
+}
+// y -= A x (6x6 * 6) by one warp (lanes 0..5)
+__device__ inline void warp_mv6_sub(const double* A, const double* x, double* y) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  if (lane < 6) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
+  }
+  __syncwarp();
+  if (lane < 6) y[lane] = y[lane] - s;
+  __syncwarp();
+}
+__device__ inline void warp_mv6(const double* A, const double* x, double* y) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  if (lane < 6) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += A[lane * 6 + k] * x[k];
+  }
+  __syncwarp();
+  if (lane < 6) y[lane] = s;
+  __syncwarp();
+}
+
+// ── scalar helpers of the span budget ───────────────────────────────────────
+__device__ inline bool log2_floor(double v, int* e) {
+  if (!(v > 0.0)) return false;
+  double x = v;
+  int k = 0;
+  while (x >= 2.0) { x /= 2.0; ++k; if (k > 250) return false; }
+  while (x < 1.0 && k > -250) { x *= 2.0; --k; }
+  *e = k;
+  return true;
+}
+__device__ inline int div_euclid(int a, int b) { int q = a / b; if (a % b < 0) q -= 1; return q; }
+
+// signal_log2 (newton.rs:812-861) from ||A||_F^2 and the mass blocks' ||M||_F^2.
+__device__ inline bool signal_from_norms(bool assembled, double a_norm2, double massn, int* r) {
+  if (!assembled) return false;
+  double stiff = ScalarTraits<double>::eff_zero(massn) ? 0.0 : a_norm2 / massn;
+  return log2_floor(stiff, r);
+}
+
+}  // namespace exg_newton

@@ -1,0 +1,723 @@
+// Wave schedule of the device Newton step for large islands.
+//
+// The island kernel (newton.cu) gives every island one CTA, which leaves a large island's
+// thousands of bodies to 256 threads while the rest of the GPU may sit idle. The wave schedule
+// runs the same step with every phase as a grid-wide kernel over the items of ALL large islands
+// at once, and keeps each island's control flow — the span budget loop of Newton::solve_step
+// (crates/newton/src/integrator/implicit/newton.rs:543-683), the Newton iterations and the
+// backtracking line search of newton_solve (:334-530) — as a per-island state machine that small
+// control kernels advance between the data phases. One "round" evaluates every island once (a
+// Newton iterate or a line-search probe) and, where the island needs it, assembles and solves for
+// a new direction or ends its span; rounds repeat until every island has finished the step.
+//
+// The per-item arithmetic is the island kernel's (newton_ops.cuh), and every reduction over an
+// island's items runs in a fixed order (maxima through order-independent integer atomics, sums
+// warp-strided in index order), so a world's result does not depend on the other islands in the
+// wave. A round is one CUDA graph, captured once per structural change.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+#include "newton_ops.cuh"
+
+namespace {
+
+using namespace exg_newton;
+
+enum WaveState { WS_START = 0, WS_ITER = 1, WS_PROBE = 2, WS_DIR = 3, WS_END = 4, WS_DONE = 5 };
+enum WaveEval { EV_NONE = 0, EV_FULL = 1, EV_JAC = 2, EV_PLAIN = 3 };
+enum WaveFlag {
+  F_START = 1,       // load the world state, best = vm
+  F_COPY_BEST = 2,   // best = vm
+  F_MASS0 = 4,       // mass0 = mass
+  F_ACCEPT = 8,      // vm = trial
+  F_BASE = 16,       // base = vm
+  F_TRIAL = 32,      // trial = base + alpha dv
+  F_COMMIT = 64,     // commit the span
+};
+
+struct WaveCtl {
+  unsigned long long remaining;  // span budget units left (of 2^kMaxDepth)
+  unsigned long long worst_bits; // max of the round's node residuals (non-negative doubles order as integers)
+  double span, half, pf, vf, best, rnorm, carried_norm, alpha, a_norm2, massn, last_best;
+  int state, eval, flags, depth;
+  int spans, iters, maxdepth, it;
+  int carried, lane, converged, assembled;
+  int nz, singular, commit_converged, active;
+};
+
+struct WaveArgs {
+  NewtonDeviceArrays A;
+  WorldRef W;
+  WaveCtl* ctl;
+  const int* isl;       // wave slot -> island
+  int n_isl;
+  const int2* body;     // (slot, island body)
+  int n_body;
+  const int2* dyn;      // (slot, dynamic node)
+  int n_dyn;
+  const int2* joint;    // (slot, island joint)
+  int n_joint;
+  const int2* cell;     // (slot, assembly cell)
+  int n_cell;
+  const int2* level;    // (slot, node) grouped by elimination level
+  const int* dyn_first; // first dynamic-node item of each wave slot (n_isl + 1 entries)
+  double* nodesq;       // per dynamic-node item: a sum of squares to reduce per island
+  int* live;            // islands not yet done after the round
+};
+
+int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
+  long long g = (items + threads - 1) / threads;
+  long long cap = (long long)std::max(1, dev->sm_count) * per_sm;
+  return (int)std::max<long long>(1, std::min(g, cap));
+}
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
+
+// ── per-island control ──────────────────────────────────────────────────────
+// Step start: every island of an active world begins its span budget; load the external wrench.
+__global__ void k_w_init(WaveArgs a) {
+  for (int k = gtid(); k < a.n_isl; k += gthreads()) {
+    WaveCtl& c = a.ctl[k];
+    const IslandDesc& d = a.A.desc[a.isl[k]];
+    c.active = a.W.w_active[d.world];
+    c.state = c.active ? WS_START : WS_DONE;
+    c.remaining = 1ull << kMaxDepth;
+    c.depth = 0;
+    c.spans = c.iters = c.maxdepth = 0;
+    c.last_best = 0.0;
+    c.flags = 0;
+    c.eval = EV_NONE;
+  }
+}
+
+__global__ void k_w_external(WaveArgs a) {
+  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+    int2 it = a.body[t];
+    if (!a.ctl[it.x].active) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_load_external(c, it.y);
+  }
+}
+
+// Round start: islands starting a span choose its length (the top of solve_step's budget loop);
+// islands at an iterate or a probe choose what to evaluate.
+__global__ void k_w_begin(WaveArgs a) {
+  for (int k = gtid(); k < a.n_isl; k += gthreads()) {
+    WaveCtl& c = a.ctl[k];
+    c.flags = 0;
+    c.eval = EV_NONE;
+    c.worst_bits = 0ull;
+    if (c.state == WS_START) {
+      unsigned long long units = 1ull << (kMaxDepth - c.depth);
+      while (units > c.remaining) { ++c.depth; units >>= 1; }
+      const IslandDesc& d = a.A.desc[a.isl[k]];
+      double span = a.W.wparams[d.world].dt;
+      for (int t = 0; t < c.depth; ++t) span = span / 2.0;
+      c.span = span;
+      c.half = span / 2.0;
+      const double scale = (a.W.wparams[d.world].newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) ? 0.5 : 1.0;
+      c.pf = -(c.half * c.half) * scale;
+      c.vf = -c.half;
+      ++c.spans;
+      c.maxdepth = max(c.maxdepth, c.depth);
+      c.best = kHuge;
+      c.converged = 0;
+      c.assembled = 0;
+      c.a_norm2 = 0.0;
+      c.carried = 0;
+      c.it = 0;
+      c.flags = F_START;
+      c.state = WS_ITER;
+    }
+    if (c.state == WS_ITER) {
+      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const exg_step_params_t& wp = a.W.wparams[d.world];
+      const int max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
+      if (c.it >= max_newton) {
+        c.state = WS_END;
+      } else {
+        ++c.iters;
+        c.eval = c.carried ? EV_JAC : EV_FULL;
+      }
+    } else if (c.state == WS_PROBE) {
+      c.eval = EV_PLAIN;
+    }
+  }
+}
+
+// After the evaluation: the iterate's convergence test or the probe's acceptance test.
+__global__ void k_w_after_eval(WaveArgs a) {
+  for (int k = gtid(); k < a.n_isl; k += gthreads()) {
+    WaveCtl& c = a.ctl[k];
+    if (c.eval == EV_FULL || c.eval == EV_JAC) {
+      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const exg_step_params_t& wp = a.W.wparams[d.world];
+      double rnorm;
+      if (c.eval == EV_JAC) {
+        rnorm = c.carried_norm;
+      } else {
+        rnorm = __longlong_as_double((long long)c.worst_bits);
+        c.flags |= F_MASS0;
+      }
+      c.carried = 0;
+      c.rnorm = rnorm;
+      if (rnorm < c.best) {
+        c.best = rnorm;
+        c.flags |= F_COPY_BEST;
+      }
+      if (rnorm <= wp.tol * wp.tol) {
+        c.converged = 1;
+        c.state = WS_END;
+      } else if (!(rnorm < kHuge)) {
+        c.state = WS_END;
+      } else {
+        c.state = WS_DIR;
+        c.nz = 0;
+        c.singular = 0;
+      }
+    } else if (c.eval == EV_PLAIN) {
+      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const exg_step_params_t& wp = a.W.wparams[d.world];
+      const int max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
+      double tnorm = __longlong_as_double((long long)c.worst_bits);
+      bool acc = tnorm < c.rnorm;
+      if (c.lane == 0 || acc) c.flags |= F_MASS0;
+      if (acc) {
+        c.flags |= F_ACCEPT;
+        c.carried = 1;
+        c.carried_norm = tnorm;
+        ++c.it;
+        c.state = c.it < max_newton ? WS_ITER : WS_END;
+      } else {
+        c.alpha = c.alpha / 2.0;
+        ++c.lane;
+        if (c.lane < kLineSearchLanes) c.flags |= F_TRIAL;
+        else c.state = WS_END;  // no probe decreased the residual: vm still holds the base
+      }
+    }
+  }
+}
+
+// After the solve: no correction at all hands over to sub-division (newton.rs:449-456);
+// otherwise the line search starts at alpha = 1.
+__global__ void k_w_after_solve(WaveArgs a) {
+  for (int k = gtid(); k < a.n_isl; k += gthreads()) {
+    WaveCtl& c = a.ctl[k];
+    c.flags &= ~(F_COPY_BEST | F_ACCEPT | F_TRIAL);  // done by the post-evaluation copy pass
+    if (c.state != WS_DIR) continue;
+    c.assembled = 1;
+    if (!c.nz) {
+      c.state = WS_END;
+      continue;
+    }
+    c.flags |= F_BASE | F_TRIAL;
+    c.lane = 0;
+    c.alpha = 1.0;
+    c.state = WS_PROBE;
+  }
+}
+
+// End of a span (the bottom of solve_step's budget loop): sub-divide, or commit and move on.
+__global__ void k_w_end(WaveArgs a) {
+  for (int k = gtid(); k < a.n_isl; k += gthreads()) {
+    WaveCtl& c = a.ctl[k];
+    c.flags &= ~(F_BASE | F_TRIAL);
+    if (c.state != WS_END) continue;
+    c.last_best = c.best;
+    const bool finite = c.best < kHuge;
+    const bool last = c.depth == kMaxDepth;
+    int r;
+    const bool sig = signal_from_norms(c.assembled != 0, c.a_norm2, c.massn, &r);
+    if (!c.converged && !last) {
+      int down = sig ? div_euclid(r - kThresholdLog2, kPerHalvingLog2) + 1 : 1;
+      c.depth += min(max(down, 1), kMaxDepth - c.depth);
+      c.state = WS_START;
+      continue;
+    }
+    if (c.converged || finite) {
+      c.flags |= F_COMMIT;
+      c.commit_converged = c.converged;
+    }
+    unsigned long long units = 1ull << (kMaxDepth - c.depth);
+    c.remaining -= units;
+    auto aligned = [&](int dd) {
+      if (dd <= 0) return false;
+      unsigned long long bigger = 1ull << (kMaxDepth - (dd - 1));
+      return bigger <= c.remaining && c.remaining % bigger == 0;
+    };
+    if (c.remaining > 0 && c.converged && aligned(c.depth) && sig) {
+      int up = div_euclid(kThresholdLog2 - r, kPerHalvingLog2);
+      while (up > 0 && aligned(c.depth)) { --c.depth; --up; }
+    }
+    if (c.remaining > 0) {
+      c.state = WS_START;
+    } else {
+      c.state = WS_DONE;
+      const int island = a.isl[k];
+      a.A.stats[4 * island + 0] = c.spans;
+      a.A.stats[4 * island + 1] = c.iters;
+      a.A.stats[4 * island + 2] = c.maxdepth;
+      a.A.stats[4 * island + 3] = (c.last_best < kHuge) ? 0 : 1;
+      a.A.residual[island] = c.last_best;
+    }
+  }
+}
+
+__global__ void k_w_count(WaveArgs a) {
+  __shared__ int n;
+  if (threadIdx.x == 0) n = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int k = threadIdx.x; k < a.n_isl; k += blockDim.x) mine += a.ctl[k].state != WS_DONE;
+  atomicAdd(&n, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) *a.live = n;
+}
+
+// ── data phases over all islands' items ─────────────────────────────────────
+__global__ void k_w_start(WaveArgs a) {
+  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+    int2 it = a.body[t];
+    if (!(a.ctl[it.x].flags & F_START)) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_load_world_state(c, it.y);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c.s.best[6 * it.y + k] = c.s.vm[6 * it.y + k];
+  }
+}
+
+__global__ void k_w_pre(WaveArgs a) {
+  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+    int2 it = a.body[t];
+    const WaveCtl& w = a.ctl[it.x];
+    if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_pre(c, w.eval == EV_FULL ? c.s.vm : c.s.trial, w.half, it.y);
+  }
+}
+
+// Joint tasks of one law (joint items are grouped by law; items [first, first + n) carry LAW),
+// one instantiation per law and task kind so each keeps its own register budget:
+//   slices: [0, 4 n) Jacobian slices, for an iterate (afresh or carried over from a probe);
+//   values: [0, n) FP64 values, for an iterate evaluated afresh (mixed path; in FP64 the slices'
+//           value parts are the values) and for a probe. A carried iterate keeps the values the
+//           accepted probe left at the same point.
+template <bool MIXED, int LAW>
+__global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
+  for (int t = gtid(); t < 4 * n; t += gthreads()) {
+    int2 it = a.joint[first + (t >> 2)];
+    const int ev = a.ctl[it.x].eval;
+    if (ev != EV_FULL && ev != EV_JAC) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_joint_slice<MIXED, LAW>(c, c.s.vm, it.y, t & 3, ev == EV_FULL);
+  }
+}
+
+template <bool MIXED, int LAW>
+__global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, int n) {
+  for (int t = gtid(); t < n; t += gthreads()) {
+    int2 it = a.joint[first + t];
+    const int ev = a.ctl[it.x].eval;
+    if (!(ev == EV_PLAIN || (ev == EV_FULL && MIXED))) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_joint_value<LAW>(c, ev == EV_PLAIN ? c.s.trial : c.s.vm, it.y);
+  }
+}
+
+template <bool MIXED, int LAW>
+void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
+  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 4LL * n, 128, 16), 128, 0, s>>>(a, first, n);
+  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, 16), 128, 0, s>>>(a, first, n);
+}
+
+template <bool MIXED>
+void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_first, cudaStream_t s) {
+  for (int L = 0; L < 4; ++L) {
+    const int first = law_first[L], n = law_first[L + 1] - first;
+    if (n == 0) continue;
+    if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, s);
+    else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, s);
+    else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, s);
+    else launch_joints_of<MIXED, 3>(dev, a, first, n, s);
+  }
+}
+
+__global__ void k_w_post(WaveArgs a) {
+  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+    int2 it = a.dyn[t];
+    WaveCtl& w = a.ctl[it.x];
+    if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    double worst = op_post(c, w.eval == EV_FULL ? c.s.vm : c.s.trial, w.half, it.y);
+    // non-negative doubles (and NaN, which must win as nan_max makes it win) order as integers
+    atomicMax(&w.worst_bits, (unsigned long long)__double_as_longlong(worst));
+  }
+}
+
+// Body copies of the control decisions, in a fixed order per body.
+__global__ void k_w_copy_bodies(WaveArgs a) {
+  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+    int2 it = a.body[t];
+    const WaveCtl& w = a.ctl[it.x];
+    const int f = w.flags;
+    if (!(f & (F_COPY_BEST | F_ACCEPT | F_BASE | F_TRIAL))) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    const int q = it.y;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (f & F_COPY_BEST) c.s.best[6 * q + k] = c.s.vm[6 * q + k];
+      if (f & F_ACCEPT) c.s.vm[6 * q + k] = c.s.trial[6 * q + k];
+      if (f & F_BASE) c.s.base[6 * q + k] = c.s.vm[6 * q + k];
+    }
+    if (f & F_TRIAL) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) op_trial(c, w.alpha, 6 * q + k);
+    }
+  }
+}
+
+// mass0 = mass, one thread per block entry (consecutive threads, consecutive entries).
+__global__ void k_w_copy_mass0(WaveArgs a) {
+  for (long long t = gtid(); t < 36LL * a.n_dyn; t += gthreads()) {
+    int2 it = a.dyn[t / 36];
+    if (!(a.ctl[it.x].flags & F_MASS0)) continue;
+    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    const size_t e = 36 * (size_t)it.y + (size_t)(t % 36);
+    c.s.mass0[e] = c.s.mass[e];
+  }
+}
+
+// Assembly, one thread per block entry (a warp covers consecutive entries of one cell, so its
+// Jacobian reads are contiguous).
+template <bool MIXED>
+__global__ void k_w_assemble(WaveArgs a) {
+  for (long long t = gtid(); t < 36LL * a.n_cell; t += gthreads()) {
+    int2 it = a.cell[t / 36];
+    const WaveCtl& w = a.ctl[it.x];
+    if (w.state != WS_DIR) continue;
+    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    bool counts;
+    op_assemble<MIXED>(c, w.pf, w.vf, it.y, (int)(t % 36), &counts);
+  }
+}
+
+// Per dynamic node, a fixed-order sum of squares: of its assembled blocks (the diagonal, and the
+// two parent couplings of a non-root node) for ||A||_F^2, or of its mass0 block for ||M||_F^2.
+__global__ void k_w_node_sq(WaveArgs a, int want_state, int mass) {
+  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+    int2 it = a.dyn[t];
+    const WaveCtl& w = a.ctl[it.x];
+    if (w.state != want_state || (mass && !w.assembled)) continue;
+    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    const size_t o = 36 * (size_t)it.y;
+    double s = 0.0;
+    if (mass) {
+      for (int e = 0; e < 36; ++e) s += c.s.mass0[o + e] * c.s.mass0[o + e];
+    } else {
+      for (int e = 0; e < 36; ++e) s += c.s.D[o + e] * c.s.D[o + e];
+      if (c.A.dn_parent[c.d.dyn_off + it.y] >= 0) {
+        for (int e = 0; e < 36; ++e) s += c.s.Acp[o + e] * c.s.Acp[o + e];
+        for (int e = 0; e < 36; ++e) s += c.s.Apc[o + e] * c.s.Apc[o + e];
+      }
+    }
+    a.nodesq[t] = s;
+  }
+}
+
+// One CTA per island: the sum of its node values, thread-strided in index order and then a
+// fixed-shape tree, so the result does not depend on scheduling.
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int want_state, int mass) {
+  __shared__ double part[kSumThreads];
+  for (int k = blockIdx.x; k < a.n_isl; k += gridDim.x) {
+    const WaveCtl& w = a.ctl[k];
+    if (w.state != want_state || (mass && !w.assembled)) continue;
+    const int first = a.dyn_first[k], count = a.dyn_first[k + 1] - first;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < count; t += kSumThreads) s += a.nodesq[first + t];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = kSumThreads / 2; h > 0; h >>= 1) {
+      if (threadIdx.x < h) part[threadIdx.x] += part[threadIdx.x + h];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (mass) a.ctl[k].massn = part[0];
+      else a.ctl[k].a_norm2 = part[0];
+    }
+    __syncthreads();
+  }
+}
+
+// Elimination, one warp per node of level L (leaves to roots): subtract the children's Schur
+// terms, invert the pivot block, and for a non-root node form its own terms for the parent —
+// S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's slot until the back
+// substitution writes dv) — so a parent only sums finished products; a root solves for dv.
+// The products and their order are the island kernel's.
+__global__ void k_w_solve_down(WaveArgs a, int first, int count) {
+  const int warp = gtid() >> 5, nwarps = gthreads() >> 5, lane = threadIdx.x & 31;
+  for (int t = warp; t < count; t += nwarps) {
+    int2 it = a.level[first + t];
+    WaveCtl& w = a.ctl[it.x];
+    if (w.state != WS_DIR) continue;
+    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    const int i = it.y;
+    double* D = c.s.D + 36 * (size_t)i;
+    double* b = c.s.bvec + 6 * i;
+    if (lane < 6) b[lane] = c.s.rhs[6 * i + lane];
+    const int* chp = c.A.ch_ptr + c.d.dyn_off;
+    for (int u = chp[i]; u < chp[i + 1]; ++u) {
+      const int ch = c.A.ch_idx[u];
+      const double* P = c.s.S + 36 * (size_t)ch;
+      D[lane] = D[lane] - P[lane];
+      if (lane < 4) D[32 + lane] = D[32 + lane] - P[32 + lane];
+      if (lane < 6) b[lane] = b[lane] - c.s.dv[6 * ch + lane];
+    }
+    __syncwarp();
+    double* Dinv = c.s.Dinv + 36 * (size_t)i;
+    bool ok = warp_inverse6(D, Dinv);
+    if (!ok && lane == 0) atomicOr(&w.singular, 1);
+    if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
+      double* S = c.s.S + 36 * (size_t)i;
+      warp_mm6<false>(c.s.Apc + 36 * (size_t)i, Dinv, S);
+      warp_mv6(S, b, c.s.dv + 6 * i);                 // q = S b
+      warp_mm6<false>(S, c.s.Acp + 36 * (size_t)i, S);  // P = S Acp, in place
+    } else {
+      warp_mv6(Dinv, b, c.s.dv + 6 * i);
+    }
+  }
+}
+
+// Back substitution, one warp per node of level L >= 1 (roots to leaves).
+__global__ void k_w_solve_up(WaveArgs a, int first, int count) {
+  const int warp = gtid() >> 5, nwarps = gthreads() >> 5;
+  for (int t = warp; t < count; t += nwarps) {
+    int2 it = a.level[first + t];
+    if (a.ctl[it.x].state != WS_DIR) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    const int i = it.y;
+    const int p = c.A.dn_parent[c.d.dyn_off + i];
+    warp_mv6_sub(c.s.Acp + 36 * (size_t)i, c.s.dv + 6 * p, c.s.bvec + 6 * i);
+    warp_mv6(c.s.Dinv + 36 * (size_t)i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+  }
+}
+
+// A singular pivot makes the whole correction NaN (the line search then rejects it); otherwise
+// record whether any component is non-zero.
+__global__ void k_w_nz(WaveArgs a) {
+  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+    int2 it = a.dyn[t];
+    WaveCtl& w = a.ctl[it.x];
+    if (w.state != WS_DIR) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    double* dv = c.s.dv + 6 * it.y;
+    int nz = 0;
+    if (w.singular) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dv[k] = __longlong_as_double(0x7ff8000000000000LL);
+      nz = 1;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) nz |= dv[k] != 0.0;
+    }
+    if (nz && !w.nz) atomicOr(&w.nz, 1);
+  }
+}
+
+// Span end: the best iterate back into vm, then (after the control kernel) the commit.
+__global__ void k_w_restore(WaveArgs a) {
+  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+    int2 it = a.body[t];
+    if (a.ctl[it.x].state != WS_END) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c.s.vm[6 * it.y + k] = c.s.best[6 * it.y + k];
+  }
+}
+
+__global__ void k_w_commit(WaveArgs a) {
+  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+    int2 it = a.dyn[t];
+    const WaveCtl& w = a.ctl[it.x];
+    if (!(w.flags & F_COMMIT)) continue;
+    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    op_commit(c, w.span, w.half, w.commit_converged != 0, it.y);
+  }
+}
+
+
+}  // namespace
+
+// ── host: wave structure and rounds ──────────────────────────────────────────
+bool NewtonWorld::wave_island(const IslandDesc& d) const {
+  return d.m >= wave_min_dyn_ && d.n_levels <= wave_max_levels_;
+}
+
+int NewtonWorld::build_wave(cudaStream_t s) {
+  std::vector<int> isl, dyn_first{0};
+  std::vector<int2> body, dyn, joint, cell;
+  int max_levels = 0;
+  for (int I = 0; I < (int)desc_.size(); ++I)
+    if (alive_[I] && wave_island(desc_[I])) isl.push_back(I);
+  for (int k = 0; k < (int)isl.size(); ++k) {
+    const IslandDesc& d = desc_[isl[k]];
+    for (int q = 0; q < d.nb; ++q) body.push_back(make_int2(k, q));
+    for (int i = 0; i < d.m; ++i) dyn.push_back(make_int2(k, i));
+    dyn_first.push_back((int)dyn.size());
+    for (int q = 0; q < d.nj; ++q) joint.push_back(make_int2(k, q));
+    for (int t = 0; t < 3 * d.m; ++t) cell.push_back(make_int2(k, t));
+    max_levels = std::max(max_levels, d.n_levels);
+  }
+  // joint items grouped by law (a warp then evaluates one law), islands in order within a law
+  auto law_of = [&](const int2& x) { return h_jl_law[desc_[isl[x.x]].joint_off + x.y]; };
+  std::stable_sort(joint.begin(), joint.end(), [&](const int2& x, const int2& y) { return law_of(x) < law_of(y); });
+  for (int L = 0; L <= 4; ++L)
+    wave_law_first_[L] = (int)(std::lower_bound(joint.begin(), joint.end(), L,
+                                                [&](const int2& x, int v) { return law_of(x) < v; }) - joint.begin());
+  // nodes by elimination level across the wave's islands
+  std::vector<std::vector<int2>> by(max_levels);
+  for (int k = 0; k < (int)isl.size(); ++k) {
+    const IslandDesc& d = desc_[isl[k]];
+    for (int L = 0; L < d.n_levels; ++L)
+      for (int u = h_lv_ptr[d.lv_off + L]; u < h_lv_ptr[d.lv_off + L + 1]; ++u)
+        by[L].push_back(make_int2(k, h_lv_nodes[d.dyn_off + u]));
+  }
+  std::vector<int2> level;
+  wave_level_ptr_.assign(1, 0);
+  for (int L = 0; L < max_levels; ++L) {
+    level.insert(level.end(), by[L].begin(), by[L].end());
+    wave_level_ptr_.push_back((int)level.size());
+  }
+  int rc = EXG_OK;
+  auto up = [&](auto& d, const auto& h) {
+    if (rc == EXG_OK) rc = d.assign(h.data(), (long long)h.size(), s);
+  };
+  up(dw_isl_, isl);
+  up(dw_dyn_first_, dyn_first);
+  up(dw_body_, body);
+  up(dw_dyn_, dyn);
+  up(dw_joint_, joint);
+  up(dw_cell_, cell);
+  up(dw_level_, level);
+  if (rc == EXG_OK) rc = dw_ctl_.reserve(std::max<long long>((long long)isl.size(), 1) * (long long)sizeof(WaveCtl), s);
+  if (rc == EXG_OK) rc = dw_nodesq_.reserve(std::max<long long>((long long)dyn.size(), 1), s);
+  if (rc == EXG_OK) rc = dw_live_.reserve(1, s);
+  if (rc != EXG_OK) return rc;
+  n_wave_ = (int)isl.size();
+  wave_counts_[0] = (int)body.size();
+  wave_counts_[1] = (int)dyn.size();
+  wave_counts_[2] = (int)joint.size();
+  wave_counts_[3] = (int)cell.size();
+  if (wave_graph_) cudaGraphExecDestroy(wave_graph_);
+  wave_graph_ = nullptr;
+  return EXG_OK;
+}
+
+int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
+  if (n_wave_ == 0) return EXG_OK;
+  WaveArgs a;
+  a.A = arr;
+  a.W = WorldRef{w.pose,    w.mom,    w.mass,   w.inertia, w.kinematic,  w.diagonal, w.pos_mass,
+                 w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
+  a.ctl = reinterpret_cast<WaveCtl*>(dw_ctl_.ptr);
+  a.isl = dw_isl_.ptr;
+  a.n_isl = n_wave_;
+  a.body = dw_body_.ptr;
+  a.n_body = wave_counts_[0];
+  a.dyn = dw_dyn_.ptr;
+  a.n_dyn = wave_counts_[1];
+  a.joint = dw_joint_.ptr;
+  a.n_joint = wave_counts_[2];
+  a.cell = dw_cell_.ptr;
+  a.n_cell = wave_counts_[3];
+  a.level = dw_level_.ptr;
+  a.dyn_first = dw_dyn_first_.ptr;
+  a.nodesq = dw_nodesq_.ptr;
+  a.live = dw_live_.ptr;
+  const bool mixed = w.precision == EXG_PRECISION_MIXED;
+  const int T = 256;
+  const int g_isl = grid_for(dev, a.n_isl, T, 4);
+  const int g_body = grid_for(dev, a.n_body, T, 8);
+  const int g_dyn = grid_for(dev, a.n_dyn, T, 8);
+  const int g_cell = grid_for(dev, 36LL * a.n_cell, T, 8);
+  const int g_entry = grid_for(dev, 36LL * a.n_dyn, T, 8);
+  const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
+  int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
+  k_w_init<<<g_isl, T, 0, s>>>(a);
+  k_w_external<<<g_body, T, 0, s>>>(a);
+  int rc = exg_after_launch(dev);
+  if (rc != EXG_OK) return rc;
+  static_assert(sizeof(WorldRef) <= sizeof(wave_graph_world_), "world snapshot too small");
+  if (wave_graph_ && std::memcmp(wave_graph_world_, &a.W, sizeof(WorldRef)) != 0) {
+    cudaGraphExecDestroy(wave_graph_);  // a world array moved since the capture
+    wave_graph_ = nullptr;
+  }
+  if (!wave_graph_) {
+    std::memcpy(wave_graph_world_, &a.W, sizeof(WorldRef));
+    // one round, captured once per structure
+    cudaGraph_t g;
+    EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    k_w_begin<<<g_isl, T, 0, s>>>(a);
+    k_w_start<<<g_body, T, 0, s>>>(a);
+    k_w_pre<<<g_body, T, 0, s>>>(a);
+    if (mixed) launch_joints_by_law<true>(dev, a, wave_law_first_, s);
+    else launch_joints_by_law<false>(dev, a, wave_law_first_, s);
+    k_w_post<<<g_dyn, T, 0, s>>>(a);
+    k_w_after_eval<<<g_isl, T, 0, s>>>(a);
+    k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+    k_w_copy_mass0<<<g_entry, T, 0, s>>>(a);
+    if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
+    else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
+    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);
+    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
+    const int nl = (int)wave_level_ptr_.size() - 1;
+    for (int L = nl - 1; L >= 0; --L) {
+      int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
+      k_w_solve_down<<<grid_for(dev, 32LL * count, T, 8), T, 0, s>>>(a, first, count);
+    }
+    for (int L = 1; L < nl; ++L) {
+      int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
+      k_w_solve_up<<<grid_for(dev, 32LL * count, T, 8), T, 0, s>>>(a, first, count);
+    }
+    k_w_nz<<<g_dyn, T, 0, s>>>(a);
+    k_w_after_solve<<<g_isl, T, 0, s>>>(a);
+    k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+    k_w_restore<<<g_body, T, 0, s>>>(a);
+    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_END, 1);
+    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_END, 1);
+    k_w_end<<<g_isl, T, 0, s>>>(a);
+    k_w_commit<<<g_dyn, T, 0, s>>>(a);
+    k_w_count<<<1, 1024, 0, s>>>(a);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    EXG_CUDA_TRY(le);
+    EXG_CUDA_TRY(e);
+    cudaError_t ie = cudaGraphInstantiate(&wave_graph_, g, 0);
+    cudaGraphDestroy(g);
+    EXG_CUDA_TRY(ie);
+    wave_graph_kernels_ = 22 + 2 * nl;
+  }
+  if (!h_live_) EXG_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&h_live_), sizeof(int)));
+  // Rounds until every island has finished the step. Each round advances every unfinished
+  // island by one evaluation, and a step takes a bounded number of them (spans x iterations x
+  // probes), so the loop's bound is never the reason it stops for a well-formed island.
+  const int kMaxRounds = (1 << kMaxDepth) * 2 * 32 * (kLineSearchLanes + 1);
+  int rounds = 0;
+  for (;;) {
+    // a few rounds between checks: nearly every island needs several
+    const int batch = rounds < 4 ? 4 : 1;
+    for (int r = 0; r < batch; ++r) {
+      EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
+      dev->launches.fetch_add(wave_graph_kernels_);
+    }
+    rounds += batch;
+    EXG_CUDA_TRY(cudaMemcpyAsync(h_live_, dw_live_.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    EXG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (*h_live_ == 0) break;
+    if (rounds >= kMaxRounds) return EXG_ERR_FATAL;
+  }
+  prof_end(dev, tok, s);
+  last_wave_rounds_ = rounds;
+  return EXG_OK;
+}

@@ -70,6 +70,20 @@ class NewtonWorld {
   // Summed SM cycles per phase since creation (kPhases values).
   int read_phase_cycles(long long* out);
   int live_islands() const { return n_live_; }
+  // Islands with at least min_dyn dynamic bodies and at most max_levels elimination levels take
+  // the wave schedule (newton_wave.cu); the others the island kernel.
+  void set_wave_threshold(int min_dyn, int max_levels) {
+    wave_min_dyn_ = min_dyn;
+    wave_max_levels_ = max_levels;
+    dirty_ = true;
+  }
+  int wave_min_dyn() const { return wave_min_dyn_; }
+  int wave_max_levels() const { return wave_max_levels_; }
+  bool has_wave() const { return n_wave_ > 0; }
+  // The wave schedule's step (host synchronous between rounds; call outside stream capture,
+  // after the step's other kernels on the same stream).
+  int run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s);
+  int last_wave_rounds() const { return last_wave_rounds_; }
 
  private:
   struct WorldSrc {  // what rebuilding a world's islands needs
@@ -80,6 +94,23 @@ class NewtonWorld {
   };
   int build_world(int slot, const WorldSrc& src);
   void compact();
+  bool wave_island(const IslandDesc& d) const;
+  int build_wave(cudaStream_t s);
+  // wave schedule
+  int wave_min_dyn_ = 32, wave_max_levels_ = 64;
+  int n_cta_ = 0, n_wave_ = 0;
+  int wave_counts_[4] = {0, 0, 0, 0};  // body, dynamic node, joint and cell items
+  int wave_law_first_[5] = {0, 0, 0, 0, 0};  // joint items of law L: [first[L], first[L+1])
+  std::vector<int> wave_level_ptr_;
+  DevArr<int> dw_isl_, dw_dyn_first_, dw_live_;
+  DevArr<int2> dw_body_, dw_dyn_, dw_joint_, dw_cell_, dw_level_;
+  DevArr<unsigned char> dw_ctl_;
+  DevArr<double> dw_nodesq_;
+  cudaGraphExec_t wave_graph_ = nullptr;
+  unsigned char wave_graph_world_[160] = {0};  // the world arrays the round graph was captured with
+  int wave_graph_kernels_ = 0;
+  int* h_live_ = nullptr;
+  int last_wave_rounds_ = 0;
   std::vector<WorldSrc> src_;
   bool dirty_ = true;
   int n_live_ = 0;

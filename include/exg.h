@@ -261,6 +261,18 @@ EXG_API int exg_server_wait(exg_server_t server, uint64_t id, int32_t timeout_ms
 EXG_API int exg_server_stats(exg_server_t server, exg_server_stats_t* out);
 EXG_API int exg_server_reset_stats(exg_server_t server);
 EXG_API int exg_server_destroy(exg_server_t server);
+/* ── schedule options of a world handle ──
+ * Implicit islands run one of two device schedules with the same per-item arithmetic: the island
+ * kernel (one CTA per island, the whole step in one launch) or the wave schedule (every phase a
+ * grid-wide kernel over all large islands, rounds of a captured graph). An island takes the wave
+ * schedule when it has at least EXG_OPT_WAVE_MIN_BODIES dynamic bodies and at most
+ * EXG_OPT_WAVE_MAX_LEVELS elimination levels. The choice depends on the island alone, so a world
+ * steps the same in every batch with the same options. */
+#define EXG_OPT_WAVE_MIN_BODIES 1
+#define EXG_OPT_WAVE_MAX_LEVELS 2
+#define EXG_OPT_LAST_WAVE_ROUNDS 3 /* read only: rounds the wave schedule ran in the last step */
+EXG_API int exg_world_set_option(exg_world_t world, int32_t option, int64_t value);
+EXG_API int exg_world_get_option(exg_world_t world, int32_t option, int64_t* value);
 /* SM clock cycles the implicit step spent per phase since the handle was created, summed over
  * islands: [0] PRE, [1] joint values + Jacobian, [2] gather + POST, [3] assembly, [4] linear
  * solve, [5] line search, [6] commit, [7] other. Zero for worlds without implicit islands. */

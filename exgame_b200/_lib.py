@@ -52,6 +52,8 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_int32)]),
     "exg_pool_release": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "exg_pool_free": (ctypes.c_int, [_vp, _vp]),
+    "exg_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "exg_host_free": (ctypes.c_int, [_vp]),
     "exg_world_footprint": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _vp, ctypes.POINTER(ctypes.c_int64)]),
     "exg_server_create": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
     "exg_server_submit": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, ctypes.c_int32, _vp, ctypes.c_int32,
@@ -241,8 +243,12 @@ class DeviceWorld:
     def step(self, n_steps=1):
         check(lib().exg_world_step(self.handle, int(n_steps)), "exg_world_step")
 
-    def bodies(self):
-        out = np.zeros(self.n, dtype=BODY_DTYPE)
+    def bodies(self, out=None):
+        """Every body of the handle (into `out` when given, e.g. a host_bodies buffer)."""
+        if out is None:
+            out = np.zeros(self.n, dtype=BODY_DTYPE)
+        if out.dtype != BODY_DTYPE or len(out) != self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous BODY_DTYPE array of the handle's body count")
         check(lib().exg_world_get_bodies(self.handle, ptr(out), self.n), "exg_world_get_bodies")
         return out
 
@@ -383,6 +389,20 @@ class DevicePool(DeviceWorld):
         s = np.zeros((), dtype=WORLD_STATS_DTYPE)
         check(lib().exg_batch_world_stats(self.handle, int(slot), ptr(s)), "exg_batch_world_stats")
         return s
+
+
+def host_bodies(n):
+    """A zeroed BODY_DTYPE array of n records in page-locked host memory (exg_host_alloc), freed
+    when the array is collected. Record copies to and from the device run at the link's rate."""
+    import weakref
+    nbytes = max(1, int(n) * BODY_DTYPE.itemsize)
+    p = ctypes.c_void_p()
+    check(lib().exg_host_alloc(nbytes, ctypes.byref(p)), "exg_host_alloc")
+    buf = (ctypes.c_char * nbytes).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=BODY_DTYPE, count=int(n))
+    arr[...] = np.zeros((), dtype=BODY_DTYPE)
+    weakref.finalize(buf, lib().exg_host_free, ctypes.c_void_p(p.value))
+    return arr
 
 
 def world_footprint(n_bodies, n_joints, params):

@@ -130,6 +130,46 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
   for (int c = 0; c < 6; ++c) mom_out[(size_t)c * b.n + i] = mom[c];
 }
 
+// Host records <-> the pool's component-major rows. Record k belongs to body first + k, or to
+// body dst[k] when a map is given (the whole handle's used slots in slot order).
+__global__ void k_bodies_scatter(const exg_body_t* __restrict__ rec, int count, int first, const int* __restrict__ dst,
+                                 double* pose, double* mom, double* mass, double* inertia, double* size, int* kin,
+                                 int* diag, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const exg_body_t& r = rec[k];
+  const int i = dst ? dst[k] : first + k;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) pose[(size_t)c * n + i] = r.pose[c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) mom[(size_t)c * n + i] = r.momentum[c];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) inertia[(size_t)c * n + i] = r.inertia[c];
+  mass[i] = r.mass;
+  size[i] = r.size;
+  kin[i] = r.kinematic;
+  diag[i] = r.diagonal;
+}
+
+__global__ void k_bodies_gather(exg_body_t* __restrict__ rec, int count, int first, const int* __restrict__ dst,
+                                const double* pose, const double* mom, const double* mass, const double* inertia,
+                                const double* size, const int* kin, const int* diag, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  exg_body_t& r = rec[k];
+  const int i = dst ? dst[k] : first + k;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) r.pose[c] = pose[(size_t)c * n + i];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) r.momentum[c] = mom[(size_t)c * n + i];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) r.inertia[c] = inertia[(size_t)c * n + i];
+  r.mass = mass[i];
+  r.size = size[i];
+  r.kinematic = kin[i];
+  r.diagonal = diag[i];
+}
+
 BodyView view_of(const DeviceWorld& w) {
   return BodyView{w.pose, w.mom, w.mass, w.inertia, w.kinematic, w.diagonal, w.n};
 }
@@ -153,5 +193,21 @@ int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStrea
                                                          w.w_body_off, w.w_active, w.conn, w.nj, w.inc_start, w.inc_cnt,
                                                          w.inc_ref);
   prof_end(dev, tok, s);
+  return exg_after_launch(dev);
+}
+
+int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
+                          const int* dst, cudaStream_t s) {
+  if (count <= 0) return EXG_OK;
+  k_bodies_scatter<<<(count + 127) / 128, 128, 0, s>>>(rec, count, first, dst, w.pose, w.mom, w.mass, w.inertia, w.size,
+                                                       w.kinematic, w.diagonal, w.n);
+  return exg_after_launch(dev);
+}
+
+int launch_bodies_gather(exg_device_s* dev, const DeviceWorld& w, exg_body_t* rec, int count, int first,
+                         const int* dst, cudaStream_t s) {
+  if (count <= 0) return EXG_OK;
+  k_bodies_gather<<<(count + 127) / 128, 128, 0, s>>>(rec, count, first, dst, w.pose, w.mom, w.mass, w.inertia, w.size,
+                                                      w.kinematic, w.diagonal, w.n);
   return exg_after_launch(dev);
 }

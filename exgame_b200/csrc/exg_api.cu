@@ -48,6 +48,9 @@ struct exg_world_s {
   bool dirty = true;
   DevArr<GravItem> items_d;
   DevArr<double> partial_d;
+  DevArr<exg_body_t> stage_d;  // host record staging
+  DevArr<int> map_d;           // record -> body of the whole handle's used slots
+  bool map_dirty = true;
   std::vector<void*> allocations;
 
   template <class T> int alloc(T** out, size_t count) {
@@ -67,6 +70,8 @@ struct exg_world_s {
     delete newton;
     items_d.release();
     partial_d.release();
+    stage_d.release();
+    map_d.release();
     for (void* p : allocations) cudaFree(p);
   }
 };
@@ -236,71 +241,59 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
   return EXG_OK;
 }
 
-static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count) {
+// Host records in and out: one copy of the records to (from) a device staging array and one
+// kernel between the records and the rows. dst (device, count entries) maps record k to its body;
+// null means bodies first .. first + count - 1.
+static int stage_reserve(exg_world_s* W, long long count) {
+  if (W->stage_d.cap >= count) return EXG_OK;
+  W->stage_d.release();  // staging contents never outlive a call
+  return W->stage_d.reserve(count, W->dev->stream);
+}
+
+static int upload_records(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count, const int* dst) {
   if (count <= 0) return EXG_OK;
-  DeviceWorld& w = W->w;
-  const int n = w.n;
-  std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
-      size(count);
-  std::vector<int> kin(count), diag(count);
-  for (int32_t i = 0; i < count; ++i) {
-    for (int c = 0; c < 8; ++c) pose[(size_t)c * count + i] = bodies[i].pose[c];
-    for (int c = 0; c < 6; ++c) mom[(size_t)c * count + i] = bodies[i].momentum[c];
-    for (int c = 0; c < 9; ++c) inertia[(size_t)c * count + i] = bodies[i].inertia[c];
-    mass[i] = bodies[i].mass;
-    size[i] = bodies[i].size;
-    kin[i] = bodies[i].kinematic;
-    diag[i] = bodies[i].diagonal;
-  }
   cudaStream_t s = W->dev->stream;
-  for (int c = 0; c < 8; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(w.pose + (size_t)c * n + first, pose.data() + (size_t)c * count, sizeof(double) * count,
-                                 cudaMemcpyHostToDevice, s));
-  for (int c = 0; c < 6; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(w.mom + (size_t)c * n + first, mom.data() + (size_t)c * count, sizeof(double) * count,
-                                 cudaMemcpyHostToDevice, s));
-  for (int c = 0; c < 9; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(w.inertia + (size_t)c * n + first, inertia.data() + (size_t)c * count,
-                                 sizeof(double) * count, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.mass + first, mass.data(), sizeof(double) * count, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.size + first, size.data(), sizeof(double) * count, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.kinematic + first, kin.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(w.diagonal + first, diag.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
+  int rc = stage_reserve(W, count);
+  if (rc != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaMemcpyAsync(W->stage_d.ptr, bodies, sizeof(exg_body_t) * (size_t)count, cudaMemcpyHostToDevice, s));
+  if ((rc = launch_bodies_scatter(W->dev, W->w, W->stage_d.ptr, count, first, dst, s)) != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   return EXG_OK;
 }
 
-static int download_bodies(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count) {
+static int download_records(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count, const int* dst) {
   if (count <= 0) return EXG_OK;
-  DeviceWorld& w = W->w;
-  const int n = w.n;
-  std::vector<double> pose(8 * (size_t)count), mom(6 * (size_t)count), mass(count), inertia(9 * (size_t)count),
-      size(count);
-  std::vector<int> kin(count), diag(count);
   cudaStream_t s = W->dev->stream;
-  for (int c = 0; c < 8; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(pose.data() + (size_t)c * count, w.pose + (size_t)c * n + first, sizeof(double) * count,
-                                 cudaMemcpyDeviceToHost, s));
-  for (int c = 0; c < 6; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(mom.data() + (size_t)c * count, w.mom + (size_t)c * n + first, sizeof(double) * count,
-                                 cudaMemcpyDeviceToHost, s));
-  for (int c = 0; c < 9; ++c)
-    EXG_CUDA_TRY(cudaMemcpyAsync(inertia.data() + (size_t)c * count, w.inertia + (size_t)c * n + first,
-                                 sizeof(double) * count, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(mass.data(), w.mass + first, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(size.data(), w.size + first, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(kin.data(), w.kinematic + first, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
-  EXG_CUDA_TRY(cudaMemcpyAsync(diag.data(), w.diagonal + first, sizeof(int) * count, cudaMemcpyDeviceToHost, s));
+  int rc = stage_reserve(W, count);
+  if (rc != EXG_OK) return rc;
+  if ((rc = launch_bodies_gather(W->dev, W->w, W->stage_d.ptr, count, first, dst, s)) != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaMemcpyAsync(out, W->stage_d.ptr, sizeof(exg_body_t) * (size_t)count, cudaMemcpyDeviceToHost, s));
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
-  for (int32_t i = 0; i < count; ++i) {
-    for (int c = 0; c < 8; ++c) out[i].pose[c] = pose[(size_t)c * count + i];
-    for (int c = 0; c < 6; ++c) out[i].momentum[c] = mom[(size_t)c * count + i];
-    for (int c = 0; c < 9; ++c) out[i].inertia[c] = inertia[(size_t)c * count + i];
-    out[i].mass = mass[i];
-    out[i].size = size[i];
-    out[i].kinematic = kin[i];
-    out[i].diagonal = diag[i];
-  }
+  return EXG_OK;
+}
+
+static int upload_bodies(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count) {
+  return upload_records(W, bodies, first, count, nullptr);
+}
+
+static int download_bodies(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count) {
+  return download_records(W, out, first, count, nullptr);
+}
+
+// The whole handle's record map: used slots in slot order, each at its body range.
+static int ensure_record_map(exg_world_s* W, long long* total) {
+  long long n = 0;
+  for (auto& ws : W->slots) if (ws.used) n += ws.n;
+  *total = n;
+  if (!W->map_dirty) return EXG_OK;
+  std::vector<int> map;
+  map.reserve((size_t)n);
+  for (auto& ws : W->slots)
+    if (ws.used)
+      for (int i = 0; i < ws.n; ++i) map.push_back(ws.body_off + i);
+  int rc = W->map_d.assign(map.data(), (long long)map.size(), W->dev->stream);
+  if (rc != EXG_OK) return rc;
+  W->map_dirty = false;
   return EXG_OK;
 }
 
@@ -468,6 +461,7 @@ static int pool_admit(exg_world_s* W, const exg_body_t* bodies, int n, const exg
   if (p.integrator == EXG_NEWTON) ++W->n_implicit; else ++W->n_explicit;
   ++W->n_used;
   W->dirty = true;
+  W->map_dirty = true;
   *slot_out = slot;
   return EXG_OK;
 }
@@ -487,6 +481,7 @@ static int pool_release(exg_world_s* W, int slot) {
   ws = WorldSlot();
   --W->n_used;
   W->dirty = true;
+  W->map_dirty = true;
   return EXG_OK;
 }
 
@@ -603,6 +598,19 @@ int exg_pool_free(exg_world_t W, exg_pool_usage_t* out) {
   out->worlds_capacity = W->w_cap;
   out->largest_free_bodies = W->body_alloc.largest_free();
   out->largest_free_joints = W->joint_alloc.largest_free();
+  return EXG_OK;
+}
+
+int exg_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return EXG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  EXG_CUDA_TRY(cudaMallocHost(out, bytes));
+  return EXG_OK;
+}
+
+int exg_host_free(void* p) {
+  if (!p) return EXG_ERR_INVALID_ARGUMENT;
+  EXG_CUDA_TRY(cudaFreeHost(p));
   return EXG_OK;
 }
 
@@ -767,35 +775,23 @@ int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
-  for (auto& ws : W->slots) if (ws.used) total += ws.n;
+  int rc = ensure_record_map(W, &total);
+  if (rc != EXG_OK) return rc;
   if (n != total) return EXG_ERR_INVALID_ARGUMENT;
-  long long at = 0;
-  for (auto& ws : W->slots) {
-    if (!ws.used) continue;
-    int rc = download_bodies(W, out + at, ws.body_off, ws.n);
-    if (rc != EXG_OK) return rc;
-    at += ws.n;
-  }
-  return EXG_OK;
+  return download_records(W, out, 0, n, W->map_d.ptr);
 }
 
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
   if (!W || !bodies) return EXG_ERR_INVALID_ARGUMENT;
+  for (int32_t i = 0; i < n; ++i)
+    if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
-  for (auto& ws : W->slots) if (ws.used) total += ws.n;
+  int rc = ensure_record_map(W, &total);
+  if (rc != EXG_OK) return rc;
   if (n != total) return EXG_ERR_INVALID_ARGUMENT;
-  for (int32_t i = 0; i < n; ++i)
-    if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  long long at = 0;
-  for (auto& ws : W->slots) {
-    if (!ws.used) continue;
-    int rc = upload_bodies(W, bodies + at, ws.body_off, ws.n);
-    if (rc != EXG_OK) return rc;
-    at += ws.n;
-  }
-  return EXG_OK;
+  return upload_records(W, bodies, 0, n, W->map_d.ptr);
 }
 
 int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n) {

@@ -123,3 +123,8 @@ int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStrea
 int launch_joints_stage(exg_device_s* dev, const exg_joint_t* joints, int nj, const double* pose_aos, const double* vel_aos,
                         double dt, double warp, int jacobian, double* out, cudaStream_t s);
 int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);
+// records <-> rows: record k is body first + k, or body dst[k] when dst is not null
+int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
+                          const int* dst, cudaStream_t s);
+int launch_bodies_gather(exg_device_s* dev, const DeviceWorld& w, exg_body_t* rec, int count, int first,
+                         const int* dst, cudaStream_t s);

@@ -212,6 +212,11 @@ EXG_API int exg_pool_set_steps(exg_world_t pool, int32_t slot, int32_t steps);
 /* Steps left per slot for slots [0, n_slots) (-1: no limit; 0 for a free slot or a world whose
  * budget is spent). */
 EXG_API int exg_pool_steps_left(exg_world_t pool, int32_t* out, int32_t n_slots);
+/* Page-locked host memory for record buffers: exg_world_get/set_bodies and the batch accessors copy
+ * from and into such buffers at the link's full rate (pageable buffers are staged by the driver). */
+EXG_API int exg_host_alloc(size_t bytes, void** out);
+EXG_API int exg_host_free(void* ptr);
+
 /* Device bytes a world holds while admitted to a pool: its body and joint rows, gravity partial
  * sums and, for the implicit integrator, its island structure and per-step scratch (an upper
  * estimate: every body counted as dynamic, one island). */

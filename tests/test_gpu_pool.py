@@ -175,3 +175,24 @@ def test_server_poll_and_zero_step_requests(device):
     with pytest.raises(_lib.ExgError):
         srv.poll(r1)  # collected already: unknown id
     srv.close()
+
+
+def test_whole_handle_records_follow_slot_order_through_page_locked_buffers(device):
+    """exg_world_get/set_bodies on a pool with a released slot in the middle: the records are the
+    used slots in slot order, and a page-locked buffer round-trips them exactly."""
+    worlds = world_set()
+    pool = _lib.DevicePool(device, max_bodies=4096, max_joints=4096, max_worlds=8)
+    s = [pool.admit(*worlds[k]) for k in (1, 2, 5, 6)]
+    pool.release(s[1])
+    pool.step(2)
+    buf = _lib.host_bodies(pool.n)
+    pool.bodies(out=buf)
+    want = np.concatenate([pool.world_bodies(k) for k in sorted(pool.counts)])
+    assert same(buf, want)
+    buf["momentum"] *= 0.5
+    pool.set_bodies(buf)
+    back = pool.bodies()
+    assert same(back, buf)
+    k = sorted(pool.counts)[1]
+    assert same(pool.world_bodies(k), buf[pool.counts[sorted(pool.counts)[0]]:][:pool.counts[k]])
+    pool.close()

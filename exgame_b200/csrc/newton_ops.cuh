@@ -172,14 +172,16 @@ __device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
 // duals; the values that enter the residual always come from an FP64 evaluation (op_joint_value,
 // or in FP64 the dual's value part, which equals it bit for bit: write_conn on slice 0), so the
 // converged iterate is an FP64 solution whatever the Jacobian's precision.
+// The slice's 42 values go to `dst` when given (a staging buffer), else to the island's scratch.
 template <bool MIXED, int LAW = -1>
-__device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int slice, bool write_conn) {
+__device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int slice, bool write_conn,
+                                      typename JacType<MIXED>::T* dst = nullptr) {
   const int joff = c.d.joint_off;
   const int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
   const int law = LAW >= 0 ? LAW : c.A.jl_law[joff + q];
   const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
   if (MIXED) {
-    float* o = jac_slice<true>(c, q, slice);
+    float* o = dst ? reinterpret_cast<float*>(dst) : jac_slice<true>(c, q, slice);
     float pa[8], pb[8], va[6], vb[6], val[6], dd[36];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { pa[k] = float(c.s.mid[8 * a + k]); pb[k] = float(c.s.mid[8 * b + k]); }
@@ -191,7 +193,7 @@ __device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int 
 #pragma unroll
     for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
   } else {
-    double* o = jac_slice<false>(c, q, slice);
+    double* o = dst ? reinterpret_cast<double*>(dst) : jac_slice<false>(c, q, slice);
     double val[6], dd[36];
     joint_jacobian_slice<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, x + 6 * a, x + 6 * b, c.P.dt, c.P.warp,
                                  slice, val, dd);
@@ -497,6 +499,63 @@ __device__ inline void warp_mv6(const double* A, const double* x, double* y) {
   __syncwarp();
   if (lane < 6) y[lane] = s;
   __syncwarp();
+}
+
+// ── the same block operations for one thread ────────────────────────────────
+// Each does per entry exactly the arithmetic of its warp-cooperative counterpart above (same
+// operand order, same sums in the same order), so a node solved by one thread matches a node
+// solved by one warp bit for bit; a thread holds the whole block in registers, so no shuffles.
+
+// Gauss-Jordan inverse of a (row-major 6x6) with partial pivoting into out. Returns false if a
+// pivot is zero or not finite. Only the right half of [A | I] is kept past the column being
+// eliminated: the left half's columns to the left of it are never read again.
+__device__ __forceinline__ bool thread_inverse6(const double* a, double* out) {
+  double M[6][12];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) M[r][c] = a[r * 6 + c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) M[r][6 + c] = (r == c) ? 1.0 : 0.0;
+  }
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(M[k][k]);
+#pragma unroll
+    for (int r = k + 1; r < 6; ++r) {
+      double x = fabs(M[r][k]);
+      if (x > best) { best = x; piv = r; }
+    }
+#pragma unroll
+    for (int c = k; c < 12; ++c) {  // swap rows k and piv by selects (registers stay registers)
+      const double mk = M[k][c];
+      double mp = mk;
+#pragma unroll
+      for (int r = k + 1; r < 6; ++r) mp = (r == piv) ? M[r][c] : mp;
+#pragma unroll
+      for (int r = k + 1; r < 6; ++r) M[r][c] = (r == piv) ? mk : M[r][c];
+      M[k][c] = mp;
+    }
+    const double pv = M[k][k];
+    if (!(fabs(pv) > 0.0) || !isfinite(pv)) ok = false;
+    const double ip = 1.0 / pv;
+#pragma unroll
+    for (int c = k; c < 12; ++c) M[k][c] = M[k][c] * ip;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r == k) continue;
+      const double f = M[r][k];
+#pragma unroll
+      for (int c = k; c < 12; ++c) M[r][c] = M[r][c] - f * M[k][c];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out[r * 6 + c] = M[r][6 + c];
+  return ok;
 }
 
 // ── scalar helpers of the span budget ───────────────────────────────────────

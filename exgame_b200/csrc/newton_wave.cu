@@ -303,14 +303,42 @@ __global__ void k_w_pre(WaveArgs a) {
 //   values: [0, n) FP64 values, for an iterate evaluated afresh (mixed path; in FP64 the slices'
 //           value parts are the values) and for a probe. A carried iterate keeps the values the
 //           accepted probe left at the same point.
+// The four slices of a joint are four adjacent lanes; a warp holds 8 joints. Each lane writes its
+// slice into the warp's staging block in shared memory, and the warp then stores each joint's four
+// contiguous slices (4 x 42 values, 16-byte aligned) with 16-byte stores spread over the lanes.
 template <bool MIXED, int LAW>
 __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
-  for (int t = gtid(); t < 4 * n; t += gthreads()) {
-    int2 it = a.joint[first + (t >> 2)];
-    const int ev = a.ctl[it.x].eval;
-    if (ev != EV_FULL && ev != EV_JAC) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
-    op_joint_slice<MIXED, LAW>(c, c.s.vm, it.y, t & 3, ev == EV_FULL);
+  typedef typename JacType<MIXED>::T J;
+  constexpr int kJoint = 4 * kJacStride;  // values per joint
+  __shared__ __align__(16) J stage[4][8][kJoint];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int total = 4 * n;
+  for (int base = gtid() - lane; base < total; base += gthreads()) {  // warp-uniform loop
+    const int t = base + lane;
+    bool on = false;
+    int2 it = make_int2(0, 0);
+    if (t < total) {
+      it = a.joint[first + (t >> 2)];
+      const int ev = a.ctl[it.x].eval;
+      if (ev == EV_FULL || ev == EV_JAC) {
+        on = true;
+        Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+        op_joint_slice<MIXED, LAW>(c, c.s.vm, it.y, t & 3, ev == EV_FULL, &stage[wib][lane >> 2][(t & 3) * kJacStride]);
+      }
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, on);
+    __syncwarp();
+    for (int j = 0; j < 8; ++j) {
+      if (!((active >> (4 * j)) & 1u)) continue;  // the joint's island did not evaluate slices
+      const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
+      const IslandDesc& d = a.A.desc[a.isl[jt.x]];
+      J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) + (size_t)jt.y * kJoint;
+      const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
+      float4* dst4 = reinterpret_cast<float4*>(dstj);
+      constexpr int kVec = kJoint * (int)sizeof(J) / 16;
+      for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
+    }
+    __syncwarp();
   }
 }
 
@@ -388,17 +416,39 @@ __global__ void k_w_copy_mass0(WaveArgs a) {
   }
 }
 
-// Assembly, one thread per block entry (a warp covers consecutive entries of one cell, so its
-// Jacobian reads are contiguous).
+// Assembly, one warp per cell: lane e holds entry e (lanes 0..3 also entries 32..35), the term
+// list is read once per warp, and a term's Jacobian rows are contiguous across the lanes.
 template <bool MIXED>
 __global__ void k_w_assemble(WaveArgs a) {
-  for (long long t = gtid(); t < 36LL * a.n_cell; t += gthreads()) {
-    int2 it = a.cell[t / 36];
+  const int lane = threadIdx.x & 31;
+  for (int t = gtid() >> 5; t < a.n_cell; t += gthreads() >> 5) {
+    int2 it = a.cell[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
     Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
-    bool counts;
-    op_assemble<MIXED>(c, w.pf, w.vf, it.y, (int)(t % 36), &counts);
+    const int cell = it.y, i = cell / 3, kind = cell % 3;
+    const int e0 = lane, e1 = lane + 32;
+    const bool has1 = e1 < 36;
+    double acc0 = (kind == 0) ? c.s.mass0[36 * (size_t)i + e0] : 0.0;
+    double acc1 = (kind == 0 && has1) ? c.s.mass0[36 * (size_t)i + e1] : 0.0;
+    const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+    for (int k = p0; k < p1; ++k) {
+      const int term = c.A.cell_terms[k];
+      const int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
+      const auto* jp = jac_slice<MIXED>(c, q, ce) + 6;
+      const auto* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
+      double pv = double(jp[e0]), vv = double(jv[e0]);
+      if (re) { pv = -pv; vv = -vv; }
+      acc0 = acc0 + w.pf * pv + w.vf * vv;
+      if (has1) {
+        double pv1 = double(jp[e1]), vv1 = double(jv[e1]);
+        if (re) { pv1 = -pv1; vv1 = -vv1; }
+        acc1 = acc1 + w.pf * pv1 + w.vf * vv1;
+      }
+    }
+    double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
+    dst[36 * (size_t)i + e0] = acc0;
+    if (has1) dst[36 * (size_t)i + e1] = acc1;
   }
 }
 
@@ -450,56 +500,104 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int wa
   }
 }
 
-// Elimination, one warp per node of level L (leaves to roots): subtract the children's Schur
-// terms, invert the pivot block, and for a non-root node form its own terms for the parent —
-// S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's slot until the back
-// substitution writes dv) — so a parent only sums finished products; a root solves for dv.
-// The products and their order are the island kernel's.
+// Elimination, one thread per node of level L (leaves to roots), the node's blocks in registers:
+// subtract the children's Schur terms, invert the pivot block, and for a non-root node form its own
+// terms for the parent — S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's
+// slot until the back substitution writes dv) — so a parent only sums finished products; a root
+// solves for dv. The arithmetic per entry is the island kernel's (newton_ops.cuh).
 __global__ void k_w_solve_down(WaveArgs a, int first, int count) {
-  const int warp = gtid() >> 5, nwarps = gthreads() >> 5, lane = threadIdx.x & 31;
-  for (int t = warp; t < count; t += nwarps) {
+  for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
     Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
     const int i = it.y;
-    double* D = c.s.D + 36 * (size_t)i;
-    double* b = c.s.bvec + 6 * i;
-    if (lane < 6) b[lane] = c.s.rhs[6 * i + lane];
+    double D[36], b[6];
+#pragma unroll
+    for (int e = 0; e < 36; ++e) D[e] = c.s.D[36 * (size_t)i + e];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) b[r] = c.s.rhs[6 * i + r];
     const int* chp = c.A.ch_ptr + c.d.dyn_off;
     for (int u = chp[i]; u < chp[i + 1]; ++u) {
       const int ch = c.A.ch_idx[u];
       const double* P = c.s.S + 36 * (size_t)ch;
-      D[lane] = D[lane] - P[lane];
-      if (lane < 4) D[32 + lane] = D[32 + lane] - P[32 + lane];
-      if (lane < 6) b[lane] = b[lane] - c.s.dv[6 * ch + lane];
+#pragma unroll
+      for (int e = 0; e < 36; ++e) D[e] = D[e] - P[e];
+#pragma unroll
+      for (int r = 0; r < 6; ++r) b[r] = b[r] - c.s.dv[6 * ch + r];
     }
-    __syncwarp();
-    double* Dinv = c.s.Dinv + 36 * (size_t)i;
-    bool ok = warp_inverse6(D, Dinv);
-    if (!ok && lane == 0) atomicOr(&w.singular, 1);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) c.s.bvec[6 * i + r] = b[r];
+    double Dinv[36];
+    if (!thread_inverse6(D, Dinv)) atomicOr(&w.singular, 1);
+#pragma unroll
+    for (int e = 0; e < 36; ++e) c.s.Dinv[36 * (size_t)i + e] = Dinv[e];
     if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
-      double* S = c.s.S + 36 * (size_t)i;
-      warp_mm6<false>(c.s.Apc + 36 * (size_t)i, Dinv, S);
-      warp_mv6(S, b, c.s.dv + 6 * i);                 // q = S b
-      warp_mm6<false>(S, c.s.Acp + 36 * (size_t)i, S);  // P = S Acp, in place
+      const double* Apc = c.s.Apc + 36 * (size_t)i;
+      const double* Acp = c.s.Acp + 36 * (size_t)i;
+      double* P = c.s.S + 36 * (size_t)i;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        double Sr[6];
+#pragma unroll
+        for (int cc = 0; cc < 6; ++cc) {
+          double v = 0.0;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) v += Apc[r * 6 + k] * Dinv[k * 6 + cc];
+          Sr[cc] = v;
+        }
+        double q = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) q += Sr[k] * b[k];
+        c.s.dv[6 * i + r] = q;
+#pragma unroll
+        for (int cc = 0; cc < 6; ++cc) {
+          double v = 0.0;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) v += Sr[k] * Acp[k * 6 + cc];
+          P[r * 6 + cc] = v;
+        }
+      }
     } else {
-      warp_mv6(Dinv, b, c.s.dv + 6 * i);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v += Dinv[r * 6 + k] * b[k];
+        c.s.dv[6 * i + r] = v;
+      }
     }
   }
 }
 
-// Back substitution, one warp per node of level L >= 1 (roots to leaves).
+// Back substitution, one thread per node of level L >= 1 (roots to leaves).
 __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
-  const int warp = gtid() >> 5, nwarps = gthreads() >> 5;
-  for (int t = warp; t < count; t += nwarps) {
+  for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
     if (a.ctl[it.x].state != WS_DIR) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
     const int i = it.y;
     const int p = c.A.dn_parent[c.d.dyn_off + i];
-    warp_mv6_sub(c.s.Acp + 36 * (size_t)i, c.s.dv + 6 * p, c.s.bvec + 6 * i);
-    warp_mv6(c.s.Dinv + 36 * (size_t)i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+    const double* Acp = c.s.Acp + 36 * (size_t)i;
+    const double* Dinv = c.s.Dinv + 36 * (size_t)i;
+    double xp[6], b[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) xp[k] = c.s.dv[6 * p + k];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double v = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v += Acp[r * 6 + k] * xp[k];
+      b[r] = c.s.bvec[6 * i + r] - v;
+      c.s.bvec[6 * i + r] = b[r];
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double v = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v += Dinv[r * 6 + k] * b[k];
+      c.s.dv[6 * i + r] = v;
+    }
   }
 }
 
@@ -640,7 +738,7 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, 8);
   const int g_dyn = grid_for(dev, a.n_dyn, T, 8);
-  const int g_cell = grid_for(dev, 36LL * a.n_cell, T, 8);
+  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, 8);
   const int g_entry = grid_for(dev, 36LL * a.n_dyn, T, 8);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
@@ -674,11 +772,11 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     const int nl = (int)wave_level_ptr_.size() - 1;
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_down<<<grid_for(dev, 32LL * count, T, 8), T, 0, s>>>(a, first, count);
+      k_w_solve_down<<<grid_for(dev, count, 128, 16), 128, 0, s>>>(a, first, count);
     }
     for (int L = 1; L < nl; ++L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_up<<<grid_for(dev, 32LL * count, T, 8), T, 0, s>>>(a, first, count);
+      k_w_solve_up<<<grid_for(dev, count, 128, 16), 128, 0, s>>>(a, first, count);
     }
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);

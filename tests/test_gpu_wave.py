@@ -91,8 +91,9 @@ def test_wave_agrees_with_island_kernel(device, precision):
     a.step(5)
     b = wave_world(device, bodies, joints, params)
     b.step(5)
-    pe, me = state_error(a.bodies(), b.bodies())
-    assert pe < 1e-12 and me < 1e-9, (pe, me)
+    # the same per-item arithmetic in both schedules: the states agree bit for bit
+    x, y = a.bodies(), b.bodies()
+    assert np.array_equal(x["pose"], y["pose"]) and np.array_equal(x["momentum"], y["momentum"])
     sa, sb = a.stats(), b.stats()
     assert sa["last_newton_iterations"] == sb["last_newton_iterations"]
     assert sa["last_spans"] == sb["last_spans"]

@@ -32,10 +32,13 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from exgame_b200 import _lib, scenarios  # noqa: E402
+from exgame_b200 import _lib, scenarios, sharding  # noqa: E402
 from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED  # noqa: E402
 
 METRIC = "body-steps/s"
+WORLDS = 4096      # config-3 batch size (--worlds)
+SHARD = False      # --shard: one batch split over the ranks instead of one batch per rank
+WORLD_SIZE = 1
 FP64_FMA_PER_SM_CLK = 64
 FP32_FMA_PER_SM_CLK = 128
 
@@ -69,13 +72,21 @@ def workload(name, rank):
         return [(gb, gj, gp), (cb, cj, cp)], cfg
     if name in ("c3", "c3-f64"):
         prec = PRECISION_MIXED if name == "c3" else PRECISION_F64
-        worlds = scenarios.config3_worlds(4096, seed=3 + rank, precision=prec, exact_jacobian=bool(prec))
+        nw = WORLDS
+        if SHARD:  # one batch for the whole job, each rank its body-balanced share (strong scaling)
+            sizes = scenarios.config3_sizes(nw, seed=3)
+            mine = set(sharding.rank_share(sizes, rank, WORLD_SIZE))
+            allw = scenarios.config3_worlds(nw, seed=3, precision=prec, exact_jacobian=bool(prec),
+                                            only=sorted(mine))
+            worlds = allw
+        else:  # each rank its own seeded batch (weak scaling)
+            worlds = scenarios.config3_worlds(nw, seed=3 + rank, precision=prec, exact_jacobian=bool(prec))
         n = sum(len(b) for b, _, _ in worlds)
-        cfg = {"workload": "4096 independent worlds, body counts log-uniform in [8, 8192]: gravity worlds "
+        cfg = {"workload": f"{nw} independent worlds, body counts log-uniform in [8, 8192]: gravity worlds "
                            "(LieEuler, dt 1e-3) and random joint trees (Newton tol 1e-10, dt 1e-2), one batched launch "
                            "set per step, " + ("mixed precision, exact mid-point Newton matrix" if prec else "f64")
                            + " (config 3)",
-               "bodies": n, "worlds": 4096, "dtype": "f32 forces / f64 state" if prec else "f64"}
+               "bodies": n, "worlds": len(worlds), "dtype": "f32 forces / f64 state" if prec else "f64"}
         return worlds, cfg
     raise SystemExit(f"unknown workload {name}")
 
@@ -266,13 +277,13 @@ def run_ours(args, rank, world_size, local_rank):
     launches = dev.kernel_launches() - launches0
     torch.cuda.synchronize()
     t = t_dev
+    dist = None
     if world_size > 1:
         import torch.distributed as dist
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+        t = sharding.max_over_ranks(t, dist, device="cuda")
         dist.barrier()
-    value = n_bodies * args.steps * world_size / t
+    total_bodies = sharding.sum_over_ranks(n_bodies, dist, device="cuda") if world_size > 1 else n_bodies
+    value = total_bodies * args.steps / t
 
     # end to end through the public API: host state in, step, host state out
     host_in = []
@@ -292,11 +303,8 @@ def run_ours(args, rank, world_size, local_rank):
     dev.synchronize()
     t_e2e = time.perf_counter() - t0
     if world_size > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = {"value": n_bodies * e2e_steps * world_size / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
+        t_e2e = sharding.max_over_ranks(t_e2e, dist, device="cuda")
+    e2e = {"value": total_bodies * e2e_steps / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(h2d), "steps": e2e_steps}
 
     # dominant kernel, timed live with events on the library stream over a profiled pass
@@ -457,6 +465,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3-f64"])
+    ap.add_argument("--worlds", type=int, default=4096, help="worlds of the config-3 batch")
+    ap.add_argument("--shard", action="store_true",
+                    help="split one batch over the ranks by body count (strong scaling) instead of one batch per rank")
     ap.add_argument("--serve-rates", default="100,1000,10000",
                     help="request rates (req/s) of the served sweep at N=1; empty to skip")
     ap.add_argument("--serve-requests", type=int, default=300)
@@ -469,6 +480,8 @@ def main():
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     threads = os.cpu_count() or 1
+    global WORLDS, SHARD, WORLD_SIZE
+    WORLDS, SHARD, WORLD_SIZE = args.worlds, args.shard, world_size
 
     if args.impl == "reference":
         if rank != 0:
@@ -518,9 +531,10 @@ def main():
         line = {
             "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world_size, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["t"] / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": r["cfg"]["dtype"],
+            "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": r["cfg"]["dtype"],
             "data": "synthetic (seeded; the reference publishes no dataset)",
-            "config": dict(r["cfg"], parallelism=f"replicas x{world_size} (independent worlds)",
+            "config": dict(r["cfg"], parallelism=(f"worlds sharded over {world_size} ranks by body count" if args.shard
+                                                  else f"replicas x{world_size} (independent worlds)"),
                            l2="flushed between timed steps (256 MB write)"),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
             "clocks": r["clocks"], "plain_path": r["plain"], "serving": serving,

@@ -217,17 +217,21 @@ def config3_sizes(n_worlds=4096, seed=3, lo=8, hi=8192):
     return np.rint(np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_worlds))).astype(np.int64)
 
 
-def config3_worlds(n_worlds=4096, seed=3, precision=PRECISION_F64, lo=8, hi=8192, exact_jacobian=False):
+def config3_worlds(n_worlds=4096, seed=3, precision=PRECISION_F64, lo=8, hi=8192, exact_jacobian=False, only=None):
     """4096 independent worlds, body counts log-uniform in [8, 8192]: even-numbered worlds are
     gravity worlds (config 0 distributions, LieEuler, dt 1e-3), odd-numbered ones are random
-    trees (config 1 laws and parameters, implicit Newton tol 1e-10, dt 1e-2)."""
+    trees (config 1 laws and parameters, implicit Newton tol 1e-10, dt 1e-2). `only` keeps a
+    subset of the world indices (each world's content depends on its index alone)."""
     sizes = config3_sizes(n_worlds, seed, lo, hi)
     gp = step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=precision, G=1.0, softening=0.05,
                      dt=1e-3)
     tp = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-2, tol=1e-10,
                      exact_jacobian=exact_jacobian)
     worlds = []
+    keep = None if only is None else set(only)
     for k, n in enumerate(sizes):
+        if keep is not None and k not in keep:  # a rank's share: the same worlds, the others skipped
+            continue
         if k % 2 == 0:
             worlds.append((gravity_world(int(n), 100.0, seed * 100003 + k), np.zeros(0, dtype=JOINT_DTYPE), gp))
         else:

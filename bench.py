@@ -32,7 +32,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from exgame_b200 import _lib, scenarios, sharding  # noqa: E402
+from exgame_b200 import _lib, autotune, scenarios, sharding  # noqa: E402
 from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED  # noqa: E402
 
 METRIC = "body-steps/s"
@@ -253,6 +253,7 @@ def run_ours(args, rank, world_size, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
     dev = _lib.Device(local_rank)
+    tuning = autotune.autotune(dev) if args.autotune else None  # launch shapes only: results do not change
     parts, cfg = workload(args.workload, rank)
     worlds = make_worlds(dev, parts)
     n_bodies = sum(len(b) for (b, _, _) in parts)
@@ -340,7 +341,7 @@ def run_ours(args, rank, world_size, local_rank):
                            "per world, one pass after a warm pass (device time, L2 flushed before the pass)"}
     return {
         "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
-        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain, "dev": dev,
+        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain, "dev": dev, "tuning": tuning,
     }
 
 
@@ -466,6 +467,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3-f64"])
     ap.add_argument("--worlds", type=int, default=4096, help="worlds of the config-3 batch")
+    ap.add_argument("--autotune", type=int, default=1, help="tune launch shapes on this GPU first")
     ap.add_argument("--shard", action="store_true",
                     help="split one batch over the ranks by body count (strong scaling) instead of one batch per rank")
     ap.add_argument("--serve-rates", default="100,1000,10000",
@@ -533,7 +535,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": r["t"] / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": r["cfg"]["dtype"],
             "data": "synthetic (seeded; the reference publishes no dataset)",
-            "config": dict(r["cfg"], parallelism=(f"worlds sharded over {world_size} ranks by body count" if args.shard
+            "config": dict(r["cfg"], autotune=r["tuning"], parallelism=(f"worlds sharded over {world_size} ranks by body count" if args.shard
                                                   else f"replicas x{world_size} (independent worlds)"),
                            l2="flushed between timed steps (256 MB write)"),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,

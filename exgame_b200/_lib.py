@@ -35,6 +35,8 @@ SIGNATURES = {
     "exg_device_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "exg_device_profile": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "exg_device_profile_read": (ctypes.c_int, [_vp, ctypes.c_int32, _c_double_p, ctypes.POINTER(ctypes.c_int64)]),
+    "exg_device_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
+    "exg_device_get_tuning": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "exg_law_lookup": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
     "exg_world_create": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, ctypes.c_int32, _vp, ctypes.POINTER(_vp)]),
     "exg_world_destroy": (ctypes.c_int, [_vp]),
@@ -203,6 +205,16 @@ class Device:
         s = ctypes.c_void_p()
         check(lib().exg_device_stream(self.handle, ctypes.byref(s)))
         return s.value
+
+    TUNE_GRAVITY_CTAS_PER_SM, TUNE_WAVE_BLOCKS_PER_SM, TUNE_WAVE_MIN_BODIES = 1, 2, 3
+
+    def set_tuning(self, key, value):
+        check(lib().exg_device_set_tuning(self.handle, int(key), int(value)), "exg_device_set_tuning")
+
+    def get_tuning(self, key):
+        v = ctypes.c_int32()
+        check(lib().exg_device_get_tuning(self.handle, int(key), ctypes.byref(v)), "exg_device_get_tuning")
+        return v.value
 
     def profile(self, enable):
         check(lib().exg_device_profile(self.handle, int(bool(enable))))

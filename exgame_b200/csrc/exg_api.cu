@@ -146,6 +146,37 @@ int exg_device_profile_read(exg_device_t dev, int32_t kind, double* total_ms, in
 
 int exg_abi_version(void) { return EXG_ABI_VERSION; }
 
+int exg_device_set_tuning(exg_device_t dev, int32_t key, int32_t value) {
+  if (!dev) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(dev->mu);
+  switch (key) {
+    case EXG_TUNE_GRAVITY_CTAS_PER_SM:
+      if (value < 1 || value > 64) return EXG_ERR_INVALID_ARGUMENT;
+      dev->tune_gravity_ctas_per_sm = value;
+      return EXG_OK;
+    case EXG_TUNE_WAVE_BLOCKS_PER_SM:
+      if (value < 1 || value > 32) return EXG_ERR_INVALID_ARGUMENT;
+      dev->tune_wave_blocks_per_sm = value;
+      return EXG_OK;
+    case EXG_TUNE_WAVE_MIN_BODIES:
+      if (value < 1) return EXG_ERR_INVALID_ARGUMENT;
+      dev->tune_wave_min_bodies = value;
+      return EXG_OK;
+    default:
+      return EXG_ERR_INVALID_ARGUMENT;
+  }
+}
+
+int exg_device_get_tuning(exg_device_t dev, int32_t key, int32_t* value) {
+  if (!dev || !value) return EXG_ERR_INVALID_ARGUMENT;
+  switch (key) {
+    case EXG_TUNE_GRAVITY_CTAS_PER_SM: *value = dev->tune_gravity_ctas_per_sm; return EXG_OK;
+    case EXG_TUNE_WAVE_BLOCKS_PER_SM: *value = dev->tune_wave_blocks_per_sm; return EXG_OK;
+    case EXG_TUNE_WAVE_MIN_BODIES: *value = dev->tune_wave_min_bodies; return EXG_OK;
+    default: return EXG_ERR_INVALID_ARGUMENT;
+  }
+}
+
 const char* exg_status_string(int status) {
   switch (status) {
     case EXG_OK: return "ok";
@@ -371,6 +402,7 @@ static int pool_init(exg_world_s* W, exg_device_s* dev, int b_cap, int j_cap, in
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   W->newton = new (std::nothrow) NewtonWorld();
   if (!W->newton) return EXG_ERR_OUT_OF_MEMORY;
+  W->newton->set_wave_threshold(dev->tune_wave_min_bodies, W->newton->wave_max_levels());
   return EXG_OK;
 }
 

@@ -37,6 +37,10 @@ struct exg_device_s {
   std::vector<cudaEvent_t> free_events;
   double prof_ms[PROF_KINDS] = {0};
   long long prof_count[PROF_KINDS] = {0};
+  // launch-shape tuning (exg_device_set_tuning; results do not depend on any of these)
+  int tune_gravity_ctas_per_sm = 32;  // persistent one-warp CTAs of the mixed gravity kernel
+  int tune_wave_blocks_per_sm = 8;    // grid cap of the wave's 256-thread data kernels (128-thread: twice)
+  int tune_wave_min_bodies = 32;      // default wave threshold of new world handles
 };
 
 // Brackets one launch with events when profiling is on (no-op otherwise).

@@ -355,8 +355,9 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
 
 template <bool MIXED, int LAW>
 void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
-  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 4LL * n, 128, 16), 128, 0, s>>>(a, first, n);
-  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, 16), 128, 0, s>>>(a, first, n);
+  const int per = 2 * dev->tune_wave_blocks_per_sm;
+  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 4LL * n, 128, per), 128, 0, s>>>(a, first, n);
+  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, s>>>(a, first, n);
 }
 
 template <bool MIXED>
@@ -736,10 +737,10 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   const bool mixed = w.precision == EXG_PRECISION_MIXED;
   const int T = 256;
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
-  const int g_body = grid_for(dev, a.n_body, T, 8);
-  const int g_dyn = grid_for(dev, a.n_dyn, T, 8);
-  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, 8);
-  const int g_entry = grid_for(dev, 36LL * a.n_dyn, T, 8);
+  const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
+  const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
+  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
+  const int g_entry = grid_for(dev, 36LL * a.n_dyn, T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
   k_w_init<<<g_isl, T, 0, s>>>(a);
@@ -747,12 +748,14 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   int rc = exg_after_launch(dev);
   if (rc != EXG_OK) return rc;
   static_assert(sizeof(WorldRef) <= sizeof(wave_graph_world_), "world snapshot too small");
-  if (wave_graph_ && std::memcmp(wave_graph_world_, &a.W, sizeof(WorldRef)) != 0) {
+  if (wave_graph_ && (std::memcmp(wave_graph_world_, &a.W, sizeof(WorldRef)) != 0 ||
+                      wave_graph_tuning_ != dev->tune_wave_blocks_per_sm)) {
     cudaGraphExecDestroy(wave_graph_);  // a world array moved since the capture
     wave_graph_ = nullptr;
   }
   if (!wave_graph_) {
     std::memcpy(wave_graph_world_, &a.W, sizeof(WorldRef));
+    wave_graph_tuning_ = dev->tune_wave_blocks_per_sm;
     // one round, captured once per structure
     cudaGraph_t g;
     EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -772,11 +775,11 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     const int nl = (int)wave_level_ptr_.size() - 1;
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_down<<<grid_for(dev, count, 128, 16), 128, 0, s>>>(a, first, count);
+      k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
     }
     for (int L = 1; L < nl; ++L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_up<<<grid_for(dev, count, 128, 16), 128, 0, s>>>(a, first, count);
+      k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
     }
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);

@@ -109,6 +109,7 @@ class NewtonWorld {
   cudaGraphExec_t wave_graph_ = nullptr;
   unsigned char wave_graph_world_[160] = {0};  // the world arrays the round graph was captured with
   int wave_graph_kernels_ = 0;
+  int wave_graph_tuning_ = 0;  // the launch-shape tuning the round graph was captured with
   int* h_live_ = nullptr;
   int last_wave_rounds_ = 0;
   std::vector<WorldSrc> src_;

@@ -158,6 +158,18 @@ EXG_API int exg_device_profile(exg_device_t dev, int32_t enable);
 EXG_API int exg_device_profile_read(exg_device_t dev, int32_t kind, double* total_ms, int64_t* launches);
 EXG_API int exg_abi_version(void);
 
+/* Launch-shape tuning of a device (exgame_b200.autotune measures and sets these). No result
+ * depends on them: they change how work is spread over the SMs, not the arithmetic.
+ *   GRAVITY_CTAS_PER_SM  persistent CTAs per SM of the mixed gravity kernel (1..64, default 32)
+ *   WAVE_BLOCKS_PER_SM   grid cap per SM of the wave schedule's data kernels (1..32, default 8)
+ *   WAVE_MIN_BODIES      wave threshold given to world handles created afterwards (default 32;
+ *                        the island kernel and the wave give identical results) */
+#define EXG_TUNE_GRAVITY_CTAS_PER_SM 1
+#define EXG_TUNE_WAVE_BLOCKS_PER_SM 2
+#define EXG_TUNE_WAVE_MIN_BODIES 3
+EXG_API int exg_device_set_tuning(exg_device_t dev, int32_t key, int32_t value);
+EXG_API int exg_device_get_tuning(exg_device_t dev, int32_t key, int32_t* value);
+
 /* ── law registry (MessageKind::from((shader_name, jacobian)), accelerator/mod.rs:118-132) ── */
 EXG_API int exg_law_lookup(const char* shader_name, int32_t* law_out, int32_t* n_params_out);
 

@@ -1,0 +1,60 @@
+"""The launch-shape autotuner: every tuned value leaves results bit-identical, and the tuner picks
+one of its candidates for each knob."""
+import numpy as np
+import pytest
+
+from exgame_b200 import _lib, autotune, scenarios
+from exgame_b200.abi import GRAVITY_PLUMMER, JOINT_DTYPE, LIE_EULER, NEWTON, PRECISION_MIXED, step_params
+
+pytestmark = pytest.mark.gpu
+D = _lib.Device
+
+
+def mixed_batch():
+    worlds = [(scenarios.gravity_world(3000, 50.0, seed=1), np.zeros(0, dtype=JOINT_DTYPE),
+               step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=PRECISION_MIXED,
+                           softening=0.05, dt=1e-3))]
+    for k, n in enumerate((20, 300, 900)):
+        b, j = scenarios.tree_world(n, seed=30 + k)
+        worlds.append((b, j, step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10,
+                                         exact_jacobian=True)))
+    return worlds
+
+
+def run(device, worlds, g, w, t):
+    device.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, g)
+    device.set_tuning(D.TUNE_WAVE_BLOCKS_PER_SM, w)
+    device.set_tuning(D.TUNE_WAVE_MIN_BODIES, t)
+    batch = _lib.DeviceBatch(device, worlds)
+    batch.step(3)
+    out = batch.bodies()
+    batch.close()
+    return out
+
+
+def test_tuning_never_changes_results(device):
+    worlds = mixed_batch()
+    defaults = [device.get_tuning(k) for k in (1, 2, 3)]
+    try:
+        ref = run(device, worlds, 32, 8, 32)
+        for g, w, t in ((8, 4, 1), (21, 16, 256), (1, 1, 1 << 20)):
+            got = run(device, worlds, g, w, t)
+            assert np.array_equal(got["pose"], ref["pose"]) and np.array_equal(got["momentum"], ref["momentum"])
+    finally:
+        for k, v in zip((1, 2, 3), defaults):
+            device.set_tuning(k, v)
+
+
+def test_autotune_picks_candidates(device):
+    defaults = [device.get_tuning(k) for k in (1, 2, 3)]
+    try:
+        r = autotune.autotune(device, gravity_bodies=8192, trees=8, tree_bodies=600, steps=2)
+        assert r["gravity_ctas_per_sm"] in autotune.GRAVITY_CTAS
+        assert r["wave_blocks_per_sm"] in autotune.WAVE_BLOCKS
+        assert r["wave_min_bodies"] in autotune.WAVE_THRESHOLDS
+        assert device.get_tuning(D.TUNE_GRAVITY_CTAS_PER_SM) == r["gravity_ctas_per_sm"]
+        with pytest.raises(_lib.ExgError):
+            device.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, 0)
+    finally:
+        for k, v in zip((1, 2, 3), defaults):
+            device.set_tuning(k, v)

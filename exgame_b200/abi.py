@@ -37,6 +37,7 @@ STEP_PARAMS_DTYPE = np.dtype(
         ("tol", "<f8"),
         ("max_newton", "<i4"),
         ("reserved1", "<i4"),
+        ("field_accel", "<f8", (3,)),
     ],
     align=True,
 )
@@ -96,7 +97,7 @@ NEWTON_EXACT_POSE_FACTOR = 1
 
 
 def step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, precision=PRECISION_F64, G=1.0, softening=0.0,
-                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32, exact_jacobian=False):
+                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32, exact_jacobian=False, field=(0.0, 0.0, 0.0)):
     p = np.zeros((), dtype=STEP_PARAMS_DTYPE)
     p["newton_flags"] = NEWTON_EXACT_POSE_FACTOR if exact_jacobian else 0
     p["integrator"] = integrator
@@ -108,4 +109,5 @@ def step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, precision=PRECISI
     p["warp"] = warp
     p["tol"] = tol
     p["max_newton"] = max_newton
+    p["field_accel"] = field
     return p

@@ -77,6 +77,7 @@ __global__ void k_integrate_explicit(BodyView b, double* __restrict__ pose_out, 
     tot[4] = pm.z * f[0] - pm.x * f[2];
     tot[5] = pm.x * f[1] - pm.y * f[0];
   }
+  add_uniform_field(wparams[wid].field_accel, reinterpret_cast<const double4*>(pos_mass)[i], tot);
   for (int q = inc_start[i], qe = inc_start[i] + inc_cnt[i]; q < qe; ++q) {
     int ref = inc_ref[q];
     int k = ref >> 1, end = ref & 1;

@@ -84,4 +84,18 @@ EXG_HD void world_velocity(const double* pose8, const double* mom6, const double
   screw_to6(wb, wv6);
 }
 
+// UniformField (crates/newton/src/field.rs:29-47): the world force F = m a of a constant
+// acceleration a (mass from the charge, 0 for kinematic bodies), added to the world wrench w6
+// (force, torque about the world origin) as a force through the body's centre: (F, p x F).
+EXG_HD void add_uniform_field(const double* a, const double4& pm, double* w6) {
+  if (a[0] == 0.0 && a[1] == 0.0 && a[2] == 0.0) return;
+  const double f[3] = {pm.w * a[0], pm.w * a[1], pm.w * a[2]};
+  w6[0] += f[0];
+  w6[1] += f[1];
+  w6[2] += f[2];
+  w6[3] += pm.y * f[2] - pm.z * f[1];
+  w6[4] += pm.z * f[0] - pm.x * f[2];
+  w6[5] += pm.x * f[1] - pm.y * f[0];
+}
+
 }  // namespace exg

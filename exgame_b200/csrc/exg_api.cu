@@ -2,6 +2,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <cmath>
 #include <new>
 #include <string>
 #include "exg_internal.cuh"
@@ -262,6 +263,8 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
   if (p->precision != EXG_PRECISION_F64 && p->precision != EXG_PRECISION_MIXED) return EXG_ERR_INVALID_ARGUMENT;
   if (p->gravity_law == EXG_GRAVITY_PLUMMER && !(p->softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   if (!(p->dt > 0.0) || !(p->warp >= 1.0)) return EXG_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(p->field_accel[k])) return EXG_ERR_INVALID_ARGUMENT;
   for (int32_t i = 0; i < n; ++i)
     if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   for (int32_t k = 0; k < nj; ++k) {

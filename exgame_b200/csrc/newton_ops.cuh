@@ -346,25 +346,28 @@ __device__ inline void op_load_world_state(const Ctx& c, int q) {
   for (int k = 0; k < 6; ++k) { c.s.vm[6 * q + k] = wv[k]; c.s.snap[6 * q + k] = p6[k]; }
 }
 
-// External wrench of island body q: gravity (F, p x F), frozen over the whole step.
+// External wrench of island body q: gravity (F, p x F) and the uniform field, frozen over the whole
+// step.
 __device__ inline void op_load_external(const Ctx& c, int q) {
   double* e = c.s.ext + 6 * q;
 #pragma unroll
   for (int k = 0; k < 6; ++k) e[k] = 0.0;
-  if (c.P.splits <= 0) return;
   int g = c.gbody(q);
-  int il = g - c.P.wbody_off;
   double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
-  double f[3];
-  for (int k = 0; k < 3; ++k) {
-    double acc = 0.0;
-    for (int s = 0; s < c.P.splits; ++s) acc += c.P.part[(size_t)s * 3 * c.P.nw + (size_t)k * c.P.nw + il];
-    f[k] = c.P.G * pm.w * acc;
+  if (c.P.splits > 0) {
+    int il = g - c.P.wbody_off;
+    double f[3];
+    for (int k = 0; k < 3; ++k) {
+      double acc = 0.0;
+      for (int s = 0; s < c.P.splits; ++s) acc += c.P.part[(size_t)s * 3 * c.P.nw + (size_t)k * c.P.nw + il];
+      f[k] = c.P.G * pm.w * acc;
+    }
+    e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
+    e[3] = pm.y * f[2] - pm.z * f[1];
+    e[4] = pm.z * f[0] - pm.x * f[2];
+    e[5] = pm.x * f[1] - pm.y * f[0];
   }
-  e[0] = f[0]; e[1] = f[1]; e[2] = f[2];
-  e[3] = pm.y * f[2] - pm.z * f[1];
-  e[4] = pm.z * f[0] - pm.x * f[2];
-  e[5] = pm.x * f[1] - pm.y * f[0];
+  add_uniform_field(c.W.wparams[c.d.world].field_accel, pm, e);
 }
 
 // commit_span (newton.rs:708-753) for dynamic node i: M = M0 * exp(span v), P = 2 P_mid - P_n

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define EXG_ABI_VERSION 1
+#define EXG_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define EXG_API __attribute__((visibility("default")))
@@ -126,6 +126,10 @@ typedef struct {
   double tol;
   int32_t max_newton; /* per span; the reference uses 32 (newton.rs:355) */
   int32_t reserved1;
+  /* UniformField (crates/newton/src/field.rs:17-47): a constant world acceleration; every body
+   * gets the world force m * field_accel (kinematic bodies, mass 0, none), added to the external
+   * wrench beside gravity. Zero: no field. */
+  double field_accel[3];
 } exg_step_params_t;
 
 /* Per-world counters of the last step. */

@@ -57,6 +57,7 @@ void* orc_world_create(const exg_body_t* bodies, int n_bodies, const exg_joint_t
   w->wp.ns_warm = ns_warm;
   w->wp.ns_seed = ns_seed;
   w->wp.exact_pose_factor = (p->newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) != 0;
+  for (int k = 0; k < 3; ++k) w->wp.field[k] = p->field_accel[k];
   w->build();
   return w;
 }

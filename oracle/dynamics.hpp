@@ -316,6 +316,7 @@ struct WorldParams {
   int ns_warm = 2, ns_seed = 24;
   int solver = SOLVER_EXACT;
   bool exact_pose_factor = false;  // -half^2/2 on the pose columns instead of the reference's -half^2
+  double field[3] = {0.0, 0.0, 0.0};  // UniformField world acceleration (field.rs:17-47)
 };
 
 // ── One island's implicit mid-point Newton step ─────────────────────────────
@@ -756,6 +757,17 @@ struct OWorld {
       if (wp.gravity.law == GRAVITY_OFF) continue;
       V3<double> p = body_position(bodies[i]);
       external[i] = Wrench<double>::make(f[i], p.cross(f[i]));
+    }
+    // UniformField (field.rs:29-47): F = m a on every body (kinematic bodies have mass 0), added
+    // after gravity as a force through the body's centre: (F, p x F) about the world origin.
+    if (wp.field[0] != 0.0 || wp.field[1] != 0.0 || wp.field[2] != 0.0) {
+      for (size_t i = 0; i < n; ++i) {
+        if (bodies[i].kinematic) continue;
+        const double m = bodies[i].mass;
+        V3<double> F{m * wp.field[0], m * wp.field[1], m * wp.field[2]};
+        V3<double> p = body_position(bodies[i]);
+        external[i] = external[i] + Wrench<double>::make(F, p.cross(F));
+      }
     }
     if (wp.integrator == NEWTON) {
       for (Island& isl : islands) {

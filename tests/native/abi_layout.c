@@ -14,7 +14,7 @@ int main(void) {
   SZ(exg_step_params_t); OFF(exg_step_params_t, integrator); OFF(exg_step_params_t, gravity_law);
   OFF(exg_step_params_t, precision); OFF(exg_step_params_t, newton_flags); OFF(exg_step_params_t, G);
   OFF(exg_step_params_t, softening); OFF(exg_step_params_t, dt); OFF(exg_step_params_t, warp);
-  OFF(exg_step_params_t, tol); OFF(exg_step_params_t, max_newton);
+  OFF(exg_step_params_t, tol); OFF(exg_step_params_t, max_newton); OFF(exg_step_params_t, field_accel);
   SZ(exg_world_stats_t); OFF(exg_world_stats_t, steps); OFF(exg_world_stats_t, last_spans);
   OFF(exg_world_stats_t, last_newton_iterations); OFF(exg_world_stats_t, max_depth_reached);
   OFF(exg_world_stats_t, fatal); OFF(exg_world_stats_t, last_residual);

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_library_loads_without_device_and_binds():
     L = _lib.lib()
-    assert L.exg_abi_version() == 1
+    assert L.exg_abi_version() == 2
     assert L.exg_status_string(-1).decode() == "no kernel for this joint law"
 
 
@@ -42,7 +42,7 @@ def test_record_layouts_match_c(oracle):
     L = oracle.lib()
     assert BODY_DTYPE.itemsize == L.orc_body_size() == 208
     assert JOINT_DTYPE.itemsize == L.orc_joint_size() == 96
-    assert STEP_PARAMS_DTYPE.itemsize == 64
+    assert STEP_PARAMS_DTYPE.itemsize == 88
     assert WORLD_STATS_DTYPE.itemsize == 32
 
 

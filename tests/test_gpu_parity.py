@@ -242,3 +242,24 @@ def test_newton_phase_cycles_reported(device):
     dw.step(2)
     ph = dw.phase_cycles()
     assert ph["joints+jacobian"] > 0 and ph["solve"] > 0 and ph["line search"] > 0
+
+
+@pytest.mark.parametrize("scheme", [LIE_EULER, NEWTON])
+def test_uniform_field_matches_oracle(device, oracle, scheme):
+    """UniformField (field.rs:17-47) beside gravity: a jointed tree with a kinematic body in a field
+    of weight plus a crosswind, explicit and implicit, both Newton schedules."""
+    bodies, joints = scenarios.tree_world(30, seed=81)
+    bodies[4]["kinematic"] = 1
+    bodies[4]["mass"] = 0.0
+    params = step_params(integrator=scheme, gravity_law=GRAVITY_PLUMMER, softening=0.05, dt=1e-2 if scheme == NEWTON else 1e-3,
+                         tol=1e-10, field=(0.0, 1.5, -9.81))
+    steps = 10 if scheme == NEWTON else 100
+    ow = oracle.OracleWorld(bodies, joints, params)
+    ow.step(steps)
+    for min_bodies in ((1 << 20, 1) if scheme == NEWTON else (1 << 20,)):
+        dw = _lib.DeviceWorld(device, bodies, joints, params)
+        dw.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, min_bodies)
+        dw.step(steps)
+        pe, me = state_error(ow.bodies(), dw.bodies())
+        assert pe < 1e-9 and me < 1e-7, (min_bodies, pe, me)
+        dw.close()

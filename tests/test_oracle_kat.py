@@ -381,3 +381,26 @@ def test_exact_pose_factor_converges_to_the_same_step(oracle):
     pb = np.array([position(x) for x in ex.bodies()])
     assert np.abs(pa - pb).max() < 1e-8
     assert its_ex < its_ref
+
+
+def test_uniform_field_applies_m_times_accel_and_ignores_kinematic(oracle):
+    """field.rs:54-97: with a world acceleration of gravity along -z plus a sideways +y wind, a
+    dynamic body of mass 2 at the origin gets the world force m a; a kinematic body gets none.
+    Restated through one LieEuler step: the momentum change is m a dt, the kinematic body is
+    untouched."""
+    from exgame_b200.abi import LIE_EULER, step_params
+    m, a, dt = 2.0, (0.0, 1.5, -9.81), 0.01
+    bs = np.array([body((0, 0, 0), (0, 0, 0), mass=m), body((3, 0, 0), kinematic=True)])
+    w = oracle.OracleWorld(bs, np.zeros(0, dtype=JOINT_DTYPE), step_params(integrator=LIE_EULER, dt=dt, field=a))
+    w.step(1)
+    out = w.bodies()
+    assert np.allclose(out[0]["momentum"][:3], np.array(a) * m * dt, rtol=0, atol=1e-15)
+    assert np.array_equal(out[1]["momentum"], bs[1]["momentum"]) and np.array_equal(out[1]["pose"], bs[1]["pose"])
+    # a free body in the field falls as p = 1/2 a t^2 under the implicit step too
+    from exgame_b200.abi import NEWTON
+    bs2 = np.array([body((1, 2, 3), (0, 0, 0), mass=m)])
+    w2 = oracle.OracleWorld(bs2, np.zeros(0, dtype=JOINT_DTYPE),
+                            step_params(integrator=NEWTON, dt=dt, tol=1e-12, field=a))
+    w2.step(10)
+    mom = w2.bodies()[0]["momentum"]
+    assert np.allclose(mom[:3], np.array(a) * m * dt * 10, rtol=1e-9, atol=1e-12)

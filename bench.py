@@ -33,7 +33,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from exgame_b200 import _lib, autotune, scenarios, sharding  # noqa: E402
-from exgame_b200.abi import BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED  # noqa: E402
+from exgame_b200.abi import (BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED,  # noqa: E402
+                             PRECISION_MIXED_FAST)
 
 METRIC = "body-steps/s"
 WORLDS = 4096      # config-3 batch size (--worlds)
@@ -182,7 +183,7 @@ def dominant_kernel(dev, cfg_name, parts, steps, bench_worlds):
             if int(p["gravity_law"]) != GRAVITY_OFF and len(b) > 1:
                 pairs += float(len(b)) ** 2
         flops = 20.0 * pairs
-        bound = "fp32" if int(parts[0][2]["precision"]) == PRECISION_MIXED else "fp64"
+        bound = "fp32" if int(parts[0][2]["precision"]) != PRECISION_F64 else "fp64"
     label = kinds[kind] + (f" ({20} flop per directed pair)" if kind == 0 else "")
     if kind == 3:
         label = "Newton step of the implicit islands (island kernel + wave rounds)"
@@ -334,6 +335,20 @@ def run_ours(args, rank, world_size, local_rank):
     grav = gravity_roofline(dev, parts, worlds, sms, sm_mhz) if kind != 0 else None
     if grav:
         roofline["gravity"] = grav
+        if int(parts[0][2]["precision"]) == PRECISION_MIXED:
+            # the single-FP32 form of the same kernel on the same gravity worlds, for comparison
+            gparts = []
+            for b, j, p in parts:
+                if int(p["gravity_law"]) != GRAVITY_OFF and len(b) > 1:
+                    q = p.copy()
+                    q["precision"] = PRECISION_MIXED_FAST
+                    gparts.append((b, j, q))
+            gw = make_worlds(dev, gparts)
+            fast = gravity_roofline(dev, gparts, gw, sms, sm_mhz)
+            for w in gw:
+                w.close()
+            fast["note"] += "; MIXED_FAST (single FP32 positions), for comparison"
+            roofline["gravity_fast"] = fast
     plain = None
     if args.plain and len(parts) > 1:
         plain = {"value": plain_path(dev, parts, flush), "unit": METRIC,
@@ -355,7 +370,7 @@ def gravity_roofline(dev, parts, worlds, sms, sm_mhz):
         w.step(1)
     ms, nl = dev.profile_read(0)
     dev.profile(False)
-    mixed = int(parts[0][2]["precision"]) == PRECISION_MIXED
+    mixed = int(parts[0][2]["precision"]) != PRECISION_F64
     per_clk = FP32_FMA_PER_SM_CLK if mixed else FP64_FMA_PER_SM_CLK
     peak = 2.0 * per_clk * sms * sm_mhz * 1e6 / 1e12
     achieved = 20.0 * pairs / (ms / 1e3 / max(nl, 1)) / 1e12

@@ -90,7 +90,7 @@ LAW_N_PARAMS = (10, 10, 2, 1)
 
 EXPLICIT_EULER, SYMPLECTIC_EULER, LIE_EULER, NEWTON = 0, 1, 2, 3
 GRAVITY_OFF, GRAVITY_SIZE_CORE, GRAVITY_PLUMMER = 0, 1, 2
-PRECISION_F64, PRECISION_MIXED = 0, 1
+PRECISION_F64, PRECISION_MIXED, PRECISION_MIXED_FAST = 0, 1, 2
 
 
 NEWTON_EXACT_POSE_FACTOR = 1

@@ -260,7 +260,7 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
   if (n < 0 || nj < 0 || (n > 0 && !bodies) || (nj > 0 && !joints) || !p) return EXG_ERR_INVALID_ARGUMENT;
   if (p->integrator < 0 || p->integrator > EXG_NEWTON) return EXG_ERR_INVALID_ARGUMENT;
   if (p->gravity_law < 0 || p->gravity_law > EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
-  if (p->precision != EXG_PRECISION_F64 && p->precision != EXG_PRECISION_MIXED) return EXG_ERR_INVALID_ARGUMENT;
+  if (p->precision < EXG_PRECISION_F64 || p->precision > EXG_PRECISION_MIXED_FAST) return EXG_ERR_INVALID_ARGUMENT;
   if (p->gravity_law == EXG_GRAVITY_PLUMMER && !(p->softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   if (!(p->dt > 0.0) || !(p->warp >= 1.0)) return EXG_ERR_INVALID_ARGUMENT;
   for (int k = 0; k < 3; ++k)
@@ -594,7 +594,7 @@ int exg_world_create(exg_device_t dev, const exg_body_t* bodies, int32_t n, cons
 
 int exg_pool_create(exg_device_t dev, const exg_pool_config_t* cfg, exg_world_t* out) {
   if (!dev || !cfg || !out || cfg->max_bodies <= 0 || cfg->max_joints < 0 || cfg->max_worlds <= 0) return EXG_ERR_INVALID_ARGUMENT;
-  if (cfg->precision != EXG_PRECISION_F64 && cfg->precision != EXG_PRECISION_MIXED) return EXG_ERR_INVALID_ARGUMENT;
+  if (cfg->precision < EXG_PRECISION_F64 || cfg->precision > EXG_PRECISION_MIXED_FAST) return EXG_ERR_INVALID_ARGUMENT;
   if (cfg->max_bodies > (1LL << 30) || cfg->max_joints > (1LL << 29)) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(dev->mu);
   cudaSetDevice(dev->ordinal);

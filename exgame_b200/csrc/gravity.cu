@@ -171,6 +171,13 @@ __device__ __forceinline__ float rsqrt_ftz(float x) {
   return r;
 }
 
+// COMP (the MIXED precision): positions relative to the tile reference are carried as FP32 pairs
+// hi + lo (the remainder of the FP64 difference), and a pair's difference is (hi_j - hi_i) +
+// (lo_j - lo_i): the first term is exact for nearby bodies (Sterbenz), so a close pair's
+// separation is accurate to FP32 rounding of the separation itself rather than of the distance to
+// the tile reference. Without it (MIXED_FAST) a close pair far from the reference carries that
+// reference distance's rounding, which dense clusters amplify over many steps.
+template <bool COMP>
 __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const double4* __restrict__ pm,
                                                                      const double* __restrict__ size,
                                                                      const GravItem* __restrict__ items, int n_items,
@@ -180,7 +187,7 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
                                                                      const int* __restrict__ w_active) {
   constexpr int T = kGravTile;
   constexpr int H = kMixThreads;
-  __shared__ float4 tq[T][2];
+  __shared__ float4 tq[T][COMP ? 3 : 2];
   __shared__ float tsz2[T];
   __shared__ float tisz3[T];
   __shared__ int cur;
@@ -198,14 +205,19 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
     int il[kMixKI];
     bool v[kMixKI];
     float px[kMixKI], py[kMixKI], pz[kMixKI], sz2[kMixKI], isz3[kMixKI];
+    float lx[kMixKI], ly[kMixKI], lz[kMixKI];
 #pragma unroll
     for (int h = 0; h < kMixKI; ++h) {
       il[h] = g.i0 + threadIdx.x + h * H;
       v[h] = il[h] < g.n;
       const double4 p = v[h] ? wpm[il[h]] : c;
-      px[h] = float(p.x - c.x);
-      py[h] = float(p.y - c.y);
-      pz[h] = float(p.z - c.z);
+      const double rx = p.x - c.x, ry = p.y - c.y, rz = p.z - c.z;
+      px[h] = float(rx);
+      py[h] = float(ry);
+      pz[h] = float(rz);
+      lx[h] = COMP ? float(rx - double(px[h])) : 0.f;
+      ly[h] = COMP ? float(ry - double(py[h])) : 0.f;
+      lz[h] = COMP ? float(rz - double(pz[h])) : 0.f;
       sz2[h] = 0.f;
       isz3[h] = 0.f;
       if (core_law && v[h]) {
@@ -216,6 +228,8 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
     }
     const float2 nxA = f2(-px[0], -px[1]), nyA = f2(-py[0], -py[1]), nzA = f2(-pz[0], -pz[1]);
     const float2 nxB = f2(-px[2], -px[3]), nyB = f2(-py[2], -py[3]), nzB = f2(-pz[2], -pz[3]);
+    const float2 mxA = f2(-lx[0], -lx[1]), myA = f2(-ly[0], -ly[1]), mzA = f2(-lz[0], -lz[1]);
+    const float2 mxB = f2(-lx[2], -lx[3]), myB = f2(-ly[2], -ly[3]), mzB = f2(-lz[2], -lz[3]);
     const float e2 = float(g.eps2);
     const float2 eps2 = f2(e2, e2);
     double acc[kMixKI][3];
@@ -226,12 +240,18 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
       for (int h = 0; h < kMixKI; ++h) {
         const int slot = threadIdx.x + h * H;
         const int j = base + slot;
-        float x = 0.f, y = 0.f, z = 0.f, m = 0.f;
+        float x = 0.f, y = 0.f, z = 0.f, m = 0.f, xl = 0.f, yl = 0.f, zl = 0.f;
         if (j < g.j1) {
           const double4 q = wpm[j];
-          x = float(q.x - c.x);
-          y = float(q.y - c.y);
-          z = float(q.z - c.z);
+          const double rx = q.x - c.x, ry = q.y - c.y, rz = q.z - c.z;
+          x = float(rx);
+          y = float(ry);
+          z = float(rz);
+          if (COMP) {
+            xl = float(rx - double(x));
+            yl = float(ry - double(y));
+            zl = float(rz - double(z));
+          }
           m = float(q.w);
           if (core_law) {
             const double sd = size[g.body_off + j];
@@ -244,6 +264,7 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
         }
         tq[slot][0] = make_float4(x, x, y, y);
         tq[slot][1] = make_float4(z, z, m, m);
+        if (COMP) tq[slot][COMP ? 2 : 0] = make_float4(xl, yl, zl, 0.f);
       }
       __syncthreads();
       float a[kMixKI][3];
@@ -253,8 +274,18 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
         for (int k = 0; k < T; ++k) {
           const float4 u = tq[k][0], w = tq[k][1];
           const float2 qx = f2(u.x, u.y), qy = f2(u.z, u.w), qz = f2(w.x, w.y), qm = f2(w.z, w.w);
-          const float2 dxA = __fadd2_rn(qx, nxA), dyA = __fadd2_rn(qy, nyA), dzA = __fadd2_rn(qz, nzA);
-          const float2 dxB = __fadd2_rn(qx, nxB), dyB = __fadd2_rn(qy, nyB), dzB = __fadd2_rn(qz, nzB);
+          float2 dxA = __fadd2_rn(qx, nxA), dyA = __fadd2_rn(qy, nyA), dzA = __fadd2_rn(qz, nzA);
+          float2 dxB = __fadd2_rn(qx, nxB), dyB = __fadd2_rn(qy, nyB), dzB = __fadd2_rn(qz, nzB);
+          if (COMP) {  // add the difference of the remainders
+            const float4 l = tq[k][COMP ? 2 : 0];
+            const float2 lxj = f2(l.x, l.x), lyj = f2(l.y, l.y), lzj = f2(l.z, l.z);
+            dxA = __fadd2_rn(dxA, __fadd2_rn(lxj, mxA));
+            dyA = __fadd2_rn(dyA, __fadd2_rn(lyj, myA));
+            dzA = __fadd2_rn(dzA, __fadd2_rn(lzj, mzA));
+            dxB = __fadd2_rn(dxB, __fadd2_rn(lxj, mxB));
+            dyB = __fadd2_rn(dyB, __fadd2_rn(lyj, myB));
+            dzB = __fadd2_rn(dzB, __fadd2_rn(lzj, mzB));
+          }
           const float2 rA = __ffma2_rn(dxA, dxA, __ffma2_rn(dyA, dyA, __ffma2_rn(dzA, dzA, eps2)));
           const float2 rB = __ffma2_rn(dxB, dxB, __ffma2_rn(dyB, dyB, __ffma2_rn(dzB, dzB, eps2)));
           const float2 iA = f2(rsqrt_ftz(rA.x), rsqrt_ftz(rA.y)), iB = f2(rsqrt_ftz(rB.x), rsqrt_ftz(rB.y));
@@ -278,7 +309,13 @@ __global__ void __launch_bounds__(kMixThreads) k_gravity_items_mixed(const doubl
           for (int h = 0; h < kMixKI; ++h) {
             // core radius of the higher-slot body (gravity.rs:126-131); coincident bodies exert
             // nothing (|d| < 1e-9, gravity.rs:119-122)
-            const float dx = u.x - px[h], dy = u.z - py[h], dz = w.x - pz[h];
+            float dx = u.x - px[h], dy = u.z - py[h], dz = w.x - pz[h];
+            if (COMP) {
+              const float4 l = tq[k][COMP ? 2 : 0];
+              dx = dx + (l.x - lx[h]);
+              dy = dy + (l.y - ly[h]);
+              dz = dz + (l.z - lz[h]);
+            }
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const bool j_hi = jg > il[h];
             const float s2 = j_hi ? ts2 : sz2[h];
@@ -378,7 +415,10 @@ int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double
   const double4* pm = reinterpret_cast<const double4*>(pos_mass);
   int tok = prof_begin(dev, PROF_GRAVITY, s);
   if (precision == EXG_PRECISION_MIXED)
-    k_gravity_items_mixed<<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm)), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
+    k_gravity_items_mixed<true><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm)), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
+                                                                             world_of_body, w_active);
+  else if (precision == EXG_PRECISION_MIXED_FAST)
+    k_gravity_items_mixed<false><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm)), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
                                                                              world_of_body, w_active);
   else
     k_gravity_items<double><<<std::min(n_items, sms * 16), kGravThreads, 0, s>>>(pm, size, items, n_items, head,

@@ -694,7 +694,7 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   int* head = d_queue.ptr + n_cta_;
   // persistent CTAs: as many as can be resident at once
   static int resident[2] = {0, 0};
-  const int mixed = w.precision == EXG_PRECISION_MIXED;
+  const int mixed = w.precision != EXG_PRECISION_F64;
   if (resident[mixed] == 0) {
     int per_sm = 0;
     cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<true>, kThreads, 0)

@@ -734,7 +734,7 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   a.dyn_first = dw_dyn_first_.ptr;
   a.nodesq = dw_nodesq_.ptr;
   a.live = dw_live_.ptr;
-  const bool mixed = w.precision == EXG_PRECISION_MIXED;
+  const bool mixed = w.precision != EXG_PRECISION_F64;
   const int T = 256;
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);

@@ -99,10 +99,14 @@ typedef enum {
 
 typedef enum { EXG_EXPLICIT_EULER = 0, EXG_SYMPLECTIC_EULER = 1, EXG_LIE_EULER = 2, EXG_NEWTON = 3 } exg_integrator;
 typedef enum { EXG_GRAVITY_OFF = 0, EXG_GRAVITY_SIZE_CORE = 1, EXG_GRAVITY_PLUMMER = 2 } exg_gravity_law;
-/* F64: every stage in double precision (the plain path). MIXED: forces and the linear
- * solve's inner iterations in FP32, pose/momentum accumulation, the Newton residual and the
- * final block-inverse correction in FP64. */
-typedef enum { EXG_PRECISION_F64 = 0, EXG_PRECISION_MIXED = 1 } exg_precision;
+/* F64: every stage in double precision (the plain path). MIXED: gravity pair terms and the Newton
+ * Jacobian's derivative slices in FP32; poses, momenta, joint wrench values, the residual and
+ * convergence test, the assembled system and its solve in FP64. Gravity takes pair separations
+ * from double-single (hi + lo FP32) positions, so a close pair's separation is accurate to its
+ * own FP32 rounding. MIXED_FAST: as MIXED with single FP32 positions relative to the gravity tile's
+ * reference body (faster; the rounding of that reference distance then enters close pairs, which
+ * dense clusters amplify over many steps). */
+typedef enum { EXG_PRECISION_F64 = 0, EXG_PRECISION_MIXED = 1, EXG_PRECISION_MIXED_FAST = 2 } exg_precision;
 
 /* Step configuration: Epoch dt/warp (crates/aristotle/src/epoch.rs:17-60), the integrator
  * (crates/newton/src/integrator/implicit/mod.rs:44-49), the gravity field and the Newton

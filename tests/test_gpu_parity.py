@@ -12,7 +12,8 @@ import pytest
 
 from exgame_b200 import _lib, scenarios
 from exgame_b200.abi import (GRAVITY_OFF, GRAVITY_PLUMMER, GRAVITY_SIZE_CORE, JOINT_DTYPE, LIE_EULER, NEWTON,
-                             PRECISION_F64, PRECISION_MIXED, SYMPLECTIC_EULER, EXPLICIT_EULER, step_params)
+                             PRECISION_F64, PRECISION_MIXED, PRECISION_MIXED_FAST, SYMPLECTIC_EULER, EXPLICIT_EULER,
+                             step_params)
 
 pytestmark = pytest.mark.gpu
 
@@ -60,19 +61,20 @@ def test_gravity_stage_fp64_matches_oracle(device, oracle, law, n):
     assert np.abs(got - want).max() <= 1e-12 * scale
 
 
+@pytest.mark.parametrize("precision", [PRECISION_MIXED, PRECISION_MIXED_FAST])
 @pytest.mark.parametrize("law", [GRAVITY_SIZE_CORE, GRAVITY_PLUMMER])
-def test_gravity_stage_mixed_error_bound(device, oracle, law):
-    """FP32 pair terms with tile-relative positions and FP64 tile accumulation. Bounds: median
-    per-body relative force error below 1e-6, and every body's error below 5e-5 of the root mean
-    square force (a body whose pulls nearly cancel has a small net force, so its own relative
-    error is not the right yardstick)."""
+def test_gravity_stage_mixed_error_bound(device, oracle, law, precision):
+    """FP32 pair terms (on double-single separations in MIXED, tile-relative FP32 positions in
+    MIXED_FAST) and FP64 tile accumulation. Bounds: median per-body relative force error below
+    1e-6, and every body's error below 5e-5 of the root mean square force (a body whose pulls
+    nearly cancel has a small net force, so its own relative error is not the right yardstick)."""
     n = 4096
     bodies = scenarios.gravity_world(n, 1000.0, seed=9)
     pm = pos_mass(bodies)
     d_pm, d_size = dev_tensor(pm), dev_tensor(np.ascontiguousarray(bodies["size"]))
     d_f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
-    _lib.check(_lib.lib().exg_gravity_forces(device.handle, vp(d_pm), vp(d_size), n, law, 1.0, 0.05, PRECISION_MIXED,
+    _lib.check(_lib.lib().exg_gravity_forces(device.handle, vp(d_pm), vp(d_size), n, law, 1.0, 0.05, precision,
                                              vp(d_f)))
     got = d_f.cpu().numpy().reshape(n, 3)
     want = oracle.gravity_forces(bodies, law, 1.0, 0.05)
@@ -263,3 +265,24 @@ def test_uniform_field_matches_oracle(device, oracle, scheme):
         pe, me = state_error(ow.bodies(), dw.bodies())
         assert pe < 1e-9 and me < 1e-7, (min_bodies, pe, me)
         dw.close()
+
+
+def test_mixed_gravity_world_1000_steps_within_1e6_of_f64(device, oracle):
+    """The mixed path's accuracy target: a config-0 cluster (1024 bodies in a ball of radius 100,
+    Plummer 0.05, LieEuler, dt 1e-3) after 1000 steps against the f64 oracle — relative pose
+    error at most 1e-6. The single-FP32 form (MIXED_FAST) is stated beside it: its close pairs
+    carry the rounding of their distance to the tile reference, which the cluster amplifies."""
+    bodies = scenarios.gravity_world(1024, 100.0, seed=7)
+    kw = dict(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, softening=0.05, dt=1e-3)
+    ow = oracle.OracleWorld(bodies, np.zeros(0, dtype=JOINT_DTYPE), step_params(**kw))
+    ow.step(1000)
+    want = ow.bodies()
+    dw = _lib.DeviceWorld(device, bodies, np.zeros(0, dtype=JOINT_DTYPE), step_params(precision=PRECISION_MIXED, **kw))
+    dw.step(1000)
+    pe, me = state_error(want, dw.bodies())
+    assert pe <= 1e-6, pe
+    fw = _lib.DeviceWorld(device, bodies, np.zeros(0, dtype=JOINT_DTYPE),
+                          step_params(precision=PRECISION_MIXED_FAST, **kw))
+    fw.step(1000)
+    pf, mf = state_error(want, fw.bodies())
+    assert pf < 1e-4 and pf > pe, (pf, pe)

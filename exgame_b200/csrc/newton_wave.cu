@@ -28,7 +28,6 @@ enum WaveEval { EV_NONE = 0, EV_FULL = 1, EV_JAC = 2, EV_PLAIN = 3 };
 enum WaveFlag {
   F_START = 1,       // load the world state, best = vm
   F_COPY_BEST = 2,   // best = vm
-  F_MASS0 = 4,       // mass0 = mass
   F_ACCEPT = 8,      // vm = trial
   F_BASE = 16,       // base = vm
   F_TRIAL = 32,      // trial = base + alpha dv
@@ -43,6 +42,7 @@ struct WaveCtl {
   int spans, iters, maxdepth, it;
   int carried, lane, converged, assembled;
   int nz, singular, commit_converged, active;
+  int mflip;  // 1: the scratch's mass and mass0 blocks trade places (see wave_ctx)
 };
 
 struct WaveArgs {
@@ -74,6 +74,20 @@ int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 
+// An island's context in the wave. "mass0 = mass" (the island kernel copies 36 values per node)
+// is a swap of the two block arrays' roles here: the evaluation writes the blocks into `mass`, and
+// adopting them as mass0 flips mflip, so the next evaluation writes into the other array.
+__device__ __forceinline__ Ctx wave_ctx(const WaveArgs& a, int k) {
+  Ctx c = make_ctx(a.A, a.W, a.isl[k]);
+  if (a.ctl[k].mflip) { double* t = c.s.mass; c.s.mass = c.s.mass0; c.s.mass0 = t; }
+  return c;
+}
+__device__ __forceinline__ Ctx wave_ctx_lite(const WaveArgs& a, int k) {
+  Ctx c = make_ctx_lite(a.A, a.W, a.isl[k]);
+  if (a.ctl[k].mflip) { double* t = c.s.mass; c.s.mass = c.s.mass0; c.s.mass0 = t; }
+  return c;
+}
+
 // ── per-island control ──────────────────────────────────────────────────────
 // Step start: every island of an active world begins its span budget; load the external wrench.
 __global__ void k_w_init(WaveArgs a) {
@@ -88,6 +102,7 @@ __global__ void k_w_init(WaveArgs a) {
     c.last_best = 0.0;
     c.flags = 0;
     c.eval = EV_NONE;
+    c.mflip = 0;
   }
 }
 
@@ -95,7 +110,7 @@ __global__ void k_w_external(WaveArgs a) {
   for (int t = gtid(); t < a.n_body; t += gthreads()) {
     int2 it = a.body[t];
     if (!a.ctl[it.x].active) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     op_load_external(c, it.y);
   }
 }
@@ -158,7 +173,7 @@ __global__ void k_w_after_eval(WaveArgs a) {
         rnorm = c.carried_norm;
       } else {
         rnorm = __longlong_as_double((long long)c.worst_bits);
-        c.flags |= F_MASS0;
+        c.mflip ^= 1;  // mass0 = mass
       }
       c.carried = 0;
       c.rnorm = rnorm;
@@ -182,7 +197,7 @@ __global__ void k_w_after_eval(WaveArgs a) {
       const int max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
       double tnorm = __longlong_as_double((long long)c.worst_bits);
       bool acc = tnorm < c.rnorm;
-      if (c.lane == 0 || acc) c.flags |= F_MASS0;
+      if (c.lane == 0 || acc) c.mflip ^= 1;  // mass0 = mass
       if (acc) {
         c.flags |= F_ACCEPT;
         c.carried = 1;
@@ -280,7 +295,7 @@ __global__ void k_w_start(WaveArgs a) {
   for (int t = gtid(); t < a.n_body; t += gthreads()) {
     int2 it = a.body[t];
     if (!(a.ctl[it.x].flags & F_START)) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     op_load_world_state(c, it.y);
 #pragma unroll
     for (int k = 0; k < 6; ++k) c.s.best[6 * it.y + k] = c.s.vm[6 * it.y + k];
@@ -292,7 +307,7 @@ __global__ void k_w_pre(WaveArgs a) {
     int2 it = a.body[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     op_pre(c, w.eval == EV_FULL ? c.s.vm : c.s.trial, w.half, it.y);
   }
 }
@@ -322,7 +337,7 @@ __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, i
       const int ev = a.ctl[it.x].eval;
       if (ev == EV_FULL || ev == EV_JAC) {
         on = true;
-        Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+        Ctx c = wave_ctx(a, it.x);
         op_joint_slice<MIXED, LAW>(c, c.s.vm, it.y, t & 3, ev == EV_FULL, &stage[wib][lane >> 2][(t & 3) * kJacStride]);
       }
     }
@@ -348,7 +363,7 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
     int2 it = a.joint[first + t];
     const int ev = a.ctl[it.x].eval;
     if (!(ev == EV_PLAIN || (ev == EV_FULL && MIXED))) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     op_joint_value<LAW>(c, ev == EV_PLAIN ? c.s.trial : c.s.vm, it.y);
   }
 }
@@ -377,7 +392,7 @@ __global__ void k_w_post(WaveArgs a) {
     int2 it = a.dyn[t];
     WaveCtl& w = a.ctl[it.x];
     if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     double worst = op_post(c, w.eval == EV_FULL ? c.s.vm : c.s.trial, w.half, it.y);
     // non-negative doubles (and NaN, which must win as nan_max makes it win) order as integers
     atomicMax(&w.worst_bits, (unsigned long long)__double_as_longlong(worst));
@@ -391,7 +406,7 @@ __global__ void k_w_copy_bodies(WaveArgs a) {
     const WaveCtl& w = a.ctl[it.x];
     const int f = w.flags;
     if (!(f & (F_COPY_BEST | F_ACCEPT | F_BASE | F_TRIAL))) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     const int q = it.y;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
@@ -406,16 +421,6 @@ __global__ void k_w_copy_bodies(WaveArgs a) {
   }
 }
 
-// mass0 = mass, one thread per block entry (consecutive threads, consecutive entries).
-__global__ void k_w_copy_mass0(WaveArgs a) {
-  for (long long t = gtid(); t < 36LL * a.n_dyn; t += gthreads()) {
-    int2 it = a.dyn[t / 36];
-    if (!(a.ctl[it.x].flags & F_MASS0)) continue;
-    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
-    const size_t e = 36 * (size_t)it.y + (size_t)(t % 36);
-    c.s.mass0[e] = c.s.mass[e];
-  }
-}
 
 // Assembly, one warp per cell: lane e holds entry e (lanes 0..3 also entries 32..35), the term
 // list is read once per warp, and a term's Jacobian rows are contiguous across the lanes.
@@ -426,7 +431,7 @@ __global__ void k_w_assemble(WaveArgs a) {
     int2 it = a.cell[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
-    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx_lite(a, it.x);
     const int cell = it.y, i = cell / 3, kind = cell % 3;
     const int e0 = lane, e1 = lane + 32;
     const bool has1 = e1 < 36;
@@ -460,7 +465,7 @@ __global__ void k_w_node_sq(WaveArgs a, int want_state, int mass) {
     int2 it = a.dyn[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != want_state || (mass && !w.assembled)) continue;
-    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx_lite(a, it.x);
     const size_t o = 36 * (size_t)it.y;
     double s = 0.0;
     if (mass) {
@@ -511,7 +516,7 @@ __global__ void k_w_solve_down(WaveArgs a, int first, int count) {
     int2 it = a.level[first + t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
-    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx_lite(a, it.x);
     const int i = it.y;
     double D[36], b[6];
 #pragma unroll
@@ -576,7 +581,7 @@ __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
   for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
     if (a.ctl[it.x].state != WS_DIR) continue;
-    Ctx c = make_ctx_lite(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx_lite(a, it.x);
     const int i = it.y;
     const int p = c.A.dn_parent[c.d.dyn_off + i];
     const double* Acp = c.s.Acp + 36 * (size_t)i;
@@ -609,7 +614,7 @@ __global__ void k_w_nz(WaveArgs a) {
     int2 it = a.dyn[t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     double* dv = c.s.dv + 6 * it.y;
     int nz = 0;
     if (w.singular) {
@@ -629,7 +634,7 @@ __global__ void k_w_restore(WaveArgs a) {
   for (int t = gtid(); t < a.n_body; t += gthreads()) {
     int2 it = a.body[t];
     if (a.ctl[it.x].state != WS_END) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
 #pragma unroll
     for (int k = 0; k < 6; ++k) c.s.vm[6 * it.y + k] = c.s.best[6 * it.y + k];
   }
@@ -640,7 +645,7 @@ __global__ void k_w_commit(WaveArgs a) {
     int2 it = a.dyn[t];
     const WaveCtl& w = a.ctl[it.x];
     if (!(w.flags & F_COMMIT)) continue;
-    Ctx c = make_ctx(a.A, a.W, a.isl[it.x]);
+    Ctx c = wave_ctx(a, it.x);
     op_commit(c, w.span, w.half, w.commit_converged != 0, it.y);
   }
 }
@@ -740,7 +745,6 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
   const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
   const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
-  const int g_entry = grid_for(dev, 36LL * a.n_dyn, T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
   k_w_init<<<g_isl, T, 0, s>>>(a);
@@ -767,7 +771,6 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     k_w_post<<<g_dyn, T, 0, s>>>(a);
     k_w_after_eval<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
-    k_w_copy_mass0<<<g_entry, T, 0, s>>>(a);
     if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
     k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);

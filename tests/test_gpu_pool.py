@@ -196,3 +196,28 @@ def test_whole_handle_records_follow_slot_order_through_page_locked_buffers(devi
     k = sorted(pool.counts)[1]
     assert same(pool.world_bodies(k), buf[pool.counts[sorted(pool.counts)[0]]:][:pool.counts[k]])
     pool.close()
+
+
+def test_server_fails_a_non_finite_world_and_serves_the_rest(device):
+    """A request whose world is not finite (a NaN momentum) fails with EXG_ERR_FATAL (the
+    reference's EvalError::Fatal of a guarded site), while the requests beside it complete and
+    equal their worlds stepped alone."""
+    worlds = world_set()
+    bad_b, bad_j, bad_p = worlds[6]
+    bad_b = bad_b.copy()
+    bad_b["momentum"][3, 0] = np.nan
+    srv = _lib.Server(device, max_bodies=8192, max_joints=8192, max_worlds=8, steps_per_tick=4)
+    good = [srv.submit(*worlds[k], 6) for k in (1, 5, 7)]
+    bad = srv.submit(bad_b, bad_j, bad_p, 6)
+    for k, rid in zip((1, 5, 7), good):
+        out, info = srv.wait(rid, timeout_ms=120000)
+        assert same(out, alone(device, worlds[k], 6)), k
+    with pytest.raises(_lib.ExgError) as e:
+        srv.wait(bad, timeout_ms=120000)
+    assert e.value.name == "EXG_ERR_FATAL"
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 3
+    # the loop is still serving
+    out, _ = srv.wait(srv.submit(*worlds[0], 2), timeout_ms=60000)
+    assert same(out, alone(device, worlds[0], 2))
+    srv.close()

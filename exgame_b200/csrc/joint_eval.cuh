@@ -30,10 +30,15 @@ EXG_HD void joint_plain(int law, const double* prm, const R* pose_a, const R* po
 }
 
 // One slice: value[6] of the wrench on a and d[6][6] = d(wrench on a component r)/d(axis 6s+c),
-// stored d[r*6 + c].
-template <class R>
-EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
-                                 const R* vel_b, double dt, double warp, int slice, R* value6, R* d36) {
+// stored d[r*6 + c]. With N = 3 one call evaluates half a slice — the axes 6s + 3h .. 6s + 3h + 2
+// (h = half) — and fills columns 3h .. 3h + 2 of d (value6 as well); each derivative column is
+// computed by the same dual operations whatever N is, so two halves give the full slice's values
+// bit for bit with about half the live state per thread.
+template <class R, int N = 6>
+EXG_HD void joint_jacobian_part(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
+                                const R* vel_b, double dt, double warp, int slice, int half, R* value6, R* d36) {
+  static_assert(N == 6 || N == 3, "a slice is evaluated whole or in halves");
+  const int c0 = N == 6 ? 0 : 3 * half;
   if (law == LAW_TORSIONAL) {
     // The couple -k (w_a - w_b) depends on the angular velocities only, linearly: its Jacobian is
     // -k I (velocity A) and +k I (velocity B) on the torque rows, zero elsewhere — exactly what the
@@ -46,17 +51,19 @@ EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, co
 #pragma unroll
     for (int r = 0; r < 6; ++r) value6[r] = w6[r];
 #pragma unroll
-    for (int k = 0; k < 36; ++k) d36[k] = R(0.0);
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < N; ++c) d36[r * 6 + c0 + c] = R(0.0);
     if (slice >= 2) {
       R k = -R(prm[0] / (warp * warp));
       R g = slice == 2 ? k : -k;
-      d36[3 * 6 + 3] = g;
-      d36[4 * 6 + 4] = g;
-      d36[5 * 6 + 5] = g;
+#pragma unroll
+      for (int r = 3; r < 6; ++r)
+        if (r >= c0 && r < c0 + N) d36[r * 6 + r] = g;
     }
     return;
   }
-  using D = Dual<6, R>;
+  using D = Dual<N, R>;
   D ma[8], mb[8], va[6], vb[6];
 #pragma unroll
   for (int i = 0; i < 8; ++i) { ma[i] = D(0.0); ma[i].v = pose_a[i]; mb[i] = D(0.0); mb[i].v = pose_b[i]; }
@@ -66,7 +73,11 @@ EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, co
     // pose seed: (1 + delta) * base with delta = Twist(seed lin, seed ang), value 0
     D seed6[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) { seed6[i] = D(0.0); seed6[i].g[i] = R(1); }
+    for (int i = 0; i < 6; ++i) {
+      seed6[i] = D(0.0);
+#pragma unroll
+      for (int c = 0; c < N; ++c) seed6[i].g[c] = (i == c0 + c) ? R(1) : R(0);  // static register index
+    }
     D delta[6], one_delta[8];
     screw_from6(seed6, delta);
     one_delta[0] = D(1.0);
@@ -80,7 +91,10 @@ EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, co
   } else {
     D* v = (slice == 2) ? va : vb;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) v[i].g[i] = R(1);
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        if (i == c0 + c) v[i].g[c] = R(1);
   }
   D ta[6], tb[6], wa[6], w6[6];
   screw_from6(va, ta);
@@ -91,8 +105,14 @@ EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, co
   for (int r = 0; r < 6; ++r) {
     value6[r] = w6[r].v;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) d36[r * 6 + c] = w6[r].g[c];
+    for (int c = 0; c < N; ++c) d36[r * 6 + c0 + c] = w6[r].g[c];
   }
+}
+
+template <class R>
+EXG_HD void joint_jacobian_slice(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
+                                 const R* vel_b, double dt, double warp, int slice, R* value6, R* d36) {
+  joint_jacobian_part<R, 6>(law, prm, pose_a, pose_b, vel_a, vel_b, dt, warp, slice, 0, value6, d36);
 }
 
 }  // namespace exg

@@ -172,6 +172,33 @@ __device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
 // duals; the values that enter the residual always come from an FP64 evaluation (op_joint_value,
 // or in FP64 the dual's value part, which equals it bit for bit: write_conn on slice 0), so the
 // converged iterate is an FP64 solution whatever the Jacobian's precision.
+// Half of slice `slice` (axes 6 slice + 3 half .. + 2) of joint q at (mid, x), into the slice's
+// 42-value record at dst: its three derivative columns and (half 0) the value part. Two halves
+// make the slice bit for bit (joint_jacobian_part).
+template <bool MIXED, int LAW = -1>
+__device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q, int slice, int half, bool write_conn,
+                                           typename JacType<MIXED>::T* dst) {
+  typedef typename JacType<MIXED>::T J;
+  const int joff = c.d.joint_off;
+  const int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
+  const int law = LAW >= 0 ? LAW : c.A.jl_law[joff + q];
+  const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
+  J pa[8], pb[8], va[6], vb[6], val[6];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) { pa[k] = J(c.s.mid[8 * a + k]); pb[k] = J(c.s.mid[8 * b + k]); }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) { va[k] = J(x[6 * a + k]); vb[k] = J(x[6 * b + k]); }
+  joint_jacobian_part<J, 3>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst + 6);
+  if (half == 0) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) dst[r] = val[r];
+  }
+  if (!MIXED && write_conn && slice == 0 && half == 0) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = double(val[r]);
+  }
+}
+
 // The slice's 42 values go to `dst` when given (a staging buffer), else to the island's scratch.
 template <bool MIXED, int LAW = -1>
 __device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int slice, bool write_conn,

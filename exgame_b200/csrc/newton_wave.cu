@@ -318,34 +318,38 @@ __global__ void k_w_pre(WaveArgs a) {
 //   values: [0, n) FP64 values, for an iterate evaluated afresh (mixed path; in FP64 the slices'
 //           value parts are the values) and for a probe. A carried iterate keeps the values the
 //           accepted probe left at the same point.
-// The four slices of a joint are four adjacent lanes; a warp holds 8 joints. Each lane writes its
-// slice into the warp's staging block in shared memory, and the warp then stores each joint's four
-// contiguous slices (4 x 42 values, 16-byte aligned) with 16-byte stores spread over the lanes.
+// A joint's four slices are evaluated as eight half slices (3 axes each: half the dual state per
+// thread, so more threads fit on an SM) by eight adjacent lanes; a warp holds 4 joints. Each lane
+// writes its part of the joint's slice records into the warp's staging block in shared memory,
+// and the warp then stores each joint's four contiguous records (4 x 42 values, 16-byte aligned)
+// with 16-byte stores spread over the lanes.
 template <bool MIXED, int LAW>
 __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
   typedef typename JacType<MIXED>::T J;
   constexpr int kJoint = 4 * kJacStride;  // values per joint
-  __shared__ __align__(16) J stage[4][8][kJoint];
+  __shared__ __align__(16) J stage[4][4][kJoint];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int total = 4 * n;
+  const int total = 8 * n;
   for (int base = gtid() - lane; base < total; base += gthreads()) {  // warp-uniform loop
     const int t = base + lane;
     bool on = false;
     int2 it = make_int2(0, 0);
     if (t < total) {
-      it = a.joint[first + (t >> 2)];
+      it = a.joint[first + (t >> 3)];
       const int ev = a.ctl[it.x].eval;
       if (ev == EV_FULL || ev == EV_JAC) {
         on = true;
         Ctx c = wave_ctx(a, it.x);
-        op_joint_slice<MIXED, LAW>(c, c.s.vm, it.y, t & 3, ev == EV_FULL, &stage[wib][lane >> 2][(t & 3) * kJacStride]);
+        const int slice = (t >> 1) & 3, half = t & 1;
+        op_joint_half_slice<MIXED, LAW>(c, c.s.vm, it.y, slice, half, ev == EV_FULL,
+                                        &stage[wib][lane >> 3][slice * kJacStride]);
       }
     }
     const unsigned active = __ballot_sync(0xffffffffu, on);
     __syncwarp();
-    for (int j = 0; j < 8; ++j) {
-      if (!((active >> (4 * j)) & 1u)) continue;  // the joint's island did not evaluate slices
-      const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
+    for (int j = 0; j < 4; ++j) {
+      if (!((active >> (8 * j)) & 1u)) continue;  // the joint's island did not evaluate slices
+      const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 8 * j), __shfl_sync(0xffffffffu, it.y, 8 * j));
       const IslandDesc& d = a.A.desc[a.isl[jt.x]];
       J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) + (size_t)jt.y * kJoint;
       const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
@@ -371,7 +375,7 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
 template <bool MIXED, int LAW>
 void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
   const int per = 2 * dev->tune_wave_blocks_per_sm;
-  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 4LL * n, 128, per), 128, 0, s>>>(a, first, n);
+  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 8LL * n, 128, per), 128, 0, s>>>(a, first, n);
   k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, s>>>(a, first, n);
 }
 

@@ -40,4 +40,31 @@ void dh_coad(const double* w6, const double* t6, double* o6) {
   double w[6], t[6], r[6]; exg::screw_from6(w6, w); exg::screw_from6(t6, t); exg::coad_bracket(w, t, r); exg::screw_to6(r, o6);
 }
 void dh_rotation_part(const double* m8, double* o8) { exg::motor_rotation_part(m8, o8); }
+// full 12 x 25 block from eight half slices (3 axes each), FP64 and FP32
+void dh_joint_jacobian_halves(int law, const double* prm, const double* pa, const double* pb, const double* va,
+                              const double* vb, double dt, double warp, double* out300) {
+  for (int s = 0; s < 4; ++s) {
+    double v[6], d[36];
+    for (int h = 0; h < 2; ++h) exg::joint_jacobian_part<double, 3>(law, prm, pa, pb, va, vb, dt, warp, s, h, v, d);
+    for (int r = 0; r < 6; ++r) {
+      out300[r * 25] = v[r];
+      out300[(6 + r) * 25] = -v[r];
+      for (int c = 0; c < 6; ++c) {
+        out300[r * 25 + 1 + 6 * s + c] = d[r * 6 + c];
+        out300[(6 + r) * 25 + 1 + 6 * s + c] = -d[r * 6 + c];
+      }
+    }
+  }
+}
+void dh_jacobian_slices_f32(int law, const double* prm, const float* pa, const float* pb, const float* va,
+                            const float* vb, double dt, double warp, int halves, float* out168) {
+  for (int s = 0; s < 4; ++s) {
+    float* o = out168 + 42 * s;
+    if (halves) {
+      for (int h = 0; h < 2; ++h) exg::joint_jacobian_part<float, 3>(law, prm, pa, pb, va, vb, dt, warp, s, h, o, o + 6);
+    } else {
+      exg::joint_jacobian_part<float, 6>(law, prm, pa, pb, va, vb, dt, warp, s, 0, o, o + 6);
+    }
+  }
+}
 }

@@ -70,3 +70,33 @@ def test_joint_plain_and_jacobian_match_oracle(dh, oracle, law):
         wj = oracle.jacobian_eval(law, prm, pa, pb, va, vb, 0.016, 1.3)
         assert np.allclose(jac.reshape(12, 25), wj, rtol=1e-12, atol=1e-12)
         assert np.array_equal(jac.reshape(12, 25)[:, 0], out)  # Jacobian kernel value == plain value
+
+
+def test_half_slices_equal_whole_slices_bit_for_bit(dh):
+    """A Jacobian slice evaluated as two 3-axis halves (what the wave's joint kernels do) equals the
+    6-axis slice bit for bit, in FP64 and FP32, for every law."""
+    rng = np.random.default_rng(12)
+    from exgame_b200 import _lib
+    for law in range(4):
+        for _ in range(5):
+            prm = rng.normal(size=10)
+            prm[6:9] = np.abs(prm[6:9]) + 0.5
+            prm[9] = 1e-6
+            if law >= 2:
+                prm[:2] = np.abs(prm[:2])
+            pa = _lib.motor_exp(rng.normal(size=6), 1.0)
+            pb = _lib.motor_exp(rng.normal(size=6), 1.0)
+            va, vb = rng.normal(size=6), rng.normal(size=6)
+            whole, halves = np.zeros(300), np.zeros(300)
+            args = (law, P(prm), P(pa), P(pb), P(va), P(vb), ctypes.c_double(0.016), ctypes.c_double(1.3))
+            dh.dh_joint_jacobian(*args, P(whole))
+            dh.dh_joint_jacobian_halves.argtypes = dh.dh_joint_jacobian.argtypes
+            dh.dh_joint_jacobian_halves(*args, P(halves))
+            assert np.array_equal(whole, halves), law
+            f = [np.ascontiguousarray(x, dtype=np.float32) for x in (pa, pb, va, vb)]
+            o6, o3 = np.zeros(168, np.float32), np.zeros(168, np.float32)
+            dh.dh_jacobian_slices_f32(law, P(prm), *[P(x) for x in f], ctypes.c_double(0.016), ctypes.c_double(1.3), 0,
+                                      P(o6))
+            dh.dh_jacobian_slices_f32(law, P(prm), *[P(x) for x in f], ctypes.c_double(0.016), ctypes.c_double(1.3), 1,
+                                      P(o3))
+            assert np.array_equal(o6, o3), law

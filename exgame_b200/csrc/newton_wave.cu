@@ -429,7 +429,7 @@ __global__ void k_w_copy_bodies(WaveArgs a) {
 // Assembly, one warp per cell: lane e holds entry e (lanes 0..3 also entries 32..35), the term
 // list is read once per warp, and a term's Jacobian rows are contiguous across the lanes.
 template <bool MIXED>
-__global__ void k_w_assemble(WaveArgs a) {
+__global__ void __launch_bounds__(256, 8) k_w_assemble(WaveArgs a) {
   const int lane = threadIdx.x & 31;
   for (int t = gtid() >> 5; t < a.n_cell; t += gthreads() >> 5) {
     int2 it = a.cell[t];

@@ -391,7 +391,7 @@ void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_f
   }
 }
 
-__global__ void k_w_post(WaveArgs a) {
+__global__ void __launch_bounds__(256, 2) k_w_post(WaveArgs a) {
   for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
     int2 it = a.dyn[t];
     WaveCtl& w = a.ctl[it.x];

@@ -785,6 +785,7 @@ static int step_locked(exg_world_s* W, int32_t n_steps) {
     }
   }
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (W->newton->has_wave() && (rc = W->newton->wave_after_steps(W->dev)) != EXG_OK) return rc;
   W->stats.steps += n_steps;
   W->stats.last_spans = 1;
   if (W->n_implicit > 0) {

@@ -359,7 +359,6 @@ long long newton_footprint_bytes(int nb, int nj) {
 
 NewtonWorld::~NewtonWorld() {
   if (wave_graph_) cudaGraphExecDestroy(wave_graph_);
-  if (h_live_) cudaFreeHost(h_live_);
   for (DevArr<int>* a : {&dw_isl_, &dw_dyn_first_, &dw_live_}) a->release();
   for (DevArr<int2>* a : {&dw_body_, &dw_dyn_, &dw_joint_, &dw_cell_, &dw_level_}) a->release();
   dw_ctl_.release();

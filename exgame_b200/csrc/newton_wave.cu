@@ -62,7 +62,7 @@ struct WaveArgs {
   const int2* level;    // (slot, node) grouped by elimination level
   const int* dyn_first; // first dynamic-node item of each wave slot (n_isl + 1 entries)
   double* nodesq;       // per dynamic-node item: a sum of squares to reduce per island
-  int* live;            // islands not yet done after the round
+  int* live;            // counters, see kLive* below
 };
 
 int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
@@ -70,6 +70,15 @@ int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
   long long cap = (long long)std::max(1, dev->sm_count) * per_sm;
   return (int)std::max<long long>(1, std::min(g, cap));
 }
+
+// Device counters of the wave (a.live): islands still stepping after the last round, rounds of
+// this step, the round cap reached with islands unfinished, and cumulative rounds / direction
+// sections / end sections (for the host's count of launched kernels).
+enum { kLiveIslands = 0, kLiveRounds = 1, kLiveOverflow = 2, kLiveTotalRounds = 3, kLiveTotalDir = 4,
+       kLiveTotalEnd = 5, kLiveCount = 6 };
+// Rounds one step may take before the wave gives up on it (EXG_ERR_FATAL); a step of a
+// well-formed island needs at most spans x iterations x (1 + probes), far fewer in practice.
+constexpr int kMaxRoundsPerStep = 1 << 17;
 
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
@@ -91,6 +100,10 @@ __device__ __forceinline__ Ctx wave_ctx_lite(const WaveArgs& a, int k) {
 // ── per-island control ──────────────────────────────────────────────────────
 // Step start: every island of an active world begins its span budget; load the external wrench.
 __global__ void k_w_init(WaveArgs a) {
+  if (gtid() == 0) {
+    a.live[kLiveRounds] = 0;
+    a.live[kLiveOverflow] = 0;
+  }
   for (int k = gtid(); k < a.n_isl; k += gthreads()) {
     WaveCtl& c = a.ctl[k];
     const IslandDesc& d = a.A.desc[a.isl[k]];
@@ -279,7 +292,25 @@ __global__ void k_w_end(WaveArgs a) {
   }
 }
 
-__global__ void k_w_count(WaveArgs a) {
+// Whether any island is in `state` after the previous kernels: the condition of the round's
+// direction (WS_DIR) or span-end (WS_END) section. One block.
+__global__ void k_w_cond(WaveArgs a, cudaGraphConditionalHandle h, int state, int counter) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int k = threadIdx.x; k < a.n_isl; k += blockDim.x) mine |= a.ctl[k].state == state;
+  if (mine) atomicOr(&any, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (any) atomicAdd(&a.live[counter], 1);
+    cudaGraphSetConditional(h, any ? 1u : 0u);
+  }
+}
+
+// Round end: islands still stepping; the loop's condition (some island unfinished and the cap not
+// reached). One block.
+__global__ void k_w_count(WaveArgs a, cudaGraphConditionalHandle h_loop) {
   __shared__ int n;
   if (threadIdx.x == 0) n = 0;
   __syncthreads();
@@ -287,7 +318,14 @@ __global__ void k_w_count(WaveArgs a) {
   for (int k = threadIdx.x; k < a.n_isl; k += blockDim.x) mine += a.ctl[k].state != WS_DONE;
   atomicAdd(&n, mine);
   __syncthreads();
-  if (threadIdx.x == 0) *a.live = n;
+  if (threadIdx.x == 0) {
+    a.live[kLiveIslands] = n;
+    const int r = ++a.live[kLiveRounds];
+    ++a.live[kLiveTotalRounds];
+    const bool over = n > 0 && r >= kMaxRoundsPerStep;
+    if (over) a.live[kLiveOverflow] = 1;
+    cudaGraphSetConditional(h_loop, (n > 0 && !over) ? 1u : 0u);
+  }
 }
 
 // ── data phases over all islands' items ─────────────────────────────────────
@@ -710,7 +748,11 @@ int NewtonWorld::build_wave(cudaStream_t s) {
   up(dw_level_, level);
   if (rc == EXG_OK) rc = dw_ctl_.reserve(std::max<long long>((long long)isl.size(), 1) * (long long)sizeof(WaveCtl), s);
   if (rc == EXG_OK) rc = dw_nodesq_.reserve(std::max<long long>((long long)dyn.size(), 1), s);
-  if (rc == EXG_OK) rc = dw_live_.reserve(1, s);
+  if (rc == EXG_OK && dw_live_.cap == 0) {
+    std::vector<int> z(kLiveCount, 0);
+    rc = dw_live_.assign(z.data(), kLiveCount, s);
+    seen_rounds_ = seen_dir_ = seen_end_ = 0;
+  }
   if (rc != EXG_OK) return rc;
   n_wave_ = (int)isl.size();
   wave_counts_[0] = (int)body.size();
@@ -743,15 +785,17 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   a.dyn_first = dw_dyn_first_.ptr;
   a.nodesq = dw_nodesq_.ptr;
   a.live = dw_live_.ptr;
-  const bool mixed = w.precision != EXG_PRECISION_F64;
   const int T = 256;
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
-  const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
-  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
-  const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
+  if (wave_graph_ && wave_mixed_ != (w.precision != EXG_PRECISION_F64)) {
+    cudaGraphExecDestroy(wave_graph_);
+    wave_graph_ = nullptr;
+  }
+  wave_mixed_ = w.precision != EXG_PRECISION_F64;
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
   k_w_init<<<g_isl, T, 0, s>>>(a);
+  dev->launches.fetch_add(1, std::memory_order_relaxed);
   k_w_external<<<g_body, T, 0, s>>>(a);
   int rc = exg_after_launch(dev);
   if (rc != EXG_OK) return rc;
@@ -764,9 +808,68 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   if (!wave_graph_) {
     std::memcpy(wave_graph_world_, &a.W, sizeof(WorldRef));
     wave_graph_tuning_ = dev->tune_wave_blocks_per_sm;
-    // one round, captured once per structure
-    cudaGraph_t g;
-    EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    rc = build_wave_graph(dev, &a, s);
+    if (rc != EXG_OK) return rc;
+  }
+  EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
+  prof_end(dev, tok, s);
+  return EXG_OK;
+}
+
+// The step's rounds as one graph: WHILE (some island unfinished) { evaluation; IF (some island
+// needs a direction) { assembly, elimination, line-search start }; IF (some span ends) { commit } }.
+// The conditions are set on the device (k_w_cond, k_w_count), so a step needs no host round trip.
+int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStream_t s) {
+  const WaveArgs& a = *static_cast<const WaveArgs*>(args);
+  const bool mixed = a.W.n >= 0 && wave_mixed_;
+  const int T = 256;
+  const int g_isl = grid_for(dev, a.n_isl, T, 4);
+  const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
+  const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
+  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
+  const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
+  const int nl = (int)wave_level_ptr_.size() - 1;
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t G = nullptr;
+  EXG_CUDA_TRY(cudaGraphCreate(&G, 0));
+  struct Guard { cudaGraph_t g; ~Guard() { if (g) cudaGraphDestroy(g); } } guard{G};
+  cudaGraphConditionalHandle h_loop, h_dir, h_end;
+  EXG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_loop, G, 1, cudaGraphCondAssignDefault));
+  EXG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_dir, G, 0, cudaGraphCondAssignDefault));
+  EXG_CUDA_TRY(cudaGraphConditionalHandleCreate(&h_end, G, 0, cudaGraphCondAssignDefault));
+  auto conditional = [&](cudaGraph_t parent, const cudaGraphNode_t* deps, size_t nd, cudaGraphConditionalHandle h,
+                         cudaGraphConditionalNodeType type, cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, parent, deps, nd, &p);
+    if (e == cudaSuccess) *body = p.conditional.phGraph_out[0];
+    return e;
+  };
+  // capture launches into `graph` after `deps`; returns the new tail
+  std::vector<cudaGraphNode_t> tail;
+  auto capture = [&](cudaGraph_t graph, const std::vector<cudaGraphNode_t>& deps, auto&& launches) -> cudaError_t {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                  mode);
+    if (e != cudaSuccess) return e;
+    launches();
+    cudaError_t le = cudaGetLastError();
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* d = nullptr;
+    size_t n = 0;
+    cudaError_t ie = cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, &d, &n);
+    if (ie == cudaSuccess) tail.assign(d, d + n);
+    cudaGraph_t out;
+    cudaError_t ee = cudaStreamEndCapture(s, &out);
+    return le != cudaSuccess ? le : (ie != cudaSuccess ? ie : ee);
+  };
+  cudaGraphNode_t loop, if_dir, if_end;
+  cudaGraph_t B, BD, BE;
+  EXG_CUDA_TRY(conditional(G, nullptr, 0, h_loop, cudaGraphCondTypeWhile, &loop, &B));
+  // evaluation of every island at its iterate or probe
+  EXG_CUDA_TRY(capture(B, {}, [&] {
     k_w_begin<<<g_isl, T, 0, s>>>(a);
     k_w_start<<<g_body, T, 0, s>>>(a);
     k_w_pre<<<g_body, T, 0, s>>>(a);
@@ -775,11 +878,15 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     k_w_post<<<g_dyn, T, 0, s>>>(a);
     k_w_after_eval<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+    k_w_cond<<<1, 1024, 0, s>>>(a, h_dir, WS_DIR, kLiveTotalDir);
+  }));
+  EXG_CUDA_TRY(conditional(B, tail.data(), tail.size(), h_dir, cudaGraphCondTypeIf, &if_dir, &BD));
+  // direction: assembly, elimination level by level, back substitution, line-search start
+  EXG_CUDA_TRY(capture(BD, {}, [&] {
     if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
     k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);
     k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
-    const int nl = (int)wave_level_ptr_.size() - 1;
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
       k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
@@ -791,41 +898,40 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+  }));
+  EXG_CUDA_TRY(capture(B, {if_dir}, [&] { k_w_cond<<<1, 1024, 0, s>>>(a, h_end, WS_END, kLiveTotalEnd); }));
+  EXG_CUDA_TRY(conditional(B, tail.data(), tail.size(), h_end, cudaGraphCondTypeIf, &if_end, &BE));
+  // span end: the best iterate back, the stiffness signal, sub-division or commit
+  EXG_CUDA_TRY(capture(BE, {}, [&] {
     k_w_restore<<<g_body, T, 0, s>>>(a);
     k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_END, 1);
     k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_END, 1);
     k_w_end<<<g_isl, T, 0, s>>>(a);
     k_w_commit<<<g_dyn, T, 0, s>>>(a);
-    k_w_count<<<1, 1024, 0, s>>>(a);
-    cudaError_t le = cudaGetLastError();
-    cudaError_t e = cudaStreamEndCapture(s, &g);
-    EXG_CUDA_TRY(le);
-    EXG_CUDA_TRY(e);
-    cudaError_t ie = cudaGraphInstantiate(&wave_graph_, g, 0);
-    cudaGraphDestroy(g);
-    EXG_CUDA_TRY(ie);
-    wave_graph_kernels_ = 22 + 2 * nl;
-  }
-  if (!h_live_) EXG_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&h_live_), sizeof(int)));
-  // Rounds until every island has finished the step. Each round advances every unfinished
-  // island by one evaluation, and a step takes a bounded number of them (spans x iterations x
-  // probes), so the loop's bound is never the reason it stops for a well-formed island.
-  const int kMaxRounds = (1 << kMaxDepth) * 2 * 32 * (kLineSearchLanes + 1);
-  int rounds = 0;
-  for (;;) {
-    // a few rounds between checks: nearly every island needs several
-    const int batch = rounds < 4 ? 4 : 1;
-    for (int r = 0; r < batch; ++r) {
-      EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
-      dev->launches.fetch_add(wave_graph_kernels_);
-    }
-    rounds += batch;
-    EXG_CUDA_TRY(cudaMemcpyAsync(h_live_, dw_live_.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
-    EXG_CUDA_TRY(cudaStreamSynchronize(s));
-    if (*h_live_ == 0) break;
-    if (rounds >= kMaxRounds) return EXG_ERR_FATAL;
-  }
-  prof_end(dev, tok, s);
-  last_wave_rounds_ = rounds;
+  }));
+  EXG_CUDA_TRY(capture(B, {if_end}, [&] { k_w_count<<<1, 1024, 0, s>>>(a, h_loop); }));
+  EXG_CUDA_TRY(cudaGraphInstantiate(&wave_graph_, G, 0));
+  int joint_kernels = 0;
+  for (int L = 0; L < 4; ++L)
+    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += 2;  // slices and values
+  wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
+  wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
+  wave_kernels_end_ = 5;
   return EXG_OK;
+}
+
+// After a synchronised step: the wave's launched-kernel count and whether a step hit the round
+// cap (reported as EXG_ERR_FATAL).
+int NewtonWorld::wave_after_steps(exg_device_s* dev) {
+  if (n_wave_ == 0 || dw_live_.cap < kLiveCount) return EXG_OK;
+  int v[kLiveCount];
+  EXG_CUDA_TRY(cudaMemcpy(v, dw_live_.ptr, sizeof v, cudaMemcpyDeviceToHost));
+  last_wave_rounds_ = v[kLiveRounds];
+  const long long dr = v[kLiveTotalRounds] - seen_rounds_, dd = v[kLiveTotalDir] - seen_dir_,
+                  de = v[kLiveTotalEnd] - seen_end_;
+  seen_rounds_ = v[kLiveTotalRounds];
+  seen_dir_ = v[kLiveTotalDir];
+  seen_end_ = v[kLiveTotalEnd];
+  dev->launches.fetch_add((uint64_t)(dr * wave_kernels_eval_ + dd * wave_kernels_dir_ + de * wave_kernels_end_));
+  return v[kLiveOverflow] ? EXG_ERR_FATAL : EXG_OK;
 }

@@ -83,6 +83,8 @@ class NewtonWorld {
   // The wave schedule's step (host synchronous between rounds; call outside stream capture,
   // after the step's other kernels on the same stream).
   int run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s);
+  // After the stream is synchronised: launched-kernel accounting, round-cap check.
+  int wave_after_steps(exg_device_s* dev);
   int last_wave_rounds() const { return last_wave_rounds_; }
 
  private:
@@ -108,9 +110,11 @@ class NewtonWorld {
   DevArr<double> dw_nodesq_;
   cudaGraphExec_t wave_graph_ = nullptr;
   unsigned char wave_graph_world_[160] = {0};  // the world arrays the round graph was captured with
-  int wave_graph_kernels_ = 0;
+  int build_wave_graph(exg_device_s* dev, const void* args, cudaStream_t s);
+  bool wave_mixed_ = false;
+  int wave_kernels_eval_ = 0, wave_kernels_dir_ = 0, wave_kernels_end_ = 0;
+  long long seen_rounds_ = 0, seen_dir_ = 0, seen_end_ = 0;
   int wave_graph_tuning_ = 0;  // the launch-shape tuning the round graph was captured with
-  int* h_live_ = nullptr;
   int last_wave_rounds_ = 0;
   std::vector<WorldSrc> src_;
   bool dirty_ = true;

@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int wa
 // terms for the parent — S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's
 // slot until the back substitution writes dv) — so a parent only sums finished products; a root
 // solves for dv. The arithmetic per entry is the island kernel's (newton_ops.cuh).
-__global__ void k_w_solve_down(WaveArgs a, int first, int count) {
+__global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, int count) {
   for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
     WaveCtl& w = a.ctl[it.x];

@@ -574,7 +574,9 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
             else if (par[row] == col) target = 3 * row + 1;
             else if (par[col] == row) target = 3 * col + 2;
             else return EXG_ERR_UNSUPPORTED;
-            cells[target].push_back(q * 4 + re * 2 + ce);
+            // term: joint * 4 + row end * 2 + column end, bit kTermTorsional for the torsional law
+            const int tors = s_jl_law[jl0 + q] == LAW_TORSIONAL ? exg_newton::kTermTorsional : 0;
+            cells[target].push_back((q * 4 + re * 2 + ce) | tors);
           }
         }
       }

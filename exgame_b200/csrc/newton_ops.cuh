@@ -20,6 +20,9 @@ constexpr double kHuge = 1e9;
 constexpr double kFloor2 = 1e-9 * 1e-9;
 constexpr int kJacStride = 42;  // per (joint, slice): value[6] + d[36]
 constexpr int kLineSearchLanes = 8;
+// Assembly terms carry this bit when the joint's law is the torsional damper, whose Jacobian
+// slices are known in closed form (joint_jacobian_part): the wave reads no slices for them.
+constexpr int kTermTorsional = 1 << 30;
 
 struct Scratch {
   double *vm, *base, *best, *trial, *mid, *snap, *ext, *conn, *jac, *mass, *mass0, *rhs, *scale, *D, *Dinv, *Acp, *Apc, *S,
@@ -330,7 +333,7 @@ __device__ inline double op_assemble(const Ctx& c, double pf, double vf, int cel
   double acc = (kind == 0) ? c.s.mass0[36 * (size_t)i + e] : 0.0;
   int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
   for (int k = p0; k < p1; ++k) {
-    int term = c.A.cell_terms[k];
+    int term = c.A.cell_terms[k] & ~kTermTorsional;
     int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
     const auto* jp = jac_slice<MIXED>(c, q, ce) + 6;
     const auto* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;

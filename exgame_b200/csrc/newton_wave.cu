@@ -404,7 +404,8 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
   for (int t = gtid(); t < n; t += gthreads()) {
     int2 it = a.joint[first + t];
     const int ev = a.ctl[it.x].eval;
-    if (!(ev == EV_PLAIN || (ev == EV_FULL && MIXED))) continue;
+    // (no torsional slices are evaluated, so in FP64 the torsional values come from here too)
+    if (!(ev == EV_PLAIN || (ev == EV_FULL && (MIXED || LAW == LAW_TORSIONAL)))) continue;
     Ctx c = wave_ctx(a, it.x);
     op_joint_value<LAW>(c, ev == EV_PLAIN ? c.s.trial : c.s.vm, it.y);
   }
@@ -413,7 +414,8 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
 template <bool MIXED, int LAW>
 void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
   const int per = 2 * dev->tune_wave_blocks_per_sm;
-  k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 8LL * n, 128, per), 128, 0, s>>>(a, first, n);
+  if (LAW != LAW_TORSIONAL)  // the assembly knows the torsional slices in closed form
+    k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 8LL * n, 128, per), 128, 0, s>>>(a, first, n);
   k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, s>>>(a, first, n);
 }
 
@@ -480,16 +482,31 @@ __global__ void __launch_bounds__(256, 8) k_w_assemble(WaveArgs a) {
     double acc0 = (kind == 0) ? c.s.mass0[36 * (size_t)i + e0] : 0.0;
     double acc1 = (kind == 0 && has1) ? c.s.mass0[36 * (size_t)i + e1] : 0.0;
     const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+    typedef typename JacType<MIXED>::T J;
     for (int k = p0; k < p1; ++k) {
-      const int term = c.A.cell_terms[k];
+      const int raw = c.A.cell_terms[k];
+      const int term = raw & ~kTermTorsional;
       const int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
-      const auto* jp = jac_slice<MIXED>(c, q, ce) + 6;
-      const auto* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
-      double pv = double(jp[e0]), vv = double(jv[e0]);
+      double pv, vv, pv1 = 0.0, vv1 = 0.0;
+      if (raw & kTermTorsional) {
+        // the torsional couple's slices (joint_jacobian_part, value for value): zero pose columns,
+        // g = -/+ c / warp^2 on the angular diagonal of the velocity columns
+        const double warp = c.W.wparams[c.d.world].warp;
+        const J kk = -J(c.A.jl_params[10 * (size_t)(c.d.joint_off + q)] / (warp * warp));
+        const double g = double(ce == 0 ? kk : -kk);
+        pv = 0.0;
+        vv = (e0 >= 21 && e0 % 7 == 0) ? g : 0.0;  // entries (3,3), (4,4)
+        if (has1) vv1 = (e1 == 35) ? g : 0.0;      // entry (5,5)
+      } else {
+        const J* jp = jac_slice<MIXED>(c, q, ce) + 6;
+        const J* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
+        pv = double(jp[e0]);
+        vv = double(jv[e0]);
+        if (has1) { pv1 = double(jp[e1]); vv1 = double(jv[e1]); }
+      }
       if (re) { pv = -pv; vv = -vv; }
       acc0 = acc0 + w.pf * pv + w.vf * vv;
       if (has1) {
-        double pv1 = double(jp[e1]), vv1 = double(jv[e1]);
         if (re) { pv1 = -pv1; vv1 = -vv1; }
         acc1 = acc1 + w.pf * pv1 + w.vf * vv1;
       }
@@ -913,7 +930,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(cudaGraphInstantiate(&wave_graph_, G, 0));
   int joint_kernels = 0;
   for (int L = 0; L < 4; ++L)
-    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += 2;  // slices and values
+    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 2;
   wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
   wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
   wave_kernels_end_ = 5;

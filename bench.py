@@ -214,10 +214,15 @@ def newton_bytes_last_step(batch, parts):
     return total, iters
 
 
+WAVE_HOST_ROUNDS = 0  # --wave-host-rounds: profiler-friendly wave rounds (same arithmetic)
+
+
 def make_worlds(dev, parts):
-    if len(parts) == 1:
-        return [_lib.DeviceWorld(dev, *parts[0])]
-    return [_lib.DeviceBatch(dev, parts)]
+    ws = [_lib.DeviceWorld(dev, *parts[0])] if len(parts) == 1 else [_lib.DeviceBatch(dev, parts)]
+    if WAVE_HOST_ROUNDS:
+        for w in ws:
+            w.set_option(_lib.DeviceWorld.OPT_WAVE_HOST_ROUNDS, 1)
+    return ws
 
 
 def plain_path(dev, parts, flush, passes=1):
@@ -483,6 +488,8 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3-f64"])
     ap.add_argument("--worlds", type=int, default=4096, help="worlds of the config-3 batch")
     ap.add_argument("--autotune", type=int, default=1, help="tune launch shapes on this GPU first")
+    ap.add_argument("--wave-host-rounds", type=int, default=0,
+                    help="drive the wave's rounds from the host (for profilers that skip conditional graph nodes)")
     ap.add_argument("--shard", action="store_true",
                     help="split one batch over the ranks by body count (strong scaling) instead of one batch per rank")
     ap.add_argument("--serve-rates", default="100,1000,10000",
@@ -497,8 +504,8 @@ def main():
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     threads = os.cpu_count() or 1
-    global WORLDS, SHARD, WORLD_SIZE
-    WORLDS, SHARD, WORLD_SIZE = args.worlds, args.shard, world_size
+    global WORLDS, SHARD, WORLD_SIZE, WAVE_HOST_ROUNDS
+    WORLDS, SHARD, WORLD_SIZE, WAVE_HOST_ROUNDS = args.worlds, args.shard, world_size, args.wave_host_rounds
 
     if args.impl == "reference":
         if rank != 0:

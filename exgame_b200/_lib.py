@@ -273,7 +273,7 @@ class DeviceWorld:
         check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
         return s
 
-    OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS = 1, 2, 3
+    OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS, OPT_WAVE_HOST_ROUNDS = 1, 2, 3, 4
 
     def set_option(self, option, value):
         check(lib().exg_world_set_option(self.handle, int(option), int(value)), "exg_world_set_option")

@@ -698,6 +698,10 @@ int exg_world_set_option(exg_world_t W, int32_t option, int64_t value) {
       if (value < 1 || value > (1LL << 30)) return EXG_ERR_INVALID_ARGUMENT;
       W->newton->set_wave_threshold(W->newton->wave_min_dyn(), (int)value);
       break;
+    case EXG_OPT_WAVE_HOST_ROUNDS:
+      if (value != 0 && value != 1) return EXG_ERR_INVALID_ARGUMENT;
+      W->newton->set_wave_host_loop(value != 0);
+      return EXG_OK;
     default:
       return EXG_ERR_INVALID_ARGUMENT;
   }
@@ -712,6 +716,7 @@ int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
     case EXG_OPT_WAVE_MIN_BODIES: *value = W->newton->wave_min_dyn(); return EXG_OK;
     case EXG_OPT_WAVE_MAX_LEVELS: *value = W->newton->wave_max_levels(); return EXG_OK;
     case EXG_OPT_LAST_WAVE_ROUNDS: *value = W->newton->last_wave_rounds(); return EXG_OK;
+    case EXG_OPT_WAVE_HOST_ROUNDS: *value = W->newton->wave_host_loop() ? 1 : 0; return EXG_OK;
     default: return EXG_ERR_INVALID_ARGUMENT;
   }
 }

@@ -328,6 +328,21 @@ __global__ void k_w_count(WaveArgs a, cudaGraphConditionalHandle h_loop) {
   }
 }
 
+// Round end of the host-driven form: islands still stepping, the round counters. One block.
+__global__ void k_w_count_flat(WaveArgs a) {
+  __shared__ int n;
+  if (threadIdx.x == 0) n = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int k = threadIdx.x; k < a.n_isl; k += blockDim.x) mine += a.ctl[k].state != WS_DONE;
+  atomicAdd(&n, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.live[kLiveIslands] = n;
+    ++a.live[kLiveRounds];
+  }
+}
+
 // ── data phases over all islands' items ─────────────────────────────────────
 __global__ void k_w_start(WaveArgs a) {
   for (int t = gtid(); t < a.n_body; t += gthreads()) {
@@ -818,18 +833,99 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   if (rc != EXG_OK) return rc;
   static_assert(sizeof(WorldRef) <= sizeof(wave_graph_world_), "world snapshot too small");
   if (wave_graph_ && (std::memcmp(wave_graph_world_, &a.W, sizeof(WorldRef)) != 0 ||
-                      wave_graph_tuning_ != dev->tune_wave_blocks_per_sm)) {
+                      wave_graph_tuning_ != dev->tune_wave_blocks_per_sm || wave_graph_host_loop_ != wave_host_loop_)) {
     cudaGraphExecDestroy(wave_graph_);  // a world array moved since the capture
     wave_graph_ = nullptr;
   }
   if (!wave_graph_) {
     std::memcpy(wave_graph_world_, &a.W, sizeof(WorldRef));
     wave_graph_tuning_ = dev->tune_wave_blocks_per_sm;
-    rc = build_wave_graph(dev, &a, s);
+    wave_graph_host_loop_ = wave_host_loop_;
+    rc = wave_host_loop_ ? build_wave_round_graph(dev, &a, s) : build_wave_graph(dev, &a, s);
     if (rc != EXG_OK) return rc;
   }
-  EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
+  if (!wave_host_loop_) {
+    EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
+    prof_end(dev, tok, s);
+    return EXG_OK;
+  }
+  // Host-driven form: one flat round graph (every section launched, islands that do not need it
+  // skip it) replayed until a device counter says every island is done.
+  int v[kLiveCount];
+  int rounds = 0;
+  for (;;) {
+    const int batch = rounds < 4 ? 4 : 1;
+    for (int r = 0; r < batch; ++r) {
+      EXG_CUDA_TRY(cudaGraphLaunch(wave_graph_, s));
+      dev->launches.fetch_add(wave_kernels_eval_ + wave_kernels_dir_ + wave_kernels_end_);
+    }
+    rounds += batch;
+    EXG_CUDA_TRY(cudaMemcpyAsync(v, dw_live_.ptr, sizeof v, cudaMemcpyDeviceToHost, s));
+    EXG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (v[kLiveIslands] == 0) break;
+    if (rounds >= kMaxRoundsPerStep) return EXG_ERR_FATAL;
+  }
   prof_end(dev, tok, s);
+  last_wave_rounds_ = rounds;
+  return EXG_OK;
+}
+
+// The host-driven form's round: the same kernels as the conditional graph's body, every section
+// unconditional. For tools that do not follow kernels into conditional graph nodes (profilers).
+int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cudaStream_t s) {
+  const WaveArgs& a = *static_cast<const WaveArgs*>(args);
+  const bool mixed = wave_mixed_;
+  const int T = 256;
+  const int g_isl = grid_for(dev, a.n_isl, T, 4);
+  const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
+  const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
+  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
+  const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
+  const int nl = (int)wave_level_ptr_.size() - 1;
+  cudaGraph_t g;
+  EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  k_w_begin<<<g_isl, T, 0, s>>>(a);
+  k_w_start<<<g_body, T, 0, s>>>(a);
+  k_w_pre<<<g_body, T, 0, s>>>(a);
+  if (mixed) launch_joints_by_law<true>(dev, a, wave_law_first_, s);
+  else launch_joints_by_law<false>(dev, a, wave_law_first_, s);
+  k_w_post<<<g_dyn, T, 0, s>>>(a);
+  k_w_after_eval<<<g_isl, T, 0, s>>>(a);
+  k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+  if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
+  else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
+  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);
+  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
+  for (int L = nl - 1; L >= 0; --L) {
+    int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
+    k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+  }
+  for (int L = 1; L < nl; ++L) {
+    int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
+    k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+  }
+  k_w_nz<<<g_dyn, T, 0, s>>>(a);
+  k_w_after_solve<<<g_isl, T, 0, s>>>(a);
+  k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
+  k_w_restore<<<g_body, T, 0, s>>>(a);
+  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_END, 1);
+  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_END, 1);
+  k_w_end<<<g_isl, T, 0, s>>>(a);
+  k_w_commit<<<g_dyn, T, 0, s>>>(a);
+  k_w_count_flat<<<1, 1024, 0, s>>>(a);
+  cudaError_t le = cudaGetLastError();
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  EXG_CUDA_TRY(le);
+  EXG_CUDA_TRY(e);
+  cudaError_t ie = cudaGraphInstantiate(&wave_graph_, g, 0);
+  cudaGraphDestroy(g);
+  EXG_CUDA_TRY(ie);
+  int joint_kernels = 0;
+  for (int L = 0; L < 4; ++L)
+    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 2;
+  wave_kernels_eval_ = 6 + joint_kernels;
+  wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
+  wave_kernels_end_ = 6;
   return EXG_OK;
 }
 
@@ -940,7 +1036,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
 // After a synchronised step: the wave's launched-kernel count and whether a step hit the round
 // cap (reported as EXG_ERR_FATAL).
 int NewtonWorld::wave_after_steps(exg_device_s* dev) {
-  if (n_wave_ == 0 || dw_live_.cap < kLiveCount) return EXG_OK;
+  if (n_wave_ == 0 || dw_live_.cap < kLiveCount || wave_graph_host_loop_) return EXG_OK;
   int v[kLiveCount];
   EXG_CUDA_TRY(cudaMemcpy(v, dw_live_.ptr, sizeof v, cudaMemcpyDeviceToHost));
   last_wave_rounds_ = v[kLiveRounds];

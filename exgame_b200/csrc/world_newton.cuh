@@ -86,6 +86,10 @@ class NewtonWorld {
   // After the stream is synchronised: launched-kernel accounting, round-cap check.
   int wave_after_steps(exg_device_s* dev);
   int last_wave_rounds() const { return last_wave_rounds_; }
+  // Rounds driven from the host (one flat round graph per launch) instead of the conditional graph:
+  // the same arithmetic, for profilers that do not follow kernels into conditional graph nodes.
+  void set_wave_host_loop(bool on) { wave_host_loop_ = on; }
+  bool wave_host_loop() const { return wave_host_loop_; }
 
  private:
   struct WorldSrc {  // what rebuilding a world's islands needs
@@ -111,6 +115,8 @@ class NewtonWorld {
   cudaGraphExec_t wave_graph_ = nullptr;
   unsigned char wave_graph_world_[160] = {0};  // the world arrays the round graph was captured with
   int build_wave_graph(exg_device_s* dev, const void* args, cudaStream_t s);
+  int build_wave_round_graph(exg_device_s* dev, const void* args, cudaStream_t s);
+  bool wave_host_loop_ = false, wave_graph_host_loop_ = false;
   bool wave_mixed_ = false;
   int wave_kernels_eval_ = 0, wave_kernels_dir_ = 0, wave_kernels_end_ = 0;
   long long seen_rounds_ = 0, seen_dir_ = 0, seen_end_ = 0;

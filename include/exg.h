@@ -296,6 +296,10 @@ EXG_API int exg_server_destroy(exg_server_t server);
 #define EXG_OPT_WAVE_MIN_BODIES 1
 #define EXG_OPT_WAVE_MAX_LEVELS 2
 #define EXG_OPT_LAST_WAVE_ROUNDS 3 /* read only: rounds the wave schedule ran in the last step */
+/* 1: the wave's rounds are replayed from the host (one flat graph per round, a device counter read
+ * between them) instead of running inside one conditional graph; identical results. For profilers
+ * that do not follow kernels into conditional graph nodes. */
+#define EXG_OPT_WAVE_HOST_ROUNDS 4
 EXG_API int exg_world_set_option(exg_world_t world, int32_t option, int64_t value);
 EXG_API int exg_world_get_option(exg_world_t world, int32_t option, int64_t* value);
 /* SM clock cycles the implicit step spent per phase since the handle was created, summed over

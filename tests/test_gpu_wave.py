@@ -141,3 +141,23 @@ def test_wave_in_a_pool_with_churn(device):
         assert np.array_equal(got["pose"], want["pose"]) and np.array_equal(got["momentum"], want["momentum"])
         alone.close()
     pool.close()
+
+
+def test_host_driven_rounds_equal_the_conditional_graph(device):
+    """The profiler-friendly form (rounds replayed from the host) steps bit-identically to the
+    conditional graph, and reports its round count."""
+    worlds = []
+    for k, n in enumerate((40, 400, 1200)):
+        b, j = scenarios.tree_world(n, seed=120 + k)
+        worlds.append((b, j, step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10,
+                                         exact_jacobian=True)))
+    out = []
+    for host in (0, 1):
+        batch = _lib.DeviceBatch(device, worlds)
+        batch.set_option(W.OPT_WAVE_MIN_BODIES, 1)
+        batch.set_option(W.OPT_WAVE_HOST_ROUNDS, host)
+        batch.step(3)
+        assert batch.get_option(W.OPT_LAST_WAVE_ROUNDS) > 0
+        out.append(batch.bodies())
+        batch.close()
+    assert np.array_equal(out[0]["pose"], out[1]["pose"]) and np.array_equal(out[0]["momentum"], out[1]["momentum"])

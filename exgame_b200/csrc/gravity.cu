@@ -4,19 +4,20 @@
 // Work decomposition: a work item is an i-tile of kGravTile bodies of one world against a
 // j-range of the same world (bodies of different worlds never interact). Items are listed
 // largest-first and pulled by persistent CTAs through an atomic counter, so worlds of very
-// uneven size (8 .. 8192 bodies) share the GPU without a tail of idle SMs. Within an item each
-// thread owns one i-body; j-bodies are staged through shared memory in tiles of kGravTile and
-// read back as broadcasts. The item writes its partial sum  sum_j m_j r_ij / core^3  to its own
-// slot; consumers add a world's splits in index order and multiply by G m_i, so results do not
-// depend on scheduling (no atomics on the data).
+// uneven size (8 .. 8192 bodies) share the GPU without a tail of idle SMs. j-bodies are staged
+// through shared memory in tiles of kGravTile and read back as broadcasts. The item writes its
+// partial sum  sum_j m_j r_ij / core^3  to its own slot; consumers add a world's splits in index
+// order and multiply by G m_i, so results do not depend on scheduling (no atomics on the data).
 //
 // Kinematic bodies carry m = 0 in the charge array and so exert no force (the reference gives
 // them no gravitational charge, gravity.rs:485-497).
 //
-// Precision: R = double is the plain path. R = float is the mixed path: positions are taken
-// relative to the item's first i-body (one double subtraction per staged j-body, amortised over
-// the tile), pair terms are FP32 with the hardware reciprocal square root, and each j-tile's FP32
-// partial is flushed into an FP64 accumulator, so rounding does not grow with the world size.
+// Precision: k_gravity_items<double> is the plain (F64) path, two i-bodies per thread.
+// k_gravity_items_mixed is the mixed path (one warp per item, four i-bodies per thread as two
+// FP32x2 packs): positions relative to the item's first i-body (one double subtraction per staged
+// body), FP32 pair terms with the hardware reciprocal square root, each j-tile's FP32 partial
+// flushed into an FP64 accumulator so rounding does not grow with the world size; its COMP form
+// (precision MIXED) also carries the FP32 remainder of every relative position.
 #include <algorithm>
 #include <mutex>
 #include "exg_internal.cuh"

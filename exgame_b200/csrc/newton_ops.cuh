@@ -18,7 +18,7 @@ constexpr int kThresholdLog2 = 8;   // THRESHOLD_LOG2
 constexpr int kPerHalvingLog2 = 4;  // PER_HALVING_LOG2
 constexpr double kHuge = 1e9;
 constexpr double kFloor2 = 1e-9 * 1e-9;
-constexpr int kJacStride = 42;  // per (joint, slice): value[6] + d[36]
+constexpr int kJacStride = 36;  // per (joint, slice): d[36] (144 B in FP32, 16-byte aligned records)
 constexpr int kLineSearchLanes = 8;
 // Assembly terms carry this bit when the joint's law is the torsional damper, whose Jacobian
 // slices are known in closed form (joint_jacobian_part): the wave reads no slices for them.
@@ -150,7 +150,8 @@ __device__ inline void op_pre(const Ctx& c, const double* x, double half, int q)
 }
 
 // Jacobian slice storage: FP32 in the mixed path (the slices are FP32 duals, so nothing is lost),
-// FP64 otherwise. Slice s of joint q: value[6] then d[36], at (q * 4 + s) * kJacStride.
+// FP64 otherwise. Slice s of joint q: its 6x6 derivative block d[36] (row-major) at (q * 4 + s) *
+// kJacStride. The slices' value parts are not stored: the residual takes the FP64 values (conn).
 template <bool MIXED> struct JacType { typedef double T; };
 template <> struct JacType<true> { typedef float T; };
 template <bool MIXED>
@@ -176,8 +177,8 @@ __device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
 // or in FP64 the dual's value part, which equals it bit for bit: write_conn on slice 0), so the
 // converged iterate is an FP64 solution whatever the Jacobian's precision.
 // Half of slice `slice` (axes 6 slice + 3 half .. + 2) of joint q at (mid, x), into the slice's
-// 42-value record at dst: its three derivative columns and (half 0) the value part. Two halves
-// make the slice bit for bit (joint_jacobian_part).
+// record at dst: its three derivative columns. Two halves make the slice bit for bit
+// (joint_jacobian_part).
 template <bool MIXED, int LAW = -1>
 __device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q, int slice, int half, bool write_conn,
                                            typename JacType<MIXED>::T* dst) {
@@ -191,18 +192,14 @@ __device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q,
   for (int k = 0; k < 8; ++k) { pa[k] = J(c.s.mid[8 * a + k]); pb[k] = J(c.s.mid[8 * b + k]); }
 #pragma unroll
   for (int k = 0; k < 6; ++k) { va[k] = J(x[6 * a + k]); vb[k] = J(x[6 * b + k]); }
-  joint_jacobian_part<J, 3>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst + 6);
-  if (half == 0) {
-#pragma unroll
-    for (int r = 0; r < 6; ++r) dst[r] = val[r];
-  }
+  joint_jacobian_part<J, 3>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst);
   if (!MIXED && write_conn && slice == 0 && half == 0) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = double(val[r]);
   }
 }
 
-// The slice's 42 values go to `dst` when given (a staging buffer), else to the island's scratch.
+// The slice's 36 derivatives go to `dst` when given (a staging buffer), else to the island's scratch.
 template <bool MIXED, int LAW = -1>
 __device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int slice, bool write_conn,
                                       typename JacType<MIXED>::T* dst = nullptr) {
@@ -219,18 +216,14 @@ __device__ inline void op_joint_slice(const Ctx& c, const double* x, int q, int 
     for (int k = 0; k < 6; ++k) { va[k] = float(x[6 * a + k]); vb[k] = float(x[6 * b + k]); }
     joint_jacobian_slice<float>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, val, dd);
 #pragma unroll
-    for (int r = 0; r < 6; ++r) o[r] = val[r];
-#pragma unroll
-    for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+    for (int k = 0; k < 36; ++k) o[k] = dd[k];
   } else {
     double* o = dst ? reinterpret_cast<double*>(dst) : jac_slice<false>(c, q, slice);
     double val[6], dd[36];
     joint_jacobian_slice<double>(law, prm, c.s.mid + 8 * a, c.s.mid + 8 * b, x + 6 * a, x + 6 * b, c.P.dt, c.P.warp,
                                  slice, val, dd);
 #pragma unroll
-    for (int r = 0; r < 6; ++r) o[r] = val[r];
-#pragma unroll
-    for (int k = 0; k < 36; ++k) o[6 + k] = dd[k];
+    for (int k = 0; k < 36; ++k) o[k] = dd[k];
     if (write_conn && slice == 0) {
 #pragma unroll
       for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = val[r];
@@ -335,8 +328,8 @@ __device__ inline double op_assemble(const Ctx& c, double pf, double vf, int cel
   for (int k = p0; k < p1; ++k) {
     int term = c.A.cell_terms[k] & ~kTermTorsional;
     int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
-    const auto* jp = jac_slice<MIXED>(c, q, ce) + 6;
-    const auto* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
+    const auto* jp = jac_slice<MIXED>(c, q, ce);
+    const auto* jv = jac_slice<MIXED>(c, q, 2 + ce);
     double pv = double(jp[r * 6 + col]), vv = double(jv[r * 6 + col]);
     if (re) { pv = -pv; vv = -vv; }
     acc = acc + pf * pv + vf * vv;

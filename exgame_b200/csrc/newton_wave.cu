@@ -374,7 +374,7 @@ __global__ void k_w_pre(WaveArgs a) {
 // A joint's four slices are evaluated as eight half slices (3 axes each: half the dual state per
 // thread, so more threads fit on an SM) by eight adjacent lanes; a warp holds 4 joints. Each lane
 // writes its part of the joint's slice records into the warp's staging block in shared memory,
-// and the warp then stores each joint's four contiguous records (4 x 42 values, 16-byte aligned)
+// and the warp then stores each joint's four contiguous records (4 x 36 values, 16-byte aligned)
 // with 16-byte stores spread over the lanes.
 template <bool MIXED, int LAW>
 __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
@@ -481,54 +481,91 @@ __global__ void k_w_copy_bodies(WaveArgs a) {
 }
 
 
-// Assembly, one warp per cell: lane e holds entry e (lanes 0..3 also entries 32..35), the term
-// list is read once per warp, and a term's Jacobian rows are contiguous across the lanes.
+// Four entries of a 6x6 block from 16-byte aligned storage.
+__device__ __forceinline__ void load4(const float* p, float o[4]) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w;
+}
+__device__ __forceinline__ void load4(const double* p, double o[4]) {
+  const double2 x = reinterpret_cast<const double2*>(p)[0], y = reinterpret_cast<const double2*>(p)[1];
+  o[0] = x.x; o[1] = x.y; o[2] = y.x; o[3] = y.y;
+}
+
+// Entries e0 .. e0+3 of one assembly term's pose (p) and velocity (v) blocks in slice precision;
+// returns whether the row end flips their sign. A torsional term has them in closed form
+// (joint_jacobian_part, value for value): zero pose columns, g = -/+ c / warp^2 on the angular
+// diagonal (entries 21, 28, 35) of the velocity columns.
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 8) k_w_assemble(WaveArgs a) {
-  const int lane = threadIdx.x & 31;
-  for (int t = gtid() >> 5; t < a.n_cell; t += gthreads() >> 5) {
-    int2 it = a.cell[t];
+__device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, typename JacType<MIXED>::T p[4],
+                                         typename JacType<MIXED>::T v[4]) {
+  typedef typename JacType<MIXED>::T J;
+  const int term = raw & ~kTermTorsional;
+  const int q = term >> 2, ce = term & 1;
+  if (raw & kTermTorsional) {
+    const double warp = c.W.wparams[c.d.world].warp;
+    const J kk = -J(c.A.jl_params[10 * (size_t)(c.d.joint_off + q)] / (warp * warp));
+    const J g = ce == 0 ? kk : -kk;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int e = e0 + m;
+      p[m] = J(0);
+      v[m] = (e >= 21 && e % 7 == 0) ? g : J(0);
+    }
+  } else {
+    load4(jac_slice<MIXED>(c, q, ce) + e0, p);
+    load4(jac_slice<MIXED>(c, q, 2 + ce) + e0, v);
+  }
+  return (term >> 1) & 1;
+}
+
+// acc += pf p + vf v entry by entry, in FP64, with the term's sign (as op_assemble adds a term).
+template <typename J>
+__device__ __forceinline__ void asm_add(double acc[4], double pf, double vf, bool re, const J p[4], const J v[4]) {
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    double pv = double(p[m]), vv = double(v[m]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc[m] = acc[m] + pf * pv + vf * vv;
+  }
+}
+
+// Assembly, three cells per warp: nine lanes per cell, lane l holding entries 4l .. 4l+3, so a
+// term's block is one 16-byte load per lane (FP32 slices) and the output two. Terms are taken two
+// at a time, both terms' loads in flight before either is added; every entry still adds the mass
+// block and then its terms in cell order, as op_assemble does.
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
+  typedef typename JacType<MIXED>::T J;
+  const int lane = threadIdx.x & 31, grp = lane / 9, e0 = 4 * (lane - 9 * grp);
+  for (int t0 = 3 * (gtid() >> 5); t0 < a.n_cell; t0 += 3 * (gthreads() >> 5)) {
+    const int t = t0 + grp;
+    if (grp >= 3 || t >= a.n_cell) continue;
+    const int2 it = a.cell[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
-    Ctx c = wave_ctx_lite(a, it.x);
+    const Ctx c = wave_ctx_lite(a, it.x);
+    const double pf = w.pf, vf = w.vf;
     const int cell = it.y, i = cell / 3, kind = cell % 3;
-    const int e0 = lane, e1 = lane + 32;
-    const bool has1 = e1 < 36;
-    double acc0 = (kind == 0) ? c.s.mass0[36 * (size_t)i + e0] : 0.0;
-    double acc1 = (kind == 0 && has1) ? c.s.mass0[36 * (size_t)i + e1] : 0.0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (kind == 0) load4(c.s.mass0 + 36 * (size_t)i + e0, acc);
+    const int* terms = c.A.cell_terms;
     const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
-    typedef typename JacType<MIXED>::T J;
-    for (int k = p0; k < p1; ++k) {
-      const int raw = c.A.cell_terms[k];
-      const int term = raw & ~kTermTorsional;
-      const int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
-      double pv, vv, pv1 = 0.0, vv1 = 0.0;
-      if (raw & kTermTorsional) {
-        // the torsional couple's slices (joint_jacobian_part, value for value): zero pose columns,
-        // g = -/+ c / warp^2 on the angular diagonal of the velocity columns
-        const double warp = c.W.wparams[c.d.world].warp;
-        const J kk = -J(c.A.jl_params[10 * (size_t)(c.d.joint_off + q)] / (warp * warp));
-        const double g = double(ce == 0 ? kk : -kk);
-        pv = 0.0;
-        vv = (e0 >= 21 && e0 % 7 == 0) ? g : 0.0;  // entries (3,3), (4,4)
-        if (has1) vv1 = (e1 == 35) ? g : 0.0;      // entry (5,5)
-      } else {
-        const J* jp = jac_slice<MIXED>(c, q, ce) + 6;
-        const J* jv = jac_slice<MIXED>(c, q, 2 + ce) + 6;
-        pv = double(jp[e0]);
-        vv = double(jv[e0]);
-        if (has1) { pv1 = double(jp[e1]); vv1 = double(jv[e1]); }
-      }
-      if (re) { pv = -pv; vv = -vv; }
-      acc0 = acc0 + w.pf * pv + w.vf * vv;
-      if (has1) {
-        if (re) { pv1 = -pv1; vv1 = -vv1; }
-        acc1 = acc1 + w.pf * pv1 + w.vf * vv1;
-      }
+    int k = p0;
+    for (; k + 1 < p1; k += 2) {
+      J pa[4], va[4], pb[4], vb[4];
+      const bool ra = asm_term<MIXED>(c, terms[k], e0, pa, va);
+      const bool rb = asm_term<MIXED>(c, terms[k + 1], e0, pb, vb);
+      asm_add(acc, pf, vf, ra, pa, va);
+      asm_add(acc, pf, vf, rb, pb, vb);
     }
-    double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
-    dst[36 * (size_t)i + e0] = acc0;
-    if (has1) dst[36 * (size_t)i + e1] = acc1;
+    if (k < p1) {
+      J pa[4], va[4];
+      const bool ra = asm_term<MIXED>(c, terms[k], e0, pa, va);
+      asm_add(acc, pf, vf, ra, pa, va);
+    }
+    double* dst = (kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc)) + 36 * (size_t)i + e0;
+    reinterpret_cast<double2*>(dst)[0] = make_double2(acc[0], acc[1]);
+    reinterpret_cast<double2*>(dst)[1] = make_double2(acc[2], acc[3]);
   }
 }
 
@@ -879,7 +916,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
   const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
-  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
+  const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
   cudaGraph_t g;
@@ -939,7 +976,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
   const int g_dyn = grid_for(dev, a.n_dyn, T, dev->tune_wave_blocks_per_sm);
-  const int g_cell = grid_for(dev, 32LL * a.n_cell, T, dev->tune_wave_blocks_per_sm);
+  const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;

@@ -152,6 +152,23 @@ __global__ void k_bodies_scatter(const exg_body_t* __restrict__ rec, int count, 
   diag[i] = r.diagonal;
 }
 
+// Records staged for exg_world_set_bodies / exg_batch_set_world, checked before any is written:
+// flags[0] = some dynamic record has no positive mass (the call is refused), flags[1] = some
+// record's kinematic flag differs from its body's current one (implicit worlds rebuild islands).
+__global__ void k_records_check(const exg_body_t* __restrict__ rec, int count, int first, const int* __restrict__ dst,
+                                const int* __restrict__ kin, int* flags) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false, changed = false;
+  if (k < count) {
+    const exg_body_t& r = rec[k];
+    const int i = dst ? dst[k] : first + k;
+    bad = !r.kinematic && !(r.mass > 0.0);
+    changed = (r.kinematic != 0) != (kin[i] != 0);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags, 1);
+  if (__syncthreads_or(changed) && threadIdx.x == 0) atomicOr(flags + 1, 1);
+}
+
 __global__ void k_bodies_gather(exg_body_t* __restrict__ rec, int count, int first, const int* __restrict__ dst,
                                 const double* pose, const double* mom, const double* mass, const double* inertia,
                                 const double* size, const int* kin, const int* diag, int n) {
@@ -202,6 +219,13 @@ int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_bod
   if (count <= 0) return EXG_OK;
   k_bodies_scatter<<<(count + 127) / 128, 128, 0, s>>>(rec, count, first, dst, w.pose, w.mom, w.mass, w.inertia, w.size,
                                                        w.kinematic, w.diagonal, w.n);
+  return exg_after_launch(dev);
+}
+
+int launch_records_check(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
+                         const int* dst, int* flags, cudaStream_t s) {
+  if (count <= 0) return EXG_OK;
+  k_records_check<<<(count + 255) / 256, 256, 0, s>>>(rec, count, first, dst, w.kinematic, flags);
   return exg_after_launch(dev);
 }
 

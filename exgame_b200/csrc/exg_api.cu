@@ -50,6 +50,7 @@ struct exg_world_s {
   DevArr<GravItem> items_d;
   DevArr<double> partial_d;
   DevArr<exg_body_t> stage_d;  // host record staging
+  DevArr<int> flags_d;         // record check flags (set_records)
   DevArr<int> map_d;           // record -> body of the whole handle's used slots
   bool map_dirty = true;
   std::vector<void*> allocations;
@@ -72,6 +73,7 @@ struct exg_world_s {
     items_d.release();
     partial_d.release();
     stage_d.release();
+    flags_d.release();
     map_d.release();
     for (void* p : allocations) cudaFree(p);
   }
@@ -302,6 +304,51 @@ static int download_records(exg_world_s* W, exg_body_t* out, int32_t first, int3
   if (rc != EXG_OK) return rc;
   if ((rc = launch_bodies_gather(W->dev, W->w, W->stage_d.ptr, count, first, dst, s)) != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaMemcpyAsync(out, W->stage_d.ptr, sizeof(exg_body_t) * (size_t)count, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  return EXG_OK;
+}
+
+// Records that replace bodies of live worlds (exg_world_set_bodies: every used slot in slot order,
+// slot < 0; exg_batch_set_world: one slot). The staged records are checked on the device before
+// any is written: a dynamic record without positive mass refuses the call, and kinematic flags
+// that differ from the current ones rebuild the islands of the implicit worlds they belong to
+// (all or none: a structure error restores the worlds already rebuilt).
+static int set_records(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count, const int* dst,
+                       int slot) {
+  if (count <= 0) return EXG_OK;
+  cudaStream_t s = W->dev->stream;
+  int rc = stage_reserve(W, count);
+  if (rc != EXG_OK) return rc;
+  if (W->flags_d.cap < 2 && (rc = W->flags_d.reserve(2, s)) != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaMemcpyAsync(W->stage_d.ptr, bodies, sizeof(exg_body_t) * (size_t)count, cudaMemcpyHostToDevice, s));
+  EXG_CUDA_TRY(cudaMemsetAsync(W->flags_d.ptr, 0, 2 * sizeof(int), s));
+  if ((rc = launch_records_check(W->dev, W->w, W->stage_d.ptr, count, first, dst, W->flags_d.ptr, s)) != EXG_OK)
+    return rc;
+  int flags[2] = {0, 0};
+  EXG_CUDA_TRY(cudaMemcpyAsync(flags, W->flags_d.ptr, sizeof(flags), cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  if (flags[0]) return EXG_ERR_INVALID_ARGUMENT;
+  if (flags[1]) {
+    std::vector<std::pair<int, std::vector<char>>> done;  // rebuilt slots with their previous flags
+    long long k = 0;
+    for (int t = 0; t < (int)W->slots.size(); ++t) {
+      const WorldSlot& ws = W->slots[t];
+      if (!ws.used || (slot >= 0 && t != slot)) continue;
+      const exg_body_t* b = bodies + k;
+      k += ws.n;
+      if (ws.params.integrator != EXG_NEWTON || !W->newton->kin_differs(t, b, ws.n)) continue;
+      std::vector<char> kin(ws.n);
+      for (int i = 0; i < ws.n; ++i) kin[i] = b[i].kinematic != 0;
+      std::vector<char> old = W->newton->kin_of(t);
+      if ((rc = W->newton->rebuild_world(t, kin)) != EXG_OK) {
+        for (auto& d : done) W->newton->rebuild_world(d.first, d.second);
+        return rc;
+      }
+      done.emplace_back(t, std::move(old));
+      W->dirty = true;
+    }
+  }
+  if ((rc = launch_bodies_scatter(W->dev, W->w, W->stage_d.ptr, count, first, dst, s)) != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaStreamSynchronize(s));
   return EXG_OK;
 }
@@ -824,15 +871,13 @@ int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
 
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
   if (!W || !bodies) return EXG_ERR_INVALID_ARGUMENT;
-  for (int32_t i = 0; i < n; ++i)
-    if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
   int rc = ensure_record_map(W, &total);
   if (rc != EXG_OK) return rc;
   if (n != total) return EXG_ERR_INVALID_ARGUMENT;
-  return upload_records(W, bodies, 0, n, W->map_d.ptr);
+  return set_records(W, bodies, 0, n, W->map_d.ptr, -1);
 }
 
 int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n) {
@@ -848,9 +893,7 @@ int exg_batch_set_world(exg_world_t W, int32_t world, const exg_body_t* bodies, 
     return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
-  for (int32_t i = 0; i < n; ++i)
-    if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
-  return upload_bodies(W, bodies, W->slots[world].body_off, n);
+  return set_records(W, bodies, W->slots[world].body_off, n, nullptr, world);
 }
 
 int exg_world_stats(exg_world_t W, exg_world_stats_t* out) {

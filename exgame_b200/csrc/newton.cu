@@ -634,6 +634,35 @@ void NewtonWorld::remove_world(int slot) {
   dirty_ = true;
 }
 
+bool NewtonWorld::kin_differs(int slot, const exg_body_t* bodies, int n) const {
+  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live) return false;
+  const std::vector<char>& k = src_[slot].kin;
+  if ((int)k.size() != n) return true;
+  for (int i = 0; i < n; ++i)
+    if (k[i] != (bodies[i].kinematic != 0)) return true;
+  return false;
+}
+
+std::vector<char> NewtonWorld::kin_of(int slot) const {
+  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live) return {};
+  return src_[slot].kin;
+}
+
+int NewtonWorld::rebuild_world(int slot, const std::vector<char>& kin) {
+  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live || src_[slot].kin.size() != kin.size())
+    return EXG_ERR_INVALID_ARGUMENT;
+  WorldSrc old = src_[slot], next = src_[slot];
+  next.kin = kin;
+  remove_world(slot);
+  int rc = build_world(slot, next);
+  if (rc != EXG_OK) {
+    if (build_world(slot, old) == EXG_OK) src_[slot] = old;  // accepted before
+    return rc;
+  }
+  src_[slot] = std::move(next);
+  return EXG_OK;
+}
+
 int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
   (void)dev;
   if (!dirty_) return EXG_OK;

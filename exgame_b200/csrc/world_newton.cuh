@@ -60,6 +60,13 @@ class NewtonWorld {
   int add_world(exg_device_s* dev, int slot, int body_off, const exg_body_t* bodies, int n, const exg_joint_t* joints,
                 int nj);
   void remove_world(int slot);
+  // Whether the world's kinematic flags differ from `bodies` (its islands were built from them).
+  bool kin_differs(int slot, const exg_body_t* bodies, int n) const;
+  // The kinematic flags the world's islands were built from.
+  std::vector<char> kin_of(int slot) const;
+  // Rebuild the world's islands for new kinematic flags (same joints); on a structure error the
+  // world keeps its previous islands.
+  int rebuild_world(int slot, const std::vector<char>& kin);
   // Upload pending structure and the island queue (host synchronous; call outside stream capture).
   int sync(exg_device_s* dev, cudaStream_t s);
   bool dirty() const { return dirty_; }

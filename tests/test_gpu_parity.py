@@ -267,6 +267,59 @@ def test_uniform_field_matches_oracle(device, oracle, scheme):
         dw.close()
 
 
+def test_set_bodies_kinematic_change_rebuilds_islands(device, oracle):
+    """Records set between steps may turn a body kinematic (or back): the implicit world's islands
+    are rebuilt from the new flags, on both Newton schedules, and the steps that follow match an
+    oracle world made from the same records; the batch accessor does the same for one world."""
+    bodies, joints = scenarios.tree_world(40, seed=83)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
+    for min_bodies in (1 << 20, 1):
+        dw = _lib.DeviceWorld(device, bodies, joints, params)
+        dw.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, min_bodies)
+        dw.step(3)
+        for kin, mass in ((1, 0.0), (0, bodies[7]["mass"])):
+            rec = dw.bodies()
+            rec[7]["kinematic"], rec[7]["mass"] = kin, mass
+            dw.set_bodies(rec)
+            ow = oracle.OracleWorld(rec, joints, params)
+            dw.step(4)
+            ow.step(4)
+            pe, me = state_error(ow.bodies(), dw.bodies())
+            assert pe < 1e-9 and me < 1e-7, (min_bodies, kin, pe, me)
+        dw.close()
+    other, oj = scenarios.chain_world(6, seed=84)
+    batch = _lib.DeviceBatch(device, [(bodies, joints, params), (other, oj, params)])
+    batch.step(2)
+    rec = batch.world_bodies(0)
+    rec[3]["kinematic"], rec[3]["mass"] = 1, 0.0
+    batch.set_world_bodies(0, rec)
+    ow = oracle.OracleWorld(rec, joints, params)
+    batch.step(3)
+    ow.step(3)
+    pe, me = state_error(ow.bodies(), batch.world_bodies(0))
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+    batch.close()
+
+
+def test_set_bodies_refuses_massless_dynamic_record(device):
+    """A dynamic record without positive mass refuses exg_world_set_bodies as a whole: nothing of
+    the call is written, and the world steps on from its previous state."""
+    bodies, joints = scenarios.tree_world(20, seed=85)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
+    dw = _lib.DeviceWorld(device, bodies, joints, params)
+    dw.step(2)
+    before = dw.bodies()
+    rec = before.copy()
+    rec["pose"][:, 0] += 1.0
+    rec[5]["mass"] = 0.0
+    with pytest.raises(_lib.ExgError):
+        dw.set_bodies(rec)
+    after = dw.bodies()
+    assert np.array_equal(before["pose"], after["pose"]) and np.array_equal(before["mass"], after["mass"])
+    dw.step(1)
+    dw.close()
+
+
 def test_mixed_gravity_world_1000_steps_within_1e6_of_f64(device, oracle):
     """The mixed path's accuracy target: a config-0 cluster (1024 bodies in a ball of radius 100,
     Plummer 0.05, LieEuler, dt 1e-3) after 1000 steps against the f64 oracle — relative pose

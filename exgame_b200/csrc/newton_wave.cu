@@ -530,9 +530,9 @@ __device__ __forceinline__ void asm_add(double acc[4], double pf, double vf, boo
 }
 
 // Assembly, three cells per warp: nine lanes per cell, lane l holding entries 4l .. 4l+3, so a
-// term's block is one 16-byte load per lane (FP32 slices) and the output two. Terms are taken two
-// at a time, both terms' loads in flight before either is added; every entry still adds the mass
-// block and then its terms in cell order, as op_assemble does.
+// term's block is one 16-byte load per lane (FP32 slices) and the output two. Every entry adds
+// the mass block and then its terms in cell order, as op_assemble does. (Taking two terms at a
+// time, or fewer CTAs per SM with more registers, measured slower.)
 template <bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
   typedef typename JacType<MIXED>::T J;
@@ -550,15 +550,7 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
     if (kind == 0) load4(c.s.mass0 + 36 * (size_t)i + e0, acc);
     const int* terms = c.A.cell_terms;
     const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
-    int k = p0;
-    for (; k + 1 < p1; k += 2) {
-      J pa[4], va[4], pb[4], vb[4];
-      const bool ra = asm_term<MIXED>(c, terms[k], e0, pa, va);
-      const bool rb = asm_term<MIXED>(c, terms[k + 1], e0, pb, vb);
-      asm_add(acc, pf, vf, ra, pa, va);
-      asm_add(acc, pf, vf, rb, pb, vb);
-    }
-    if (k < p1) {
+    for (int k = p0; k < p1; ++k) {
       J pa[4], va[4];
       const bool ra = asm_term<MIXED>(c, terms[k], e0, pa, va);
       asm_add(acc, pf, vf, ra, pa, va);

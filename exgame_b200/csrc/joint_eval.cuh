@@ -34,7 +34,8 @@ EXG_HD void joint_plain(int law, const double* prm, const R* pose_a, const R* po
 // (h = half) — and fills columns 3h .. 3h + 2 of d (value6 as well); each derivative column is
 // computed by the same dual operations whatever N is, so two halves give the full slice's values
 // bit for bit with about half the live state per thread.
-template <class R, int N = 6>
+// KIND = 0 / 1 promises a pose / twist slice at compile time (-1: decided by `slice`).
+template <class R, int N = 6, int KIND = -1>
 EXG_HD void joint_jacobian_part(int law, const double* prm, const R* pose_a, const R* pose_b, const R* vel_a,
                                 const R* vel_b, double dt, double warp, int slice, int half, R* value6, R* d36) {
   static_assert(N == 6 || N == 3, "a slice is evaluated whole or in halves");
@@ -64,12 +65,25 @@ EXG_HD void joint_jacobian_part(int law, const double* prm, const R* pose_a, con
     return;
   }
   using D = Dual<N, R>;
-  D ma[8], mb[8], va[6], vb[6];
+  // the wrench's value and its N partial columns into value6 / d36
+  auto emit = [&](const D* wa) {
+    D w6[6];
+    screw_to6(wa, w6);
 #pragma unroll
-  for (int i = 0; i < 8; ++i) { ma[i] = D(0.0); ma[i].v = pose_a[i]; mb[i] = D(0.0); mb[i].v = pose_b[i]; }
+    for (int r = 0; r < 6; ++r) {
+      value6[r] = w6[r].v;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) { va[i] = D(0.0); va[i].v = vel_a[i]; vb[i] = D(0.0); vb[i].v = vel_b[i]; }
-  if (slice < 2) {
+      for (int c = 0; c < N; ++c) d36[r * 6 + c0 + c] = w6[r].g[c];
+    }
+  };
+  // Each branch ends in its own emit: the two paths share no arrays after the branch, which
+  // keeps them in registers.
+  if (KIND == 0 || (KIND < 0 && slice < 2)) {
+    D ma[8], mb[8], va[6], vb[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { va[i] = D(0.0); va[i].v = vel_a[i]; vb[i] = D(0.0); vb[i].v = vel_b[i]; }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { ma[i] = D(0.0); ma[i].v = pose_a[i]; mb[i] = D(0.0); mb[i].v = pose_b[i]; }
     // pose seed: (1 + delta) * base with delta = Twist(seed lin, seed ang), value 0
     D seed6[6];
 #pragma unroll
@@ -83,29 +97,41 @@ EXG_HD void joint_jacobian_part(int law, const double* prm, const R* pose_a, con
     one_delta[0] = D(1.0);
     one_delta[7] = D(0.0);
     static_for<0, 6>([&](auto i) { one_delta[slot_of(EVEN, BIV[i])] = delta[i]; });
-    D* base = (slice == 0) ? ma : mb;
-    D moved[8];
+    // the seeded pose (a or b) by selects, so the arrays stay in registers
+    const bool on_a = slice == 0;
+    D base[8], moved[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) base[i] = on_a ? ma[i] : mb[i];
     gp<EVEN, EVEN, EVEN>(one_delta, base, moved);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) base[i] = moved[i];
+    for (int i = 0; i < 8; ++i) {
+      ma[i] = on_a ? moved[i] : ma[i];
+      mb[i] = on_a ? mb[i] : moved[i];
+    }
+    D ta[6], tb[6], wa[6];
+    screw_from6(va, ta);
+    screw_from6(vb, tb);
+    law_wrench<D, D>(law, prm, ma, mb, ta, tb, dt, warp, wa);
+    emit(wa);
   } else {
-    D* v = (slice == 2) ? va : vb;
+    // twist seed: the poses carry no partials, so the laws' pose chains run plain
+    D va[6], vb[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) { va[i] = D(0.0); va[i].v = vel_a[i]; vb[i] = D(0.0); vb[i].v = vel_b[i]; }
+    const bool on_a = slice == 2;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-      for (int c = 0; c < N; ++c)
-        if (i == c0 + c) v[i].g[c] = R(1);
-  }
-  D ta[6], tb[6], wa[6], w6[6];
-  screw_from6(va, ta);
-  screw_from6(vb, tb);
-  law_wrench(law, prm, ma, mb, ta, tb, dt, warp, wa);
-  screw_to6(wa, w6);
-#pragma unroll
-  for (int r = 0; r < 6; ++r) {
-    value6[r] = w6[r].v;
-#pragma unroll
-    for (int c = 0; c < N; ++c) d36[r * 6 + c0 + c] = w6[r].g[c];
+      for (int c = 0; c < N; ++c) {
+        const R one = (i == c0 + c) ? R(1) : R(0);  // static register index
+        va[i].g[c] = on_a ? one : R(0);
+        vb[i].g[c] = on_a ? R(0) : one;
+      }
+    D ta[6], tb[6], wa[6];
+    screw_from6(va, ta);
+    screw_from6(vb, tb);
+    law_wrench<D, R>(law, prm, pose_a, pose_b, ta, tb, dt, warp, wa);
+    emit(wa);
   }
 }
 

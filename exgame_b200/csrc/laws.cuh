@@ -16,21 +16,35 @@ namespace exg {
 
 enum : int { LAW_SIMPLE = 0, LAW_CRITICAL = 1, LAW_PERPENDICULAR = 2, LAW_TORSIONAL = 3 };
 
-template <class S>
-EXG_HD void law_axial(int law, const double* prm, const S* ma, const S* mb, const S* ta, const S* tb, double dt, double warp,
-                      S* wa) {
-  S la[3] = {S(prm[0]), S(prm[1]), S(prm[2])};
-  S lb[3] = {S(prm[3]), S(prm[4]), S(prm[5])};
-  S pa[4], pb[4], line[6];
+// Pose-only intermediates are computed in P and lifted to S where they meet the twists. P = S
+// is the plain evaluation and the pose slices of the Jacobian; P = R with S = Dual<N, R> gives the
+// twist slices, whose pose chain has no partials, at plain cost (same values: a dual's value part
+// is the plain evaluation).
+template <class S> struct Lift {
+  static EXG_HD S from(const S& x) { return x; }
+};
+template <int N, class R> struct Lift<Dual<N, R>> {
+  static EXG_HD Dual<N, R> from(const Dual<N, R>& x) { return x; }
+  static EXG_HD Dual<N, R> from(const R& x) { Dual<N, R> r; r.v = x; return r; }
+};
+
+template <class S, class P = S>
+EXG_HD void law_axial(int law, const double* prm, const P* ma, const P* mb, const S* ta, const S* tb, double dt,
+                      double warp, S* wa) {
+  P la[3] = {P(prm[0]), P(prm[1]), P(prm[2])};
+  P lb[3] = {P(prm[3]), P(prm[4]), P(prm[5])};
+  P pa[4], pb[4], line[6];
   anchor_point(ma, la, pa);
   anchor_point(mb, lb, pb);
   point_join(pa, pb, line);
-  S d = soft_weight_norm(line, S(prm[9]));
-  S raw[6], unit[6], rel[6];
+  P dp = soft_weight_norm(line, P(prm[9]));
+  P raw[6];
   wrench_from_line(line, raw);
-  S inv_d = S(1.0) / d;
+  P inv_d = P(1.0) / dp;
+  S unit[6], rel[6];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) { unit[i] = raw[i] * inv_d; rel[i] = ta[i] - tb[i]; }
+  for (int i = 0; i < 6; ++i) { unit[i] = Lift<S>::from(raw[i] * inv_d); rel[i] = ta[i] - tb[i]; }
+  const S d = Lift<S>::from(dp);
   S d_dot = screw_power(unit, rel);
   S f;
   if (law == LAW_SIMPLE) {
@@ -47,32 +61,36 @@ EXG_HD void law_axial(int law, const double* prm, const S* ma, const S* mb, cons
   for (int i = 0; i < 6; ++i) wa[i] = unit[i] * nf;
 }
 
-template <class S>
-EXG_HD void law_perpendicular(const double* prm, const S* ma, const S* mb, const S* ta, const S* tb, double warp, S* wa) {
-  S zero[3] = {S(0.0), S(0.0), S(0.0)};
-  S pa[4], pb[4], line[6];
+template <class S, class P = S>
+EXG_HD void law_perpendicular(const double* prm, const P* ma, const P* mb, const S* ta, const S* tb, double warp,
+                              S* wa) {
+  P zero[3] = {P(0.0), P(0.0), P(0.0)};
+  P pa[4], pb[4], line[6];
   anchor_point(ma, zero, pa);
   anchor_point(mb, zero, pb);
   point_join(pa, pb, line);
-  S d = soft_weight_norm(line, S(prm[1]));
+  P d = soft_weight_norm(line, P(prm[1]));
   S b_eff = S(prm[0] / (warp * warp));
-  S dir[3], n[3];
+  P dir[3], cp[3];
   line_direction(line, dir);
-  S inv_d = S(1.0) / d;
+  P inv_d = P(1.0) / d;
+  point_coords(pa, cp);
+  S n[3], ca[3], pas[4];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) n[i] = dir[i] * inv_d;
+  for (int i = 0; i < 3; ++i) { n[i] = Lift<S>::from(dir[i] * inv_d); ca[i] = Lift<S>::from(cp[i]); }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) pas[i] = Lift<S>::from(pa[i]);
   S rel[6], v[3];
 #pragma unroll
   for (int i = 0; i < 6; ++i) rel[i] = ta[i] - tb[i];
-  velocity_at(rel, pa, v);
+  velocity_at(rel, pas, v);
   S vn = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
-  S ca[3], tip[3];
-  point_coords(pa, ca);
+  S tip[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) tip[i] = ca[i] + (v[i] - n[i] * vn) * (-b_eff);
   S pt[4], l2[6];
   point_make(tip, pt);
-  point_join(pt, pa, l2);
+  point_join(pt, pas, l2);
   wrench_from_line(l2, wa);
 }
 
@@ -88,11 +106,11 @@ EXG_HD void law_torsional(const double* prm, const S* ta, const S* tb, double wa
   screw_from_phys(zero, tq, wa);
 }
 
-template <class S>
-EXG_HD void law_wrench(int law, const double* prm, const S* ma, const S* mb, const S* ta, const S* tb, double dt, double warp,
-                       S* wa) {
-  if (law <= LAW_CRITICAL) law_axial(law, prm, ma, mb, ta, tb, dt, warp, wa);
-  else if (law == LAW_PERPENDICULAR) law_perpendicular(prm, ma, mb, ta, tb, warp, wa);
+template <class S, class P = S>
+EXG_HD void law_wrench(int law, const double* prm, const P* ma, const P* mb, const S* ta, const S* tb, double dt,
+                       double warp, S* wa) {
+  if (law <= LAW_CRITICAL) law_axial<S, P>(law, prm, ma, mb, ta, tb, dt, warp, wa);
+  else if (law == LAW_PERPENDICULAR) law_perpendicular<S, P>(prm, ma, mb, ta, tb, warp, wa);
   else law_torsional(prm, ta, tb, warp, wa);
 }
 

@@ -80,7 +80,12 @@ __device__ void phase_pre(const Ctx& c, const double* v, double half) {
 template <bool MIXED>
 __device__ void phase_joints(const Ctx& c, const double* v, bool jac) {
   if (jac) {
-    for (int t = threadIdx.x; t < 4 * c.d.nj; t += blockDim.x) op_joint<MIXED>(c, v, t >> 2, t & 3, true);
+    // a warp takes 16 joints and one kind of slice (pose 0, 1 or twist 2, 3), so it follows one path
+    const int total = 64 * ((c.d.nj + 15) / 16);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int w = t >> 5, l = t & 31, q = (w >> 1) * 16 + (l >> 1);
+      if (q < c.d.nj) op_joint<MIXED>(c, v, q, 2 * (w & 1) + (l & 1), true);
+    }
   } else {
     for (int q = threadIdx.x; q < c.d.nj; q += blockDim.x) op_joint<MIXED>(c, v, q, 0, false);
   }

@@ -179,7 +179,7 @@ __device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
 // Half of slice `slice` (axes 6 slice + 3 half .. + 2) of joint q at (mid, x), into the slice's
 // record at dst: its three derivative columns. Two halves make the slice bit for bit
 // (joint_jacobian_part).
-template <bool MIXED, int LAW = -1>
+template <bool MIXED, int LAW = -1, int KIND = -1>
 __device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q, int slice, int half, bool write_conn,
                                            typename JacType<MIXED>::T* dst) {
   typedef typename JacType<MIXED>::T J;
@@ -192,7 +192,7 @@ __device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q,
   for (int k = 0; k < 8; ++k) { pa[k] = J(c.s.mid[8 * a + k]); pb[k] = J(c.s.mid[8 * b + k]); }
 #pragma unroll
   for (int k = 0; k < 6; ++k) { va[k] = J(x[6 * a + k]); vb[k] = J(x[6 * b + k]); }
-  joint_jacobian_part<J, 3>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst);
+  joint_jacobian_part<J, 3, KIND>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst);
   if (!MIXED && write_conn && slice == 0 && half == 0) {
 #pragma unroll
     for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = double(val[r]);

@@ -372,42 +372,43 @@ __global__ void k_w_pre(WaveArgs a) {
 //           value parts are the values) and for a probe. A carried iterate keeps the values the
 //           accepted probe left at the same point.
 // A joint's four slices are evaluated as eight half slices (3 axes each: half the dual state per
-// thread, so more threads fit on an SM) by eight adjacent lanes; a warp holds 4 joints. Each lane
-// writes its part of the joint's slice records into the warp's staging block in shared memory,
-// and the warp then stores each joint's four contiguous records (4 x 36 values, 16-byte aligned)
-// with 16-byte stores spread over the lanes.
-template <bool MIXED, int LAW>
+// thread, so more threads fit on an SM), in two launches: KIND 0 the pose slices (0, 1), KIND 1 the
+// twist slices (2, 3), whose laws run their pose chains without partials and so need far fewer
+// registers. A warp takes 8 joints, four lanes each. Each lane writes its part of the slice
+// records into the warp's staging block in shared memory, and the warp then stores each joint's
+// two contiguous records (2 x 36 values, 16-byte aligned) with 16-byte stores.
+template <bool MIXED, int LAW, int KIND>
 __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
   typedef typename JacType<MIXED>::T J;
-  constexpr int kJoint = 4 * kJacStride;  // values per joint
-  __shared__ __align__(16) J stage[4][4][kJoint];
+  constexpr int kHalf = 2 * kJacStride;  // values per joint and kind
+  __shared__ __align__(16) J stage[4][8][kHalf];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int total = 8 * n;
-  for (int base = gtid() - lane; base < total; base += gthreads()) {  // warp-uniform loop
-    const int t = base + lane;
+  const long long total = 32LL * ((n + 7) / 8);
+  for (long long base = gtid() - lane; base < total; base += gthreads()) {  // warp-uniform loop
+    const int jq = (int)(base >> 5) * 8 + (lane >> 2), slice = 2 * KIND + ((lane >> 1) & 1), half = lane & 1;
     bool on = false;
     int2 it = make_int2(0, 0);
-    if (t < total) {
-      it = a.joint[first + (t >> 3)];
+    if (jq < n) {
+      it = a.joint[first + jq];
       const int ev = a.ctl[it.x].eval;
       if (ev == EV_FULL || ev == EV_JAC) {
         on = true;
         Ctx c = wave_ctx(a, it.x);
-        const int slice = (t >> 1) & 3, half = t & 1;
-        op_joint_half_slice<MIXED, LAW>(c, c.s.vm, it.y, slice, half, ev == EV_FULL,
-                                        &stage[wib][lane >> 3][slice * kJacStride]);
+        op_joint_half_slice<MIXED, LAW, KIND>(c, c.s.vm, it.y, slice, half, ev == EV_FULL,
+                                        &stage[wib][lane >> 2][(slice & 1) * kJacStride]);
       }
     }
     const unsigned active = __ballot_sync(0xffffffffu, on);
     __syncwarp();
-    for (int j = 0; j < 4; ++j) {
-      if (!((active >> (8 * j)) & 1u)) continue;  // the joint's island did not evaluate slices
-      const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 8 * j), __shfl_sync(0xffffffffu, it.y, 8 * j));
+    for (int j = 0; j < 8; ++j) {
+      if (!((active >> (4 * j)) & 1u)) continue;  // no joint here, or its island did not evaluate slices
+      const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
       const IslandDesc& d = a.A.desc[a.isl[jt.x]];
-      J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) + (size_t)jt.y * kJoint;
+      J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
+                (size_t)jt.y * 4 * kJacStride + KIND * kHalf;
       const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
       float4* dst4 = reinterpret_cast<float4*>(dstj);
-      constexpr int kVec = kJoint * (int)sizeof(J) / 16;
+      constexpr int kVec = kHalf * (int)sizeof(J) / 16;
       for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
     }
     __syncwarp();
@@ -429,8 +430,11 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
 template <bool MIXED, int LAW>
 void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
   const int per = 2 * dev->tune_wave_blocks_per_sm;
-  if (LAW != LAW_TORSIONAL)  // the assembly knows the torsional slices in closed form
-    k_w_joint_slices<MIXED, LAW><<<grid_for(dev, 8LL * n, 128, per), 128, 0, s>>>(a, first, n);
+  if (LAW != LAW_TORSIONAL) {  // the assembly knows the torsional slices in closed form
+    const int g = grid_for(dev, 32LL * ((n + 7) / 8), 128, per);
+    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);
+    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);
+  }
   k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, s>>>(a, first, n);
 }
 
@@ -951,7 +955,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   EXG_CUDA_TRY(ie);
   int joint_kernels = 0;
   for (int L = 0; L < 4; ++L)
-    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 2;
+    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels;
   wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
   wave_kernels_end_ = 6;
@@ -1055,7 +1059,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(cudaGraphInstantiate(&wave_graph_, G, 0));
   int joint_kernels = 0;
   for (int L = 0; L < 4; ++L)
-    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 2;
+    if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
   wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
   wave_kernels_end_ = 5;

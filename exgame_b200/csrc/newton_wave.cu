@@ -554,9 +554,16 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
     if (kind == 0) load4(c.s.mass0 + 36 * (size_t)i + e0, acc);
     const int* terms = c.A.cell_terms;
     const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+    // the group's nine lanes fetch nine term indices at a time and pass them round by shuffle, so
+    // a term's block loads wait on no index load of their own
+    const unsigned gmask = 0x1ffu << (9 * grp);
+    const int sub = e0 >> 2;
+    int mine = 0;
     for (int k = p0; k < p1; ++k) {
+      const int j = (k - p0) % 9;
+      if (j == 0) mine = (k + sub < p1) ? terms[k + sub] : 0;
       J pa[4], va[4];
-      const bool ra = asm_term<MIXED>(c, terms[k], e0, pa, va);
+      const bool ra = asm_term<MIXED>(c, __shfl_sync(gmask, mine, 9 * grp + j), e0, pa, va);
       asm_add(acc, pf, vf, ra, pa, va);
     }
     double* dst = (kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc)) + 36 * (size_t)i + e0;
@@ -613,6 +620,20 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int wa
   }
 }
 
+// N doubles (N even) between registers and 16-byte aligned memory, two at a time.
+template <int N>
+__device__ __forceinline__ void ld_n(const double* p, double* o) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int e = 0; e < N / 2; ++e) { const double2 x = q[e]; o[2 * e] = x.x; o[2 * e + 1] = x.y; }
+}
+template <int N>
+__device__ __forceinline__ void st_n(double* p, const double* v) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int e = 0; e < N / 2; ++e) q[e] = make_double2(v[2 * e], v[2 * e + 1]);
+}
+
 // Elimination, one thread per node of level L (leaves to roots), the node's blocks in registers:
 // subtract the children's Schur terms, invert the pivot block, and for a non-root node form its own
 // terms for the parent — S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's
@@ -626,64 +647,78 @@ __global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, 
     Ctx c = wave_ctx_lite(a, it.x);
     const int i = it.y;
     double D[36], b[6];
-#pragma unroll
-    for (int e = 0; e < 36; ++e) D[e] = c.s.D[36 * (size_t)i + e];
-#pragma unroll
-    for (int r = 0; r < 6; ++r) b[r] = c.s.rhs[6 * i + r];
+    ld_n<36>(c.s.D + 36 * (size_t)i, D);
+    ld_n<6>(c.s.rhs + 6 * (size_t)i, b);
     const int* chp = c.A.ch_ptr + c.d.dyn_off;
     for (int u = chp[i]; u < chp[i + 1]; ++u) {
       const int ch = c.A.ch_idx[u];
-      const double* P = c.s.S + 36 * (size_t)ch;
+      const double2* P = reinterpret_cast<const double2*>(c.s.S + 36 * (size_t)ch);
 #pragma unroll
-      for (int e = 0; e < 36; ++e) D[e] = D[e] - P[e];
+      for (int e = 0; e < 18; ++e) {
+        const double2 x = P[e];
+        D[2 * e] = D[2 * e] - x.x;
+        D[2 * e + 1] = D[2 * e + 1] - x.y;
+      }
+      const double2* q = reinterpret_cast<const double2*>(c.s.dv + 6 * (size_t)ch);
 #pragma unroll
-      for (int r = 0; r < 6; ++r) b[r] = b[r] - c.s.dv[6 * ch + r];
+      for (int r = 0; r < 3; ++r) {
+        const double2 x = q[r];
+        b[2 * r] = b[2 * r] - x.x;
+        b[2 * r + 1] = b[2 * r + 1] - x.y;
+      }
     }
-#pragma unroll
-    for (int r = 0; r < 6; ++r) c.s.bvec[6 * i + r] = b[r];
+    st_n<6>(c.s.bvec + 6 * (size_t)i, b);
     double Dinv[36];
     if (!thread_inverse6(D, Dinv)) atomicOr(&w.singular, 1);
-#pragma unroll
-    for (int e = 0; e < 36; ++e) c.s.Dinv[36 * (size_t)i + e] = Dinv[e];
+    st_n<36>(c.s.Dinv + 36 * (size_t)i, Dinv);
     if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
-      const double* Apc = c.s.Apc + 36 * (size_t)i;
+      double dv[6];
       const double* Acp = c.s.Acp + 36 * (size_t)i;
-      double* P = c.s.S + 36 * (size_t)i;
+      const double* Apc = c.s.Apc + 36 * (size_t)i;
+      double2* P = reinterpret_cast<double2*>(c.s.S + 36 * (size_t)i);
 #pragma unroll
       for (int r = 0; r < 6; ++r) {
-        double Sr[6];
+        double ar[6], Sr[6], Pr[6];
+        ld_n<6>(Apc + 6 * r, ar);
 #pragma unroll
         for (int cc = 0; cc < 6; ++cc) {
           double v = 0.0;
 #pragma unroll
-          for (int k = 0; k < 6; ++k) v += Apc[r * 6 + k] * Dinv[k * 6 + cc];
+          for (int k = 0; k < 6; ++k) v += ar[k] * Dinv[k * 6 + cc];
           Sr[cc] = v;
         }
         double q = 0.0;
 #pragma unroll
         for (int k = 0; k < 6; ++k) q += Sr[k] * b[k];
-        c.s.dv[6 * i + r] = q;
+        dv[r] = q;
+        // row r of P = S Acp, each entry summed over k in order (rows of Acp as 16-byte loads)
 #pragma unroll
-        for (int cc = 0; cc < 6; ++cc) {
-          double v = 0.0;
+        for (int cc = 0; cc < 6; ++cc) Pr[cc] = 0.0;
 #pragma unroll
-          for (int k = 0; k < 6; ++k) v += Sr[k] * Acp[k * 6 + cc];
-          P[r * 6 + cc] = v;
+        for (int k = 0; k < 6; ++k) {
+          double ak[6];
+          ld_n<6>(Acp + 6 * k, ak);
+#pragma unroll
+          for (int cc = 0; cc < 6; ++cc) Pr[cc] += Sr[k] * ak[cc];
         }
+#pragma unroll
+        for (int e = 0; e < 3; ++e) P[3 * r + e] = make_double2(Pr[2 * e], Pr[2 * e + 1]);
       }
+      st_n<6>(c.s.dv + 6 * (size_t)i, dv);
     } else {
+      double dv[6];
 #pragma unroll
       for (int r = 0; r < 6; ++r) {
         double v = 0.0;
 #pragma unroll
         for (int k = 0; k < 6; ++k) v += Dinv[r * 6 + k] * b[k];
-        c.s.dv[6 * i + r] = v;
+        dv[r] = v;
       }
+      st_n<6>(c.s.dv + 6 * (size_t)i, dv);
     }
   }
 }
 
-// Back substitution, one thread per node of level L >= 1 (roots to leaves).
 __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
   for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
@@ -693,24 +728,29 @@ __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
     const int p = c.A.dn_parent[c.d.dyn_off + i];
     const double* Acp = c.s.Acp + 36 * (size_t)i;
     const double* Dinv = c.s.Dinv + 36 * (size_t)i;
-    double xp[6], b[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) xp[k] = c.s.dv[6 * p + k];
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      double v = 0.0;
-#pragma unroll
-      for (int k = 0; k < 6; ++k) v += Acp[r * 6 + k] * xp[k];
-      b[r] = c.s.bvec[6 * i + r] - v;
-      c.s.bvec[6 * i + r] = b[r];
-    }
+    double xp[6], b[6], x[6];
+    ld_n<6>(c.s.dv + 6 * (size_t)p, xp);
+    ld_n<6>(c.s.bvec + 6 * (size_t)i, b);
 #pragma unroll
     for (int r = 0; r < 6; ++r) {
+      double ar[6];
+      ld_n<6>(Acp + 6 * r, ar);
       double v = 0.0;
 #pragma unroll
-      for (int k = 0; k < 6; ++k) v += Dinv[r * 6 + k] * b[k];
-      c.s.dv[6 * i + r] = v;
+      for (int k = 0; k < 6; ++k) v += ar[k] * xp[k];
+      b[r] = b[r] - v;
     }
+    st_n<6>(c.s.bvec + 6 * (size_t)i, b);
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double dr[6];
+      ld_n<6>(Dinv + 6 * r, dr);
+      double v = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) v += dr[k] * b[k];
+      x[r] = v;
+    }
+    st_n<6>(c.s.dv + 6 * (size_t)i, x);
   }
 }
 

@@ -149,6 +149,21 @@ __device__ inline void op_pre(const Ctx& c, const double* x, double half, int q)
   for (int k = 0; k < 8; ++k) c.s.mid[8 * q + k] = m[k];
 }
 
+// N doubles (N even) between registers and 16-byte aligned memory, two at a time (every scratch
+// array starts on a 16-byte boundary and holds its items at even offsets).
+template <int N>
+__device__ __forceinline__ void ld_n(const double* p, double* o) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int e = 0; e < N / 2; ++e) { const double2 x = q[e]; o[2 * e] = x.x; o[2 * e + 1] = x.y; }
+}
+template <int N>
+__device__ __forceinline__ void st_n(double* p, const double* v) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int e = 0; e < N / 2; ++e) q[e] = make_double2(v[2 * e], v[2 * e + 1]);
+}
+
 // Jacobian slice storage: FP32 in the mixed path (the slices are FP32 duals, so nothing is lost),
 // FP64 otherwise. Slice s of joint q: its 6x6 derivative block d[36] (row-major) at (q * 4 + s) *
 // kJacStride. The slices' value parts are not stored: the residual takes the FP64 values (conn).
@@ -250,18 +265,19 @@ __device__ inline double op_post(const Ctx& c, const double* x, double half, int
   int q = c.A.dn_body[c.d.dyn_off + i];
   int g = c.gbody(q);
   double tot[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) tot[k] = c.s.ext[6 * q + k];
+  ld_n<6>(c.s.ext + 6 * (size_t)q, tot);
   int p0 = c.A.ib_inc_ptr[c.d.inc_off + q], p1 = c.A.ib_inc_ptr[c.d.inc_off + q + 1];
   for (int t = p0; t < p1; ++t) {
     int ref = c.A.ib_inc_ref[t];
     int jq = ref >> 1;
+    double w[6];
+    ld_n<6>(c.s.conn + 6 * (size_t)jq, w);
     if (ref & 1) {
 #pragma unroll
-      for (int k = 0; k < 6; ++k) tot[k] = tot[k] - c.s.conn[6 * jq + k];
+      for (int k = 0; k < 6; ++k) tot[k] = tot[k] - w[k];
     } else {
 #pragma unroll
-      for (int k = 0; k < 6; ++k) tot[k] = tot[k] + c.s.conn[6 * jq + k];
+      for (int k = 0; k < 6; ++k) tot[k] = tot[k] + w[k];
     }
   }
   double I9[9];
@@ -269,10 +285,10 @@ __device__ inline double op_post(const Ctx& c, const double* x, double half, int
   for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
   const bool diag = c.W.diagonal[g] != 0;
   const double mass = c.W.mass[g];
-  const double* mid = c.s.mid + 8 * q;
-  double inv[8];
+  double mid[8], inv[8];
+  ld_n<8>(c.s.mid + 8 * (size_t)q, mid);
   motor_reverse(mid, inv);
-  double* blk = c.s.mass + 36 * (size_t)i;
+  double blk[36];
 #pragma unroll
   for (int col = 0; col < 6; ++col) {
     double e6[6] = {0, 0, 0, 0, 0, 0};
@@ -289,26 +305,25 @@ __device__ inline double op_post(const Ctx& c, const double* x, double half, int
 #pragma unroll
     for (int r = 0; r < 6; ++r) blk[r * 6 + col] = c6[r];
   }
-  const double* vv = x + 6 * q;
-  double p[6], nn[6], hh[6], res[6];
+  st_n<36>(c.s.mass + 36 * (size_t)i, blk);
+  double vv[6], p[6], nn[6], hh[6], res[6];
+  ld_n<6>(x + 6 * (size_t)q, vv);
+  ld_n<6>(c.s.snap + 6 * (size_t)q, nn);
 #pragma unroll
   for (int r = 0; r < 6; ++r) {
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) acc += blk[r * 6 + k] * vv[k];
     p[r] = acc;
-    nn[r] = c.s.snap[6 * q + r];
     hh[r] = tot[r] * half;
   }
 #pragma unroll
   for (int r = 0; r < 6; ++r) res[r] = -(p[r] - nn[r] - hh[r]);
-#pragma unroll
-  for (int r = 0; r < 6; ++r) c.s.rhs[6 * i + r] = res[r];
+  st_n<6>(c.s.rhs + 6 * (size_t)i, res);
   auto sq3 = [](const double* v) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; };
   double lin = fmax(fmax(fmax(sq3(p), sq3(nn)), sq3(hh)), kFloor2);
   double ang = fmax(fmax(fmax(sq3(p + 3), sq3(nn + 3)), sq3(hh + 3)), kFloor2);
-  c.s.scale[2 * i] = lin;
-  c.s.scale[2 * i + 1] = ang;
+  reinterpret_cast<double2*>(c.s.scale)[i] = make_double2(lin, ang);
   worst = nan_max(worst, sq3(res) / lin);
   worst = nan_max(worst, sq3(res + 3) / ang);
   return worst;

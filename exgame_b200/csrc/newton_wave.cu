@@ -582,13 +582,22 @@ __global__ void k_w_node_sq(WaveArgs a, int want_state, int mass) {
     Ctx c = wave_ctx_lite(a, it.x);
     const size_t o = 36 * (size_t)it.y;
     double s = 0.0;
+    auto add_sq = [&](const double* blk) {  // entries in order, read two at a time
+      const double2* b2 = reinterpret_cast<const double2*>(blk + o);
+#pragma unroll 6
+      for (int e = 0; e < 18; ++e) {
+        const double2 v = b2[e];
+        s += v.x * v.x;
+        s += v.y * v.y;
+      }
+    };
     if (mass) {
-      for (int e = 0; e < 36; ++e) s += c.s.mass0[o + e] * c.s.mass0[o + e];
+      add_sq(c.s.mass0);
     } else {
-      for (int e = 0; e < 36; ++e) s += c.s.D[o + e] * c.s.D[o + e];
+      add_sq(c.s.D);
       if (c.A.dn_parent[c.d.dyn_off + it.y] >= 0) {
-        for (int e = 0; e < 36; ++e) s += c.s.Acp[o + e] * c.s.Acp[o + e];
-        for (int e = 0; e < 36; ++e) s += c.s.Apc[o + e] * c.s.Apc[o + e];
+        add_sq(c.s.Acp);
+        add_sq(c.s.Apc);
       }
     }
     a.nodesq[t] = s;
@@ -618,20 +627,6 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int wa
     }
     __syncthreads();
   }
-}
-
-// N doubles (N even) between registers and 16-byte aligned memory, two at a time.
-template <int N>
-__device__ __forceinline__ void ld_n(const double* p, double* o) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-#pragma unroll
-  for (int e = 0; e < N / 2; ++e) { const double2 x = q[e]; o[2 * e] = x.x; o[2 * e + 1] = x.y; }
-}
-template <int N>
-__device__ __forceinline__ void st_n(double* p, const double* v) {
-  double2* q = reinterpret_cast<double2*>(p);
-#pragma unroll
-  for (int e = 0; e < N / 2; ++e) q[e] = make_double2(v[2 * e], v[2 * e + 1]);
 }
 
 // Elimination, one thread per node of level L (leaves to roots), the node's blocks in registers:

@@ -135,20 +135,6 @@ __device__ inline double nan_max(double a, double b) {
   return a > b ? a : b;
 }
 
-// ── per-item operations ─────────────────────────────────────────────────────
-// PRE (functions::pre): mid = exp(half/2 x) * pose of island body q.
-__device__ inline void op_pre(const Ctx& c, const double* x, double half, int q) {
-  int g = c.gbody(q);
-  double pose[8], vb[6], e[8], m[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
-  screw_from6(x + 6 * q, vb);
-  twist_exp(vb, half, e);
-  motor_compose(pose, e, m);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) c.s.mid[8 * q + k] = m[k];
-}
-
 // N doubles (N even) between registers and 16-byte aligned memory, two at a time (every scratch
 // array starts on a 16-byte boundary and holds its items at even offsets).
 template <int N>
@@ -162,6 +148,20 @@ __device__ __forceinline__ void st_n(double* p, const double* v) {
   double2* q = reinterpret_cast<double2*>(p);
 #pragma unroll
   for (int e = 0; e < N / 2; ++e) q[e] = make_double2(v[2 * e], v[2 * e + 1]);
+}
+
+// ── per-item operations ─────────────────────────────────────────────────────
+// PRE (functions::pre): mid = exp(half/2 x) * pose of island body q.
+__device__ inline void op_pre(const Ctx& c, const double* x, double half, int q) {
+  int g = c.gbody(q);
+  double pose[8], xv[6], vb[6], e[8], m[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+  ld_n<6>(x + 6 * (size_t)q, xv);
+  screw_from6(xv, vb);
+  twist_exp(vb, half, e);
+  motor_compose(pose, e, m);
+  st_n<8>(c.s.mid + 8 * (size_t)q, m);
 }
 
 // Jacobian slice storage: FP32 in the mixed path (the slices are FP32 duals, so nothing is lost),
@@ -380,16 +380,14 @@ __device__ inline void op_load_world_state(const Ctx& c, int q) {
   screw_from6(mom, mb);
   wrench_transport(mb, pose, pw);
   screw_to6(pw, p6);
-#pragma unroll
-  for (int k = 0; k < 6; ++k) { c.s.vm[6 * q + k] = wv[k]; c.s.snap[6 * q + k] = p6[k]; }
+  st_n<6>(c.s.vm + 6 * (size_t)q, wv);
+  st_n<6>(c.s.snap + 6 * (size_t)q, p6);
 }
 
 // External wrench of island body q: gravity (F, p x F) and the uniform field, frozen over the whole
 // step.
 __device__ inline void op_load_external(const Ctx& c, int q) {
-  double* e = c.s.ext + 6 * q;
-#pragma unroll
-  for (int k = 0; k < 6; ++k) e[k] = 0.0;
+  double e[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   int g = c.gbody(q);
   double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
   if (c.P.splits > 0) {
@@ -406,6 +404,7 @@ __device__ inline void op_load_external(const Ctx& c, int q) {
     e[5] = pm.x * f[1] - pm.y * f[0];
   }
   add_uniform_field(c.W.wparams[c.d.world].field_accel, pm, e);
+  st_n<6>(c.s.ext + 6 * (size_t)q, e);
 }
 
 // commit_span (newton.rs:708-753) for dynamic node i: M = M0 * exp(span v), P = 2 P_mid - P_n
@@ -418,7 +417,10 @@ __device__ inline void op_commit(const Ctx& c, double span, double half, bool co
   for (int k = 0; k < 8; ++k) m0[k] = c.W.pose[(size_t)k * c.W.n + g];
 #pragma unroll
   for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
-  screw_from6(c.s.vm + 6 * q, vb);
+  double vq[6], snap[6];
+  ld_n<6>(c.s.vm + 6 * (size_t)q, vq);
+  ld_n<6>(c.s.snap + 6 * (size_t)q, snap);
+  screw_from6(vq, vb);
   twist_exp(vb, half, e);
   motor_compose(m0, e, pm);
   motor_reverse(pm, inv);
@@ -431,7 +433,7 @@ __device__ inline void op_commit(const Ctx& c, double span, double half, bool co
   screw_to6(pw, psm);
   double pnew[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) pnew[k] = converged ? psm[k] * 2.0 - c.s.snap[6 * q + k] : psm[k];
+  for (int k = 0; k < 6; ++k) pnew[k] = converged ? psm[k] * 2.0 - snap[k] : psm[k];
   double en[8], mnew[8], minv[8], pnb[6], pbody[6], out6[6];
   twist_exp(vb, span, en);
   motor_compose(m0, en, mnew);

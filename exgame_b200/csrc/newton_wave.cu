@@ -350,8 +350,9 @@ __global__ void k_w_start(WaveArgs a) {
     if (!(a.ctl[it.x].flags & F_START)) continue;
     Ctx c = wave_ctx(a, it.x);
     op_load_world_state(c, it.y);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) c.s.best[6 * it.y + k] = c.s.vm[6 * it.y + k];
+    double v[6];
+    ld_n<6>(c.s.vm + 6 * (size_t)it.y, v);
+    st_n<6>(c.s.best + 6 * (size_t)it.y, v);
   }
 }
 
@@ -470,16 +471,29 @@ __global__ void k_w_copy_bodies(WaveArgs a) {
     const int f = w.flags;
     if (!(f & (F_COPY_BEST | F_ACCEPT | F_BASE | F_TRIAL))) continue;
     Ctx c = wave_ctx(a, it.x);
-    const int q = it.y;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      if (f & F_COPY_BEST) c.s.best[6 * q + k] = c.s.vm[6 * q + k];
-      if (f & F_ACCEPT) c.s.vm[6 * q + k] = c.s.trial[6 * q + k];
-      if (f & F_BASE) c.s.base[6 * q + k] = c.s.vm[6 * q + k];
+    const size_t o = 6 * (size_t)it.y;
+    double v[6];
+    ld_n<6>(c.s.vm + o, v);
+    if (f & F_COPY_BEST) st_n<6>(c.s.best + o, v);
+    if (f & F_ACCEPT) {
+      ld_n<6>(c.s.trial + o, v);
+      st_n<6>(c.s.vm + o, v);
     }
-    if (f & F_TRIAL) {
+    if (f & F_BASE) st_n<6>(c.s.base + o, v);
+    if (f & F_TRIAL) {  // op_trial for the body's six entries
+      const int i = c.A.ib_order[c.d.body_off + it.y];
+      double bs[6], tr[6];
+      ld_n<6>(c.s.base + o, bs);
+      if (i >= 0) {
+        double d[6];
+        ld_n<6>(c.s.dv + 6 * (size_t)i, d);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) op_trial(c, w.alpha, 6 * q + k);
+        for (int k = 0; k < 6; ++k) tr[k] = bs[k] + d[k] * w.alpha;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tr[k] = bs[k];
+      }
+      st_n<6>(c.s.trial + o, tr);
     }
   }
 }
@@ -757,15 +771,18 @@ __global__ void k_w_nz(WaveArgs a) {
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
     Ctx c = wave_ctx(a, it.x);
-    double* dv = c.s.dv + 6 * it.y;
+    double* dv = c.s.dv + 6 * (size_t)it.y;
     int nz = 0;
     if (w.singular) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) dv[k] = __longlong_as_double(0x7ff8000000000000LL);
+      const double nan = __longlong_as_double(0x7ff8000000000000LL);
+      const double v[6] = {nan, nan, nan, nan, nan, nan};
+      st_n<6>(dv, v);
       nz = 1;
     } else {
+      double v[6];
+      ld_n<6>(dv, v);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) nz |= dv[k] != 0.0;
+      for (int k = 0; k < 6; ++k) nz |= v[k] != 0.0;
     }
     if (nz && !w.nz) atomicOr(&w.nz, 1);
   }
@@ -777,8 +794,9 @@ __global__ void k_w_restore(WaveArgs a) {
     int2 it = a.body[t];
     if (a.ctl[it.x].state != WS_END) continue;
     Ctx c = wave_ctx(a, it.x);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) c.s.vm[6 * it.y + k] = c.s.best[6 * it.y + k];
+    double v[6];
+    ld_n<6>(c.s.best + 6 * (size_t)it.y, v);
+    st_n<6>(c.s.vm + 6 * (size_t)it.y, v);
   }
 }
 

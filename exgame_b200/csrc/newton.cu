@@ -365,9 +365,10 @@ long long newton_footprint_bytes(int nb, int nj) {
 NewtonWorld::~NewtonWorld() {
   if (wave_graph_) cudaGraphExecDestroy(wave_graph_);
   for (DevArr<int>* a : {&dw_isl_, &dw_dyn_first_, &dw_live_}) a->release();
-  for (DevArr<int2>* a : {&dw_body_, &dw_dyn_, &dw_joint_, &dw_cell_, &dw_level_}) a->release();
+  for (DevArr<int2>* a : {&dw_body_, &dw_dyn_, &dw_joint_, &dw_cell_, &dw_level_, &dw_cell_terms_}) a->release();
   dw_ctl_.release();
   dw_nodesq_.release();
+  dw_desc_.release();
   d_desc.release();
   for (DevArr<int>* a : {&d_isl_body, &d_jl_law, &d_jl_a, &d_jl_b, &d_ib_order, &d_ib_inc_ptr, &d_ib_inc_ref, &d_dn_body,
                          &d_dn_parent, &d_lv_ptr, &d_lv_nodes, &d_ch_ptr, &d_ch_idx, &d_cell_ptr, &d_cell_terms, &d_stats,

@@ -119,6 +119,20 @@ __device__ inline Ctx make_ctx(const NewtonDeviceArrays& A, const WorldRef& W, i
   return c;
 }
 
+// A context from a descriptor the caller already holds (the wave keeps a copy per wave slot);
+// c.island is then not set. `params` resolves the world's step parameters.
+__device__ __forceinline__ Ctx make_ctx_desc(const NewtonDeviceArrays& A, const WorldRef& W, const IslandDesc& d,
+                                             bool params) {
+  Ctx c;
+  c.A = A;
+  c.W = W;
+  c.island = -1;
+  c.d = d;
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  if (params) resolve_params(c);
+  return c;
+}
+
 // The island's structure and scratch only (for operations that read no world parameter).
 __device__ inline Ctx make_ctx_lite(const NewtonDeviceArrays& A, const WorldRef& W, int island) {
   Ctx c;

@@ -50,6 +50,7 @@ struct WaveArgs {
   WorldRef W;
   WaveCtl* ctl;
   const int* isl;       // wave slot -> island
+  const IslandDesc* wdesc;  // wave slot -> the island's descriptor (a copy, one load less)
   int n_isl;
   const int2* body;     // (slot, island body)
   int n_body;
@@ -58,6 +59,7 @@ struct WaveArgs {
   const int2* joint;    // (slot, island joint)
   int n_joint;
   const int2* cell;     // (slot, assembly cell)
+  const int2* cell_range;  // per cell item: [p0, p1) of its terms in A.cell_terms
   int n_cell;
   const int2* level;    // (slot, node) grouped by elimination level
   const int* dyn_first; // first dynamic-node item of each wave slot (n_isl + 1 entries)
@@ -87,12 +89,12 @@ __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 // is a swap of the two block arrays' roles here: the evaluation writes the blocks into `mass`, and
 // adopting them as mass0 flips mflip, so the next evaluation writes into the other array.
 __device__ __forceinline__ Ctx wave_ctx(const WaveArgs& a, int k) {
-  Ctx c = make_ctx(a.A, a.W, a.isl[k]);
+  Ctx c = make_ctx_desc(a.A, a.W, a.wdesc[k], true);
   if (a.ctl[k].mflip) { double* t = c.s.mass; c.s.mass = c.s.mass0; c.s.mass0 = t; }
   return c;
 }
 __device__ __forceinline__ Ctx wave_ctx_lite(const WaveArgs& a, int k) {
-  Ctx c = make_ctx_lite(a.A, a.W, a.isl[k]);
+  Ctx c = make_ctx_desc(a.A, a.W, a.wdesc[k], false);
   if (a.ctl[k].mflip) { double* t = c.s.mass; c.s.mass = c.s.mass0; c.s.mass0 = t; }
   return c;
 }
@@ -106,7 +108,7 @@ __global__ void k_w_init(WaveArgs a) {
   }
   for (int k = gtid(); k < a.n_isl; k += gthreads()) {
     WaveCtl& c = a.ctl[k];
-    const IslandDesc& d = a.A.desc[a.isl[k]];
+    const IslandDesc& d = a.wdesc[k];
     c.active = a.W.w_active[d.world];
     c.state = c.active ? WS_START : WS_DONE;
     c.remaining = 1ull << kMaxDepth;
@@ -139,7 +141,7 @@ __global__ void k_w_begin(WaveArgs a) {
     if (c.state == WS_START) {
       unsigned long long units = 1ull << (kMaxDepth - c.depth);
       while (units > c.remaining) { ++c.depth; units >>= 1; }
-      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const IslandDesc& d = a.wdesc[k];
       double span = a.W.wparams[d.world].dt;
       for (int t = 0; t < c.depth; ++t) span = span / 2.0;
       c.span = span;
@@ -159,7 +161,7 @@ __global__ void k_w_begin(WaveArgs a) {
       c.state = WS_ITER;
     }
     if (c.state == WS_ITER) {
-      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const IslandDesc& d = a.wdesc[k];
       const exg_step_params_t& wp = a.W.wparams[d.world];
       const int max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
       if (c.it >= max_newton) {
@@ -179,7 +181,7 @@ __global__ void k_w_after_eval(WaveArgs a) {
   for (int k = gtid(); k < a.n_isl; k += gthreads()) {
     WaveCtl& c = a.ctl[k];
     if (c.eval == EV_FULL || c.eval == EV_JAC) {
-      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const IslandDesc& d = a.wdesc[k];
       const exg_step_params_t& wp = a.W.wparams[d.world];
       double rnorm;
       if (c.eval == EV_JAC) {
@@ -205,7 +207,7 @@ __global__ void k_w_after_eval(WaveArgs a) {
         c.singular = 0;
       }
     } else if (c.eval == EV_PLAIN) {
-      const IslandDesc& d = a.A.desc[a.isl[k]];
+      const IslandDesc& d = a.wdesc[k];
       const exg_step_params_t& wp = a.W.wparams[d.world];
       const int max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
       double tnorm = __longlong_as_double((long long)c.worst_bits);
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, i
     for (int j = 0; j < 8; ++j) {
       if (!((active >> (4 * j)) & 1u)) continue;  // no joint here, or its island did not evaluate slices
       const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
-      const IslandDesc& d = a.A.desc[a.isl[jt.x]];
+      const IslandDesc& d = a.wdesc[jt.x];
       J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
                 (size_t)jt.y * 4 * kJacStride + KIND * kHalf;
       const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
@@ -558,7 +560,7 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
   for (int t0 = 3 * (gtid() >> 5); t0 < a.n_cell; t0 += 3 * (gthreads() >> 5)) {
     const int t = t0 + grp;
     if (grp >= 3 || t >= a.n_cell) continue;
-    const int2 it = a.cell[t];
+    const int2 it = a.cell[t], range = a.cell_range[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
     const Ctx c = wave_ctx_lite(a, it.x);
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (kind == 0) load4(c.s.mass0 + 36 * (size_t)i + e0, acc);
     const int* terms = c.A.cell_terms;
-    const int p0 = c.A.cell_ptr[c.d.cell_off + cell], p1 = c.A.cell_ptr[c.d.cell_off + cell + 1];
+    const int p0 = range.x, p1 = range.y;
     // the group's nine lanes fetch nine term indices at a time and pass them round by shuffle, so
     // a term's block loads wait on no index load of their own
     const unsigned gmask = 0x1ffu << (9 * grp);
@@ -820,7 +822,7 @@ bool NewtonWorld::wave_island(const IslandDesc& d) const {
 
 int NewtonWorld::build_wave(cudaStream_t s) {
   std::vector<int> isl, dyn_first{0};
-  std::vector<int2> body, dyn, joint, cell;
+  std::vector<int2> body, dyn, joint, cell, cell_range;
   int max_levels = 0;
   for (int I = 0; I < (int)desc_.size(); ++I)
     if (alive_[I] && wave_island(desc_[I])) isl.push_back(I);
@@ -830,7 +832,10 @@ int NewtonWorld::build_wave(cudaStream_t s) {
     for (int i = 0; i < d.m; ++i) dyn.push_back(make_int2(k, i));
     dyn_first.push_back((int)dyn.size());
     for (int q = 0; q < d.nj; ++q) joint.push_back(make_int2(k, q));
-    for (int t = 0; t < 3 * d.m; ++t) cell.push_back(make_int2(k, t));
+    for (int t = 0; t < 3 * d.m; ++t) {
+      cell.push_back(make_int2(k, t));
+      cell_range.push_back(make_int2(h_cell_ptr[d.cell_off + t], h_cell_ptr[d.cell_off + t + 1]));
+    }
     max_levels = std::max(max_levels, d.n_levels);
   }
   // joint items grouped by law (a warp then evaluates one law), islands in order within a law
@@ -857,12 +862,16 @@ int NewtonWorld::build_wave(cudaStream_t s) {
   auto up = [&](auto& d, const auto& h) {
     if (rc == EXG_OK) rc = d.assign(h.data(), (long long)h.size(), s);
   };
+  std::vector<IslandDesc> wdesc;
+  for (int I : isl) wdesc.push_back(desc_[I]);
   up(dw_isl_, isl);
+  up(dw_desc_, wdesc);
   up(dw_dyn_first_, dyn_first);
   up(dw_body_, body);
   up(dw_dyn_, dyn);
   up(dw_joint_, joint);
   up(dw_cell_, cell);
+  up(dw_cell_terms_, cell_range);
   up(dw_level_, level);
   if (rc == EXG_OK) rc = dw_ctl_.reserve(std::max<long long>((long long)isl.size(), 1) * (long long)sizeof(WaveCtl), s);
   if (rc == EXG_OK) rc = dw_nodesq_.reserve(std::max<long long>((long long)dyn.size(), 1), s);
@@ -890,6 +899,7 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
                  w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
   a.ctl = reinterpret_cast<WaveCtl*>(dw_ctl_.ptr);
   a.isl = dw_isl_.ptr;
+  a.wdesc = dw_desc_.ptr;
   a.n_isl = n_wave_;
   a.body = dw_body_.ptr;
   a.n_body = wave_counts_[0];
@@ -898,6 +908,7 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   a.joint = dw_joint_.ptr;
   a.n_joint = wave_counts_[2];
   a.cell = dw_cell_.ptr;
+  a.cell_range = dw_cell_terms_.ptr;
   a.n_cell = wave_counts_[3];
   a.level = dw_level_.ptr;
   a.dyn_first = dw_dyn_first_.ptr;

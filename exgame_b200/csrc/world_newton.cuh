@@ -116,7 +116,9 @@ class NewtonWorld {
   int wave_law_first_[5] = {0, 0, 0, 0, 0};  // joint items of law L: [first[L], first[L+1])
   std::vector<int> wave_level_ptr_;
   DevArr<int> dw_isl_, dw_dyn_first_, dw_live_;
+  DevArr<IslandDesc> dw_desc_;  // island descriptors in wave-slot order
   DevArr<int2> dw_body_, dw_dyn_, dw_joint_, dw_cell_, dw_level_;
+  DevArr<int2> dw_cell_terms_;  // per cell item: its term range in cell_terms (absolute)
   DevArr<unsigned char> dw_ctl_;
   DevArr<double> dw_nodesq_;
   cudaGraphExec_t wave_graph_ = nullptr;

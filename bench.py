@@ -9,8 +9,9 @@ with log-uniform step counts through the native request loop, p50/p99 latency).
 
 A step is one Mechanism::step of the whole workload (every body advanced by dt). `value` is
 body-steps/s from CUDA events on the library's stream with the state resident in HBM; `e2e` is the
-same metric through the public API with host buffers (the step's inputs copied in from host
-memory and its result read back inside the timed region). Under torchrun each rank steps its own
+same metric through the public API with page-locked host buffers: each step the dynamic state
+(pose, momentum) copied in, the step, the state read back, all inside the timed region
+(`e2e.records` does the same with whole body records). Under torchrun each rank steps its own
 replica of the workload (independent worlds: weak scaling, no collective in the data path); the
 timing is the max over ranks.
 
@@ -292,27 +293,34 @@ def run_ours(args, rank, world_size, local_rank):
     total_bodies = sharding.sum_over_ranks(n_bodies, dist, device="cuda") if world_size > 1 else n_bodies
     value = total_bodies * args.steps / t
 
-    # end to end through the public API: host state in, step, host state out
-    host_in = []
-    for w in worlds:  # page-locked host buffers, as a serving host would keep them
-        h = _lib.host_bodies(w.n)
-        w.bodies(out=h)
-        host_in.append(h)
-    h2d = sum(h.nbytes for h in host_in)
-    e2e_steps = args.steps
-    dev.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        for w, h in zip(worlds, host_in):
-            w.set_bodies(h)
-            w.step(1)
-            w.bodies(out=h)
-    dev.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if world_size > 1:
-        t_e2e = sharding.max_over_ranks(t_e2e, dist, device="cuda")
-    e2e = {"value": total_bodies * e2e_steps / t_e2e, "unit": METRIC, "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(h2d), "steps": e2e_steps}
+    # end to end through the public API, page-locked host buffers as a serving host keeps them:
+    # the dynamic state (pose, momentum) in, one step, the state out (exg_world_set/get_state);
+    # beside it the same with whole records (exg_world_set/get_bodies)
+    def end_to_end(alloc, get, put):
+        host = []
+        for w in worlds:
+            h = alloc(w.n)
+            get(w, h)
+            host.append(h)
+        nbytes = sum(h.nbytes for h in host)
+        dev.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for w, h in zip(worlds, host):
+                put(w, h)
+                w.step(1)
+                get(w, h)
+        dev.synchronize()
+        t_e = time.perf_counter() - t0
+        if world_size > 1:
+            t_e = sharding.max_over_ranks(t_e, dist, device="cuda")
+        return {"value": total_bodies * args.steps / t_e, "unit": METRIC, "h2d_bytes_per_step": int(nbytes),
+                "d2h_bytes_per_step": int(nbytes), "steps": args.steps}
+
+    e2e = end_to_end(_lib.host_state, lambda w, h: w.state(out=h), lambda w, h: w.set_state(h))
+    e2e["transfer"] = "dynamic state (pose, momentum: 112 B per body) in and out every step"
+    e2e["records"] = end_to_end(_lib.host_bodies, lambda w, h: w.bodies(out=h), lambda w, h: w.set_bodies(h))
+    e2e["records"]["transfer"] = "whole body records (208 B per body) in and out every step"
 
     # dominant kernel, timed live with events on the library stream over a profiled pass
     kind, ms, nl, flops, bound, label, shares = dominant_kernel(dev, args.workload, parts, args.steps, worlds)

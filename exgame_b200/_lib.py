@@ -43,6 +43,8 @@ SIGNATURES = {
     "exg_world_step": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "exg_world_get_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_set_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
+    "exg_world_get_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
+    "exg_world_set_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_stats": (ctypes.c_int, [_vp, _vp]),
     "exg_world_energy": (ctypes.c_int, [_vp, _c_double_p]),
     "exg_batch_create": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
@@ -268,6 +270,22 @@ class DeviceWorld:
         b = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
         check(lib().exg_world_set_bodies(self.handle, ptr(b), len(b)), "exg_world_set_bodies")
 
+    def state(self, out=None):
+        """Every body's (pose[8], momentum[6]) as an (n, 14) array (into `out` when given, e.g. a
+        host_state buffer)."""
+        if out is None:
+            out = np.zeros((self.n, 14), dtype=np.float64)
+        if out.dtype != np.float64 or out.shape != (self.n, 14) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of shape (n_bodies, 14)")
+        check(lib().exg_world_get_state(self.handle, ptr(out), self.n), "exg_world_get_state")
+        return out
+
+    def set_state(self, state):
+        st = np.ascontiguousarray(state, dtype=np.float64)
+        if st.shape != (self.n, 14):
+            raise ValueError("state must have shape (n_bodies, 14)")
+        check(lib().exg_world_set_state(self.handle, ptr(st), self.n), "exg_world_set_state")
+
     def stats(self):
         s = np.zeros((), dtype=WORLD_STATS_DTYPE)
         check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
@@ -413,6 +431,20 @@ def host_bodies(n):
     buf = (ctypes.c_char * nbytes).from_address(p.value)
     arr = np.frombuffer(buf, dtype=BODY_DTYPE, count=int(n))
     arr[...] = np.zeros((), dtype=BODY_DTYPE)
+    weakref.finalize(buf, lib().exg_host_free, ctypes.c_void_p(p.value))
+    return arr
+
+
+def host_state(n):
+    """A zeroed (n, 14) float64 array in page-locked host memory, for DeviceWorld.state/set_state
+    (pose[8] then momentum[6] per body)."""
+    import weakref
+    nbytes = max(1, int(n) * 14 * 8)
+    p = ctypes.c_void_p()
+    check(lib().exg_host_alloc(nbytes, ctypes.byref(p)), "exg_host_alloc")
+    buf = (ctypes.c_char * nbytes).from_address(p.value)
+    arr = np.frombuffer(buf, dtype=np.float64, count=int(n) * 14).reshape(int(n), 14)
+    arr[...] = 0.0
     weakref.finalize(buf, lib().exg_host_free, ctypes.c_void_p(p.value))
     return arr
 

@@ -152,6 +152,38 @@ __global__ void k_bodies_scatter(const exg_body_t* __restrict__ rec, int count, 
   diag[i] = r.diagonal;
 }
 
+// Dynamic state only — per body pose[8] then momentum[6], the first 14 doubles of a record — and
+// the pool's rows. Record k belongs to body first + k, or to body dst[k] when a map is given.
+__global__ void k_state_scatter(const double* __restrict__ st, int count, int first, const int* __restrict__ dst,
+                                double* pose, double* mom, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const double2* r = reinterpret_cast<const double2*>(st + 14 * (size_t)k);
+  double v[14];
+#pragma unroll
+  for (int e = 0; e < 7; ++e) { const double2 x = r[e]; v[2 * e] = x.x; v[2 * e + 1] = x.y; }
+  const int i = dst ? dst[k] : first + k;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) pose[(size_t)c * n + i] = v[c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) mom[(size_t)c * n + i] = v[8 + c];
+}
+
+__global__ void k_state_gather(double* __restrict__ st, int count, int first, const int* __restrict__ dst,
+                               const double* pose, const double* mom, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int i = dst ? dst[k] : first + k;
+  double v[14];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) v[c] = pose[(size_t)c * n + i];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) v[8 + c] = mom[(size_t)c * n + i];
+  double2* r = reinterpret_cast<double2*>(st + 14 * (size_t)k);
+#pragma unroll
+  for (int e = 0; e < 7; ++e) r[e] = make_double2(v[2 * e], v[2 * e + 1]);
+}
+
 // Records staged for exg_world_set_bodies / exg_batch_set_world, checked before any is written:
 // flags[0] = some dynamic record has no positive mass (the call is refused), flags[1] = some
 // record's kinematic flag differs from its body's current one (implicit worlds rebuild islands).
@@ -219,6 +251,20 @@ int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_bod
   if (count <= 0) return EXG_OK;
   k_bodies_scatter<<<(count + 127) / 128, 128, 0, s>>>(rec, count, first, dst, w.pose, w.mom, w.mass, w.inertia, w.size,
                                                        w.kinematic, w.diagonal, w.n);
+  return exg_after_launch(dev);
+}
+
+int launch_state_scatter(exg_device_s* dev, const DeviceWorld& w, const double* st, int count, int first,
+                         const int* dst, cudaStream_t s) {
+  if (count <= 0) return EXG_OK;
+  k_state_scatter<<<(count + 127) / 128, 128, 0, s>>>(st, count, first, dst, w.pose, w.mom, w.n);
+  return exg_after_launch(dev);
+}
+
+int launch_state_gather(exg_device_s* dev, const DeviceWorld& w, double* st, int count, int first, const int* dst,
+                        cudaStream_t s) {
+  if (count <= 0) return EXG_OK;
+  k_state_gather<<<(count + 127) / 128, 128, 0, s>>>(st, count, first, dst, w.pose, w.mom, w.n);
   return exg_after_launch(dev);
 }
 

@@ -869,6 +869,42 @@ int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
   return download_records(W, out, 0, n, W->map_d.ptr);
 }
 
+int exg_world_get_state(exg_world_t W, double* out, int32_t n) {
+  if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  long long total = 0;
+  int rc = ensure_record_map(W, &total);
+  if (rc != EXG_OK) return rc;
+  if (n != total) return EXG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return EXG_OK;
+  if ((rc = stage_reserve(W, n)) != EXG_OK) return rc;  // 14 doubles fit in a record's slot
+  cudaStream_t s = W->dev->stream;
+  double* st = reinterpret_cast<double*>(W->stage_d.ptr);
+  if ((rc = launch_state_gather(W->dev, W->w, st, n, 0, W->map_d.ptr, s)) != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaMemcpyAsync(out, st, sizeof(double) * 14 * (size_t)n, cudaMemcpyDeviceToHost, s));
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  return EXG_OK;
+}
+
+int exg_world_set_state(exg_world_t W, const double* state, int32_t n) {
+  if (!W || !state) return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  long long total = 0;
+  int rc = ensure_record_map(W, &total);
+  if (rc != EXG_OK) return rc;
+  if (n != total) return EXG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return EXG_OK;
+  if ((rc = stage_reserve(W, n)) != EXG_OK) return rc;
+  cudaStream_t s = W->dev->stream;
+  double* st = reinterpret_cast<double*>(W->stage_d.ptr);
+  EXG_CUDA_TRY(cudaMemcpyAsync(st, state, sizeof(double) * 14 * (size_t)n, cudaMemcpyHostToDevice, s));
+  if ((rc = launch_state_scatter(W->dev, W->w, st, n, 0, W->map_d.ptr, s)) != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  return EXG_OK;
+}
+
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
   if (!W || !bodies) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(W->dev->mu);

@@ -130,6 +130,10 @@ int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStrea
 // records <-> rows: record k is body first + k, or body dst[k] when dst is not null
 int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
                           const int* dst, cudaStream_t s);
+int launch_state_scatter(exg_device_s* dev, const DeviceWorld& w, const double* st, int count, int first,
+                         const int* dst, cudaStream_t s);
+int launch_state_gather(exg_device_s* dev, const DeviceWorld& w, double* st, int count, int first, const int* dst,
+                        cudaStream_t s);
 int launch_records_check(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
                          const int* dst, int* flags, cudaStream_t s);
 int launch_bodies_gather(exg_device_s* dev, const DeviceWorld& w, exg_body_t* rec, int count, int first,

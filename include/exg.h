@@ -189,6 +189,13 @@ EXG_API int exg_world_destroy(exg_world_t w);
 EXG_API int exg_world_step(exg_world_t w, int32_t n_steps);
 EXG_API int exg_world_get_bodies(exg_world_t w, exg_body_t* out, int32_t n_bodies);
 EXG_API int exg_world_set_bodies(exg_world_t w, const exg_body_t* bodies, int32_t n_bodies);
+/* The dynamic state alone, in the record order of exg_world_get/set_bodies: per body pose[8] then
+ * momentum[6] (14 doubles, 112 B; the first two fields of exg_body_t). Mass, inertia, size and
+ * flags stay as they are on the device, so a loop that feeds states in and reads them back each
+ * step (Mechanism::step with the host reading poses, crates/newton/src/mechanism/mechanism.rs:526)
+ * moves 112 B per body each way instead of a record's 208 B. */
+EXG_API int exg_world_get_state(exg_world_t w, double* state, int32_t n_bodies);
+EXG_API int exg_world_set_state(exg_world_t w, const double* state, int32_t n_bodies);
 EXG_API int exg_world_stats(exg_world_t w, exg_world_stats_t* out);
 
 /* ── batch: many independent worlds of uneven size stepped together (Driver::step over many

@@ -198,6 +198,36 @@ def test_whole_handle_records_follow_slot_order_through_page_locked_buffers(devi
     pool.close()
 
 
+def test_state_accessors_move_pose_and_momentum_in_record_order(device):
+    """exg_world_get/set_state on a pool with a released slot in the middle: 14 doubles per body
+    (pose then momentum) in the records' order; setting states changes nothing else, and stepping
+    from them equals stepping from the same records set whole."""
+    worlds = world_set()
+    pool = _lib.DevicePool(device, max_bodies=4096, max_joints=4096, max_worlds=8)
+    s = [pool.admit(*worlds[k]) for k in (1, 2, 5, 6)]
+    pool.release(s[1])
+    pool.step(2)
+    rec = pool.bodies()
+    st = _lib.host_state(pool.n)
+    pool.state(out=st)
+    assert np.array_equal(st[:, :8], rec["pose"]) and np.array_equal(st[:, 8:], rec["momentum"])
+    st[:, 8:] *= 0.5
+    pool.set_state(st)
+    back = pool.bodies()
+    assert np.array_equal(back["momentum"], st[:, 8:]) and np.array_equal(back["pose"], st[:, :8])
+    for f in ("mass", "inertia", "size", "kinematic", "diagonal"):
+        assert np.array_equal(back[f], rec[f]), f
+    pool.step(3)
+    via_state = pool.bodies()
+    rec["momentum"] *= 0.5
+    pool.set_bodies(rec)
+    pool.step(3)
+    assert same(pool.bodies(), via_state)
+    with pytest.raises(ValueError):
+        pool.set_state(st[:-1])
+    pool.close()
+
+
 def test_server_fails_a_non_finite_world_and_serves_the_rest(device):
     """A request whose world is not finite (a NaN momentum) fails with EXG_ERR_FATAL (the
     reference's EvalError::Fatal of a guarded site), while the requests beside it complete and

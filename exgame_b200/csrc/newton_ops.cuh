@@ -194,11 +194,14 @@ template <int LAW = -1>
 __device__ inline void op_joint_value(const Ctx& c, const double* x, int q) {
   const int joff = c.d.joint_off;
   const int a = c.A.jl_a[joff + q], b = c.A.jl_b[joff + q];
-  double out[12];
-  joint_plain<double>(LAW >= 0 ? LAW : c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), c.s.mid + 8 * a, c.s.mid + 8 * b,
-                      x + 6 * a, x + 6 * b, c.P.dt, c.P.warp, out);
-#pragma unroll
-  for (int r = 0; r < 6; ++r) c.s.conn[6 * q + r] = out[r];
+  double ma[8], mb[8], xa[6], xb[6], out[12];
+  ld_n<8>(c.s.mid + 8 * (size_t)a, ma);
+  ld_n<8>(c.s.mid + 8 * (size_t)b, mb);
+  ld_n<6>(x + 6 * (size_t)a, xa);
+  ld_n<6>(x + 6 * (size_t)b, xb);
+  joint_plain<double>(LAW >= 0 ? LAW : c.A.jl_law[joff + q], c.A.jl_params + 10 * (size_t)(joff + q), ma, mb, xa, xb,
+                      c.P.dt, c.P.warp, out);
+  st_n<6>(c.s.conn + 6 * (size_t)q, out);
 }
 
 // Jacobian slice `slice` of joint q at (mid, x). MIXED evaluates the derivative slices in FP32
@@ -217,10 +220,17 @@ __device__ inline void op_joint_half_slice(const Ctx& c, const double* x, int q,
   const int law = LAW >= 0 ? LAW : c.A.jl_law[joff + q];
   const double* prm = c.A.jl_params + 10 * (size_t)(joff + q);
   J pa[8], pb[8], va[6], vb[6], val[6];
+  {
+    double ma[8], mb[8], xa[6], xb[6];
+    ld_n<8>(c.s.mid + 8 * (size_t)a, ma);
+    ld_n<8>(c.s.mid + 8 * (size_t)b, mb);
+    ld_n<6>(x + 6 * (size_t)a, xa);
+    ld_n<6>(x + 6 * (size_t)b, xb);
 #pragma unroll
-  for (int k = 0; k < 8; ++k) { pa[k] = J(c.s.mid[8 * a + k]); pb[k] = J(c.s.mid[8 * b + k]); }
+    for (int k = 0; k < 8; ++k) { pa[k] = J(ma[k]); pb[k] = J(mb[k]); }
 #pragma unroll
-  for (int k = 0; k < 6; ++k) { va[k] = J(x[6 * a + k]); vb[k] = J(x[6 * b + k]); }
+    for (int k = 0; k < 6; ++k) { va[k] = J(xa[k]); vb[k] = J(xb[k]); }
+  }
   joint_jacobian_part<J, 3, KIND>(law, prm, pa, pb, va, vb, c.P.dt, c.P.warp, slice, half, val, dst);
   if (!MIXED && write_conn && slice == 0 && half == 0) {
 #pragma unroll

@@ -381,7 +381,7 @@ __global__ void k_w_pre(WaveArgs a) {
 // records into the warp's staging block in shared memory, and the warp then stores each joint's
 // two contiguous records (2 x 36 values, 16-byte aligned) with 16-byte stores.
 template <bool MIXED, int LAW, int KIND>
-__global__ void __launch_bounds__(128) k_w_joint_slices(WaveArgs a, int first, int n) {
+__global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveArgs a, int first, int n) {
   typedef typename JacType<MIXED>::T J;
   constexpr int kHalf = 2 * kJacStride;  // values per joint and kind
   __shared__ __align__(16) J stage[4][8][kHalf];

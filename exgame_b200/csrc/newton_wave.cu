@@ -832,9 +832,29 @@ int NewtonWorld::build_wave(cudaStream_t s) {
     for (int i = 0; i < d.m; ++i) dyn.push_back(make_int2(k, i));
     dyn_first.push_back((int)dyn.size());
     for (int q = 0; q < d.nj; ++q) joint.push_back(make_int2(k, q));
-    for (int t = 0; t < 3 * d.m; ++t) {
+    // Cells in groups that read the same Jacobian slices: group p holds the diagonal of p and
+    // (parent row, p col) — both read p's parent joints at p's end — and (child row, p col) of
+    // every child c, which read c's joints at p's end, as the diagonal of p does. A slice's two
+    // readers then run side by side (one pass from DRAM); cells are independent, so the order
+    // changes no result.
+    auto emit = [&](int t) {
       cell.push_back(make_int2(k, t));
       cell_range.push_back(make_int2(h_cell_ptr[d.cell_off + t], h_cell_ptr[d.cell_off + t + 1]));
+    };
+    std::vector<int> ch_first(d.m + 1, 0), ch_list(d.m);
+    for (int i = 0; i < d.m; ++i)
+      if (h_dn_parent[d.dyn_off + i] >= 0) ++ch_first[h_dn_parent[d.dyn_off + i] + 1];
+    for (int i = 0; i < d.m; ++i) ch_first[i + 1] += ch_first[i];
+    {
+      std::vector<int> fill(ch_first.begin(), ch_first.end() - 1);
+      for (int i = 0; i < d.m; ++i)
+        if (h_dn_parent[d.dyn_off + i] >= 0) ch_list[fill[h_dn_parent[d.dyn_off + i]]++] = i;
+    }
+    for (int p = 0; p < d.m; ++p) {
+      emit(3 * p);
+      emit(3 * p + 2);
+      if (h_dn_parent[d.dyn_off + p] < 0) emit(3 * p + 1);  // a root's: no terms
+      for (int u = ch_first[p]; u < ch_first[p + 1]; ++u) emit(3 * ch_list[u] + 1);
     }
     max_levels = std::max(max_levels, d.n_levels);
   }

@@ -730,6 +730,58 @@ __global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, 
   }
 }
 
+// The same elimination with one warp per node, for narrow levels, where one thread's dependent
+// chain (loads, the 6x6 inverse, two products) would bound the level's time. Entry e of a block
+// is lane e (lanes 0..3 also e + 32); the blocks pass through the warp's shared memory to the
+// warp-cooperative operations, which do per entry exactly the single-thread arithmetic, so the two
+// kernels give the same bits.
+constexpr int kSolveWarps = 4;
+constexpr int kNarrowLevel = 2048;  // nodes: levels up to this size take the warp kernel
+__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs a, int first, int count) {
+  __shared__ __align__(16) double sh[kSolveWarps][36 * 3 + 8];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double* Dm = sh[wib];
+  double* Dinv = Dm + 36;
+  double* S = Dm + 72;
+  double* b = Dm + 108;
+  const int e1 = lane + 32;
+  const bool has1 = e1 < 36;
+  for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
+    const int2 it = a.level[first + t];
+    WaveCtl& w = a.ctl[it.x];
+    if (w.state != WS_DIR) continue;
+    const Ctx c = wave_ctx_lite(a, it.x);
+    const size_t i = it.y;
+    double d0 = c.s.D[36 * i + lane], d1 = has1 ? c.s.D[36 * i + e1] : 0.0;
+    double bb = lane < 6 ? c.s.rhs[6 * i + lane] : 0.0;
+    const int* chp = c.A.ch_ptr + c.d.dyn_off;
+    for (int u = chp[i]; u < chp[i + 1]; ++u) {
+      const size_t ch = c.A.ch_idx[u];
+      d0 = d0 - c.s.S[36 * ch + lane];
+      if (has1) d1 = d1 - c.s.S[36 * ch + e1];
+      if (lane < 6) bb = bb - c.s.dv[6 * ch + lane];
+    }
+    Dm[lane] = d0;
+    if (has1) Dm[e1] = d1;
+    if (lane < 6) {
+      b[lane] = bb;
+      c.s.bvec[6 * i + lane] = bb;
+    }
+    __syncwarp();
+    if (!warp_inverse6(Dm, Dinv) && lane == 0) atomicOr(&w.singular, 1);
+    c.s.Dinv[36 * i + lane] = Dinv[lane];
+    if (has1) c.s.Dinv[36 * i + e1] = Dinv[e1];
+    if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
+      warp_mm6<false>(c.s.Apc + 36 * i, Dinv, S);        // S = Apc Dinv
+      warp_mm6<false>(S, c.s.Acp + 36 * i, c.s.S + 36 * i);  // P = S Acp, in S's slot
+      warp_mv6(S, b, c.s.dv + 6 * i);                      // q = S b, in dv's slot
+    } else {
+      warp_mv6(Dinv, b, c.s.dv + 6 * i);
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
   for (int t = gtid(); t < count; t += gthreads()) {
     int2 it = a.level[first + t];
@@ -1015,7 +1067,10 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
   for (int L = nl - 1; L >= 0; --L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+    if (count <= kNarrowLevel)
+      k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
+    else
+      k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
   }
   for (int L = 1; L < nl; ++L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
@@ -1119,7 +1174,11 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
     k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+      if (count <= kNarrowLevel)
+        k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
+                                                                                                         count);
+      else
+        k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
     }
     for (int L = 1; L < nl; ++L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;

@@ -818,6 +818,20 @@ __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
   }
 }
 
+// Back substitution with one warp per node (lanes 0..5 one row each), for narrow levels; the
+// warp operations do the single-thread arithmetic per entry.
+__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_up_warp(WaveArgs a, int first, int count) {
+  for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
+    const int2 it = a.level[first + t];
+    if (a.ctl[it.x].state != WS_DIR) continue;
+    const Ctx c = wave_ctx_lite(a, it.x);
+    const size_t i = it.y;
+    const size_t p = c.A.dn_parent[c.d.dyn_off + i];
+    warp_mv6_sub(c.s.Acp + 36 * i, c.s.dv + 6 * p, c.s.bvec + 6 * i);
+    warp_mv6(c.s.Dinv + 36 * i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+  }
+}
+
 // A singular pivot makes the whole correction NaN (the line search then rejects it); otherwise
 // record whether any component is non-zero.
 __global__ void k_w_nz(WaveArgs a) {
@@ -1075,7 +1089,10 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   }
   for (int L = 1; L < nl; ++L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+    if (count <= kNarrowLevel)
+      k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
+    else
+      k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
   }
   k_w_nz<<<g_dyn, T, 0, s>>>(a);
   k_w_after_solve<<<g_isl, T, 0, s>>>(a);
@@ -1183,7 +1200,11 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
     }
     for (int L = 1; L < nl; ++L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
+      if (count <= kNarrowLevel)
+        k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
+                                                                                                       count);
+      else
+        k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
     }
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);

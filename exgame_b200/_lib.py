@@ -5,6 +5,7 @@ there is no CPU fallback for the compute path.
 """
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -44,6 +45,7 @@ SIGNATURES = {
     "exg_world_get_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_set_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_get_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
+    "exg_batch_set_joints": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
     "exg_world_set_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_stats": (ctypes.c_int, [_vp, _vp]),
     "exg_world_energy": (ctypes.c_int, [_vp, _c_double_p]),
@@ -194,6 +196,7 @@ class Device:
         check(lib().exg_device_create(int(ordinal), ctypes.byref(h)), "exg_device_create")
         self.handle = h
         self.ordinal = ordinal
+        self._owned = weakref.WeakSet()  # worlds, pools and servers made on this device
 
     def kernel_launches(self):
         v = ctypes.c_uint64()
@@ -229,7 +232,11 @@ class Device:
         return ms.value, n.value
 
     def close(self):
+        """Destroy the device; the worlds, pools and servers made on it are closed first (the
+        library refuses to destroy a device under live handles)."""
         if self.handle:
+            for h in list(self._owned):
+                h.close()
             lib().exg_device_destroy(self.handle)
             self.handle = None
 
@@ -252,6 +259,7 @@ class DeviceWorld:
         check(lib().exg_world_create(device.handle, ptr(self.bodies_host), len(self.bodies_host), ptr(self.joints_host),
                                      len(self.joints_host), ptr(self.params), ctypes.byref(h)), "exg_world_create")
         self.handle = h
+        device._owned.add(self)
         self.n = len(self.bodies_host)
 
     def step(self, n_steps=1):
@@ -279,6 +287,11 @@ class DeviceWorld:
             raise ValueError("out must be a contiguous float64 array of shape (n_bodies, 14)")
         check(lib().exg_world_get_state(self.handle, ptr(out), self.n), "exg_world_get_state")
         return out
+
+    def set_joints(self, joints, world=0):
+        """Replace the joints of `world` (0 for a single world; a batch index or pool slot)."""
+        j = np.ascontiguousarray(joints, dtype=JOINT_DTYPE)
+        check(lib().exg_batch_set_joints(self.handle, int(world), ptr(j), len(j)), "exg_batch_set_joints")
 
     def set_state(self, state):
         st = np.ascontiguousarray(state, dtype=np.float64)
@@ -343,6 +356,7 @@ class DeviceBatch(DeviceWorld):
                                      ptr(self.bodies_host), ptr(self.joints_host), ptr(self.params), ctypes.byref(h)),
               "exg_batch_create")
         self.handle = h
+        device._owned.add(self)
         self.n = int(self.counts.sum())
         self.n_worlds = len(worlds)
 
@@ -373,6 +387,7 @@ class DevicePool(DeviceWorld):
         h = ctypes.c_void_p()
         check(lib().exg_pool_create(device.handle, ptr(cfg), ctypes.byref(h)), "exg_pool_create")
         self.handle = h
+        device._owned.add(self)
         self.counts = {}  # slot -> body count
 
     @property
@@ -471,6 +486,7 @@ class Server:
         h = ctypes.c_void_p()
         check(lib().exg_server_create(device.handle, ptr(cfg), ctypes.byref(h)), "exg_server_create")
         self.handle = h
+        device._owned.add(self)
         self.sizes = {}
 
     def submit(self, bodies, joints, params, steps):

@@ -222,7 +222,7 @@ int exg_device_create(int32_t ordinal, exg_device_t* out) {
 }
 
 int exg_device_destroy(exg_device_t dev) {
-  if (!dev) return EXG_ERR_INVALID_ARGUMENT;
+  if (!dev || dev->handles.load() > 0) return EXG_ERR_INVALID_ARGUMENT;  // its worlds go first
   cudaSetDevice(dev->ordinal);
   cudaStreamSynchronize(dev->stream);
   prof_collect(dev);
@@ -457,6 +457,29 @@ static int pool_init(exg_world_s* W, exg_device_s* dev, int b_cap, int j_cap, in
 }
 
 // Admit one validated world into free ranges of the pool.
+// A world's joints into the pool's joint range [jo, jo + nj): batch-global body indices, the
+// incidence of its n bodies (at bo) in joint order, and the range's owner.
+static int upload_joints(exg_world_s* W, int slot, int bo, int n, long long jo, const exg_joint_t* joints, int nj) {
+  DeviceWorld& w = W->w;
+  std::vector<exg_joint_t> gj(joints, joints + nj);
+  for (auto& j : gj) { j.a += bo; j.b += bo; }
+  std::vector<int> cnt(n, 0), start(n, 0), ref(2 * (size_t)nj);
+  for (int k = 0; k < nj; ++k) { cnt[joints[k].a]++; cnt[joints[k].b]++; }
+  int acc = 0;
+  for (int i = 0; i < n; ++i) { start[i] = 2 * (int)jo + acc; acc += cnt[i]; }
+  std::vector<int> fill(start);
+  for (int k = 0; k < nj; ++k) {
+    ref[fill[joints[k].a]++ - 2 * jo] = 2 * ((int)jo + k);
+    ref[fill[joints[k].b]++ - 2 * jo] = 2 * ((int)jo + k) + 1;
+  }
+  int rc = put(W, w.joints, jo, gj.data(), nj);
+  if (rc == EXG_OK) rc = put(W, w.inc_start, bo, start.data(), n);
+  if (rc == EXG_OK) rc = put(W, w.inc_cnt, bo, cnt.data(), n);
+  if (rc == EXG_OK) rc = put(W, w.inc_ref, 2 * jo, ref.data(), 2 * (long long)nj);
+  if (rc == EXG_OK) rc = fill_int(W, w.world_of_joint, jo, nj, slot);
+  return rc;
+}
+
 static int pool_admit(exg_world_s* W, const exg_body_t* bodies, int n, const exg_joint_t* joints, int nj,
                       const exg_step_params_t& p, int* slot_out) {
   if (p.precision != W->w.precision) return EXG_ERR_INVALID_ARGUMENT;
@@ -473,23 +496,7 @@ static int pool_admit(exg_world_s* W, const exg_body_t* bodies, int n, const exg
   }
   DeviceWorld& w = W->w;
   int rc = upload_bodies(W, bodies, (int)bo, n);
-  // joints with batch-global body indices, incidence per body in joint order
-  std::vector<exg_joint_t> gj(joints, joints + nj);
-  for (auto& j : gj) { j.a += (int)bo; j.b += (int)bo; }
-  std::vector<int> cnt(n, 0), start(n, 0), ref(2 * (size_t)nj);
-  for (int k = 0; k < nj; ++k) { cnt[joints[k].a]++; cnt[joints[k].b]++; }
-  int acc = 0;
-  for (int i = 0; i < n; ++i) { start[i] = 2 * (int)jo + acc; acc += cnt[i]; }
-  std::vector<int> fill(start);
-  for (int k = 0; k < nj; ++k) {
-    ref[fill[joints[k].a]++ - 2 * jo] = 2 * ((int)jo + k);
-    ref[fill[joints[k].b]++ - 2 * jo] = 2 * ((int)jo + k) + 1;
-  }
-  if (rc == EXG_OK) rc = put(W, w.joints, jo, gj.data(), nj);
-  if (rc == EXG_OK) rc = put(W, w.inc_start, bo, start.data(), n);
-  if (rc == EXG_OK) rc = put(W, w.inc_cnt, bo, cnt.data(), n);
-  if (rc == EXG_OK) rc = put(W, w.inc_ref, 2 * jo, ref.data(), 2 * (long long)nj);
-  if (rc == EXG_OK) rc = fill_int(W, w.world_of_joint, jo, nj, slot);
+  if (rc == EXG_OK) rc = upload_joints(W, slot, (int)bo, n, jo, joints, nj);
   // gravity work items of this world alone (their j-ranges depend on the world's size only)
   WorldSlot ws;
   std::vector<GravItem> items;
@@ -567,6 +574,45 @@ static int pool_release(exg_world_s* W, int slot) {
   return EXG_OK;
 }
 
+// New joints for the world in `slot` (Islands::connect / detach and Mechanism::split / merge as
+// one edit: the islands are the connected components of the new joint graph, rebuilt on the
+// host). Its bodies stay on the device. All or nothing: a refused structure, or no room in the
+// joint range, leaves the world as it was.
+static int pool_set_joints(exg_world_s* W, int slot, const exg_joint_t* joints, int nj) {
+  WorldSlot& ws = W->slots[slot];
+  for (int k = 0; k < nj; ++k) {
+    if (joints[k].law < 0 || joints[k].law > 3) return EXG_ERR_NO_SHADER;
+    if (joints[k].a < 0 || joints[k].a >= ws.n || joints[k].b < 0 || joints[k].b >= ws.n || joints[k].a == joints[k].b)
+      return EXG_ERR_INVALID_ARGUMENT;
+  }
+  long long jo = W->joint_alloc.alloc(nj);
+  bool reused = false;  // no room beside the old list: its range is given up first
+  if (jo < 0) {
+    W->joint_alloc.release(ws.joint_off, ws.nj);
+    reused = true;
+    jo = W->joint_alloc.alloc(nj);
+    if (jo < 0) {
+      W->joint_alloc.alloc_at(ws.joint_off, ws.nj);  // just released: free
+      return EXG_ERR_OUT_OF_MEMORY;
+    }
+  }
+  int rc = EXG_OK;
+  if (ws.params.integrator == EXG_NEWTON && (rc = W->newton->replace_joints(slot, joints, nj)) != EXG_OK) {
+    W->joint_alloc.release(jo, nj);
+    if (reused) W->joint_alloc.alloc_at(ws.joint_off, ws.nj);
+    return rc;
+  }
+  if ((rc = fill_int(W, W->w.world_of_joint, ws.joint_off, ws.nj, -1)) != EXG_OK) return rc;
+  if ((rc = upload_joints(W, slot, ws.body_off, ws.n, jo, joints, nj)) != EXG_OK) return rc;
+  if (!reused) W->joint_alloc.release(ws.joint_off, ws.nj);
+  ws.joint_off = (int)jo;
+  ws.nj = nj;
+  W->w.h_joint_off[slot] = (int)jo;
+  W->w.h_nj[slot] = nj;
+  W->dirty = true;
+  return EXG_OK;
+}
+
 // Before a step after a structural change: the gravity queue of the live worlds (largest item
 // first), the partial array's size, the island queue; the step graph is re-captured.
 static int pool_prepare(exg_world_s* W) {
@@ -630,6 +676,7 @@ int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* body_cou
   }
   if (rc == EXG_OK) rc = pool_prepare(W);
   if (rc != EXG_OK) { delete W; return rc; }
+  ++dev->handles;
   *out = W;
   return EXG_OK;
 }
@@ -649,6 +696,7 @@ int exg_pool_create(exg_device_t dev, const exg_pool_config_t* cfg, exg_world_t*
   if (!W) return EXG_ERR_OUT_OF_MEMORY;
   int rc = pool_init(W, dev, (int)cfg->max_bodies, (int)cfg->max_joints, cfg->max_worlds, cfg->precision);
   if (rc != EXG_OK) { delete W; return rc; }
+  ++dev->handles;
   *out = W;
   return EXG_OK;
 }
@@ -770,10 +818,12 @@ int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
 
 int exg_world_destroy(exg_world_t W) {
   if (!W) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
-  cudaSetDevice(W->dev->ordinal);
-  cudaStreamSynchronize(W->dev->stream);
+  exg_device_s* dev = W->dev;
+  std::lock_guard<std::mutex> lock(dev->mu);
+  cudaSetDevice(dev->ordinal);
+  cudaStreamSynchronize(dev->stream);
   delete W;
+  --dev->handles;
   return EXG_OK;
 }
 
@@ -922,6 +972,14 @@ int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n
   std::lock_guard<std::mutex> lock(W->dev->mu);
   cudaSetDevice(W->dev->ordinal);
   return download_bodies(W, out, W->slots[world].body_off, n);
+}
+
+int exg_batch_set_joints(exg_world_t W, int32_t world, const exg_joint_t* joints, int32_t nj) {
+  if (!W || world < 0 || world >= W->w_cap || !W->slots[world].used || nj < 0 || (nj > 0 && !joints))
+    return EXG_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(W->dev->mu);
+  cudaSetDevice(W->dev->ordinal);
+  return pool_set_joints(W, world, joints, nj);
 }
 
 int exg_batch_set_world(exg_world_t W, int32_t world, const exg_body_t* bodies, int32_t n) {

@@ -30,6 +30,7 @@ struct exg_device_s {
   cudaStream_t stream = nullptr;
   std::atomic<uint64_t> launches{0};
   std::mutex mu;  // one submitter at a time (the reference's single worker thread)
+  std::atomic<int> handles{0};  // live world handles made on the device (batches, pools, servers' pools)
   // profiler: event pairs recorded on `stream` around each launch of a kind
   bool profiling = false;
   struct Rec { int kind; cudaEvent_t a, b; };

@@ -654,19 +654,32 @@ std::vector<char> NewtonWorld::kin_of(int slot) const {
   return src_[slot].kin;
 }
 
-int NewtonWorld::rebuild_world(int slot, const std::vector<char>& kin) {
-  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live || src_[slot].kin.size() != kin.size())
-    return EXG_ERR_INVALID_ARGUMENT;
-  WorldSrc old = src_[slot], next = src_[slot];
-  next.kin = kin;
+int NewtonWorld::rebuild_from(int slot, WorldSrc next) {
+  WorldSrc old = src_[slot];
   remove_world(slot);
   int rc = build_world(slot, next);
   if (rc != EXG_OK) {
     if (build_world(slot, old) == EXG_OK) src_[slot] = old;  // accepted before
     return rc;
   }
+  next.live = true;
   src_[slot] = std::move(next);
   return EXG_OK;
+}
+
+int NewtonWorld::rebuild_world(int slot, const std::vector<char>& kin) {
+  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live || src_[slot].kin.size() != kin.size())
+    return EXG_ERR_INVALID_ARGUMENT;
+  WorldSrc next = src_[slot];
+  next.kin = kin;
+  return rebuild_from(slot, std::move(next));
+}
+
+int NewtonWorld::replace_joints(int slot, const exg_joint_t* joints, int nj) {
+  if (slot < 0 || slot >= (int)src_.size() || !src_[slot].live || nj < 0) return EXG_ERR_INVALID_ARGUMENT;
+  WorldSrc next = src_[slot];
+  next.joints.assign(joints, joints + nj);
+  return rebuild_from(slot, std::move(next));
 }
 
 int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {

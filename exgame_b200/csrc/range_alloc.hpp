@@ -35,6 +35,20 @@ class RangeAllocator {
     }
     return -1;
   }
+  // take [off, off + len) if it lies inside one free range (false otherwise); a caller that just
+  // released a range gets the same one back this way
+  bool alloc_at(long long off, long long len) {
+    if (len <= 0) return true;
+    auto it = free_.upper_bound(off);
+    if (it == free_.begin()) return false;
+    --it;
+    const long long start = it->first, end = it->first + it->second;
+    if (off < start || off + len > end) return false;
+    free_.erase(it);
+    if (off > start) free_[start] = off - start;
+    if (end > off + len) free_[off + len] = end - (off + len);
+    return true;
+  }
   void release(long long off, long long len) {
     if (len <= 0) return;
     auto next = free_.lower_bound(off);

@@ -67,6 +67,9 @@ class NewtonWorld {
   // Rebuild the world's islands for new kinematic flags (same joints); on a structure error the
   // world keeps its previous islands.
   int rebuild_world(int slot, const std::vector<char>& kin);
+  // Rebuild the world's islands for a new joint list (world-local body indices; same bodies);
+  // on a structure error the world keeps its previous islands.
+  int replace_joints(int slot, const exg_joint_t* joints, int nj);
   // Upload pending structure and the island queue (host synchronous; call outside stream capture).
   int sync(exg_device_s* dev, cudaStream_t s);
   bool dirty() const { return dirty_; }
@@ -106,6 +109,7 @@ class NewtonWorld {
     std::vector<exg_joint_t> joints;
   };
   int build_world(int slot, const WorldSrc& src);
+  int rebuild_from(int slot, WorldSrc next);  // all or nothing
   void compact();
   bool wave_island(const IslandDesc& d) const;
   int build_wave(cudaStream_t s);

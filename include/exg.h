@@ -151,6 +151,8 @@ typedef struct exg_world_s* exg_world_t;
 
 /* ── device (replaces rembrandt::GpuAccelerator::new, crates/rembrandt/src/lib.rs:98-158) ── */
 EXG_API int exg_device_create(int32_t ordinal, exg_device_t* out);
+/* Refused (EXG_ERR_INVALID_ARGUMENT) while world handles made on the device are alive: destroy
+ * them (and servers) first. */
 EXG_API int exg_device_destroy(exg_device_t dev);
 EXG_API int exg_device_synchronize(exg_device_t dev);
 /* Number of kernels this library launched on the device so far. */
@@ -211,6 +213,16 @@ EXG_API int exg_batch_create(exg_device_t dev, int32_t n_worlds, const int32_t* 
 EXG_API int exg_batch_get_world(exg_world_t w, int32_t world, exg_body_t* out, int32_t n_bodies);
 EXG_API int exg_batch_set_world(exg_world_t w, int32_t world, const exg_body_t* bodies, int32_t n_bodies);
 EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_t* out);
+/* New joints for one world of a batch or pool (world 0 of a single world): joint records with
+ * world-local body indices, replacing the world's joint list. Adding a joint between two islands
+ * merges them, removing one may split an island (Islands::connect / detach,
+ * crates/newton/src/mechanism/islands.rs:166-299; Mechanism::split / merge,
+ * crates/newton/src/mechanism/mechanism.rs:326-434); the islands and the solver's structure are
+ * rebuilt before the next step (cache.rs:689-788). The bodies keep their state on the device.
+ * All or nothing: EXG_ERR_UNSUPPORTED (a dynamic cycle), EXG_ERR_OUT_OF_MEMORY (no room in the
+ * handle's joint capacity: a world or batch handle holds the joint count it was created with, a
+ * pool max_joints) or a bad record leaves the world as it was. */
+EXG_API int exg_batch_set_joints(exg_world_t w, int32_t world, const exg_joint_t* joints, int32_t n_joints);
 /* ── pool: worlds admitted into and released from fixed-capacity device arrays ──
  * The serving form of a batch: state stays resident while worlds come and go. A released slot's
  * ranges are reused by later admissions; exg_world_step advances every admitted world. The

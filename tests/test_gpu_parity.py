@@ -301,6 +301,74 @@ def test_set_bodies_kinematic_change_rebuilds_islands(device, oracle):
     batch.close()
 
 
+def _edge_mask(joints, a, b):
+    return ((joints["a"] == a) & (joints["b"] == b)) | ((joints["a"] == b) & (joints["b"] == a))
+
+
+@pytest.mark.parametrize("scheme", [NEWTON, LIE_EULER])
+def test_set_joints_detach_and_connect_match_oracle(device, oracle, scheme):
+    """Joints replaced between steps (exg_batch_set_joints): detaching a tree edge splits an
+    island, connecting it again merges the two; each following span matches an oracle world made
+    from the current records and the new joints, on both Newton schedules and explicitly."""
+    bodies, joints = scenarios.tree_world(40, seed=86)
+    params = step_params(integrator=scheme, gravity_law=GRAVITY_OFF, dt=1e-2 if scheme == NEWTON else 1e-3,
+                         tol=1e-10)
+    c = 17  # its parent is its one neighbour of lower index (the generator's parents precede)
+    touch = (joints["a"] == c) | (joints["b"] == c)
+    ends = np.where(joints["a"][touch] == c, joints["b"][touch], joints["a"][touch])
+    cut = joints[~_edge_mask(joints, c, int(ends[ends < c][0]))]
+    assert len(cut) == len(joints) - 3
+    steps = 4 if scheme == NEWTON else 40
+    for min_bodies in ((1 << 20, 1) if scheme == NEWTON else (1 << 20,)):
+        dw = _lib.DeviceWorld(device, bodies, joints, params)
+        dw.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, min_bodies)
+        dw.step(steps)
+        for new in (cut, joints):
+            dw.set_joints(new)
+            ow = oracle.OracleWorld(dw.bodies(), new, params)
+            dw.step(steps)
+            ow.step(steps)
+            pe, me = state_error(ow.bodies(), dw.bodies())
+            assert pe < 1e-9 and me < 1e-7, (min_bodies, len(new), pe, me)
+        dw.close()
+
+
+def test_set_joints_refuses_a_cycle_and_changes_nothing(device, oracle):
+    """A joint list that closes a cycle of dynamic bodies is refused (EXG_ERR_UNSUPPORTED) and the
+    world steps on exactly as an untouched twin; in a batch, replacing one world's joints leaves
+    the other world bit for bit as when stepped alone."""
+    bodies, joints = scenarios.tree_world(24, seed=87)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
+    loop = joints.copy()  # same count (a world handle's joint capacity is its count at creation)
+    loop[-1]["a"], loop[-1]["b"] = 5, 9  # the dropped law leaves its edge joined by the other two
+    a = _lib.DeviceWorld(device, bodies, joints, params)
+    b = _lib.DeviceWorld(device, bodies, joints, params)
+    a.step(2)
+    b.step(2)
+    with pytest.raises(_lib.ExgError) as e:
+        a.set_joints(loop)
+    assert e.value.status == -22  # EXG_ERR_UNSUPPORTED
+    a.step(3)
+    b.step(3)
+    assert np.array_equal(a.bodies()["pose"], b.bodies()["pose"])
+    a.close()
+    b.close()
+    other, oj = scenarios.chain_world(8, seed=88)
+    batch = _lib.DeviceBatch(device, [(other, oj, params), (bodies, joints, params)])
+    alone = _lib.DeviceWorld(device, other, oj, params)
+    batch.step(2)
+    ow = oracle.OracleWorld(batch.world_bodies(1), joints[3:], params)
+    batch.set_joints(joints[3:], world=1)
+    batch.step(3)
+    alone.step(5)
+    ow.step(3)
+    assert np.array_equal(batch.world_bodies(0)["pose"], alone.bodies()["pose"])
+    pe, me = state_error(ow.bodies(), batch.world_bodies(1))
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+    batch.close()
+    alone.close()
+
+
 def test_set_bodies_refuses_massless_dynamic_record(device):
     """A dynamic record without positive mass refuses exg_world_set_bodies as a whole: nothing of
     the call is written, and the world steps on from its previous state."""

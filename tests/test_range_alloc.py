@@ -25,6 +25,8 @@ def ra():
         getattr(L, fn).restype = ctypes.c_longlong
         getattr(L, fn).argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     L.ra_release.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong]
+    L.ra_alloc_at.restype = ctypes.c_int
+    L.ra_alloc_at.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong]
     L.ra_grow.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
     for fn in ("ra_capacity", "ra_largest_free", "ra_used_end"):
         getattr(L, fn).restype = ctypes.c_longlong
@@ -75,4 +77,21 @@ def test_random_admissions_and_releases_match_the_model(ra, seed):
             run = 0 if u else run + 1
             runs.append(run)
         assert ra.ra_largest_free(a) == (max(runs) if runs else 0)
+    ra.ra_free(a)
+
+
+def test_alloc_at_takes_a_given_free_range_back(ra):
+    """alloc_at claims [off, off + len) only when it lies inside one free range, splitting that
+    range; a range just released comes back at its own offset even when first fit would not."""
+    a = ra.ra_new(100)
+    assert ra.ra_alloc(a, 10) == 0
+    assert ra.ra_alloc(a, 30) == 10
+    ra.ra_release(a, 0, 10)        # free: [0, 10) and [40, 100)
+    ra.ra_release(a, 10, 30)       # coalesced: [0, 100)
+    assert ra.ra_alloc_at(a, 10, 30) == 1
+    assert ra.ra_alloc_at(a, 35, 10) == 0   # overlaps the taken range
+    assert ra.ra_alloc(a, 10) == 0          # the left remainder [0, 10)
+    assert ra.ra_alloc(a, 60) == 40         # the right remainder [40, 100)
+    assert ra.ra_largest_free(a) == 0
+    assert ra.ra_alloc_at(a, 99, 2) == 0    # past the capacity
     ra.ra_free(a)

@@ -46,6 +46,7 @@ SIGNATURES = {
     "exg_world_set_bodies": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_get_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_batch_set_joints": (ctypes.c_int, [_vp, ctypes.c_int32, _vp, ctypes.c_int32]),
+    "exg_world_stream": (ctypes.c_int, [_vp, _vp]),
     "exg_world_set_state": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_stats": (ctypes.c_int, [_vp, _vp]),
     "exg_world_energy": (ctypes.c_int, [_vp, _c_double_p]),
@@ -304,7 +305,13 @@ class DeviceWorld:
         check(lib().exg_world_stats(self.handle, ptr(s)), "exg_world_stats")
         return s
 
-    OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS, OPT_WAVE_HOST_ROUNDS = 1, 2, 3, 4
+    OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS, OPT_WAVE_HOST_ROUNDS, OPT_OWN_STREAM = 1, 2, 3, 4, 5
+
+    def stream(self):
+        """The CUDA stream (as an integer handle) this world's work runs on."""
+        s = ctypes.c_void_p()
+        check(lib().exg_world_stream(self.handle, ctypes.byref(s)), "exg_world_stream")
+        return s.value
 
     def set_option(self, option, value):
         check(lib().exg_world_set_option(self.handle, int(option), int(value)), "exg_world_set_option")

@@ -37,6 +37,8 @@ struct WorldSlot {
 // the island queue are rebuilt and the step graph re-captured before the next step.
 struct exg_world_s {
   exg_device_s* dev = nullptr;
+  std::mutex mu;               // one caller at a time on this handle
+  cudaStream_t own = nullptr;  // the handle's own stream (EXG_OPT_OWN_STREAM), else the device's
   DeviceWorld w;
   NewtonWorld* newton = nullptr;
   exg_world_stats_t stats{};
@@ -79,6 +81,19 @@ struct exg_world_s {
   }
 };
 
+// The stream a handle's work runs on.
+static inline cudaStream_t wstream(const exg_world_s* W) { return W->own ? W->own : W->dev->stream; }
+
+// Calls on one handle exclude each other. A handle on the device's stream also excludes every
+// other call that uses that stream (a graph captured there must see no foreign work), so only
+// handles with their own stream run side by side. Lock order: the handle, then the device.
+struct HandleLock {
+  std::unique_lock<std::mutex> handle, device;
+  explicit HandleLock(exg_world_s* W) : handle(W->mu) {
+    if (!W->own) device = std::unique_lock<std::mutex>(W->dev->mu);
+  }
+};
+
 static cudaEvent_t take_event(exg_device_s* dev) {
   if (!dev->free_events.empty()) {
     cudaEvent_t e = dev->free_events.back();
@@ -92,6 +107,7 @@ static cudaEvent_t take_event(exg_device_s* dev) {
 
 int prof_begin(exg_device_s* dev, int kind, cudaStream_t s) {
   if (!dev->profiling) return -1;
+  std::lock_guard<std::mutex> lock(dev->prof_mu);
   exg_device_s::Rec r{kind, take_event(dev), take_event(dev)};
   cudaEventRecord(r.a, s);
   dev->recs.push_back(r);
@@ -100,11 +116,13 @@ int prof_begin(exg_device_s* dev, int kind, cudaStream_t s) {
 
 void prof_end(exg_device_s* dev, int token, cudaStream_t s) {
   if (token < 0) return;
+  std::lock_guard<std::mutex> lock(dev->prof_mu);
   cudaEventRecord(dev->recs[token].b, s);
 }
 
-// fold recorded pairs into the per-kind totals (the stream must be idle)
+// fold recorded pairs into the per-kind totals (the device must be idle)
 static void prof_collect(exg_device_s* dev) {
+  std::lock_guard<std::mutex> lock(dev->prof_mu);
   for (auto& r : dev->recs) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
@@ -129,7 +147,7 @@ int exg_device_profile(exg_device_t dev, int32_t enable) {
   if (!dev) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(dev->mu);
   cudaSetDevice(dev->ordinal);
-  EXG_CUDA_TRY(cudaStreamSynchronize(dev->stream));
+  EXG_CUDA_TRY(cudaDeviceSynchronize());  // world handles may run on their own streams
   prof_collect(dev);
   for (int k = 0; k < PROF_KINDS; ++k) { dev->prof_ms[k] = 0.0; dev->prof_count[k] = 0; }
   dev->profiling = enable != 0;
@@ -140,7 +158,7 @@ int exg_device_profile_read(exg_device_t dev, int32_t kind, double* total_ms, in
   if (!dev || kind < 0 || kind >= PROF_KINDS || !total_ms || !launches) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(dev->mu);
   cudaSetDevice(dev->ordinal);
-  EXG_CUDA_TRY(cudaStreamSynchronize(dev->stream));
+  EXG_CUDA_TRY(cudaDeviceSynchronize());
   prof_collect(dev);
   *total_ms = dev->prof_ms[kind];
   *launches = dev->prof_count[kind];
@@ -234,7 +252,8 @@ int exg_device_destroy(exg_device_t dev) {
 
 int exg_device_synchronize(exg_device_t dev) {
   if (!dev) return EXG_ERR_INVALID_ARGUMENT;
-  EXG_CUDA_TRY(cudaStreamSynchronize(dev->stream));
+  EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));
+  EXG_CUDA_TRY(cudaDeviceSynchronize());  // every handle's stream
   return EXG_OK;
 }
 
@@ -283,12 +302,12 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
 static int stage_reserve(exg_world_s* W, long long count) {
   if (W->stage_d.cap >= count) return EXG_OK;
   W->stage_d.release();  // staging contents never outlive a call
-  return W->stage_d.reserve(count, W->dev->stream);
+  return W->stage_d.reserve(count, wstream(W));
 }
 
 static int upload_records(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count, const int* dst) {
   if (count <= 0) return EXG_OK;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   int rc = stage_reserve(W, count);
   if (rc != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaMemcpyAsync(W->stage_d.ptr, bodies, sizeof(exg_body_t) * (size_t)count, cudaMemcpyHostToDevice, s));
@@ -299,7 +318,7 @@ static int upload_records(exg_world_s* W, const exg_body_t* bodies, int32_t firs
 
 static int download_records(exg_world_s* W, exg_body_t* out, int32_t first, int32_t count, const int* dst) {
   if (count <= 0) return EXG_OK;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   int rc = stage_reserve(W, count);
   if (rc != EXG_OK) return rc;
   if ((rc = launch_bodies_gather(W->dev, W->w, W->stage_d.ptr, count, first, dst, s)) != EXG_OK) return rc;
@@ -316,7 +335,7 @@ static int download_records(exg_world_s* W, exg_body_t* out, int32_t first, int3
 static int set_records(exg_world_s* W, const exg_body_t* bodies, int32_t first, int32_t count, const int* dst,
                        int slot) {
   if (count <= 0) return EXG_OK;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   int rc = stage_reserve(W, count);
   if (rc != EXG_OK) return rc;
   if (W->flags_d.cap < 2 && (rc = W->flags_d.reserve(2, s)) != EXG_OK) return rc;
@@ -372,7 +391,7 @@ static int ensure_record_map(exg_world_s* W, long long* total) {
   for (auto& ws : W->slots)
     if (ws.used)
       for (int i = 0; i < ws.n; ++i) map.push_back(ws.body_off + i);
-  int rc = W->map_d.assign(map.data(), (long long)map.size(), W->dev->stream);
+  int rc = W->map_d.assign(map.data(), (long long)map.size(), wstream(W));
   if (rc != EXG_OK) return rc;
   W->map_dirty = false;
   return EXG_OK;
@@ -381,15 +400,15 @@ static int ensure_record_map(exg_world_s* W, long long* total) {
 static int fill_int(exg_world_s* W, int* d, long long first, long long count, int value) {
   if (count <= 0) return EXG_OK;
   std::vector<int> v(count, value);
-  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, v.data(), sizeof(int) * count, cudaMemcpyHostToDevice, W->dev->stream));
-  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, v.data(), sizeof(int) * count, cudaMemcpyHostToDevice, wstream(W)));
+  EXG_CUDA_TRY(cudaStreamSynchronize(wstream(W)));
   return EXG_OK;
 }
 
 template <class T> static int put(exg_world_s* W, T* d, long long first, const T* src, long long count) {
   if (count <= 0) return EXG_OK;
-  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, src, sizeof(T) * count, cudaMemcpyHostToDevice, W->dev->stream));
-  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  EXG_CUDA_TRY(cudaMemcpyAsync(d + first, src, sizeof(T) * count, cudaMemcpyHostToDevice, wstream(W)));
+  EXG_CUDA_TRY(cudaStreamSynchronize(wstream(W)));
   return EXG_OK;
 }
 
@@ -619,7 +638,7 @@ static int pool_prepare(exg_world_s* W) {
   if (!W->dirty) return EXG_OK;
   W->drop_graph();
   DeviceWorld& w = W->w;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   std::vector<std::pair<double, GravItem>> tmp;
   for (auto& ws : W->slots)
     if (ws.used)
@@ -706,7 +725,7 @@ int exg_pool_admit(exg_world_t W, const exg_body_t* bodies, int32_t n, const exg
   if (!W || !slot_out) return EXG_ERR_INVALID_ARGUMENT;
   int st = validate_world(bodies, n, joints, nj, params);
   if (st != EXG_OK) return st;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   int slot = -1;
   int rc = pool_admit(W, bodies, n, joints, nj, *params, &slot);
@@ -716,14 +735,14 @@ int exg_pool_admit(exg_world_t W, const exg_body_t* bodies, int32_t n, const exg
 
 int exg_pool_release(exg_world_t W, int32_t slot) {
   if (!W) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return pool_release(W, slot);
 }
 
 int exg_pool_free(exg_world_t W, exg_pool_usage_t* out) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   out->worlds_used = W->n_used;
   out->worlds_capacity = W->w_cap;
   out->largest_free_bodies = W->body_alloc.largest_free();
@@ -764,18 +783,18 @@ int exg_world_footprint(int32_t n, int32_t nj, const exg_step_params_t* p, int64
 
 int exg_pool_set_steps(exg_world_t W, int32_t slot, int32_t steps) {
   if (!W || slot < 0 || slot >= W->w_cap || !W->slots[slot].used || steps < -1) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return put(W, W->w.w_left, slot, &steps, 1);
 }
 
 int exg_pool_steps_left(exg_world_t W, int32_t* out, int32_t n_slots) {
   if (!W || !out || n_slots < 0 || n_slots > W->w_cap) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   if (n_slots == 0) return EXG_OK;
-  EXG_CUDA_TRY(cudaMemcpyAsync(out, W->w.w_left, sizeof(int32_t) * n_slots, cudaMemcpyDeviceToHost, W->dev->stream));
-  EXG_CUDA_TRY(cudaStreamSynchronize(W->dev->stream));
+  EXG_CUDA_TRY(cudaMemcpyAsync(out, W->w.w_left, sizeof(int32_t) * n_slots, cudaMemcpyDeviceToHost, wstream(W)));
+  EXG_CUDA_TRY(cudaStreamSynchronize(wstream(W)));
   for (int32_t k = 0; k < n_slots; ++k)
     if (!W->slots[k].used) out[k] = 0;
   return EXG_OK;
@@ -783,7 +802,7 @@ int exg_pool_steps_left(exg_world_t W, int32_t* out, int32_t n_slots) {
 
 int exg_world_set_option(exg_world_t W, int32_t option, int64_t value) {
   if (!W) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   switch (option) {
     case EXG_OPT_WAVE_MIN_BODIES:
       if (value < 1 || value > (1LL << 30)) return EXG_ERR_INVALID_ARGUMENT;
@@ -797,6 +816,17 @@ int exg_world_set_option(exg_world_t W, int32_t option, int64_t value) {
       if (value != 0 && value != 1) return EXG_ERR_INVALID_ARGUMENT;
       W->newton->set_wave_host_loop(value != 0);
       return EXG_OK;
+    case EXG_OPT_OWN_STREAM:
+      if (value != 0 && value != 1) return EXG_ERR_INVALID_ARGUMENT;
+      EXG_CUDA_TRY(cudaSetDevice(W->dev->ordinal));
+      EXG_CUDA_TRY(cudaStreamSynchronize(wstream(W)));  // work in flight ends where it began
+      if (value && !W->own) {
+        EXG_CUDA_TRY(cudaStreamCreateWithFlags(&W->own, cudaStreamNonBlocking));
+      } else if (!value && W->own) {
+        cudaStreamDestroy(W->own);
+        W->own = nullptr;
+      }
+      return EXG_OK;
     default:
       return EXG_ERR_INVALID_ARGUMENT;
   }
@@ -804,14 +834,22 @@ int exg_world_set_option(exg_world_t W, int32_t option, int64_t value) {
   return EXG_OK;
 }
 
+int exg_world_stream(exg_world_t W, void** out) {
+  if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
+  HandleLock lock(W);
+  *out = (void*)wstream(W);
+  return EXG_OK;
+}
+
 int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
   if (!W || !value) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   switch (option) {
     case EXG_OPT_WAVE_MIN_BODIES: *value = W->newton->wave_min_dyn(); return EXG_OK;
     case EXG_OPT_WAVE_MAX_LEVELS: *value = W->newton->wave_max_levels(); return EXG_OK;
     case EXG_OPT_LAST_WAVE_ROUNDS: *value = W->newton->last_wave_rounds(); return EXG_OK;
     case EXG_OPT_WAVE_HOST_ROUNDS: *value = W->newton->wave_host_loop() ? 1 : 0; return EXG_OK;
+    case EXG_OPT_OWN_STREAM: *value = W->own ? 1 : 0; return EXG_OK;
     default: return EXG_ERR_INVALID_ARGUMENT;
   }
 }
@@ -819,9 +857,12 @@ int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
 int exg_world_destroy(exg_world_t W) {
   if (!W) return EXG_ERR_INVALID_ARGUMENT;
   exg_device_s* dev = W->dev;
-  std::lock_guard<std::mutex> lock(dev->mu);
-  cudaSetDevice(dev->ordinal);
-  cudaStreamSynchronize(dev->stream);
+  {
+    HandleLock lock(W);  // waits for a call in flight on the handle
+    cudaSetDevice(dev->ordinal);
+    cudaStreamSynchronize(wstream(W));
+  }
+  if (W->own) cudaStreamDestroy(W->own);
   delete W;
   --dev->handles;
   return EXG_OK;
@@ -833,7 +874,7 @@ int exg_world_destroy(exg_world_t W) {
 // charges and world twists, gravity, explicit joints and integration, then the implicit islands.
 static int enqueue_step(exg_world_s* W, int* kernels) {
   DeviceWorld& w = W->w;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   uint64_t before = W->dev->launches.load();
   int rc;
   if ((rc = launch_body_pre(W->dev, w, s)) != EXG_OK) return rc;
@@ -848,7 +889,7 @@ static int enqueue_step(exg_world_s* W, int* kernels) {
 }
 
 static int step_locked(exg_world_s* W, int32_t n_steps) {
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   int rc = pool_prepare(W);
   if (rc != EXG_OK) return rc;
   if (W->n_used == 0 || n_steps == 0) return EXG_OK;
@@ -902,7 +943,7 @@ extern "C" {
 
 int exg_world_step(exg_world_t W, int32_t n_steps) {
   if (!W || n_steps < 0) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return step_locked(W, n_steps);
 }
@@ -910,7 +951,7 @@ int exg_world_step(exg_world_t W, int32_t n_steps) {
 // whole-handle accessors: the used worlds in slot order, each at its body offset
 int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
   int rc = ensure_record_map(W, &total);
@@ -921,7 +962,7 @@ int exg_world_get_bodies(exg_world_t W, exg_body_t* out, int32_t n) {
 
 int exg_world_get_state(exg_world_t W, double* out, int32_t n) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
   int rc = ensure_record_map(W, &total);
@@ -929,7 +970,7 @@ int exg_world_get_state(exg_world_t W, double* out, int32_t n) {
   if (n != total) return EXG_ERR_INVALID_ARGUMENT;
   if (n == 0) return EXG_OK;
   if ((rc = stage_reserve(W, n)) != EXG_OK) return rc;  // 14 doubles fit in a record's slot
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   double* st = reinterpret_cast<double*>(W->stage_d.ptr);
   if ((rc = launch_state_gather(W->dev, W->w, st, n, 0, W->map_d.ptr, s)) != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaMemcpyAsync(out, st, sizeof(double) * 14 * (size_t)n, cudaMemcpyDeviceToHost, s));
@@ -939,7 +980,7 @@ int exg_world_get_state(exg_world_t W, double* out, int32_t n) {
 
 int exg_world_set_state(exg_world_t W, const double* state, int32_t n) {
   if (!W || !state) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
   int rc = ensure_record_map(W, &total);
@@ -947,7 +988,7 @@ int exg_world_set_state(exg_world_t W, const double* state, int32_t n) {
   if (n != total) return EXG_ERR_INVALID_ARGUMENT;
   if (n == 0) return EXG_OK;
   if ((rc = stage_reserve(W, n)) != EXG_OK) return rc;
-  cudaStream_t s = W->dev->stream;
+  cudaStream_t s = wstream(W);
   double* st = reinterpret_cast<double*>(W->stage_d.ptr);
   EXG_CUDA_TRY(cudaMemcpyAsync(st, state, sizeof(double) * 14 * (size_t)n, cudaMemcpyHostToDevice, s));
   if ((rc = launch_state_scatter(W->dev, W->w, st, n, 0, W->map_d.ptr, s)) != EXG_OK) return rc;
@@ -957,7 +998,7 @@ int exg_world_set_state(exg_world_t W, const double* state, int32_t n) {
 
 int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
   if (!W || !bodies) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   long long total = 0;
   int rc = ensure_record_map(W, &total);
@@ -969,7 +1010,7 @@ int exg_world_set_bodies(exg_world_t W, const exg_body_t* bodies, int32_t n) {
 int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n) {
   if (!W || !out || world < 0 || world >= W->w_cap || !W->slots[world].used || n != W->slots[world].n)
     return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return download_bodies(W, out, W->slots[world].body_off, n);
 }
@@ -977,7 +1018,7 @@ int exg_batch_get_world(exg_world_t W, int32_t world, exg_body_t* out, int32_t n
 int exg_batch_set_joints(exg_world_t W, int32_t world, const exg_joint_t* joints, int32_t nj) {
   if (!W || world < 0 || world >= W->w_cap || !W->slots[world].used || nj < 0 || (nj > 0 && !joints))
     return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return pool_set_joints(W, world, joints, nj);
 }
@@ -985,7 +1026,7 @@ int exg_batch_set_joints(exg_world_t W, int32_t world, const exg_joint_t* joints
 int exg_batch_set_world(exg_world_t W, int32_t world, const exg_body_t* bodies, int32_t n) {
   if (!W || !bodies || world < 0 || world >= W->w_cap || !W->slots[world].used || n != W->slots[world].n)
     return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   return set_records(W, bodies, W->slots[world].body_off, n, nullptr, world);
 }
@@ -998,7 +1039,7 @@ int exg_world_stats(exg_world_t W, exg_world_stats_t* out) {
 
 int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) {
   if (!W || !out || world < 0 || world >= W->w_cap || !W->slots[world].used) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   *out = W->stats;
   out->last_spans = 1;
@@ -1012,7 +1053,7 @@ int exg_batch_world_stats(exg_world_t W, int32_t world, exg_world_stats_t* out) 
 
 int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lock(W->dev->mu);
+  HandleLock lock(W);
   cudaSetDevice(W->dev->ordinal);
   long long tmp[8];
   int rc = W->newton->read_phase_cycles(tmp);
@@ -1031,7 +1072,7 @@ int exg_world_energy(exg_world_t W, double* out) {
     if (rc != EXG_OK) return rc;
     std::vector<exg_joint_t> j(ws.nj);
     if (ws.nj > 0) {
-      std::lock_guard<std::mutex> lock(W->dev->mu);
+      HandleLock lock(W);
       EXG_CUDA_TRY(cudaMemcpy(j.data(), W->w.joints + ws.joint_off, sizeof(exg_joint_t) * ws.nj, cudaMemcpyDeviceToHost));
     }
     for (auto& jj : j) { jj.a -= ws.body_off; jj.b -= ws.body_off; }

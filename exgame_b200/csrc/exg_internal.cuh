@@ -32,16 +32,17 @@ struct exg_device_s {
   std::mutex mu;  // one submitter at a time (the reference's single worker thread)
   std::atomic<int> handles{0};  // live world handles made on the device (batches, pools, servers' pools)
   // profiler: event pairs recorded on `stream` around each launch of a kind
-  bool profiling = false;
+  std::atomic<bool> profiling{false};
+  std::mutex prof_mu;  // the event records below (handles on their own streams record concurrently)
   struct Rec { int kind; cudaEvent_t a, b; };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> free_events;
   double prof_ms[PROF_KINDS] = {0};
   long long prof_count[PROF_KINDS] = {0};
   // launch-shape tuning (exg_device_set_tuning; results do not depend on any of these)
-  int tune_gravity_ctas_per_sm = 32;  // persistent one-warp CTAs of the mixed gravity kernel
-  int tune_wave_blocks_per_sm = 8;    // grid cap of the wave's 256-thread data kernels (128-thread: twice)
-  int tune_wave_min_bodies = 32;      // default wave threshold of new world handles
+  std::atomic<int> tune_gravity_ctas_per_sm{32};  // persistent one-warp CTAs of the mixed gravity kernel
+  std::atomic<int> tune_wave_blocks_per_sm{8};    // grid cap of the wave's 256-thread data kernels (128-thread: twice)
+  std::atomic<int> tune_wave_min_bodies{32};      // default wave threshold of new world handles
 };
 
 // Brackets one launch with events when profiling is on (no-op otherwise).

@@ -416,10 +416,10 @@ int launch_gravity_items(exg_device_s* dev, const double* pos_mass, const double
   const double4* pm = reinterpret_cast<const double4*>(pos_mass);
   int tok = prof_begin(dev, PROF_GRAVITY, s);
   if (precision == EXG_PRECISION_MIXED)
-    k_gravity_items_mixed<true><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm)), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
+    k_gravity_items_mixed<true><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm.load())), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
                                                                              world_of_body, w_active);
   else if (precision == EXG_PRECISION_MIXED_FAST)
-    k_gravity_items_mixed<false><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm)), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
+    k_gravity_items_mixed<false><<<std::min(n_items, sms * std::max(1, dev->tune_gravity_ctas_per_sm.load())), kMixThreads, 0, s>>>(pm, size, items, n_items, head, partial,
                                                                              world_of_body, w_active);
   else
     k_gravity_items<double><<<std::min(n_items, sms * 16), kGravThreads, 0, s>>>(pm, size, items, n_items, head,

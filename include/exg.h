@@ -319,8 +319,16 @@ EXG_API int exg_server_destroy(exg_server_t server);
  * between them) instead of running inside one conditional graph; identical results. For profilers
  * that do not follow kernels into conditional graph nodes. */
 #define EXG_OPT_WAVE_HOST_ROUNDS 4
+/* 1: the handle runs on a stream of its own, and calls on it no longer wait for calls on other
+ * handles, so host threads holding different handles overlap their copies and steps on the GPU
+ * (the accelerator's worker serialises all flushes, crates/newton/src/accelerator/mod.rs:1044;
+ * here only a handle is single-writer). 0 (default): the device's stream, shared with every other
+ * handle on it; calls on such handles take turns. */
+#define EXG_OPT_OWN_STREAM 5
 EXG_API int exg_world_set_option(exg_world_t world, int32_t option, int64_t value);
 EXG_API int exg_world_get_option(exg_world_t world, int32_t option, int64_t* value);
+/* The CUDA stream (cudaStream_t) the handle's work runs on, for events around its calls. */
+EXG_API int exg_world_stream(exg_world_t world, void** stream_out);
 /* SM clock cycles the implicit step spent per phase since the handle was created, summed over
  * islands: [0] PRE, [1] joint values + Jacobian, [2] gather + POST, [3] assembly, [4] linear
  * solve, [5] line search, [6] commit, [7] other. Zero for worlds without implicit islands. */

@@ -90,3 +90,52 @@ def test_config3_sized_batch_runs(device):
     assert st["fatal"] == 0
     out = batch.bodies()
     assert np.all(np.isfinite(out["pose"])) and np.all(np.isfinite(out["momentum"]))
+
+
+def test_handles_on_their_own_streams_step_side_by_side_bit_for_bit(device):
+    """Two batch handles with EXG_OPT_OWN_STREAM, each driven by its own host thread (state in,
+    a step, state out, every step), end bit for bit where the same handles stepped one after the
+    other on the device's stream end; a third handle on the device stream steps meanwhile."""
+    import threading
+    worlds = mixed_worlds(PRECISION_MIXED)
+    halves = (worlds[:5], worlds[5:])
+    want = []
+    for part in halves:
+        b = _lib.DeviceBatch(device, part)
+        for _ in range(6):
+            st = b.state()
+            b.set_state(st)
+            b.step(1)
+        want.append(b.bodies())
+        b.close()
+    handles = [_lib.DeviceBatch(device, part) for part in halves]
+    shared = _lib.DeviceBatch(device, worlds[:3])
+    for h in handles:
+        h.set_option(_lib.DeviceWorld.OPT_OWN_STREAM, 1)
+        assert h.get_option(_lib.DeviceWorld.OPT_OWN_STREAM) == 1
+    assert handles[0].stream() != handles[1].stream() != shared.stream()
+    errors = []
+
+    def drive(h):
+        try:
+            st = _lib.host_state(h.n)
+            for _ in range(6):
+                h.state(out=st)
+                h.set_state(st)
+                h.step(1)
+        except Exception as e:  # surfaced below
+            errors.append(e)
+
+    threads = [threading.Thread(target=drive, args=(h,)) for h in handles]
+    for t in threads:
+        t.start()
+    shared.step(4)
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for h, w in zip(handles, want):
+        got = h.bodies()
+        assert np.array_equal(got["pose"], w["pose"]) and np.array_equal(got["momentum"], w["momentum"])
+        h.set_option(_lib.DeviceWorld.OPT_OWN_STREAM, 0)
+        h.close()
+    shared.close()

@@ -11,8 +11,8 @@ A step is one Mechanism::step of the whole workload (every body advanced by dt).
 body-steps/s from CUDA events on the library's stream with the state resident in HBM; `e2e` is the
 same metric through the public API with page-locked host buffers: each step the dynamic state
 (pose, momentum) copied in, the step, the state read back, all inside the timed region. The
-explicit and the implicit worlds sit in two handles on streams of their own, each driven by a host
-thread, so one's copies overlap the other's step (`e2e.one_handle`: one handle, one thread;
+explicit worlds and the two halves of the implicit ones sit in three handles on streams of their
+own, each driven by a host thread, so one's copies overlap the others' steps (`e2e.one_handle`: one handle, one thread;
 `e2e.records`: whole body records). Under torchrun each rank steps its own
 replica of the workload (independent worlds: weak scaling, no collective in the data path); the
 timing is the max over ranks.
@@ -320,11 +320,11 @@ def run_ours(args, rank, world_size, local_rank):
                 "d2h_bytes_per_step": int(nbytes), "steps": args.steps}
 
     def end_to_end_overlapped():
-        # the same state loop on two handles with streams of their own (EXG_OPT_OWN_STREAM), one
-        # holding the explicit worlds and one the implicit ones, each driven by its own host
-        # thread: one handle's copies run while the other steps
-        groups = [[p for p in parts if int(p[2]["integrator"]) != NEWTON],
-                  [p for p in parts if int(p[2]["integrator"]) == NEWTON]]
+        # the same state loop on three handles with streams of their own (EXG_OPT_OWN_STREAM): the
+        # explicit worlds, and the implicit ones in two halves; each handle is driven by its own
+        # host thread, so one handle's copies run while the others step
+        implicit = [p for p in parts if int(p[2]["integrator"]) == NEWTON]
+        groups = [[p for p in parts if int(p[2]["integrator"]) != NEWTON], implicit[0::2], implicit[1::2]]
         if not all(groups):
             return None
         hs = [_lib.DeviceBatch(dev, g) for g in groups]
@@ -360,8 +360,8 @@ def run_ours(args, rank, world_size, local_rank):
         nbytes = sum(b.nbytes for b in bufs)
         return {"value": total_bodies * args.steps / t_e, "unit": METRIC, "h2d_bytes_per_step": int(nbytes),
                 "d2h_bytes_per_step": int(nbytes), "steps": args.steps,
-                "transfer": "dynamic state in and out every step; two handles on their own streams (explicit "
-                            "and implicit worlds), one host thread each"}
+                "transfer": "dynamic state in and out every step; three handles on their own streams (the "
+                            "explicit worlds, the implicit ones in two halves), one host thread each"}
 
     one = end_to_end(_lib.host_state, lambda w, h: w.state(out=h), lambda w, h: w.set_state(h))
     one["transfer"] = "dynamic state (pose, momentum: 112 B per body) in and out every step, one handle"

@@ -430,26 +430,29 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
   }
 }
 
+// The slices of one law on s, its values on sv (independent work: slices write the Jacobian
+// records, values the joint wrenches).
 template <bool MIXED, int LAW>
-void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s) {
+void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s, cudaStream_t sv) {
   const int per = 2 * dev->tune_wave_blocks_per_sm;
   if (LAW != LAW_TORSIONAL) {  // the assembly knows the torsional slices in closed form
     const int g = grid_for(dev, 32LL * ((n + 7) / 8), 128, per);
     k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);
     k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);
   }
-  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, s>>>(a, first, n);
+  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, sv>>>(a, first, n);
 }
 
 template <bool MIXED>
-void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_first, cudaStream_t s) {
+void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_first, cudaStream_t s,
+                          cudaStream_t sv) {
   for (int L = 0; L < 4; ++L) {
     const int first = law_first[L], n = law_first[L + 1] - first;
     if (n == 0) continue;
-    if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, s);
-    else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, s);
-    else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, s);
-    else launch_joints_of<MIXED, 3>(dev, a, first, n, s);
+    if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, s, sv);
+    else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, s, sv);
+    else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, s, sv);
+    else launch_joints_of<MIXED, 3>(dev, a, first, n, s, sv);
   }
 }
 
@@ -1067,12 +1070,12 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
   cudaGraph_t g;
+  if (int rc = ensure_side()) return rc;
   EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   k_w_begin<<<g_isl, T, 0, s>>>(a);
   k_w_start<<<g_body, T, 0, s>>>(a);
   k_w_pre<<<g_body, T, 0, s>>>(a);
-  if (mixed) launch_joints_by_law<true>(dev, a, wave_law_first_, s);
-  else launch_joints_by_law<false>(dev, a, wave_law_first_, s);
+  joints_forked(dev, &a, mixed, s);
   k_w_post<<<g_dyn, T, 0, s>>>(a);
   k_w_after_eval<<<g_isl, T, 0, s>>>(a);
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
@@ -1119,6 +1122,25 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   return EXG_OK;
 }
 
+int NewtonWorld::ensure_side() {
+  if (!side_) EXG_CUDA_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  if (!fork_) EXG_CUDA_TRY(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  if (!join_) EXG_CUDA_TRY(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
+  return EXG_OK;
+}
+
+// A round's joint tasks, captured: the Jacobian slices on s and, beside them on the side stream,
+// the FP64 values; the side branch joins s again before anything that reads the values.
+void NewtonWorld::joints_forked(exg_device_s* dev, const void* args, bool mixed, cudaStream_t s) {
+  const WaveArgs& a = *static_cast<const WaveArgs*>(args);
+  cudaEventRecord(fork_, s);
+  cudaStreamWaitEvent(side_, fork_, 0);
+  if (mixed) launch_joints_by_law<true>(dev, a, wave_law_first_, s, side_);
+  else launch_joints_by_law<false>(dev, a, wave_law_first_, s, side_);
+  cudaEventRecord(join_, side_);
+  cudaStreamWaitEvent(s, join_, 0);
+}
+
 // The step's rounds as one graph: WHILE (some island unfinished) { evaluation; IF (some island
 // needs a direction) { assembly, elimination, line-search start }; IF (some span ends) { commit } }.
 // The conditions are set on the device (k_w_cond, k_w_count), so a step needs no host round trip.
@@ -1133,6 +1155,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  if (int rc = ensure_side()) return rc;
   cudaGraph_t G = nullptr;
   EXG_CUDA_TRY(cudaGraphCreate(&G, 0));
   struct Guard { cudaGraph_t g; ~Guard() { if (g) cudaGraphDestroy(g); } } guard{G};
@@ -1176,8 +1199,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
     k_w_begin<<<g_isl, T, 0, s>>>(a);
     k_w_start<<<g_body, T, 0, s>>>(a);
     k_w_pre<<<g_body, T, 0, s>>>(a);
-    if (mixed) launch_joints_by_law<true>(dev, a, wave_law_first_, s);
-    else launch_joints_by_law<false>(dev, a, wave_law_first_, s);
+    joints_forked(dev, &a, mixed, s);
     k_w_post<<<g_dyn, T, 0, s>>>(a);
     k_w_after_eval<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);

@@ -129,6 +129,11 @@ class NewtonWorld {
   unsigned char wave_graph_world_[160] = {0};  // the world arrays the round graph was captured with
   int build_wave_graph(exg_device_s* dev, const void* args, cudaStream_t s);
   int build_wave_round_graph(exg_device_s* dev, const void* args, cudaStream_t s);
+  // the side stream and events of the forked joint tasks (made before any capture)
+  int ensure_side();
+  void joints_forked(exg_device_s* dev, const void* args, bool mixed, cudaStream_t s);
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
   bool wave_host_loop_ = false, wave_graph_host_loop_ = false;
   bool wave_mixed_ = false;
   int wave_kernels_eval_ = 0, wave_kernels_dir_ = 0, wave_kernels_end_ = 0;

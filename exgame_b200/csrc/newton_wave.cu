@@ -591,13 +591,21 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
   }
 }
 
+// The islands whose span end reads the stiffness signal (not converged, sub-division left, a matrix
+// assembled in the span): only they sum ||A||_F^2 and ||M||_F^2, at span end, from the blocks of
+// their last assembly (the elimination leaves D, A_cp and A_pc as assembled), the same values the
+// island kernel sums after each assembly.
+__device__ __forceinline__ bool wants_norms(const WaveCtl& w) {
+  return w.state == WS_END && w.assembled && !w.converged && w.depth != kMaxDepth;
+}
+
 // Per dynamic node, a fixed-order sum of squares: of its assembled blocks (the diagonal, and the
 // two parent couplings of a non-root node) for ||A||_F^2, or of its mass0 block for ||M||_F^2.
-__global__ void k_w_node_sq(WaveArgs a, int want_state, int mass) {
+__global__ void k_w_node_sq(WaveArgs a, int mass) {
   for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
     int2 it = a.dyn[t];
     const WaveCtl& w = a.ctl[it.x];
-    if (w.state != want_state || (mass && !w.assembled)) continue;
+    if (!wants_norms(w)) continue;
     Ctx c = wave_ctx_lite(a, it.x);
     const size_t o = 36 * (size_t)it.y;
     double s = 0.0;
@@ -626,11 +634,11 @@ __global__ void k_w_node_sq(WaveArgs a, int want_state, int mass) {
 // One CTA per island: the sum of its node values, thread-strided in index order and then a
 // fixed-shape tree, so the result does not depend on scheduling.
 constexpr int kSumThreads = 256;
-__global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int want_state, int mass) {
+__global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int mass) {
   __shared__ double part[kSumThreads];
   for (int k = blockIdx.x; k < a.n_isl; k += gridDim.x) {
     const WaveCtl& w = a.ctl[k];
-    if (w.state != want_state || (mass && !w.assembled)) continue;
+    if (!wants_norms(w)) continue;
     const int first = a.dyn_first[k], count = a.dyn_first[k + 1] - first;
     double s = 0.0;
     for (int t = threadIdx.x; t < count; t += kSumThreads) s += a.nodesq[first + t];
@@ -1081,8 +1089,6 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
   if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
   else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);
-  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
   for (int L = nl - 1; L >= 0; --L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
     if (count <= kNarrowLevel)
@@ -1101,8 +1107,10 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   k_w_after_solve<<<g_isl, T, 0, s>>>(a);
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
   k_w_restore<<<g_body, T, 0, s>>>(a);
-  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_END, 1);
-  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_END, 1);
+  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, 0);
+  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, 0);
+  k_w_node_sq<<<g_dyn, T, 0, s>>>(a, 1);
+  k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, 1);
   k_w_end<<<g_isl, T, 0, s>>>(a);
   k_w_commit<<<g_dyn, T, 0, s>>>(a);
   k_w_count_flat<<<1, 1024, 0, s>>>(a);
@@ -1117,8 +1125,8 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   for (int L = 0; L < 4; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels;
-  wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
-  wave_kernels_end_ = 6;
+  wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;
+  wave_kernels_end_ = 8;
   return EXG_OK;
 }
 
@@ -1210,8 +1218,6 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(capture(BD, {}, [&] {
     if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_DIR, 0);
-    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_DIR, 0);
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
       if (count <= kNarrowLevel)
@@ -1237,8 +1243,10 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   // span end: the best iterate back, the stiffness signal, sub-division or commit
   EXG_CUDA_TRY(capture(BE, {}, [&] {
     k_w_restore<<<g_body, T, 0, s>>>(a);
-    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, WS_END, 1);
-    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, WS_END, 1);
+    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, 0);
+    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, 0);
+    k_w_node_sq<<<g_dyn, T, 0, s>>>(a, 1);
+    k_w_island_sum<<<g_sum, kSumThreads, 0, s>>>(a, 1);
     k_w_end<<<g_isl, T, 0, s>>>(a);
     k_w_commit<<<g_dyn, T, 0, s>>>(a);
   }));
@@ -1248,8 +1256,8 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   for (int L = 0; L < 4; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
-  wave_kernels_dir_ = 3 + nl + (nl - 1) + 3;
-  wave_kernels_end_ = 5;
+  wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;
+  wave_kernels_end_ = 7;
   return EXG_OK;
 }
 

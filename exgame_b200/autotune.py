@@ -18,7 +18,7 @@ from .abi import GRAVITY_PLUMMER, JOINT_DTYPE, LIE_EULER, NEWTON, PRECISION_MIXE
 
 GRAVITY_CTAS = (8, 12, 16, 21, 32)
 WAVE_BLOCKS = (4, 8, 16)
-WAVE_THRESHOLDS = (32, 256, 2048)
+WAVE_THRESHOLDS = (8, 16, 32, 256)
 
 
 def _time(dev, kinds, world, steps):

@@ -161,3 +161,24 @@ def test_host_driven_rounds_equal_the_conditional_graph(device):
         out.append(batch.bodies())
         batch.close()
     assert np.array_equal(out[0]["pose"], out[1]["pose"]) and np.array_equal(out[0]["momentum"], out[1]["momentum"])
+
+
+def test_wide_and_narrow_elimination_levels_agree_with_island_kernel(device):
+    """A batch whose widest elimination levels hold more than 8192 nodes, so the wave eliminates
+    them one thread per node and the narrow levels one warp per node: every world ends bit for bit
+    as the island kernel leaves it."""
+    worlds = []
+    for k in range(64):
+        b, j = scenarios.tree_world(2048, seed=400 + k)
+        worlds.append((b, j, step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10,
+                                         exact_jacobian=True)))
+    a = _lib.DeviceBatch(device, worlds)
+    a.set_option(W.OPT_WAVE_MIN_BODIES, 1 << 20)  # island kernel
+    a.step(3)
+    b = _lib.DeviceBatch(device, worlds)
+    b.set_option(W.OPT_WAVE_MIN_BODIES, 1)
+    b.step(3)
+    x, y = a.bodies(), b.bodies()
+    assert np.array_equal(x["pose"], y["pose"]) and np.array_equal(x["momentum"], y["momentum"])
+    a.close()
+    b.close()

@@ -306,6 +306,7 @@ class DeviceWorld:
         return s
 
     OPT_WAVE_MIN_BODIES, OPT_WAVE_MAX_LEVELS, OPT_LAST_WAVE_ROUNDS, OPT_WAVE_HOST_ROUNDS, OPT_OWN_STREAM = 1, 2, 3, 4, 5
+    OPT_WAVE_LEVEL_MAX_WIDTH, OPT_WAVE_LEVEL_MIN_WIDTH = 6, 7
 
     def stream(self):
         """The CUDA stream (as an integer handle) this world's work runs on."""

@@ -235,6 +235,7 @@ int exg_device_create(int32_t ordinal, exg_device_t* out) {
     delete d;
     return EXG_ERR_BACKEND;
   }
+  exg_internal_noalloc_forget(ordinal);
   *out = d;
   return EXG_OK;
 }
@@ -850,6 +851,8 @@ int exg_world_get_option(exg_world_t W, int32_t option, int64_t* value) {
     case EXG_OPT_LAST_WAVE_ROUNDS: *value = W->newton->last_wave_rounds(); return EXG_OK;
     case EXG_OPT_WAVE_HOST_ROUNDS: *value = W->newton->wave_host_loop() ? 1 : 0; return EXG_OK;
     case EXG_OPT_OWN_STREAM: *value = W->own ? 1 : 0; return EXG_OK;
+    case EXG_OPT_WAVE_LEVEL_MAX_WIDTH: *value = W->newton->wave_level_width(true); return EXG_OK;
+    case EXG_OPT_WAVE_LEVEL_MIN_WIDTH: *value = W->newton->wave_level_width(false); return EXG_OK;
     default: return EXG_ERR_INVALID_ARGUMENT;
   }
 }
@@ -1141,7 +1144,7 @@ int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t nj, c
                     double dt, double warp, int32_t jacobian, double* d_out) {
   if (!dev || nj < 0 || (nj > 0 && (!d_joints || !d_pose || !d_vel || !d_out))) return EXG_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(dev->mu);
-  cudaSetDevice(dev->ordinal);
+  EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));
   int rc = launch_joints_stage(dev, d_joints, nj, d_pose, d_vel, dt, warp, jacobian, d_out, dev->stream);
   if (rc != EXG_OK) return rc;
   EXG_CUDA_TRY(cudaStreamSynchronize(dev->stream));
@@ -1154,9 +1157,11 @@ int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double*
   if (law == EXG_GRAVITY_SIZE_CORE && n > 0 && !d_size) return EXG_ERR_INVALID_ARGUMENT;
   if (law != EXG_GRAVITY_SIZE_CORE && law != EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
   if (law == EXG_GRAVITY_PLUMMER && !(softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
+  if (precision != EXG_PRECISION_F64 && precision != EXG_PRECISION_MIXED && precision != EXG_PRECISION_MIXED_FAST)
+    return EXG_ERR_INVALID_ARGUMENT;
   if (n == 0) return EXG_OK;
   std::lock_guard<std::mutex> lock(dev->mu);
-  cudaSetDevice(dev->ordinal);
+  EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));
   cudaStream_t s = dev->stream;
   if (n == 1) {
     EXG_CUDA_TRY(cudaMemsetAsync(d_force, 0, 3 * sizeof(double), s));

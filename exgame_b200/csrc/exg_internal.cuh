@@ -19,6 +19,8 @@
   } while (0)
 
 void exg_internal_set_cuda_error(cudaError_t e, const char* what);
+// Drop the cached device address of the no-allocation gravity array on `ordinal` (gravity.cu).
+void exg_internal_noalloc_forget(int ordinal);
 
 // Kernel kinds the in-library profiler distinguishes.
 enum ProfKind { PROF_GRAVITY = 0, PROF_JOINTS = 1, PROF_INTEGRATE = 2, PROF_NEWTON = 3, PROF_BODY_PRE = 4, PROF_NEWTON_WAVE = 5,

@@ -473,6 +473,14 @@ int noalloc_scratch(int ordinal, unsigned char** out) {
 }
 }  // namespace
 
+// A new device handle looks the address up again on its first no-allocation call, so a context
+// the host re-created on that device (after cudaDeviceReset) is not served a stale address.
+void exg_internal_noalloc_forget(int ordinal) {
+  if (ordinal < 0 || ordinal >= 256) return;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  g_noalloc_addr[ordinal] = nullptr;
+}
+
 extern "C" int exg_gravity_forces_noalloc(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n,
                                           int32_t law, double G, double softening, int32_t precision, double* d_force) {
   if (!dev || n < 0 || (n > 0 && (!d_pos_mass || !d_force))) return EXG_ERR_INVALID_ARGUMENT;
@@ -480,6 +488,8 @@ extern "C" int exg_gravity_forces_noalloc(exg_device_t dev, const double* d_pos_
   if (law == EXG_GRAVITY_SIZE_CORE && n > 0 && !d_size) return EXG_ERR_INVALID_ARGUMENT;
   if (law != EXG_GRAVITY_SIZE_CORE && law != EXG_GRAVITY_PLUMMER) return EXG_ERR_INVALID_ARGUMENT;
   if (law == EXG_GRAVITY_PLUMMER && !(softening > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
+  if (precision != EXG_PRECISION_F64 && precision != EXG_PRECISION_MIXED && precision != EXG_PRECISION_MIXED_FAST)
+    return EXG_ERR_INVALID_ARGUMENT;
   if (n == 0) return EXG_OK;
   std::lock_guard<std::mutex> lock(dev->mu);
   EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));

@@ -96,6 +96,15 @@ class NewtonWorld {
   // After the stream is synchronised: launched-kernel accounting, round-cap check.
   int wave_after_steps(exg_device_s* dev);
   int last_wave_rounds() const { return last_wave_rounds_; }
+  // Widest (or narrowest) elimination level of the wave, in nodes; 0 without wave islands.
+  int wave_level_width(bool widest) const {
+    int best = 0;
+    for (size_t L = 0; L + 1 < wave_level_ptr_.size(); ++L) {
+      int wd = wave_level_ptr_[L + 1] - wave_level_ptr_[L];
+      if (L == 0 || (widest ? wd > best : wd < best)) best = wd;
+    }
+    return best;
+  }
   // Rounds driven from the host (one flat round graph per launch) instead of the conditional graph:
   // the same arithmetic, for profilers that do not follow kernels into conditional graph nodes.
   void set_wave_host_loop(bool on) { wave_host_loop_ = on; }

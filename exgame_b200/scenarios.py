@@ -3,7 +3,8 @@ configurations the measurements are quoted on).
 
 Every generator draws from numpy's PCG64 (`numpy.random.default_rng(seed)`) and returns host
 arrays in the C ABI's record layouts (BODY_DTYPE, JOINT_DTYPE) plus step parameters. Motors are
-built with the library's own host-side algebra (exg_motor_exp / exg_motor_compose).
+built with a numpy restatement of the motor algebra (motors_np), so generating a workload loads
+no part of the CUDA library.
 
   gravity_world  N point masses: positions uniform in a ball, masses log-uniform in [1, 10],
                  circular-orbit speed about the centre of mass (mass strictly inside the radius
@@ -24,7 +25,7 @@ import math
 
 import numpy as np
 
-from . import _lib
+from . import motors_np
 from .abi import (BODY_DTYPE, GRAVITY_OFF, GRAVITY_PLUMMER, JOINT_DTYPE, LIE_EULER, NEWTON, PRECISION_F64,
                   step_params)
 
@@ -32,7 +33,7 @@ IDENTITY = np.array([1.0, 0, 0, 0, 0, 0, 0, 0])
 
 
 def translation(x):
-    return _lib.motor_exp(np.array([x[0], x[1], x[2], 0.0, 0.0, 0.0]), 1.0)
+    return motors_np.twist_exp_n(np.array([x[0], x[1], x[2], 0.0, 0.0, 0.0]), 1.0)[0]
 
 
 def random_unit(rng):
@@ -74,7 +75,7 @@ def gravity_world(n, radius=100.0, seed=0, G=1.0):
     bodies = np.zeros(n, dtype=BODY_DTYPE)
     tw = np.zeros((n, 6))
     tw[:, :3] = pos
-    bodies["pose"] = _lib.motor_exp_n(tw, 1.0)
+    bodies["pose"] = motors_np.twist_exp_n(tw, 1.0)
     bodies["momentum"][:, :3] = mass[:, None] * vel
     bodies["mass"] = mass
     bodies["inertia"][:, 0] = 1.0
@@ -131,7 +132,7 @@ def _bodies_at(rng, mass, I, pos, twist_sigma):
     xi = rng.normal(0.0, twist_sigma, size=(n, 6))
     tw = np.zeros((n, 6))
     tw[:, :3] = pos
-    bodies["pose"] = _lib.motor_compose_n(_lib.motor_exp_n(xi, 1.0), _lib.motor_exp_n(tw, 1.0))
+    bodies["pose"] = motors_np.compose_n(motors_np.twist_exp_n(xi, 1.0), motors_np.twist_exp_n(tw, 1.0))
     return bodies
 
 

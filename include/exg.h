@@ -325,6 +325,11 @@ EXG_API int exg_server_destroy(exg_server_t server);
  * here only a handle is single-writer). 0 (default): the device's stream, shared with every other
  * handle on it; calls on such handles take turns. */
 #define EXG_OPT_OWN_STREAM 5
+/* Read only, after a step: the most and the fewest nodes on one elimination level of the wave
+ * schedule, across the handle's wave islands (the wave eliminates levels wider than 8192 nodes one
+ * thread per node, narrower ones one warp per node); 0 without wave islands. */
+#define EXG_OPT_WAVE_LEVEL_MAX_WIDTH 6
+#define EXG_OPT_WAVE_LEVEL_MIN_WIDTH 7
 EXG_API int exg_world_set_option(exg_world_t world, int32_t option, int64_t value);
 EXG_API int exg_world_get_option(exg_world_t world, int32_t option, int64_t* value);
 /* The CUDA stream (cudaStream_t) the handle's work runs on, for events around its calls. */
@@ -361,8 +366,9 @@ EXG_API int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32
                     const double* d_vel, double dt, double warp, int32_t jacobian, double* d_out);
 /* All-pairs gravity (crates/newton/src/gravity.rs:110-140, 438-450): d_pos_mass holds
  * [x, y, z, m] per body, d_size the core radius (SIZE_CORE law), output d_force[3*i] is the
- * world force on body i. precision MIXED runs the FP32 tile-relative kernel with compensated
- * accumulation. */
+ * world force on body i. precision MIXED runs the FP32 kernel on double-single separations,
+ * MIXED_FAST the single-FP32 one, F64 the double kernel; any other precision code is
+ * EXG_ERR_INVALID_ARGUMENT. */
 EXG_API int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law,
                        double G, double softening, int32_t precision, double* d_force);
 
@@ -376,7 +382,9 @@ EXG_API int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const
  * the process exits. Bodies are limited to EXG_NOALLOC_MAX_BODIES; larger n returns
  * EXG_ERR_INVALID_ARGUMENT before any work is queued.
  * The first call on a device looks up that array's device address (once per device, with the
- * device current); make that first call before capturing any stream into a CUDA graph.
+ * device current); make that first call before capturing any stream into a CUDA graph. The address
+ * belongs to the device's primary context: exg_device_create forgets it, so after a
+ * cudaDeviceReset create a new device handle before the next call.
  * Every call on a device uses the same array and leaves its contents behind; the call resets what
  * must start at zero. Two calls whose GPU work overlaps (from different threads or streams) race
  * on the array. The call returns after its work has finished. */

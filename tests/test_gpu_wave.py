@@ -178,6 +178,9 @@ def test_wide_and_narrow_elimination_levels_agree_with_island_kernel(device):
     b = _lib.DeviceBatch(device, worlds)
     b.set_option(W.OPT_WAVE_MIN_BODIES, 1)
     b.step(3)
+    # the batch exercises both elimination kernels: a level wider than 8192 nodes and one narrower
+    assert b.get_option(W.OPT_WAVE_LEVEL_MAX_WIDTH) > 8192
+    assert 0 < b.get_option(W.OPT_WAVE_LEVEL_MIN_WIDTH) <= 8192
     x, y = a.bodies(), b.bodies()
     assert np.array_equal(x["pose"], y["pose"]) and np.array_equal(x["momentum"], y["momentum"])
     a.close()

@@ -13,7 +13,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from exgame_b200 import _lib, scenarios
+from exgame_b200 import _lib, motors_np, scenarios
 from exgame_b200.abi import GRAVITY_PLUMMER, GRAVITY_SIZE_CORE, PRECISION_F64, PRECISION_MIXED
 
 pytestmark = pytest.mark.gpu
@@ -24,7 +24,7 @@ MAX_BODIES = 16384  # EXG_NOALLOC_MAX_BODIES in include/exg.h
 
 
 def charges(bodies):
-    p = np.array([_lib.motor_apply_point(b["pose"], np.zeros(3)) for b in bodies])
+    p = motors_np.apply_point_n(bodies["pose"], np.zeros((len(bodies), 3)))
     pm = np.zeros((len(bodies), 4))
     pm[:, :3] = p
     pm[:, 3] = bodies["mass"]
@@ -50,16 +50,21 @@ def forces(dev, fn, pm_t, size_t, n, law, precision):
 
 @pytest.mark.parametrize("precision", [PRECISION_F64, PRECISION_MIXED])
 def test_noalloc_matches_allocating_entry_point_twice(precision):
+    """Both entry points run the same work plan through the same kernels, so they agree bit for
+    bit; the sizes include the array's limit (MAX_BODIES: every work item and partial-sum slot of
+    the fixed array in use) and one body below it, each followed by a smaller call that must not
+    see what the larger one left behind."""
     L = _lib.lib()
     dev = _lib.Device(0)
-    # two different calls in a row: the second must not see anything the first left behind
-    for n, law, seed in ((3000, GRAVITY_PLUMMER, 1), (700, GRAVITY_SIZE_CORE, 2)):
+    cases = ((3000, GRAVITY_PLUMMER, 1), (700, GRAVITY_SIZE_CORE, 2), (MAX_BODIES, GRAVITY_PLUMMER, 3),
+             (1000, GRAVITY_SIZE_CORE, 4), (MAX_BODIES - 1, GRAVITY_SIZE_CORE, 5), (257, GRAVITY_PLUMMER, 6))
+    for n, law, seed in cases:
         bodies = scenarios.gravity_world(n, 50.0, seed=seed)
         pm_t, size_t = on_device(charges(bodies)), on_device(np.ascontiguousarray(bodies["size"]))
         want = forces(dev, L.exg_gravity_forces, pm_t, size_t, n, law, precision)
         got = forces(dev, L.exg_gravity_forces_noalloc, pm_t, size_t, n, law, precision)
-        scale = np.abs(want).max()
-        assert np.abs(got - want).max() <= 1e-12 * scale, (n, law)
+        assert np.isfinite(want).all()
+        assert np.array_equal(got, want), (n, law, np.abs(got - want).max())
     dev.close()
 
 
@@ -72,4 +77,16 @@ def test_noalloc_rejects_sizes_beyond_its_array():
     torch.cuda.synchronize()
     st = L.exg_gravity_forces_noalloc(dev.handle, vp(pm_t), None, n, GRAVITY_PLUMMER, 1.0, 0.05, PRECISION_F64, vp(out))
     assert st == -20  # EXG_ERR_INVALID_ARGUMENT
+    dev.close()
+
+
+def test_both_entry_points_reject_unknown_precision():
+    L = _lib.lib()
+    dev = _lib.Device(0)
+    n = 64
+    pm_t = torch.ones(4 * n, dtype=torch.float64, device="cuda")
+    out = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    for fn in (L.exg_gravity_forces, L.exg_gravity_forces_noalloc):
+        assert fn(dev.handle, vp(pm_t), None, n, GRAVITY_PLUMMER, 1.0, 0.05, 7, vp(out)) == -20
     dev.close()

@@ -75,6 +75,9 @@ SIGNATURES = {
     "exg_pool_set_steps": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
     "exg_pool_steps_left": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
+    "exg_world_island_count": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "exg_world_island_structure": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp,
+                                                  ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
     "exg_motor_compose": (ctypes.c_int, [_vp, _vp, _vp]),
     "exg_motor_inverse": (ctypes.c_int, [_vp, _vp]),
@@ -333,6 +336,28 @@ class DeviceWorld:
         e = ctypes.c_double()
         check(lib().exg_world_energy(self.handle, ctypes.byref(e)), "exg_world_energy")
         return e.value
+
+    STRUCT_KINDS = {"bodies": 1, "joint_ends": 2, "order": 3, "incidence_ptr": 4, "incidence": 5, "parent": 6,
+                    "joints": 7}
+
+    def island_count(self, world=0):
+        n = ctypes.c_int32()
+        check(lib().exg_world_island_count(self.handle, int(world), ctypes.byref(n)), "exg_world_island_count")
+        return n.value
+
+    def island_structure(self, island, kind, world=0):
+        """One integer map of an implicit island's solver structure, read back from the device
+        (kind: a key of STRUCT_KINDS). joint_ends comes as an (n_joints, 3) array: law, a, b."""
+        k = self.STRUCT_KINDS[kind]
+        n = ctypes.c_int32()
+        st = lib().exg_world_island_structure(self.handle, int(world), int(island), k, None, 0, ctypes.byref(n))
+        if st != EXG_OK and n.value == 0 and st != -20:
+            check(st, "exg_world_island_structure")
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        check(lib().exg_world_island_structure(self.handle, int(world), int(island), k, ptr(out), len(out),
+                                               ctypes.byref(n)), "exg_world_island_structure")
+        out = out[:n.value]
+        return out.reshape(-1, 3) if kind == "joint_ends" else out
 
     def close(self):
         if self.handle:

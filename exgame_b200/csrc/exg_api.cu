@@ -1064,6 +1064,28 @@ int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
   return rc;
 }
 
+int exg_world_island_count(exg_world_t W, int32_t world, int32_t* n_islands) {
+  if (!W || !n_islands) return EXG_ERR_INVALID_ARGUMENT;
+  HandleLock lock(W);
+  if (world < 0 || world >= W->w_cap || !W->slots[world].used) return EXG_ERR_INVALID_ARGUMENT;
+  *n_islands = W->newton->island_count(world);
+  return EXG_OK;
+}
+
+int exg_world_island_structure(exg_world_t W, int32_t world, int32_t island, int32_t kind, int32_t* out, int32_t cap,
+                               int32_t* len) {
+  if (!W || !len || cap < 0 || (cap > 0 && !out)) return EXG_ERR_INVALID_ARGUMENT;
+  HandleLock lock(W);
+  if (world < 0 || world >= W->w_cap || !W->slots[world].used) return EXG_ERR_INVALID_ARGUMENT;
+  EXG_CUDA_TRY(cudaSetDevice(W->dev->ordinal));
+  int rc;
+  if (W->dirty && (rc = pool_prepare(W)) != EXG_OK) return rc;  // upload pending structure first
+  int n = 0;
+  rc = W->newton->read_structure(world, island, kind, out, cap, &n);
+  *len = n;
+  return rc;
+}
+
 int exg_world_energy(exg_world_t W, double* out) {
   if (!W || !out) return EXG_ERR_INVALID_ARGUMENT;
   double e = 0.0;

@@ -407,6 +407,7 @@ void NewtonWorld::compact() {
                               &h_cell_terms})
     v->clear();
   h_jl_params.clear();
+  h_jl_id.clear();
   world_islands_.clear();
   scratch_alloc_.init(scratch_alloc_.capacity());
   n_live_ = 0;
@@ -449,6 +450,7 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
   std::vector<int> s_isl_body, s_jl_law, s_jl_a, s_jl_b, s_ib_order, s_ib_inc_ptr, s_ib_inc_ref, s_dn_body, s_dn_parent,
       s_lv_ptr, s_lv_nodes, s_ch_ptr, s_ch_idx, s_cell_ptr, s_cell_terms;
   std::vector<double> s_jl_params;
+  std::vector<int> s_jl_id;
   const int base_isl_body = (int)h_isl_body.size(), base_jl = (int)h_jl_law.size(), base_order = (int)h_ib_order.size(),
             base_inc_ptr = (int)h_ib_inc_ptr.size(), base_inc_ref = (int)h_ib_inc_ref.size(),
             base_dn = (int)h_dn_body.size(), base_lv = (int)h_lv_ptr.size(), base_ch_idx = (int)h_ch_idx.size(),
@@ -470,6 +472,7 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
       s_jl_law.push_back(jt.law);
       s_jl_a.push_back(local[jt.a]);
       s_jl_b.push_back(local[jt.b]);
+      s_jl_id.push_back(J[q]);
       for (int k = 0; k < 10; ++k) s_jl_params.push_back(jt.params[k]);
     }
     // dynamic order (island order, kinematic excluded)
@@ -617,6 +620,7 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
   cat(h_dn_body, s_dn_body); cat(h_dn_parent, s_dn_parent); cat(h_lv_ptr, s_lv_ptr); cat(h_lv_nodes, s_lv_nodes);
   cat(h_ch_ptr, s_ch_ptr); cat(h_ch_idx, s_ch_idx); cat(h_cell_ptr, s_cell_ptr); cat(h_cell_terms, s_cell_terms);
   h_jl_params.insert(h_jl_params.end(), s_jl_params.begin(), s_jl_params.end());
+  cat(h_jl_id, s_jl_id);
   if ((int)world_islands_.size() <= slot) world_islands_.resize(slot + 1);
   world_islands_[slot].clear();
   for (size_t I = 0; I < desc.size(); ++I) {
@@ -762,6 +766,57 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
     k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
+}
+
+int NewtonWorld::island_count(int slot) const {
+  if (slot < 0 || slot >= (int)world_islands_.size()) return 0;
+  return (int)world_islands_[slot].size();
+}
+
+int NewtonWorld::read_structure(int slot, int k, int kind, int* out, int cap, int* len) {
+  if (dirty_) return EXG_ERR_INVALID_ARGUMENT;
+  if (slot < 0 || slot >= (int)world_islands_.size() || k < 0 || k >= (int)world_islands_[slot].size())
+    return EXG_ERR_INVALID_ARGUMENT;
+  const IslandDesc& d = desc_[world_islands_[slot][k]];
+  std::vector<int> v;
+  cudaError_t err = cudaSuccess;
+  auto fetch = [&](const DevArr<int>& a, long long off, int n) {
+    std::vector<int> h(std::max(n, 0), 0);
+    if (n > 0 && err == cudaSuccess) err = cudaMemcpy(h.data(), a.ptr + off, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    return h;
+  };
+  switch (kind) {
+    case EXG_STRUCT_ISLAND_BODIES:
+      v = fetch(d_isl_body, d.body_off, d.nb);
+      for (int& x : v) x -= src_[slot].body_off;
+      break;
+    case EXG_STRUCT_JOINT_ENDS: {
+      std::vector<int> law = fetch(d_jl_law, d.joint_off, d.nj), a = fetch(d_jl_a, d.joint_off, d.nj),
+                       b = fetch(d_jl_b, d.joint_off, d.nj);
+      for (int q = 0; q < d.nj; ++q) { v.push_back(law[q]); v.push_back(a[q]); v.push_back(b[q]); }
+      break;
+    }
+    case EXG_STRUCT_ORDER: v = fetch(d_ib_order, d.body_off, d.nb); break;
+    case EXG_STRUCT_INCIDENCE_PTR: {
+      v = fetch(d_ib_inc_ptr, d.inc_off, d.nb + 1);
+      const int base = v.empty() ? 0 : v[0];
+      for (int& x : v) x -= base;
+      break;
+    }
+    case EXG_STRUCT_INCIDENCE: {
+      std::vector<int> p = fetch(d_ib_inc_ptr, d.inc_off, d.nb + 1);
+      v = fetch(d_ib_inc_ref, p.front(), p.back() - p.front());
+      break;
+    }
+    case EXG_STRUCT_PARENT: v = fetch(d_dn_parent, d.dyn_off, d.m); break;
+    case EXG_STRUCT_ISLAND_JOINTS: v.assign(h_jl_id.begin() + d.joint_off, h_jl_id.begin() + d.joint_off + d.nj); break;
+    default: return EXG_ERR_INVALID_ARGUMENT;
+  }
+  EXG_CUDA_TRY(err);
+  *len = (int)v.size();
+  if ((int)v.size() > cap) return EXG_ERR_INVALID_ARGUMENT;
+  if (!v.empty()) std::copy(v.begin(), v.end(), out);
+  return EXG_OK;
 }
 
 int NewtonWorld::read_phase_cycles(long long* out) {

@@ -80,6 +80,12 @@ class NewtonWorld {
   // Summed SM cycles per phase since creation (kPhases values).
   int read_phase_cycles(long long* out);
   int live_islands() const { return n_live_; }
+  // Islands of one world (a slot of the pool), in island order (ascending first body).
+  int island_count(int slot) const;
+  // One array of island k's solver structure, copied back from the device arrays the kernels
+  // read (the kinds of exg_world_island_structure); *len its length. Host synchronous; the
+  // structure must be synced.
+  int read_structure(int slot, int k, int kind, int* out, int cap, int* len);
   // Islands with at least min_dyn dynamic bodies and at most max_levels elimination levels take
   // the wave schedule (newton_wave.cu); the others the island kernel.
   void set_wave_threshold(int min_dyn, int max_levels) {
@@ -159,6 +165,7 @@ class NewtonWorld {
   std::vector<int> h_isl_body, h_jl_law, h_jl_a, h_jl_b, h_ib_order, h_ib_inc_ptr, h_ib_inc_ref, h_dn_body, h_dn_parent,
       h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
   std::vector<double> h_jl_params;
+  std::vector<int> h_jl_id;  // per island joint: the world-local joint index (host only)
   std::vector<std::vector<int>> world_islands_;
   // device mirrors
   DevArr<IslandDesc> d_desc;

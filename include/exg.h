@@ -338,6 +338,33 @@ EXG_API int exg_world_stream(exg_world_t world, void** stream_out);
  * islands: [0] PRE, [1] joint values + Jacobian, [2] gather + POST, [3] assembly, [4] linear
  * solve, [5] line search, [6] commit, [7] other. Zero for worlds without implicit islands. */
 EXG_API int exg_world_phase_cycles(exg_world_t w, int64_t out[8]);
+/* ── solver structure read-back ──
+ * The islands of one implicit world (world 0 of a single-world handle, a batch index or a pool
+ * slot) and, per island, the integer maps the kernels index by, copied back from the device. These
+ * are the reference's per-island topology and gather maps (crates/newton/src/mechanism/islands.rs;
+ * bake_incidence, crates/newton/src/accelerator/mod.rs:289-331; the solver cache's dynamic order,
+ * crates/newton/src/integrator/implicit/cache.rs:566-573, 885-897), for checking them integer for
+ * integer. Islands come in order of their first body; an explicit world has none.
+ *   ISLAND_BODIES  per island body: its world-local body index (ascending)
+ *   JOINT_ENDS     per island joint, three ints: law, end a, end b (island-local body indices)
+ *   ORDER          per island body: its index among the island's dynamic bodies, -1 if kinematic
+ *   INCIDENCE_PTR  per island body plus one: offsets into INCIDENCE
+ *   INCIDENCE      per gathered term, in gather order: island joint * 2 + end (0 = a, 1 = b)
+ *   PARENT         per dynamic body: its parent in the elimination order's tree, -1 for a root
+ *   ISLAND_JOINTS  per island joint: its world-local joint index (ascending)
+ * `cap` is the capacity of out in ints; *len receives the length even when it exceeds cap
+ * (EXG_ERR_INVALID_ARGUMENT then). */
+#define EXG_STRUCT_ISLAND_BODIES 1
+#define EXG_STRUCT_JOINT_ENDS 2
+#define EXG_STRUCT_ORDER 3
+#define EXG_STRUCT_INCIDENCE_PTR 4
+#define EXG_STRUCT_INCIDENCE 5
+#define EXG_STRUCT_PARENT 6
+#define EXG_STRUCT_ISLAND_JOINTS 7
+EXG_API int exg_world_island_count(exg_world_t w, int32_t world, int32_t* n_islands);
+EXG_API int exg_world_island_structure(exg_world_t w, int32_t world, int32_t island, int32_t kind, int32_t* out,
+                                       int32_t cap, int32_t* len);
+
 /* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
 EXG_API int exg_world_energy(exg_world_t w, double* out);
 

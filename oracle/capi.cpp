@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only. C entry points over the f64 restatement, loaded by the
 // test suite (ctypes) to check the CUDA path; the shipped library never links this.
 // Records use the public layouts of include/exg.h so one numpy array feeds both sides.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include "../include/exg.h"
@@ -74,6 +75,35 @@ void orc_world_island_stats(void* h, int k, int* spans, int* iters) {
   Island& isl = static_cast<OWorld*>(h)->islands[k];
   *spans = isl.last_spans;
   *iters = isl.last_newton_iterations;
+}
+
+// Structure of island k, in the kinds of exg_world_island_structure (include/exg.h): 1 island
+// bodies, 2 joint ends (law, a, b per joint, island-local), 3 order, 4 incidence pointers,
+// 5 incidence terms, 7 island joints. Returns the length, or -1 when it exceeds cap.
+int orc_world_island_structure(void* h, int k, int kind, int* out, int cap) {
+  OWorld* w = static_cast<OWorld*>(h);
+  if (!w->built) w->build();
+  if (k < 0 || k >= (int)w->islands.size()) return -1;
+  const Island& isl = w->islands[k];
+  std::vector<int> v, ptr, ref;
+  auto local = [&](int g) { return int(std::lower_bound(isl.bodies.begin(), isl.bodies.end(), g) - isl.bodies.begin()); };
+  switch (kind) {
+    case 1: v = isl.bodies; break;
+    case 2:
+      for (int jq : isl.joints) {
+        const OJoint& j = w->joints[jq];
+        v.push_back(j.law); v.push_back(local(j.a)); v.push_back(local(j.b));
+      }
+      break;
+    case 3: v = isl.order; break;
+    case 4: bake_incidence(isl, w->joints, ptr, ref); v = ptr; break;
+    case 5: bake_incidence(isl, w->joints, ptr, ref); v = ref; break;
+    case 7: v = isl.joints; break;
+    default: return -1;
+  }
+  if ((int)v.size() > cap) return -1;
+  std::copy(v.begin(), v.end(), out);
+  return (int)v.size();
 }
 
 // ── stage-level checks ──────────────────────────────────────────────────────

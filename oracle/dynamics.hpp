@@ -207,6 +207,28 @@ inline std::vector<Island> build_islands(int n_bodies, const std::vector<OJoint>
   return out;
 }
 
+// bake_incidence (crates/newton/src/accelerator/mod.rs:289-331; the solver cache's gather terms
+// follow the same order, integrator/implicit/cache.rs:885-897): per island body, the joint wrench
+// slots flowing into its total, in joint traversal order, end a (slot 0) before end b (slot 1).
+// CSR over island bodies: ptr[q] .. ptr[q+1] index `ref`, each entry island joint * 2 + slot.
+inline void bake_incidence(const Island& isl, const std::vector<OJoint>& joints, std::vector<int>& ptr,
+                           std::vector<int>& ref) {
+  const int n = (int)isl.bodies.size();
+  auto local = [&](int g) { return int(std::lower_bound(isl.bodies.begin(), isl.bodies.end(), g) - isl.bodies.begin()); };
+  std::vector<std::vector<int>> acc(n);
+  for (size_t q = 0; q < isl.joints.size(); ++q) {
+    const OJoint& j = joints[isl.joints[q]];
+    acc[local(j.a)].push_back(2 * (int)q + 0);
+    acc[local(j.b)].push_back(2 * (int)q + 1);
+  }
+  ptr.assign(1, 0);
+  ref.clear();
+  for (int q = 0; q < n; ++q) {
+    ref.insert(ref.end(), acc[q].begin(), acc[q].end());
+    ptr.push_back((int)ref.size());
+  }
+}
+
 // ── Explicit integrators (integrator/explicit/*.rs) ─────────────────────────
 inline void integrate_explicit(int scheme, OBody& b, const Wrench<double>& w_body, double dt) {
   if (b.kinematic) return;

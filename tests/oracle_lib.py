@@ -34,6 +34,8 @@ def lib():
         L.orc_world_energy.restype = ctypes.c_double
         L.orc_world_energy.argtypes = [ctypes.c_void_p]
         L.orc_world_island_count.argtypes = [ctypes.c_void_p]
+        L.orc_world_island_structure.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                 ctypes.c_int]
         L.orc_world_island_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int)]
         L.orc_power.restype = ctypes.c_double
@@ -91,6 +93,20 @@ class OracleWorld:
             lib().orc_world_island_stats(self.h, k, ctypes.byref(s), ctypes.byref(it))
             out.append((s.value, it.value))
         return out
+
+    STRUCT_KINDS = {"bodies": 1, "joint_ends": 2, "order": 3, "incidence_ptr": 4, "incidence": 5, "joints": 7}
+
+    def island_count(self):
+        return lib().orc_world_island_count(self.h)
+
+    def island_structure(self, island, kind):
+        """The oracle's restatement of one island map (islands, order, bake_incidence)."""
+        cap = 8 * (len(self._b) + 3 * len(self._j)) + 8
+        out = np.zeros(cap, dtype=np.int32)
+        n = lib().orc_world_island_structure(self.h, int(island), self.STRUCT_KINDS[kind], p(out), cap)
+        assert n >= 0
+        out = out[:n]
+        return out.reshape(-1, 3) if kind == "joint_ends" else out
 
     def __del__(self):
         try:

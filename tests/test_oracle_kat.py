@@ -404,3 +404,27 @@ def test_uniform_field_applies_m_times_accel_and_ignores_kinematic(oracle):
     w2.step(10)
     mom = w2.bodies()[0]["momentum"]
     assert np.allclose(mom[:3], np.array(a) * m * dt * 10, rtol=1e-9, atol=1e-12)
+
+
+def test_bake_incidence_order_known_answer(oracle):
+    """bake_incidence (crates/newton/src/accelerator/mod.rs:289-331): per body, the joint wrench
+    slots in joint traversal order, end a (slot 0) before end b (slot 1); the cache's `order`
+    enumerates the dynamic bodies in island order (integrator/implicit/cache.rs:566-573)."""
+    from exgame_b200.abi import BODY_DTYPE, JOINT_DTYPE, NEWTON, step_params
+    bodies = np.zeros(4, dtype=BODY_DTYPE)
+    bodies["pose"][:, 0] = 1.0
+    bodies["mass"] = 1.0
+    bodies["inertia"][:, [0, 4, 8]] = 1.0
+    bodies["diagonal"] = 1
+    bodies["kinematic"][1] = 1
+    joints = np.zeros(4, dtype=JOINT_DTYPE)
+    for k, (a, b) in enumerate(((0, 1), (1, 2), (2, 0), (3, 2))):
+        joints[k]["law"], joints[k]["a"], joints[k]["b"] = 3, a, b
+        joints[k]["params"][0] = 1.0
+    ow = oracle.OracleWorld(bodies, joints, step_params(integrator=NEWTON))
+    assert ow.island_count() == 1
+    assert list(ow.island_structure(0, "incidence_ptr")) == [0, 2, 4, 7, 8]
+    # body 0: j0.a, j2.b; body 1: j0.b, j1.a; body 2: j1.b, j2.a, j3.b; body 3: j3.a
+    assert list(ow.island_structure(0, "incidence")) == [0, 5, 1, 2, 3, 4, 7, 6]
+    assert list(ow.island_structure(0, "order")) == [0, -1, 1, 2]
+    assert ow.island_structure(0, "joint_ends").tolist() == [[3, 0, 1], [3, 1, 2], [3, 2, 0], [3, 3, 2]]

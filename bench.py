@@ -228,16 +228,19 @@ def make_worlds(dev, parts):
     return ws
 
 
-def plain_path(dev, parts, flush, passes=1):
+def plain_path(dev, parts, flush, passes=1, reference_matrix=False):
     """The plain path: every world FP64 and alone, one world per launch (a step of the workload is
-    one exg_world_step per world). Returns body-steps/s over `passes` passes after one warm pass."""
+    one exg_world_step per world). Returns body-steps/s over `passes` passes after one warm pass.
+    The Newton matrix is the batch's own unless `reference_matrix` (the reference's -half^2 pose
+    factor, which converges in more iterations to the same step)."""
     import torch
     stream = torch.cuda.ExternalStream(dev.stream())
     worlds = []
     for b, j, p in parts:
         q = p.copy()
         q["precision"] = PRECISION_F64
-        q["newton_flags"] = 0  # the reference's Newton matrix
+        if reference_matrix:
+            q["newton_flags"] = 0
         worlds.append(_lib.DeviceWorld(dev, b, j, q))
     for w in worlds:
         w.step(1)
@@ -414,11 +417,16 @@ def run_ours(args, rank, world_size, local_rank):
     plain = None
     if args.plain and len(parts) > 1:
         plain = {"value": plain_path(dev, parts, flush), "unit": METRIC,
-                 "sample": "every world FP64 with the reference's Newton matrix, stepped alone, one exg_world_step "
-                           "per world, one pass after a warm pass (device time, L2 flushed before the pass)"}
+                 "sample": "every world FP64 with the batch's Newton matrix, stepped alone, one exg_world_step "
+                           "per world, one pass after a warm pass (device time, L2 flushed before the pass)",
+                 "reference_matrix": {
+                     "value": plain_path(dev, parts, flush, reference_matrix=True), "unit": METRIC,
+                     "sample": "the same with the reference's Newton matrix (pose factor -half^2), which takes more "
+                               "Newton iterations to the same converged step"}}
+    err = error_vs_oracle(dev, parts, args.error_steps) if args.error_steps > 0 and rank == 0 else None
     return {
         "value": value, "t": t, "e2e": e2e, "roofline": roofline, "cfg": cfg, "launches": launches,
-        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain, "dev": dev, "tuning": tuning,
+        "clocks": clk.summary(), "n_bodies": n_bodies, "plain": plain, "dev": dev, "tuning": tuning, "error": err,
     }
 
 
@@ -512,28 +520,99 @@ def serve_sweep(dev, rates, n_requests, pool_size, tick, rank):
                                 "measured alone (device time)"}
 
 
+def error_vs_oracle(dev, parts, steps):
+    """The timed path's error against the f64 oracle on a sample of the workload's worlds: the same
+    worlds with the same parameters in a batch of their own (a world steps bit for bit the same in
+    every batch), `steps` steps on the device and in the oracle from the same initial state. Per
+    world: pose error per body relative to max(1, |pose|), the worst body; momentum relative to the
+    world's largest |p|; energy of the two states by the oracle's energy function."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    oracle_lib.lib().orc_set_threads(os.cpu_count() or 1)
+    grav = [k for k, (b, _, p) in enumerate(parts) if int(p["integrator"]) != NEWTON and len(b) <= 1024]
+    tree = [k for k, (b, _, p) in enumerate(parts) if int(p["integrator"]) == NEWTON and len(b) <= 48]
+    if len(parts) <= 2:  # single-world workloads: the worlds themselves when small enough
+        grav = [k for k, (b, _, p) in enumerate(parts) if len(b) <= 4096]
+        tree = []
+    pick = []
+    for sel in (grav, tree):
+        sel = sorted(sel, key=lambda k: len(parts[k][0]))
+        if sel:
+            pick += [sel[int(round(q * (len(sel) - 1)))] for q in (0.0, 0.5, 0.8, 1.0)]
+    pick = sorted(set(pick))
+    if not pick:
+        return None
+    sample = [parts[k] for k in pick]
+    batch = _lib.DeviceBatch(dev, sample)
+    batch.step(steps)
+    got = [batch.world_bodies(i) for i in range(len(sample))]
+    batch.close()
+    t0 = time.perf_counter()
+    ows = []
+    for b, j, p in sample:
+        q = p.copy()
+        q["precision"] = PRECISION_F64
+        ows.append(oracle_lib.OracleWorld(b, j, q))
+    oracle_lib.worlds_step(ows, steps)
+    t_orc = time.perf_counter() - t0
+    worst = {"pose_rel": 0.0, "momentum_rel": 0.0, "energy_rel": 0.0}
+    per = []
+    for (b, j, p), g, ow in zip(sample, got, ows):
+        want = ow.bodies()
+        pose = float((np.abs(g["pose"] - want["pose"]).max(axis=1) /
+                      np.maximum(1.0, np.abs(want["pose"]).max(axis=1))).max())
+        pm = float(np.abs(want["momentum"]).max())
+        mom = float(np.abs(g["momentum"] - want["momentum"]).max() / max(pm, 1e-300))
+        e_w = ow.energy()
+        e_g = oracle_lib.OracleWorld(g, j, ow._p).energy()
+        en = abs(e_g - e_w) / max(abs(e_w), 1e-300)
+        per.append({"bodies": len(b), "kind": "tree" if int(p["integrator"]) == NEWTON else "gravity",
+                    "pose_rel": pose, "momentum_rel": mom, "energy_rel": en})
+        for k, v in (("pose_rel", pose), ("momentum_rel", mom), ("energy_rel", en)):
+            worst[k] = max(worst[k], v)
+    return dict(worst, steps=steps, tolerance_pose_rel=1e-6, within=worst["pose_rel"] <= 1e-6, worlds=per,
+                oracle_seconds=t_orc,
+                sample="worlds of the timed workload (gravity up to 1024 bodies, trees up to 48 bodies, at the "
+                       "0/50/80/100 % size quantiles of each kind), the timed path's precision and Newton matrix, "
+                       "in a batch of their own, against the f64 oracle from the same initial state")
+
+
+def oracle_sample(parts):
+    """The CPU legs' bounded sample of a large batch: every 16th world in size order, so the sample
+    has the batch's size distribution. Returns (worlds, description)."""
+    if len(parts) <= 64:
+        return parts, "the whole workload"
+    order = sorted(range(len(parts)), key=lambda k: (len(parts[k][0]), k))
+    pick = sorted(order[8::16])
+    sample = [parts[k] for k in pick]
+    nb = sum(len(b) for b, _, _ in sample)
+    tot = sum(len(b) for b, _, _ in parts)
+    return sample, (f"{len(sample)} of {len(parts)} worlds (every 16th in size order), {nb} of {tot} bodies "
+                    f"({100.0 * nb / tot:.2f} %)")
+
+
 def cpu_baseline(args, threads):
-    """The oracle (C++ f64 restatement) on a bounded sample of the same workload."""
+    """The oracle (C++ f64 restatement) on a bounded sample of the same workload, worlds spread over
+    the host threads (OpenMP, largest first)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
     L = oracle_lib.lib()
     L.orc_set_threads(int(threads))
     parts, cfg = workload(args.workload, 0)
-    if len(parts) > 64:  # a bounded sample: every 16th world of the batch
-        parts = parts[::16]
+    parts, desc = oracle_sample(parts)
+    parts = sorted(parts, key=lambda x: -len(x[0]))
     worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
     n = sum(w.n for w in worlds)
     budget = args.cpu_seconds
     steps, t0 = 0, time.perf_counter()
     while True:
-        for w in worlds:
-            w.step(1)
+        oracle_lib.worlds_step(worlds, 1)
         steps += 1
         el = time.perf_counter() - t0
         if el >= budget or steps >= 100000:
             break
     return {"value": n * steps / el, "unit": METRIC, "cores": int(threads), "kind": "port",
-            "sample": f"{steps} steps of the same workload ({n} bodies) on {threads} host thread(s), {el:.1f} s"}
+            "sample": f"{steps} steps of {desc}, on {threads} host threads (worlds in parallel), {el:.1f} s"}
 
 
 def main():
@@ -556,6 +635,8 @@ def main():
     ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--error-steps", type=int, default=1000,
+                    help="steps of the sampled worlds compared with the f64 oracle after the run (0: skip)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -571,19 +652,14 @@ def main():
         import oracle_lib
         oracle_lib.lib().orc_set_threads(threads)
         parts, cfg = workload(args.workload, 0)
-        sample = f"{args.steps} timed steps after {args.warmup} warm-up steps"
-        if len(parts) > 64:  # a bounded sample: every 16th world of the batch
-            parts = parts[::16]
-            sample += ", every 16th world of the batch"
+        parts, desc = oracle_sample(parts)
+        parts = sorted(parts, key=lambda x: -len(x[0]))  # largest first over the threads
+        sample = f"{args.steps} timed steps after {args.warmup} warm-up steps of {desc}, worlds in parallel"
         worlds = [oracle_lib.OracleWorld(b, j, p) for (b, j, p) in parts]
         n = sum(w.n for w in worlds)
-        for _ in range(args.warmup):
-            for w in worlds:
-                w.step(1)
+        oracle_lib.worlds_step(worlds, args.warmup)
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            for w in worlds:
-                w.step(1)
+        oracle_lib.worlds_step(worlds, args.steps)
         el = time.perf_counter() - t0
         v = n * args.steps / el
         line = {"metric": METRIC, "value": v, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
@@ -603,7 +679,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     r = run_ours(args, rank, world_size, local_rank)
-    cpu = cpu_baseline(args, 1) if rank == 0 and world_size == 1 else None
+    cpu = cpu_baseline(args, threads) if rank == 0 and world_size == 1 else None
     serving = None
     if rank == 0 and world_size == 1 and args.serve_rates:
         rates = [float(x) for x in args.serve_rates.split(",") if x]
@@ -618,7 +694,7 @@ def main():
                                                   else f"replicas x{world_size} (independent worlds)"),
                            l2="flushed between timed steps (256 MB write)"),
             "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "cpu_baseline": cpu,
-            "clocks": r["clocks"], "plain_path": r["plain"], "serving": serving,
+            "clocks": r["clocks"], "plain_path": r["plain"], "serving": serving, "error_vs_oracle": r["error"],
         }
         print(json.dumps(line))
     if world_size > 1:

@@ -63,6 +63,25 @@ void* orc_world_create(const exg_body_t* bodies, int n_bodies, const exg_joint_t
   return w;
 }
 void orc_world_destroy(void* h) { delete static_cast<OWorld*>(h); }
+// Step n_worlds independent worlds `steps` times each on the oracle's threads: worlds of at least
+// kBigWorld bodies one after another, each using every thread inside (gravity rows, islands,
+// joints), then the smaller worlds spread over the threads one world per thread (largest first).
+void orc_worlds_step(void** handles, int n_worlds, int steps) {
+  constexpr size_t kBigWorld = 512;
+  const int nt = oracle_threads();
+  std::vector<OWorld*> big, small;
+  for (int k = 0; k < n_worlds; ++k) {
+    OWorld* w = static_cast<OWorld*>(handles[k]);
+    (w->bodies.size() >= kBigWorld ? big : small).push_back(w);
+  }
+  std::stable_sort(small.begin(), small.end(), [](OWorld* a, OWorld* b) { return a->bodies.size() > b->bodies.size(); });
+  for (OWorld* w : big)
+    for (int s = 0; s < steps; ++s) w->step();
+  const int ns = (int)small.size();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) if (nt > 1 && ns > 1)
+  for (int k = 0; k < ns; ++k)
+    for (int s = 0; s < steps; ++s) small[k]->step();
+}
 void orc_world_step(void* h, int n) { OWorld* w = static_cast<OWorld*>(h); for (int s = 0; s < n; ++s) w->step(); }
 void orc_world_get_bodies(void* h, exg_body_t* out) {
   OWorld* w = static_cast<OWorld*>(h);

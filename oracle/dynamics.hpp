@@ -23,7 +23,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
-#include <thread>
+#include <omp.h>
 #include <vector>
 #include "laws.hpp"
 
@@ -111,7 +111,10 @@ struct GravityParams { int law; double G; double eps; };
 // Per-body world force from every other body, summed in slot order (gravity.rs:530-587,
 // 438-450). SIZE_CORE: the reference law with the higher-slot body's size as the core.
 // PLUMMER: F = G m_i m_j (p_j - p_i) / (r^2 + eps^2)^(3/2).
-// Host threads the oracle's O(N^2) gravity loop may use (the CPU baseline runs it on every core).
+// Host threads the oracle may use (OpenMP): over gravity rows, over the islands of a world, over
+// an island's joints and bodies, and over worlds (orc_worlds_step). Every parallel loop writes
+// disjoint outputs and every reduction runs serially in index order afterwards, so results do not
+// depend on the thread count.
 inline int& oracle_threads() { static int t = 1; return t; }
 
 inline void gravity_forces(const std::vector<OBody>& bodies, const GravityParams& gp, std::vector<V3<double>>& force) {
@@ -120,9 +123,10 @@ inline void gravity_forces(const std::vector<OBody>& bodies, const GravityParams
   if (gp.law == GRAVITY_OFF) return;
   std::vector<V3<double>> pos(n);
   for (size_t i = 0; i < n; ++i) pos[i] = body_position(bodies[i]);
-  int nt = std::max(1, std::min<int>(oracle_threads(), (int)n));
-  auto rows = [&](size_t lo, size_t hi) {
-  for (size_t i = lo; i < hi; ++i) {
+  const int nt = std::max(1, std::min<int>(oracle_threads(), (int)n));
+#pragma omp parallel for schedule(static) num_threads(nt) if (nt > 1 && !omp_in_parallel())
+  for (long long ii = 0; ii < (long long)n; ++ii) {
+    const size_t i = (size_t)ii;
     if (bodies[i].kinematic) continue;
     double mi = bodies[i].mass;
     V3<double> acc;
@@ -145,11 +149,6 @@ inline void gravity_forces(const std::vector<OBody>& bodies, const GravityParams
     }
     force[i] = acc;
   }
-  };
-  if (nt == 1) { rows(0, n); return; }
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t) pool.emplace_back(rows, n * t / nt, n * (t + 1) / nt);
-  for (auto& th : pool) th.join();
 }
 
 inline double gravity_potential(const std::vector<OBody>& bodies, const GravityParams& gp) {
@@ -157,8 +156,13 @@ inline double gravity_potential(const std::vector<OBody>& bodies, const GravityP
   size_t n = bodies.size();
   std::vector<V3<double>> pos(n);
   for (size_t i = 0; i < n; ++i) pos[i] = body_position(bodies[i]);
-  double e = 0.0;
-  for (size_t i = 0; i < n; ++i)
+  // per-row sums in parallel, then the rows in order
+  std::vector<double> row(n, 0.0);
+  const int nt = std::max(1, std::min<int>(oracle_threads(), (int)n));
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nt) if (nt > 1 && !omp_in_parallel())
+  for (long long ii = 0; ii < (long long)n; ++ii) {
+    const size_t i = (size_t)ii;
+    double e = 0.0;
     for (size_t j = i + 1; j < n; ++j) {
       if (bodies[i].kinematic || bodies[j].kinematic) continue;
       V3<double> r = pos[j] - pos[i];
@@ -169,6 +173,10 @@ inline double gravity_potential(const std::vector<OBody>& bodies, const GravityP
         e -= d >= s ? mm / d : mm * (3.0 * s * s - r2) / (2.0 * s * s * s);
       }
     }
+    row[i] = e;
+  }
+  double e = 0.0;
+  for (size_t i = 0; i < n; ++i) e += row[i];
   return e;
 }
 
@@ -297,6 +305,38 @@ inline bool block_inverse(const Block& a, Block& inv) {
   return true;
 }
 
+
+// Block-sparse matrix over the island's dynamic bodies: per row, the blocks of the columns in its
+// sparsity pattern (the row itself and its joint neighbours, cache.rs:712-724), columns ascending.
+// Absent blocks read as zero, so the dense loops of the solvers below read it unchanged while a
+// tree island of m bodies stores O(m) blocks instead of m^2.
+struct SparseBlocks {
+  int m = 0;
+  std::vector<std::vector<int>> cols;
+  std::vector<std::vector<Block>> vals;
+  void init(int m_, const std::vector<std::vector<int>>& pattern) {
+    m = m_;
+    cols.assign(m, {});
+    vals.assign(m, {});
+    for (int i = 0; i < m; ++i) {
+      cols[i] = pattern[i];
+      std::sort(cols[i].begin(), cols[i].end());
+      vals[i].assign(cols[i].size(), zero_block());
+    }
+  }
+  const Block* find(int i, int j) const {
+    const std::vector<int>& c = cols[i];
+    auto it = std::lower_bound(c.begin(), c.end(), j);
+    return (it != c.end() && *it == j) ? &vals[i][it - c.begin()] : nullptr;
+  }
+  Block& at(int i, int j) { return const_cast<Block&>(*find(i, j)); }  // (i, j) in the pattern
+  const Block& get(int i, int j) const {
+    static const Block zero = zero_block();
+    const Block* b = find(i, j);
+    return b ? *b : zero;
+  }
+};
+
 // functions/src/lib.rs:170-247 — world mass block, residual rhs = -R and self-scale.
 inline void body_post(const OBody& b, const Motor<double>& pose_mid, const Twist<double>& solve_vel, const Wrench<double>& snap_mom,
                       const Wrench<double>& total, double half, double floor2, Block& block, double rhs[6], double scale[6]) {
@@ -354,7 +394,7 @@ struct NewtonIsland {
   std::vector<double> rhs, scale;               // 6 per dynamic body
   std::vector<double> jac;                      // 300 per island joint
   std::vector<Block> lane0_mass;                // the mass blocks lane 0 last wrote
-  std::vector<Block> A;                         // last assembled system (dense m*m for NS / exact dense)
+  SparseBlocks A;                               // last assembled system, block-sparse
   std::vector<std::vector<int>> nbrs;           // sparsity (cache.rs:712-724)
   double a_norm2 = 0.0;
   bool have_A = false;
@@ -375,7 +415,10 @@ struct NewtonIsland {
     size_t nj = isl.joints.size();
     std::vector<double> conn(nj * 12);
     if (with_jac) jac.resize(nj * 300);
-    for (size_t q = 0; q < nj; ++q) {
+    const int nt = oracle_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt) if (nt > 1 && nj > 64 && !omp_in_parallel())
+    for (long long qq = 0; qq < (long long)nj; ++qq) {
+      const size_t q = (size_t)qq;
       const OJoint& j = joints[isl.joints[q]];
       int la = local_of(j.a), lb = local_of(j.b);
       double pa[8], pb[8], va[6], vb[6];
@@ -399,11 +442,16 @@ struct NewtonIsland {
     int m = isl.m;
     mass_out.resize(m); rhs_out.resize(6 * m); scale_out.resize(6 * m);
     double floor2 = 1e-9 * 1e-9;
-    double worst = 0.0;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt) if (nt > 1 && n > 64 && !omp_in_parallel())
     for (int q = 0; q < n; ++q) {
       int i = isl.order[q];
       if (i < 0) continue;
       body_post(bodies[isl.bodies[q]], mid[q], vmid[q], snap[q], total[q], half, floor2, mass_out[i], &rhs_out[6 * i], &scale_out[6 * i]);
+    }
+    double worst = 0.0;
+    for (int q = 0; q < n; ++q) {
+      int i = isl.order[q];
+      if (i < 0) continue;
       const double* r = &rhs_out[6 * i];
       double lin2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
       double ang2 = r[3] * r[3] + r[4] * r[4] + r[5] * r[5];
@@ -433,8 +481,8 @@ struct NewtonIsland {
   // (pf * pose columns + vf * velocity columns), pf = -half^2, vf = -half.
   void assemble(double half) {
     int m = isl.m;
-    A.assign((size_t)m * m, zero_block());
-    for (int i = 0; i < m; ++i) A[(size_t)i * m + i] = lane0_mass[i];
+    A.init(m, nbrs);
+    for (int i = 0; i < m; ++i) A.at(i, i) = lane0_mass[i];
     double pf = -(half * half) * (wp.exact_pose_factor ? 0.5 : 1.0), vf = -half;
     for (size_t q = 0; q < isl.joints.size(); ++q) {
       const OJoint& j = joints[isl.joints[q]];
@@ -443,7 +491,7 @@ struct NewtonIsland {
         if (ends[re] < 0) continue;
         for (int ce = 0; ce < 2; ++ce) {
           if (ends[ce] < 0) continue;
-          Block& out = A[(size_t)ends[re] * m + ends[ce]];
+          Block& out = A.at(ends[re], ends[ce]);
           for (int col = 0; col < 6; ++col)
             for (int r = 0; r < 6; ++r) {
               int comp = re * 6 + r;
@@ -455,7 +503,8 @@ struct NewtonIsland {
       }
     }
     a_norm2 = 0.0;
-    for (const Block& b : A) a_norm2 += fro2(b);
+    for (int i = 0; i < m; ++i)  // row-major over (i, j): absent (zero) blocks add nothing
+      for (const Block& b : A.vals[i]) a_norm2 += fro2(b);
     have_A = true;
   }
 
@@ -477,12 +526,12 @@ struct NewtonIsland {
     if (tree) {
       std::vector<Block> D(m), Dinv(m);
       std::vector<double> b(rhs_in);
-      for (int i = 0; i < m; ++i) D[i] = A[(size_t)i * m + i];
+      for (int i = 0; i < m; ++i) D[i] = A.get(i, i);
       for (int h = m - 1; h >= 1; --h) {  // leaves first
         int i = bfs[h], p = parent[i];
         if (!block_inverse(D[i], Dinv[i])) return false;
-        const Block& Api = A[(size_t)p * m + i];
-        const Block& Aip = A[(size_t)i * m + p];
+        const Block& Api = A.get(p, i);
+        const Block& Aip = A.get(i, p);
         Block S = zero_block();  // Api * Dinv_i
         block_mul_acc(S, Api, Dinv[i]);
         Block T = zero_block();
@@ -496,7 +545,7 @@ struct NewtonIsland {
         double y[6];
         for (int r = 0; r < 6; ++r) y[r] = b[6 * i + r];
         if (p >= 0) {
-          const Block& Aip = A[(size_t)i * m + p];
+          const Block& Aip = A.get(i, p);
           for (int r = 0; r < 6; ++r) { double s = 0.0; for (int c = 0; c < 6; ++c) s += Aip[r * 6 + c] * dv[6 * p + c]; y[r] -= s; }
         }
         for (int r = 0; r < 6; ++r) { double s = 0.0; for (int c = 0; c < 6; ++c) s += Dinv[i][r * 6 + c] * y[c]; dv[6 * i + r] = s; }
@@ -506,7 +555,7 @@ struct NewtonIsland {
     int n = 6 * m;
     std::vector<double> a((size_t)n * n), x(rhs_in);
     for (int bi = 0; bi < m; ++bi) for (int bj = 0; bj < m; ++bj)
-      for (int r = 0; r < 6; ++r) for (int c = 0; c < 6; ++c) a[(size_t)(6 * bi + r) * n + 6 * bj + c] = A[(size_t)bi * m + bj][r * 6 + c];
+      for (int r = 0; r < 6; ++r) for (int c = 0; c < 6; ++c) a[(size_t)(6 * bi + r) * n + 6 * bj + c] = A.get(bi, bj)[r * 6 + c];
     for (int k = 0; k < n; ++k) {
       int piv = k; double best = std::fabs(a[(size_t)k * n + k]);
       for (int r = k + 1; r < n; ++r) if (std::fabs(a[(size_t)r * n + k]) > best) { best = std::fabs(a[(size_t)r * n + k]); piv = r; }
@@ -531,8 +580,8 @@ struct NewtonIsland {
     for (int i = 0; i < m; ++i) {
       double row = 0.0, col = 0.0;
       for (int j = 0; j < m; ++j) {
-        const Block& rb = A[(size_t)i * m + j];
-        const Block& cb = A[(size_t)j * m + i];
+        const Block& rb = A.get(i, j);
+        const Block& cb = A.get(j, i);
         for (int k = 0; k < 36; ++k) { row += std::fabs(rb[k]); col += std::fabs(cb[k]); }
       }
       inf = (inf > row) ? inf : row;
@@ -542,7 +591,7 @@ struct NewtonIsland {
     isl.X.assign((size_t)m * m, zero_block());
     for (int i = 0; i < m; ++i)
       for (int j = 0; j < m; ++j) {
-        const Block& src = A[(size_t)j * m + i];
+        const Block& src = A.get(j, i);
         Block& dst = isl.X[(size_t)i * m + j];
         for (int r = 0; r < 6; ++r) for (int c = 0; c < 6; ++c) dst[r * 6 + c] = src[c * 6 + r] * s;
       }
@@ -554,7 +603,7 @@ struct NewtonIsland {
     for (int i = 0; i < m; ++i)
       for (int j = 0; j < m; ++j) {
         Block acc = zero_block();
-        for (int k : nbrs[i]) block_mul_acc(acc, A[(size_t)i * m + k], isl.X[(size_t)k * m + j]);
+        for (int k : nbrs[i]) block_mul_acc(acc, A.get(i, k), isl.X[(size_t)k * m + j]);
         R[(size_t)i * m + j] = acc;
       }
     double contraction = 0.0;
@@ -792,8 +841,10 @@ struct OWorld {
       }
     }
     if (wp.integrator == NEWTON) {
-      for (Island& isl : islands) {
-        NewtonIsland ni(bodies, joints, isl, wp, external);
+      const int nt = oracle_threads(), ni_count = (int)islands.size();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) if (nt > 1 && ni_count > 1 && !omp_in_parallel())
+      for (int k = 0; k < ni_count; ++k) {
+        NewtonIsland ni(bodies, joints, islands[k], wp, external);
         ni.step(wp.dt);
       }
       return;

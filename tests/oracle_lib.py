@@ -30,6 +30,7 @@ def lib():
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_world_destroy.argtypes = [ctypes.c_void_p]
         L.orc_world_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_worlds_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_world_get_bodies.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_world_energy.restype = ctypes.c_double
         L.orc_world_energy.argtypes = [ctypes.c_void_p]
@@ -113,6 +114,12 @@ class OracleWorld:
             lib().orc_world_destroy(self.h)
         except Exception:
             pass
+
+
+def worlds_step(worlds, steps):
+    """Step independent oracle worlds `steps` times, spread over the oracle's threads (OpenMP)."""
+    hs = (ctypes.c_void_p * len(worlds))(*[w.h for w in worlds])
+    lib().orc_worlds_step(hs, len(worlds), int(steps))
 
 
 def twist_exp(t, dt=1.0):

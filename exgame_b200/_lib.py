@@ -76,6 +76,7 @@ SIGNATURES = {
     "exg_pool_steps_left": (ctypes.c_int, [_vp, _vp, ctypes.c_int32]),
     "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
     "exg_world_island_count": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+    "exg_batch_set_epoch": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double]),
     "exg_world_island_structure": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp,
                                                   ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
@@ -296,6 +297,10 @@ class DeviceWorld:
         """Replace the joints of `world` (0 for a single world; a batch index or pool slot)."""
         j = np.ascontiguousarray(joints, dtype=JOINT_DTYPE)
         check(lib().exg_batch_set_joints(self.handle, int(world), ptr(j), len(j)), "exg_batch_set_joints")
+
+    def set_epoch(self, dt, warp=1.0, world=0):
+        """dt and warp of `world` for the following steps (Epoch::standalone(dt, warp))."""
+        check(lib().exg_batch_set_epoch(self.handle, int(world), float(dt), float(warp)), "exg_batch_set_epoch")
 
     def set_state(self, state):
         st = np.ascontiguousarray(state, dtype=np.float64)

@@ -1064,6 +1064,21 @@ int exg_world_phase_cycles(exg_world_t W, int64_t out[8]) {
   return rc;
 }
 
+int exg_batch_set_epoch(exg_world_t W, int32_t world, double dt, double warp) {
+  if (!W || !(dt > 0.0) || !std::isfinite(dt) || !(warp >= 1.0) || !std::isfinite(warp)) return EXG_ERR_INVALID_ARGUMENT;
+  HandleLock lock(W);
+  if (world < 0 || world >= W->w_cap || !W->slots[world].used) return EXG_ERR_INVALID_ARGUMENT;
+  EXG_CUDA_TRY(cudaSetDevice(W->dev->ordinal));
+  exg_step_params_t p = W->slots[world].params;
+  p.dt = dt;
+  p.warp = warp;
+  int rc = put(W, W->w.wparams, world, &p, 1);
+  if (rc != EXG_OK) return rc;
+  W->slots[world].params = p;
+  W->w.h_params[world] = p;
+  return EXG_OK;
+}
+
 int exg_world_island_count(exg_world_t W, int32_t world, int32_t* n_islands) {
   if (!W || !n_islands) return EXG_ERR_INVALID_ARGUMENT;
   HandleLock lock(W);

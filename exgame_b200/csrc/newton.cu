@@ -16,6 +16,7 @@
 #include <cstring>
 #include <functional>
 #include <new>
+#include <set>
 #include "body.cuh"
 #include "newton_ops.cuh"
 
@@ -105,8 +106,16 @@ __device__ void copy_mass0(const Ctx& c) {
 template <bool MIXED>
 __device__ double phase_assemble(const Ctx& c, double half, double* red) {
   double sumsq = 0.0;
-  const int cells = 3 * c.d.m;
   const double pf = -(half * half) * c.P.pose_factor_scale, vf = -half;
+  if (c.d.solver == 1) {
+    const int cells = c.d.m + 2 * c.d.n_slots;
+    for (int t = threadIdx.x; t < cells * 36; t += blockDim.x) {
+      const double acc = op_assemble_lu<MIXED>(c, pf, vf, t / 36, t % 36);
+      sumsq += acc * acc;
+    }
+    return block_sum(sumsq, red);
+  }
+  const int cells = 3 * c.d.m;
   for (int t = threadIdx.x; t < cells * 36; t += blockDim.x) {
     bool counts;
     double acc = op_assemble<MIXED>(c, pf, vf, t / 36, t % 36, &counts);
@@ -115,9 +124,75 @@ __device__ double phase_assemble(const Ctx& c, double half, double* red) {
   return block_sum(sumsq, red);
 }
 
+// Exact solve of A dv = rhs by block LU on the island's elimination order (solver 1: dynamic
+// cycles). Level by level from the first eliminated nodes (left-looking: a node's row, column and
+// diagonal blocks receive every product of the lower levels in a fixed order, one warp per target
+// block), then per node the pivot inverse D^-1 and the scaled column S = A(j, k) D_k^-1 in place;
+// the right-hand side follows the same updates (b_k -= S_kp y_p). Back substitution from the last
+// level: x_k = D_k^-1 (y_k - sum_j A(k, j) x_j). Returns false if a pivot block is singular (dv is
+// then NaN, which the line search rejects).
+__device__ bool phase_solve_lu(const Ctx& c, int* flag) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = c.d.m;
+  const int* lv = c.A.lv_ptr + c.d.lv_off;
+  const int* nodes = c.A.lv_nodes + c.d.dyn_off;
+  const int* lg = c.A.gn_lgrp + c.d.gen_lv_off;
+  const int* rp = c.A.gn_rop_ptr + c.d.gen_off;
+  const int* sp = c.A.gn_slot_ptr + c.d.gen_off;
+  const int* scol = c.A.gn_slot_col + c.d.gen_slot_off;
+  if (threadIdx.x == 0) *flag = 1;
+  for (int t = threadIdx.x; t < 6 * m; t += blockDim.x) c.s.bvec[t] = c.s.rhs[t];
+  __syncthreads();
+  for (int L = 0; L < c.d.n_levels; ++L) {
+    for (int g = lg[L] + warp; g < lg[L + 1]; g += kWarps) {
+      const int4 G = c.A.gn_grp[g];
+      double* tgt = lu_block(c, G.x);
+      for (int o = G.y; o < G.z; ++o) {
+        const int2 op = c.A.gn_ops[o];
+        warp_mm6<true>(lu_block(c, op.x), lu_block(c, op.y), tgt);
+      }
+    }
+    for (int u = lv[L] + warp; u < lv[L + 1]; u += kWarps) {
+      const int k = nodes[u];
+      for (int t = rp[k]; t < rp[k + 1]; ++t) {
+        const int2 op = c.A.gn_rops[t];
+        warp_mv6_sub(lu_block(c, op.x), c.s.bvec + 6 * (size_t)op.y, c.s.bvec + 6 * (size_t)k);
+      }
+    }
+    __syncthreads();
+    for (int u = lv[L] + warp; u < lv[L + 1]; u += kWarps) {
+      const int k = nodes[u];
+      const bool ok = warp_inverse6(lu_block(c, k), c.s.Dinv + 36 * (size_t)k);
+      if (!ok && lane == 0) *flag = 0;
+      for (int s = sp[k]; s < sp[k + 1]; ++s) {
+        double* lo = c.s.G + 72 * (size_t)s + 36;
+        warp_mm6<false>(lo, c.s.Dinv + 36 * (size_t)k, lo);
+      }
+    }
+    __syncthreads();
+  }
+  for (int L = c.d.n_levels - 1; L >= 0; --L) {
+    for (int u = lv[L] + warp; u < lv[L + 1]; u += kWarps) {
+      const int k = nodes[u];
+      for (int s = sp[k]; s < sp[k + 1]; ++s)
+        warp_mv6_sub(c.s.G + 72 * (size_t)s, c.s.dv + 6 * (size_t)scol[s], c.s.bvec + 6 * (size_t)k);
+      warp_mv6(c.s.Dinv + 36 * (size_t)k, c.s.bvec + 6 * (size_t)k, c.s.dv + 6 * (size_t)k);
+    }
+    __syncthreads();
+  }
+  bool ok = *flag != 0;
+  __syncthreads();
+  if (!ok) {
+    for (int t = threadIdx.x; t < 6 * m; t += blockDim.x) c.s.dv[t] = __longlong_as_double(0x7ff8000000000000ULL);
+    __syncthreads();
+  }
+  return ok;
+}
+
 // Exact solve of A dv = rhs on the island's elimination forest. Returns false if a pivot
 // block is singular (dv is then NaN, which the line search rejects).
 __device__ bool phase_solve(const Ctx& c, int* flag) {
+  if (c.d.solver == 1) return phase_solve_lu(c, flag);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = c.d.m;
   const int* lv = c.A.lv_ptr + c.d.lv_off;
@@ -355,6 +430,80 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDevi
 }  // namespace
 
 // ── host: island structure ────────────────────────────────────────────────────
+namespace {
+// Block LU plan of an island whose dynamic bodies form cycles. The elimination order is minimum
+// degree on the dynamic adjacency (ties to the lowest node), eliminating a node joining its
+// remaining neighbours into a clique (the fill). later[k] are k's neighbours eliminated after it
+// in the filled graph (by position); the elimination tree's parent is the first of them, and a
+// node's level is its height in that tree, so every node a node depends on sits on a lower level.
+struct BlockLuPlan {
+  std::vector<int> pos, parent, level, slot_first;
+  std::vector<std::vector<int>> later, contrib;  // contrib[k]: the p with k in later[p], by position
+  int n_levels = 0, n_slots = 0;
+  int slot(int k, int j) const {  // the slot of the pair (k, j), j in later[k]
+    const std::vector<int>& L = later[k];
+    int lo = 0, hi = (int)L.size();
+    while (lo < hi) {
+      int mid = (lo + hi) / 2;
+      if (pos[L[mid]] < pos[j]) lo = mid + 1; else hi = mid;
+    }
+    return slot_first[k] + lo;
+  }
+  bool has(int k, int j) const {
+    int s = slot(k, j) - slot_first[k];
+    return s < (int)later[k].size() && later[k][s] == j;
+  }
+};
+
+void plan_block_lu(int m, const std::vector<std::vector<int>>& adj, BlockLuPlan& P) {
+  std::vector<std::set<int>> nb(m);
+  for (int i = 0; i < m; ++i) nb[i].insert(adj[i].begin(), adj[i].end());
+  std::set<std::pair<int, int>> queue;  // (current degree, node)
+  for (int i = 0; i < m; ++i) queue.insert({(int)nb[i].size(), i});
+  P.pos.assign(m, -1);
+  P.later.assign(m, {});
+  std::vector<int> order;
+  order.reserve(m);
+  for (int step = 0; step < m; ++step) {
+    const int v = queue.begin()->second;
+    queue.erase(queue.begin());
+    P.pos[v] = step;
+    order.push_back(v);
+    std::vector<int> ns(nb[v].begin(), nb[v].end());
+    P.later[v] = ns;
+    for (int u : ns) {
+      queue.erase({(int)nb[u].size(), u});
+      nb[u].erase(v);
+    }
+    for (size_t a = 0; a < ns.size(); ++a)
+      for (size_t b = a + 1; b < ns.size(); ++b) {
+        nb[ns[a]].insert(ns[b]);
+        nb[ns[b]].insert(ns[a]);
+      }
+    for (int u : ns) queue.insert({(int)nb[u].size(), u});
+    nb[v].clear();
+  }
+  for (int k = 0; k < m; ++k)
+    std::sort(P.later[k].begin(), P.later[k].end(), [&](int a, int b) { return P.pos[a] < P.pos[b]; });
+  P.parent.assign(m, -1);
+  P.level.assign(m, 0);
+  P.n_levels = m > 0 ? 1 : 0;
+  for (int v : order) {
+    if (P.later[v].empty()) continue;
+    const int p = P.later[v][0];
+    P.parent[v] = p;
+    P.level[p] = std::max(P.level[p], P.level[v] + 1);
+    P.n_levels = std::max(P.n_levels, P.level[p] + 1);
+  }
+  P.slot_first.assign(m + 1, 0);
+  for (int k = 0; k < m; ++k) P.slot_first[k + 1] = P.slot_first[k] + (int)P.later[k].size();
+  P.n_slots = P.slot_first[m];
+  P.contrib.assign(m, {});
+  for (int v : order)
+    for (int j : P.later[v]) P.contrib[j].push_back(v);
+}
+}  // namespace
+
 long long newton_footprint_bytes(int nb, int nj) {
   // scratch, then the structure: 13 ints per body (body list, order, incidence pointers,
   // dynamic list, parents, levels, children, 3 assembly cells), 9 per joint plus its 10 params
@@ -378,6 +527,10 @@ NewtonWorld::~NewtonWorld() {
                          &d_queue})
     a->release();
   d_jl_params.release();
+  for (DevArr<int>* a : {&d_gn_lgrp, &d_gn_rop_ptr, &d_gn_slot_ptr, &d_gn_slot_col}) a->release();
+  d_gn_grp.release();
+  d_gn_ops.release();
+  d_gn_rops.release();
   d_scratch.release();
   d_residual.release();
   d_phase.release();
@@ -408,6 +561,10 @@ void NewtonWorld::compact() {
     v->clear();
   h_jl_params.clear();
   h_jl_id.clear();
+  for (std::vector<int>* v : {&h_gn_lgrp, &h_gn_rop_ptr, &h_gn_slot_ptr, &h_gn_slot_col}) v->clear();
+  h_gn_grp.clear();
+  h_gn_ops.clear();
+  h_gn_rops.clear();
   world_islands_.clear();
   scratch_alloc_.init(scratch_alloc_.capacity());
   n_live_ = 0;
@@ -418,6 +575,10 @@ void NewtonWorld::compact() {
                          &d_dn_parent, &d_lv_ptr, &d_lv_nodes, &d_ch_ptr, &d_ch_idx, &d_cell_ptr, &d_cell_terms})
     a->size = 0;
   d_jl_params.size = 0;
+  for (DevArr<int>* a : {&d_gn_lgrp, &d_gn_rop_ptr, &d_gn_slot_ptr, &d_gn_slot_col}) a->size = 0;
+  d_gn_grp.size = 0;
+  d_gn_ops.size = 0;
+  d_gn_rops.size = 0;
   dirty_ = true;
 }
 
@@ -450,7 +611,12 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
   std::vector<int> s_isl_body, s_jl_law, s_jl_a, s_jl_b, s_ib_order, s_ib_inc_ptr, s_ib_inc_ref, s_dn_body, s_dn_parent,
       s_lv_ptr, s_lv_nodes, s_ch_ptr, s_ch_idx, s_cell_ptr, s_cell_terms;
   std::vector<double> s_jl_params;
-  std::vector<int> s_jl_id;
+  std::vector<int> s_jl_id, s_gn_lgrp, s_gn_rop_ptr, s_gn_slot_ptr, s_gn_slot_col;
+  std::vector<int4> s_gn_grp;
+  std::vector<int2> s_gn_ops, s_gn_rops;
+  const int base_gn_lgrp = (int)h_gn_lgrp.size(), base_gn_ptr = (int)h_gn_rop_ptr.size(),
+            base_gn_slot = (int)h_gn_slot_col.size(), base_gn_grp = (int)h_gn_grp.size(),
+            base_gn_ops = (int)h_gn_ops.size(), base_gn_rops = (int)h_gn_rops.size();
   const int base_isl_body = (int)h_isl_body.size(), base_jl = (int)h_jl_law.size(), base_order = (int)h_ib_order.size(),
             base_inc_ptr = (int)h_ib_inc_ptr.size(), base_inc_ref = (int)h_ib_inc_ref.size(),
             base_dn = (int)h_dn_body.size(), base_lv = (int)h_lv_ptr.size(), base_ch_idx = (int)h_ch_idx.size(),
@@ -543,7 +709,109 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
       ++comps;
     }
     for (int q = 0; q < d.nb; ++q) local[B[q]] = -1;
-    if (edges != m - comps) return EXG_ERR_UNSUPPORTED;  // a cycle among the dynamic bodies
+    d.solver = 0;
+    d.n_slots = 0;
+    d.gen_off = d.gen_lv_off = d.gen_slot_off = 0;
+    if (edges != m - comps) {
+      // a cycle among the dynamic bodies: block LU on a minimum-degree order with fill
+      BlockLuPlan P;
+      plan_block_lu(m, adj, P);
+      d.solver = 1;
+      d.n_slots = P.n_slots;
+      d.n_levels = P.n_levels;
+      d.lv_off = base_lv + (int)s_lv_ptr.size();
+      std::vector<std::vector<int>> by(P.n_levels);
+      for (int i = 0; i < m; ++i) by[P.level[i]].push_back(i);
+      {
+        int acc = 0;
+        for (int L = 0; L < P.n_levels; ++L) {
+          s_lv_ptr.push_back(acc);
+          for (int i : by[L]) s_lv_nodes.push_back(i);
+          acc += (int)by[L].size();
+        }
+        s_lv_ptr.push_back(acc);
+      }
+      {  // children of the elimination tree (for the structure read-back; the solve reads gn_*)
+        std::vector<std::vector<int>> ch(m);
+        for (int i = 0; i < m; ++i) if (P.parent[i] >= 0) ch[P.parent[i]].push_back(i);
+        for (int i = 0; i < m; ++i) {
+          s_ch_ptr.push_back(base_ch_idx + (int)s_ch_idx.size());
+          for (int x : ch[i]) s_ch_idx.push_back(x);
+        }
+        for (int i = 0; i < m; ++i) { s_dn_body.push_back(dyn_body[i]); s_dn_parent.push_back(P.parent[i]); }
+      }
+      // update groups per level: a group is one target block of a node and the ordered products
+      // subtracted from it (left-looking: every contribution comes from a lower level)
+      d.gen_lv_off = base_gn_lgrp + (int)s_gn_lgrp.size();
+      d.gen_off = base_gn_ptr + (int)s_gn_rop_ptr.size();
+      d.gen_slot_off = base_gn_slot + (int)s_gn_slot_col.size();
+      auto up_blk = [&](int k, int j) { return m + 2 * P.slot(k, j); };
+      auto lo_blk = [&](int k, int j) { return m + 2 * P.slot(k, j) + 1; };
+      for (int L = 0; L < P.n_levels; ++L) {
+        s_gn_lgrp.push_back(base_gn_grp + (int)s_gn_grp.size());
+        for (int k : by[L]) {
+          auto group = [&](int target, const std::vector<int2>& ops) {
+            if (ops.empty()) return;
+            const int first = base_gn_ops + (int)s_gn_ops.size();
+            s_gn_ops.insert(s_gn_ops.end(), ops.begin(), ops.end());
+            s_gn_grp.push_back(make_int4(target, first, first + (int)ops.size(), k));
+          };
+          std::vector<int2> ops;
+          for (int p : P.contrib[k]) ops.push_back(make_int2(lo_blk(p, k), up_blk(p, k)));  // D_k -= S_kp A_pk
+          group(k, ops);
+          for (int j : P.later[k]) {
+            std::vector<int2> opu, opl;
+            for (int p : P.contrib[k]) {
+              if (!P.has(p, j)) continue;
+              opu.push_back(make_int2(lo_blk(p, k), up_blk(p, j)));  // A_kj -= S_kp A_pj
+              opl.push_back(make_int2(lo_blk(p, j), up_blk(p, k)));  // A_jk -= S_jp A_pk
+            }
+            group(up_blk(k, j), opu);
+            group(lo_blk(k, j), opl);
+          }
+        }
+      }
+      s_gn_lgrp.push_back(base_gn_grp + (int)s_gn_grp.size());
+      for (int k = 0; k < m; ++k) {
+        s_gn_rop_ptr.push_back(base_gn_rops + (int)s_gn_rops.size());
+        for (int p : P.contrib[k]) s_gn_rops.push_back(make_int2(lo_blk(p, k), p));  // b_k -= S_kp y_p
+        s_gn_slot_ptr.push_back(P.slot_first[k]);
+        for (int j : P.later[k]) s_gn_slot_col.push_back(j);
+      }
+      s_gn_rop_ptr.push_back(base_gn_rops + (int)s_gn_rops.size());
+      s_gn_slot_ptr.push_back(P.slot_first[m]);
+      // assembly cells: the diagonal blocks, then both blocks of every slot (fill slots get none)
+      d.cell_off = base_cell_ptr + (int)s_cell_ptr.size();
+      {
+        const int n_cells = m + 2 * P.n_slots;
+        std::vector<std::vector<int>> cells(n_cells);
+        for (int q = 0; q < d.nj; ++q) {
+          int ends[2] = {order[s_jl_a[jl0 + q]], order[s_jl_b[jl0 + q]]};
+          for (int re = 0; re < 2; ++re) {
+            if (ends[re] < 0) continue;
+            for (int ce = 0; ce < 2; ++ce) {
+              if (ends[ce] < 0) continue;
+              const int row = ends[re], col = ends[ce];
+              int target;
+              if (row == col) target = row;
+              else if (P.pos[row] < P.pos[col]) target = up_blk(row, col);
+              else target = lo_blk(col, row);
+              const int tors = s_jl_law[jl0 + q] == LAW_TORSIONAL ? exg_newton::kTermTorsional : 0;
+              cells[target].push_back((q * 4 + re * 2 + ce) | tors);
+            }
+          }
+        }
+        int pos = base_cell_terms + (int)s_cell_terms.size();
+        for (int t = 0; t < n_cells; ++t) {
+          s_cell_ptr.push_back(pos);
+          for (int x : cells[t]) { s_cell_terms.push_back(x); ++pos; }
+        }
+        s_cell_ptr.push_back(pos);
+      }
+      desc.push_back(d);
+      lens.push_back((scratch_doubles(d.nb, d.nj, m, d.n_slots) + 31) & ~31LL);
+      continue;
+    }
     int nlev = 0;
     for (int i = 0; i < m; ++i) nlev = std::max(nlev, level[i] + 1);
     d.n_levels = nlev;
@@ -621,6 +889,11 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
   cat(h_ch_ptr, s_ch_ptr); cat(h_ch_idx, s_ch_idx); cat(h_cell_ptr, s_cell_ptr); cat(h_cell_terms, s_cell_terms);
   h_jl_params.insert(h_jl_params.end(), s_jl_params.begin(), s_jl_params.end());
   cat(h_jl_id, s_jl_id);
+  cat(h_gn_lgrp, s_gn_lgrp); cat(h_gn_rop_ptr, s_gn_rop_ptr); cat(h_gn_slot_ptr, s_gn_slot_ptr);
+  cat(h_gn_slot_col, s_gn_slot_col);
+  h_gn_grp.insert(h_gn_grp.end(), s_gn_grp.begin(), s_gn_grp.end());
+  h_gn_ops.insert(h_gn_ops.end(), s_gn_ops.begin(), s_gn_ops.end());
+  h_gn_rops.insert(h_gn_rops.end(), s_gn_rops.begin(), s_gn_rops.end());
   if ((int)world_islands_.size() <= slot) world_islands_.resize(slot + 1);
   world_islands_[slot].clear();
   for (size_t I = 0; I < desc.size(); ++I) {
@@ -702,6 +975,8 @@ int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
   up(d_jl_params, h_jl_params); up(d_ib_order, h_ib_order); up(d_ib_inc_ptr, h_ib_inc_ptr);
   up(d_ib_inc_ref, h_ib_inc_ref); up(d_dn_body, h_dn_body); up(d_dn_parent, h_dn_parent); up(d_lv_ptr, h_lv_ptr);
   up(d_lv_nodes, h_lv_nodes); up(d_ch_idx, h_ch_idx); up(d_cell_ptr, h_cell_ptr); up(d_cell_terms, h_cell_terms);
+  up(d_gn_lgrp, h_gn_lgrp); up(d_gn_rop_ptr, h_gn_rop_ptr); up(d_gn_slot_ptr, h_gn_slot_ptr);
+  up(d_gn_slot_col, h_gn_slot_col); up(d_gn_grp, h_gn_grp); up(d_gn_ops, h_gn_ops); up(d_gn_rops, h_gn_rops);
   if (rc != EXG_OK) return rc;
   // ch_ptr carries a sentinel after its last entry; rewrite it with the tail
   if ((long long)h_ch_ptr.size() > d_ch_ptr.size || d_ch_ptr.cap == 0) {
@@ -735,7 +1010,9 @@ int NewtonWorld::sync(exg_device_s* dev, cudaStream_t s) {
   if ((rc = d_queue.assign(q.data(), (long long)q.size(), s)) != EXG_OK) return rc;
   arr = NewtonDeviceArrays{d_desc.ptr,      d_isl_body.ptr, d_jl_law.ptr,   d_jl_a.ptr,      d_jl_b.ptr,     d_jl_params.ptr,
                            d_ib_order.ptr,  d_ib_inc_ptr.ptr, d_ib_inc_ref.ptr, d_dn_body.ptr, d_dn_parent.ptr, d_lv_ptr.ptr,
-                           d_lv_nodes.ptr,  d_ch_ptr.ptr,   d_ch_idx.ptr,   d_cell_ptr.ptr,  d_cell_terms.ptr, d_scratch.ptr,
+                           d_lv_nodes.ptr,  d_ch_ptr.ptr,   d_ch_idx.ptr,   d_cell_ptr.ptr,  d_cell_terms.ptr,
+                           d_gn_lgrp.ptr,   d_gn_grp.ptr,   d_gn_ops.ptr,   d_gn_rop_ptr.ptr, d_gn_rops.ptr,
+                           d_gn_slot_ptr.ptr, d_gn_slot_col.ptr, d_scratch.ptr,
                            d_stats.ptr,     d_residual.ptr, d_phase.ptr};
   if ((rc = build_wave(s)) != EXG_OK) return rc;
   dirty_ = false;

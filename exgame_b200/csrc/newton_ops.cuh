@@ -26,14 +26,18 @@ constexpr int kTermTorsional = 1 << 30;
 
 struct Scratch {
   double *vm, *base, *best, *trial, *mid, *snap, *ext, *conn, *jac, *mass, *mass0, *rhs, *scale, *D, *Dinv, *Acp, *Apc, *S,
-      *bvec, *dv;
+      *bvec, *dv, *G;
 };
 
-EXG_HD long long scratch_doubles(int nb, int nj, int m) {
-  return (long long)nb * (6 * 4 + 8 + 6 * 2) + (long long)nj * (6 + 4 * kJacStride) + (long long)m * (36 * 7 + 6 * 3 + 2);
+// Doubles of an island's scratch; n_slots (block-LU islands) adds the off-diagonal block pairs.
+EXG_HD long long scratch_doubles(int nb, int nj, int m, int n_slots = 0) {
+  return (long long)nb * (6 * 4 + 8 + 6 * 2) + (long long)nj * (6 + 4 * kJacStride) + (long long)m * (36 * 7 + 6 * 3 + 2) +
+         (long long)n_slots * 72;
 }
 
-__device__ inline Scratch carve(double* p, int nb, int nj, int m) {
+// The island's scratch arrays; a block-LU island's off-diagonal blocks (G) follow the common ones,
+// so a tree island's layout does not depend on the solver.
+__device__ inline Scratch carve(double* p, int nb, int nj, int m, int n_slots = 0) {
   Scratch s;
   s.vm = p; p += nb * 6;
   s.base = p; p += nb * 6;
@@ -55,6 +59,7 @@ __device__ inline Scratch carve(double* p, int nb, int nj, int m) {
   s.S = p; p += (size_t)m * 36;
   s.bvec = p; p += (size_t)m * 6;
   s.dv = p; p += (size_t)m * 6;
+  s.G = p; p += (size_t)n_slots * 72;
   return s;
 }
 
@@ -114,7 +119,7 @@ __device__ inline Ctx make_ctx(const NewtonDeviceArrays& A, const WorldRef& W, i
   c.W = W;
   c.island = island;
   c.d = A.desc[island];
-  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
   resolve_params(c);
   return c;
 }
@@ -128,7 +133,7 @@ __device__ __forceinline__ Ctx make_ctx_desc(const NewtonDeviceArrays& A, const 
   c.W = W;
   c.island = -1;
   c.d = d;
-  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
   if (params) resolve_params(c);
   return c;
 }
@@ -140,7 +145,7 @@ __device__ inline Ctx make_ctx_lite(const NewtonDeviceArrays& A, const WorldRef&
   c.W = W;
   c.island = island;
   c.d = A.desc[island];
-  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m);
+  c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
   return c;
 }
 
@@ -376,6 +381,33 @@ __device__ inline double op_assemble(const Ctx& c, double pf, double vf, int cel
   double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
   dst[36 * (size_t)i + e] = acc;
   *counts = kind == 0 || c.A.dn_parent[c.d.dyn_off + i] >= 0;
+  return acc;
+}
+
+// Block t of a block-LU island: the diagonal block of node t (t < m), else an off-diagonal block
+// of a slot (Up of slot s at m + 2s, Lo at m + 2s + 1).
+__device__ __forceinline__ double* lu_block(const Ctx& c, int t) {
+  return t < c.d.m ? c.s.D + 36 * (size_t)t : c.s.G + 36 * (size_t)(t - c.d.m);
+}
+
+// Assembly entry e of cell t of a block-LU island: the mass block (diagonal cells) then every
+// contributing joint end in cell order, with the factors of op_assemble. Writes the block's entry
+// and returns it (every block of such an island enters ||A||_F).
+template <bool MIXED>
+__device__ inline double op_assemble_lu(const Ctx& c, double pf, double vf, int t, int e) {
+  const int r = e / 6, col = e % 6;
+  double acc = (t < c.d.m) ? c.s.mass0[36 * (size_t)t + e] : 0.0;
+  const int p0 = c.A.cell_ptr[c.d.cell_off + t], p1 = c.A.cell_ptr[c.d.cell_off + t + 1];
+  for (int k = p0; k < p1; ++k) {
+    int term = c.A.cell_terms[k] & ~kTermTorsional;
+    int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
+    const auto* jp = jac_slice<MIXED>(c, q, ce);
+    const auto* jv = jac_slice<MIXED>(c, q, 2 + ce);
+    double pv = double(jp[r * 6 + col]), vv = double(jv[r * 6 + col]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc = acc + pf * pv + vf * vv;
+  }
+  lu_block(c, t)[e] = acc;
   return acc;
 }
 

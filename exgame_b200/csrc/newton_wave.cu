@@ -895,7 +895,8 @@ __global__ void k_w_commit(WaveArgs a) {
 
 // ── host: wave structure and rounds ──────────────────────────────────────────
 bool NewtonWorld::wave_island(const IslandDesc& d) const {
-  return d.m >= wave_min_dyn_ && d.n_levels <= wave_max_levels_;
+  // block-LU islands (dynamic cycles) run on the island kernel
+  return d.solver == 0 && d.m >= wave_min_dyn_ && d.n_levels <= wave_max_levels_;
 }
 
 int NewtonWorld::build_wave(cudaStream_t s) {

@@ -19,6 +19,17 @@ struct IslandDesc {
   int cell_off;          // cell_ptr[cell_off .. cell_off + 3m + 1)
   int inc_off;           // ib_inc_ptr[inc_off .. inc_off + nb + 1)
   long long scratch_off; // doubles
+  // Linear solve: 0 = block elimination on the island's tree (its dynamic bodies form a forest),
+  // 1 = block LU on a minimum-degree elimination order with fill (dynamic cycles). For solver 1
+  // the island's blocks are D[0..m) then, per off-diagonal slot s (a pair k < j in elimination
+  // order, fill included), Up = A(k, j) and Lo = A(j, k) at blocks m + 2s and m + 2s + 1; levels
+  // (lv_*) run from the first eliminated nodes up, and the gn_* arrays hold the factorization's
+  // update lists.
+  int solver;
+  int n_slots;           // off-diagonal slots (solver 1)
+  int gen_off;           // gn_rop_ptr / gn_slot_ptr [gen_off .. gen_off + m + 1)
+  int gen_lv_off;        // gn_lgrp [gen_lv_off .. gen_lv_off + n_levels + 1)
+  int gen_slot_off;      // gn_slot_col [gen_slot_off .. gen_slot_off + n_slots)
 };
 
 struct NewtonDeviceArrays {
@@ -39,6 +50,17 @@ struct NewtonDeviceArrays {
   const int* ch_idx;
   const int* cell_ptr;     // assembly terms per (node, kind)
   const int* cell_terms;   // local joint * 4 + row_end * 2 + col_end
+  // solver 1 (block LU): per level, its update groups (absolute offsets into gn_grp); a group is
+  // (target block, first op, end op) over gn_ops, each op (left block, right block): target -=
+  // left * right, in order; per node, its right-hand-side updates (absolute into gn_rops, each (the
+  // scaled block S = A(k, p) D_p^-1, p)) and its slots (island-relative, columns in gn_slot_col).
+  const int* gn_lgrp;
+  const int4* gn_grp;
+  const int2* gn_ops;
+  const int* gn_rop_ptr;
+  const int2* gn_rops;
+  const int* gn_slot_ptr;
+  const int* gn_slot_col;
   double* scratch;
   int* stats;              // per island: spans, newton iterations, max depth, fatal
   double* residual;        // per island: last span's best residual
@@ -166,11 +188,17 @@ class NewtonWorld {
       h_lv_ptr, h_lv_nodes, h_ch_ptr, h_ch_idx, h_cell_ptr, h_cell_terms;
   std::vector<double> h_jl_params;
   std::vector<int> h_jl_id;  // per island joint: the world-local joint index (host only)
+  std::vector<int> h_gn_lgrp, h_gn_rop_ptr, h_gn_slot_ptr, h_gn_slot_col;
+  std::vector<int4> h_gn_grp;
+  std::vector<int2> h_gn_ops, h_gn_rops;
   std::vector<std::vector<int>> world_islands_;
   // device mirrors
   DevArr<IslandDesc> d_desc;
   DevArr<int> d_isl_body, d_jl_law, d_jl_a, d_jl_b, d_ib_order, d_ib_inc_ptr, d_ib_inc_ref, d_dn_body, d_dn_parent,
       d_lv_ptr, d_lv_nodes, d_ch_ptr, d_ch_idx, d_cell_ptr, d_cell_terms;
+  DevArr<int> d_gn_lgrp, d_gn_rop_ptr, d_gn_slot_ptr, d_gn_slot_col;
+  DevArr<int4> d_gn_grp;
+  DevArr<int2> d_gn_ops, d_gn_rops;
   DevArr<double> d_jl_params, d_scratch, d_residual;
   DevArr<int> d_stats, d_queue;
   DevArr<long long> d_phase;

@@ -171,6 +171,52 @@ def tree_world(n, seed=2, twist_sigma=0.05, laws=(0, 2, 3)):
     return _bodies_at(rng, mass, I, pos, twist_sigma), joints
 
 
+def cloth_world(cols, rows, kick=0.5, k=100.0, zeta=0.7, mass_total=1.0, width=0.5, g=9.81, wind=1.0, dt=1.0 / 60.0,
+                tol=1e-4, precision=PRECISION_F64):
+    """The reference's curtain (crates/newton/tests/cloth_grid_stability.rs:48-110,
+    cloth_scaling.rs:40-90): a cols x rows grid in the XZ plane with spacing h = width / (cols - 1),
+    the top row kinematic at rest, every other node a point body of mass mass_total / (cols rows)
+    with unit isotropic moment; nodes whose row-major index is 1 mod 4 start at kick along +Y. An
+    axial SimpleSpringDamper (anchors at the centres, rest h, stiffness k, damping
+    zeta 2 sqrt(k m / 2), softening 1e-6) joins each node to its right and its upper neighbour, in
+    row-major order, right before up. Gravity -g along Z and a wind of `wind` along Y act as
+    uniform fields. The grid's springs close cycles among the dynamic bodies."""
+    h = width / (cols - 1.0)
+    m = mass_total / (cols * rows)
+    c = zeta * 2.0 * math.sqrt(k * (m * 0.5))
+    n = cols * rows
+    bodies = np.zeros(n, dtype=BODY_DTYPE)
+    tw = np.zeros((n, 6))
+    for row in range(rows):
+        for col in range(cols):
+            i = row * cols + col
+            tw[i, :3] = (col * h, 0.0, row * h)
+    bodies["pose"] = motors_np.twist_exp_n(tw, 1.0)
+    bodies["inertia"][:, 0] = bodies["inertia"][:, 4] = bodies["inertia"][:, 8] = 1.0
+    bodies["diagonal"] = 1
+    top = np.arange(n) >= (rows - 1) * cols
+    bodies["kinematic"] = top.astype(np.int32)
+    bodies["mass"] = np.where(top, 0.0, m)
+    bodies["size"] = np.cbrt(m / 4.0)
+    gust = (~top) & (np.arange(n) % 4 == 1)
+    bodies["momentum"][gust, 1] = m * kick
+    edges = []
+    for row in range(rows):
+        for col in range(cols):
+            i = row * cols + col
+            if col + 1 < cols:
+                edges.append((i, i + 1))
+            if row + 1 < rows:
+                edges.append((i, i + cols))
+    joints = np.zeros(len(edges), dtype=JOINT_DTYPE)
+    for q, (a, b) in enumerate(edges):
+        joints[q]["law"], joints[q]["a"], joints[q]["b"] = 0, a, b
+        joints[q]["params"][6:10] = (h, k, c, 1e-6)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=dt, tol=tol,
+                         field=(0.0, wind, -g))
+    return bodies, joints, params
+
+
 def concat_worlds(parts):
     """Concatenate (bodies, joints) pairs into one world, re-indexing the joints."""
     bodies, joints, off = [], [], 0

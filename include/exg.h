@@ -223,6 +223,11 @@ EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_
  * handle's joint capacity: a world or batch handle holds the joint count it was created with, a
  * pool max_joints) or a bad record leaves the world as it was. */
 EXG_API int exg_batch_set_joints(exg_world_t w, int32_t world, const exg_joint_t* joints, int32_t n_joints);
+/* The epoch of one world (world 0 of a single world) for the following steps: its dt and warp
+ * (Epoch::standalone(dt, warp), crates/aristotle/src/epoch.rs:17-60; the reference passes the
+ * epoch to every Mechanism::step, so a host with a variable frame time sets it before each step).
+ * dt > 0 and finite, warp >= 1; no structural change, nothing is rebuilt. */
+EXG_API int exg_batch_set_epoch(exg_world_t w, int32_t world, double dt, double warp);
 /* ── pool: worlds admitted into and released from fixed-capacity device arrays ──
  * The serving form of a batch: state stays resident while worlds come and go. A released slot's
  * ranges are reused by later admissions; exg_world_step advances every admitted world. The

@@ -333,10 +333,11 @@ def test_set_joints_detach_and_connect_match_oracle(device, oracle, scheme):
         dw.close()
 
 
-def test_set_joints_refuses_a_cycle_and_changes_nothing(device, oracle):
-    """A joint list that closes a cycle of dynamic bodies is refused (EXG_ERR_UNSUPPORTED) and the
-    world steps on exactly as an untouched twin; in a batch, replacing one world's joints leaves
-    the other world bit for bit as when stepped alone."""
+def test_set_joints_closing_a_cycle_and_a_refused_list(device, oracle):
+    """A joint list that closes a cycle of dynamic bodies moves the island to the block-LU solve
+    and the world then steps as the oracle does; a list beyond the handle's joint capacity is
+    refused (EXG_ERR_OUT_OF_MEMORY) and the world steps on exactly as an untouched twin; in a
+    batch, replacing one world's joints leaves the other world bit for bit as when stepped alone."""
     bodies, joints = scenarios.tree_world(24, seed=87)
     params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, dt=1e-2, tol=1e-10)
     loop = joints.copy()  # same count (a world handle's joint capacity is its count at creation)
@@ -345,14 +346,23 @@ def test_set_joints_refuses_a_cycle_and_changes_nothing(device, oracle):
     b = _lib.DeviceWorld(device, bodies, joints, params)
     a.step(2)
     b.step(2)
-    with pytest.raises(_lib.ExgError) as e:
-        a.set_joints(loop)
-    assert e.value.status == -22  # EXG_ERR_UNSUPPORTED
+    a.set_joints(loop)
+    ow = oracle.OracleWorld(a.bodies(), loop, params)
     a.step(3)
+    ow.step(3)
+    pe, me = state_error(ow.bodies(), a.bodies())
+    assert pe < 1e-9 and me < 1e-7, (pe, me)
+    with pytest.raises(_lib.ExgError) as e:
+        b.set_joints(np.concatenate([joints, joints[:1]]))
+    assert e.value.status == -21  # EXG_ERR_OUT_OF_MEMORY: beyond the handle's joint capacity
+    twin = _lib.DeviceWorld(device, bodies, joints, params)
+    twin.step(2)
     b.step(3)
-    assert np.array_equal(a.bodies()["pose"], b.bodies()["pose"])
+    twin.step(3)
+    assert np.array_equal(b.bodies()["pose"], twin.bodies()["pose"])
     a.close()
     b.close()
+    twin.close()
     other, oj = scenarios.chain_world(8, seed=88)
     batch = _lib.DeviceBatch(device, [(other, oj, params), (bodies, joints, params)])
     alone = _lib.DeviceWorld(device, other, oj, params)

@@ -31,8 +31,10 @@ def check_parents(dev_world, world, island, ends, order):
         if ia >= 0 and ib >= 0:
             adj.add((ia, ib))
             adj.add((ib, ia))
+    cyclic = len(adj) // 2 > m - 1
     for i, p in enumerate(par):
-        assert p == -1 or (i, p) in adj
+        # a tree island's parents are joint edges; a cyclic island's are its factor's (fill included)
+        assert p == -1 or cyclic or (i, p) in adj
     # no cycles: following parents from any node reaches a root within m hops
     for i in range(m):
         x, hops = i, 0
@@ -117,13 +119,29 @@ def test_batch_worlds_and_joint_replacement(device, oracle):
     cut = j2[(j2["a"] != j2["a"][30]) | (j2["b"] != j2["b"][30])]
     batch.set_joints(cut, world=2)
     b1, j1, p1 = worlds[1]
-    extra = np.zeros(1, dtype=JOINT_DTYPE)
-    extra[0] = j1[0]
+    extra = np.zeros(10, dtype=JOINT_DTYPE)  # more joints than the batch has room for
+    extra[:] = j1[0]
     extra["a"], extra["b"] = 3, 140
     j1b = np.concatenate([j1[:5], extra, j1[5:]])
-    with pytest.raises(_lib.ExgError):  # a dynamic cycle is refused and changes nothing
+    with pytest.raises(_lib.ExgError):  # beyond the batch's joint capacity: refused, nothing changes
         batch.set_joints(j1b, world=1)
     batch.step(1)
     assert compare(batch, oracle, b2, cut, p2, world=2) == 2
     compare(batch, oracle, b1, j1, p1, world=1)
+    # the same count with an edge moved so that it closes a cycle: accepted (block-LU island)
+    j1c = j1.copy()
+    j1c[-1]["a"], j1c[-1]["b"] = 3, 140
+    batch.set_joints(j1c, world=1)
+    batch.step(1)
+    compare(batch, oracle, b1, j1c, p1, world=1)
     batch.close()
+
+
+def test_cloth_islands_structure(device, oracle):
+    """A curtain's dynamic bodies form cycles: the island keeps the oracle's gather maps and order
+    (the block-LU solve changes only the elimination structure)."""
+    b, j, p = scenarios.cloth_world(5, 10, tol=1e-10)
+    w = _lib.DeviceWorld(device, b, j, p)
+    w.step(1)
+    assert compare(w, oracle, b, j, p) == 1
+    w.close()

@@ -77,6 +77,16 @@ SIGNATURES = {
     "exg_world_phase_cycles": (ctypes.c_int, [_vp, _vp]),
     "exg_world_island_count": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "exg_batch_set_epoch": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double]),
+    "exg_storage_create": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(_vp)]),
+    "exg_storage_destroy": (ctypes.c_int, [_vp]),
+    "exg_slot_alloc": (ctypes.c_int, [_vp, _vp, _vp]),
+    "exg_slot_free": (ctypes.c_int, [_vp, ctypes.c_uint64]),
+    "exg_slot_read": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
+    "exg_slot_write": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp]),
+    "exg_slot_read_n": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "exg_slot_write_n": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "exg_storage_info": (ctypes.c_int, [_vp, _vp]),
+    "exg_ledger_check": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "exg_world_island_structure": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp,
                                                   ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
     "exg_motor_exp": (ctypes.c_int, [_vp, ctypes.c_double, _vp]),
@@ -575,3 +585,87 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ── typed slot storage and the one-writer ledger ─────────────────────────────
+SLOT_KEY_DTYPE = np.dtype([("index", np.uint32), ("generation", np.uint32)])
+STORAGE_INFO_DTYPE = np.dtype([("buffer", np.uint64), ("elem_bytes", np.int64), ("capacity", np.int64),
+                               ("len", np.int64), ("live", np.int64), ("generation", np.uint64)])
+
+
+def _key_word(key):
+    """An exg_slot_key_t passed by value: (index, generation) packed little-endian in 64 bits."""
+    k = np.asarray(key, dtype=SLOT_KEY_DTYPE).reshape(())
+    return int(k["index"]) | (int(k["generation"]) << 32)
+
+
+class SlotStorage:
+    """Typed slot storage on the device (aristotle::World per-type storage): elements of one numpy
+    dtype, keys (index, generation), lowest free slot reused, growth that keeps indices and bumps
+    the storage's generation."""
+
+    def __init__(self, device, dtype, capacity=256):
+        self.device = device
+        self.dtype = np.dtype(dtype)
+        if self.dtype.itemsize % 4:
+            raise ValueError("element size must be a multiple of 4 bytes")
+        h = ctypes.c_void_p()
+        check(lib().exg_storage_create(device.handle, self.dtype.itemsize, int(capacity), ctypes.byref(h)),
+              "exg_storage_create")
+        self.handle = h
+        device._owned.add(self)
+
+    def alloc(self, value):
+        v = np.ascontiguousarray(np.asarray(value, dtype=self.dtype).reshape(()))
+        key = np.zeros((), dtype=SLOT_KEY_DTYPE)
+        check(lib().exg_slot_alloc(self.handle, ptr(v), ptr(key)), "exg_slot_alloc")
+        return key
+
+    def free(self, key):
+        check(lib().exg_slot_free(self.handle, _key_word(key)), "exg_slot_free")
+
+    def read(self, key):
+        out = np.zeros((), dtype=self.dtype)
+        check(lib().exg_slot_read(self.handle, _key_word(key), ptr(out)), "exg_slot_read")
+        return out
+
+    def write(self, key, value):
+        v = np.ascontiguousarray(np.asarray(value, dtype=self.dtype).reshape(()))
+        check(lib().exg_slot_write(self.handle, _key_word(key), ptr(v)), "exg_slot_write")
+
+    def read_n(self, keys):
+        k = np.ascontiguousarray(keys, dtype=SLOT_KEY_DTYPE)
+        out = np.zeros(len(k), dtype=self.dtype)
+        check(lib().exg_slot_read_n(self.handle, ptr(k), len(k), ptr(out)), "exg_slot_read_n")
+        return out
+
+    def write_n(self, keys, values):
+        k = np.ascontiguousarray(keys, dtype=SLOT_KEY_DTYPE)
+        v = np.ascontiguousarray(values, dtype=self.dtype)
+        if len(v) != len(k):
+            raise ValueError("one value per key")
+        check(lib().exg_slot_write_n(self.handle, ptr(k), len(k), ptr(v)), "exg_slot_write_n")
+
+    def info(self):
+        out = np.zeros((), dtype=STORAGE_INFO_DTYPE)
+        check(lib().exg_storage_info(self.handle, ptr(out)), "exg_storage_info")
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().exg_storage_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ledger_check(slots, n_slots):
+    """The one-writer check of a scatter map: (status, first offending position or -1)."""
+    s = np.ascontiguousarray(slots, dtype=np.int32)
+    clash = ctypes.c_int64()
+    st = lib().exg_ledger_check(ptr(s), len(s), int(n_slots), ctypes.byref(clash))
+    return st, clash.value

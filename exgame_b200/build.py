@@ -10,7 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libexg.so")
 OBJ_DIR = os.path.join(HERE, "_build")
-SOURCES = ["exg_api.cu", "gravity.cu", "joints.cu", "bodies.cu", "newton.cu", "newton_wave.cu", "server.cu"]
+SOURCES = ["exg_api.cu", "gravity.cu", "joints.cu", "bodies.cu", "newton.cu", "newton_wave.cu", "server.cu",
+           "storage.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr",

@@ -17,6 +17,8 @@ const char* kLawNames[4] = {"SimpleSpringDamper", "CriticallyDampedWarped", "Per
 const int kLawParams[4] = {10, 10, 2, 1};
 }  // namespace
 
+void exg_internal_set_message(const char* what) { g_last_error = what; }
+
 void exg_internal_set_cuda_error(cudaError_t e, const char* what) {
   g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
 }

@@ -19,6 +19,12 @@
   } while (0)
 
 void exg_internal_set_cuda_error(cudaError_t e, const char* what);
+// The message exg_status_string(EXG_ERR_BACKEND) returns on this thread until the next error.
+void exg_internal_set_message(const char* what);
+// One-writer check of a scatter map (storage.cu): every entry of slots[0, n) in [0, n_slots) and no
+// slot named twice. EXG_OK, or EXG_ERR_BACKEND with the message set and *first_clash the position
+// of the first repeated (or out-of-range) entry.
+int exg_internal_ledger(const int32_t* slots, long long n, long long n_slots, long long* first_clash, const char* what);
 // Drop the cached device address of the no-allocation gravity array on `ordinal` (gravity.cu).
 void exg_internal_noalloc_forget(int ordinal);
 

@@ -870,6 +870,42 @@ int NewtonWorld::build_world(int slot, const WorldSrc& src) {
     desc.push_back(d);
     lens.push_back((scratch_doubles(d.nb, d.nj, m) + 31) & ~31LL);
   }
+  // one-writer ledger over the maps just built (crates/newton/src/accelerator/shaders.rs:321-390):
+  // each body in one island, each joint end gathered once, each assembly term in one cell, each
+  // factor block the target of one update group; a clash refuses the world before anything changes
+  {
+    std::vector<int32_t> v;
+    for (int x : s_isl_body) v.push_back(x - body_off);
+    int rc = exg_internal_ledger(v.data(), (long long)v.size(), n, nullptr, "structure refused: island bodies");
+    for (size_t I = 0; I < desc.size() && rc == EXG_OK; ++I) {
+      const IslandDesc& d = desc[I];
+      const int li = d.inc_off - base_inc_ptr;
+      const int r0 = s_ib_inc_ptr[li] - base_inc_ref, r1 = s_ib_inc_ptr[li + d.nb] - base_inc_ref;
+      if (r1 - r0 != 2 * d.nj) {
+        exg_internal_set_message("structure refused: an island gathers a joint end twice or not at all");
+        rc = EXG_ERR_BACKEND;
+      }
+      if (rc == EXG_OK)
+        rc = exg_internal_ledger(s_ib_inc_ref.data() + r0, r1 - r0, 2LL * d.nj, nullptr,
+                                 "structure refused: gathered joint ends");
+      const int lc = d.cell_off - base_cell_ptr;
+      const int n_cells = d.solver == 1 ? d.m + 2 * d.n_slots : 3 * d.m;
+      const int t0 = s_cell_ptr[lc] - base_cell_terms, t1 = s_cell_ptr[lc + n_cells] - base_cell_terms;
+      v.assign(s_cell_terms.begin() + t0, s_cell_terms.begin() + t1);
+      for (int32_t& x : v) x &= ~exg_newton::kTermTorsional;
+      if (rc == EXG_OK) rc = exg_internal_ledger(v.data(), (long long)v.size(), 4LL * d.nj, nullptr,
+                                                 "structure refused: assembly terms");
+      if (rc == EXG_OK && d.solver == 1) {
+        const int lg = d.gen_lv_off - base_gn_lgrp;
+        const int g0 = s_gn_lgrp[lg] - base_gn_grp, g1 = s_gn_lgrp[lg + d.n_levels] - base_gn_grp;
+        v.clear();
+        for (int g = g0; g < g1; ++g) v.push_back(s_gn_grp[g].x);
+        rc = exg_internal_ledger(v.data(), (long long)v.size(), (long long)d.m + 2LL * d.n_slots, nullptr,
+                                 "structure refused: factor update targets");
+      }
+    }
+    if (rc != EXG_OK) return rc;
+  }
   // scratch ranges (grow the scratch array when the allocator has no room)
   for (size_t I = 0; I < desc.size(); ++I) {
     long long off = scratch_alloc_.alloc(lens[I]);

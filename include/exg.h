@@ -373,6 +373,53 @@ EXG_API int exg_world_island_structure(exg_world_t w, int32_t world, int32_t isl
 /* Total energy: kinetic + gravity + joint potential (crates/newton/tests/energy_drift_repro.rs:123-149). */
 EXG_API int exg_world_energy(exg_world_t w, double* out);
 
+/* ── typed slot storage (aristotle::World per-type storage, crates/aristotle/src/world.rs) ──
+ * One storage holds elements of elem_bytes (a multiple of 4, at most 65536) in one device buffer
+ * of `capacity` slots (WorldBuilder::with_storage / capacity, world.rs:498-538). A key is the slot
+ * index and the slot's generation (MapKey; WorldKey::raw_index, world.rs:479-487). Inserting takes
+ * the lowest free slot (the reference keeps its free list in slot order, RawMap::insert / remove,
+ * world.rs:300-370); a fresh slot starts at generation 0 and freeing bumps the slot's generation, so
+ * a stale or freed key is refused (EXG_ERR_INVALID_ARGUMENT) by read, write and free. Inserting into
+ * a full buffer grows it geometrically: every live slot is copied to the same position and the
+ * storage's generation is bumped (RawMap::grow, world.rs:189-211; World::generation, world.rs:
+ * 625-633), so indices survive growth while a holder of the old buffer pointer learns that it must
+ * re-bind. Device memory is not host-mapped: read and write are explicit copies; the _n forms move
+ * many slots in one gather or scatter kernel. A storage counts as a handle of its device. */
+typedef struct exg_storage_s* exg_storage_t;
+typedef struct {
+  uint32_t index;
+  uint32_t generation;
+} exg_slot_key_t;
+typedef struct {
+  void* buffer;        /* the device buffer (valid while the generation below is current) */
+  int64_t elem_bytes;
+  int64_t capacity;    /* slots the buffer holds */
+  int64_t len;         /* slots ever handed out (live or free) */
+  int64_t live;        /* live keys */
+  uint64_t generation; /* bumped by every growth */
+} exg_storage_info_t;
+EXG_API int exg_storage_create(exg_device_t dev, int64_t elem_bytes, int64_t capacity, exg_storage_t* out);
+EXG_API int exg_storage_destroy(exg_storage_t st);
+EXG_API int exg_slot_alloc(exg_storage_t st, const void* value, exg_slot_key_t* key);
+EXG_API int exg_slot_free(exg_storage_t st, exg_slot_key_t key);
+EXG_API int exg_slot_read(exg_storage_t st, exg_slot_key_t key, void* out);
+EXG_API int exg_slot_write(exg_storage_t st, exg_slot_key_t key, const void* value);
+EXG_API int exg_slot_read_n(exg_storage_t st, const exg_slot_key_t* keys, int32_t n, void* out);
+/* The batch's writes run unordered on the device, so a batch naming one slot twice is refused
+ * before anything is written (the one-writer ledger below). All keys are checked first: a stale
+ * key refuses the batch too. */
+EXG_API int exg_slot_write_n(exg_storage_t st, const exg_slot_key_t* keys, int32_t n, const void* values);
+EXG_API int exg_storage_info(exg_storage_t st, exg_storage_info_t* out);
+
+/* ── one-writer ledger (crates/newton/src/accelerator/shaders.rs:321-390) ──
+ * The check every batch of unordered writes passes before it runs: each of slots[0, n) must lie in
+ * [0, n_slots) and no slot may be named twice. EXG_OK, or EXG_ERR_BACKEND (the reference refuses
+ * the flush with EvalError::Backend) with exg_status_string naming the slot and *first_clash the
+ * position of the first offending entry. The library runs it on its own scatter maps whenever a
+ * world's structure is rebuilt (island bodies, gathered joint ends, assembly terms, factor blocks),
+ * and on every batched slot write. Host only: no device needed. */
+EXG_API int exg_ledger_check(const int32_t* slots, int64_t n, int64_t n_slots, int64_t* first_clash);
+
 /* ── host-side motor utilities (no device needed; the same algebra the kernels use) ── */
 /* Twist::exp(dt) of (linear xyz, angular xyz) -> motor (crates/clifford/src/pga3/screw.rs:297-301). */
 EXG_API int exg_motor_exp(const double twist[6], double dt, double out[8]);

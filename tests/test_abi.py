@@ -130,3 +130,14 @@ def test_pool_and_server_reject_a_missing_device():
     pc = np.zeros((), dtype=abi.POOL_CONFIG_DTYPE)
     pc["max_bodies"], pc["max_worlds"] = 1024, 4
     assert _lib.lib().exg_pool_create(None, _lib.ptr(pc), ctypes.byref(h)) == -20
+
+
+def test_ledger_refuses_a_second_writer_and_out_of_range_slots():
+    """The one-writer check (crates/newton/src/accelerator/shaders.rs:321-390) is host only."""
+    assert _lib.ledger_check([3, 1, 4, 0, 2], 5) == (0, -1)
+    st, at = _lib.ledger_check([3, 1, 4, 1, 2], 5)
+    assert st == -5 and at == 3
+    assert "second writer" in _lib.lib().exg_status_string(st).decode()
+    st, at = _lib.ledger_check([0, 7], 5)
+    assert st == -5 and at == 1
+    assert _lib.ledger_check([], 0) == (0, -1)

@@ -26,6 +26,10 @@ def _nvcc():
 
 def build(verbose=False, force=False):
     os.makedirs(OBJ_DIR, exist_ok=True)
+    # the traced joint laws first: csrc/user_laws.cuh (rewritten only when its text changes)
+    sys.path.insert(0, os.path.dirname(HERE))
+    from exgame_b200 import viete
+    viete.generate()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
     headers.append(os.path.join(HERE, "..", "include", "exg.h"))
     newest_header = max(os.path.getmtime(h) for h in headers)

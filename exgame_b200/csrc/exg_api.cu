@@ -8,6 +8,7 @@
 #include "exg_internal.cuh"
 #include "body.cuh"
 #include "world_newton.cuh"
+#include "laws.cuh"
 #include "slab.cuh"
 
 namespace {
@@ -274,6 +275,12 @@ int exg_law_lookup(const char* name, int32_t* law_out, int32_t* n_params_out) {
       if (n_params_out) *n_params_out = kLawParams[k];
       return EXG_OK;
     }
+  for (int k = 0; k < exg::kUserLaws; ++k)  // the traced laws (user_laws.cuh)
+    if (std::strcmp(name, exg::kUserLawTable[k].name) == 0) {
+      if (law_out) *law_out = exg::kUserLawFirst + k;
+      if (n_params_out) *n_params_out = exg::kUserLawTable[k].n_params;
+      return EXG_OK;
+    }
   return EXG_ERR_NO_SHADER;
 }
 
@@ -292,7 +299,7 @@ static int validate_world(const exg_body_t* bodies, int32_t n, const exg_joint_t
   for (int32_t i = 0; i < n; ++i)
     if (!bodies[i].kinematic && !(bodies[i].mass > 0.0)) return EXG_ERR_INVALID_ARGUMENT;
   for (int32_t k = 0; k < nj; ++k) {
-    if (joints[k].law < 0 || joints[k].law > 3) return EXG_ERR_NO_SHADER;
+    if (joints[k].law < 0 || joints[k].law >= exg::kUserLawFirst + exg::kUserLaws) return EXG_ERR_NO_SHADER;
     if (joints[k].a < 0 || joints[k].a >= n || joints[k].b < 0 || joints[k].b >= n || joints[k].a == joints[k].b)
       return EXG_ERR_INVALID_ARGUMENT;
   }
@@ -603,7 +610,7 @@ static int pool_release(exg_world_s* W, int slot) {
 static int pool_set_joints(exg_world_s* W, int slot, const exg_joint_t* joints, int nj) {
   WorldSlot& ws = W->slots[slot];
   for (int k = 0; k < nj; ++k) {
-    if (joints[k].law < 0 || joints[k].law > 3) return EXG_ERR_NO_SHADER;
+    if (joints[k].law < 0 || joints[k].law >= exg::kUserLawFirst + exg::kUserLaws) return EXG_ERR_NO_SHADER;
     if (joints[k].a < 0 || joints[k].a >= ws.n || joints[k].b < 0 || joints[k].b >= ws.n || joints[k].a == joints[k].b)
       return EXG_ERR_INVALID_ARGUMENT;
   }

@@ -8,7 +8,8 @@
 //   PerpendicularDamperWarped  crates/joints/src/perpendicular_damper_warped.rs:107-162
 //   TorsionalDamperWarped      crates/joints/src/torsional_damper_warped.rs:93-123
 // Instantiated with S = double (plain f64 path), float (mixed path) and Dual<6, R> (one
-// 6-axis slice of the 24-axis Jacobian per evaluation).
+// 6-axis slice of the 24-axis Jacobian per evaluation). Law ids from kUserLawFirst on are the
+// traced laws of user_laws.cuh, with the same signature.
 #pragma once
 #include "geom.cuh"
 
@@ -27,6 +28,12 @@ template <int N, class R> struct Lift<Dual<N, R>> {
   static EXG_HD Dual<N, R> from(const Dual<N, R>& x) { return x; }
   static EXG_HD Dual<N, R> from(const R& x) { Dual<N, R> r; r.v = x; return r; }
 };
+
+}  // namespace exg
+// Laws traced from their scalar-generic form at build time (exgame_b200/viete.py): law ids from
+// kUserLawFirst on.
+#include "user_laws.cuh"
+namespace exg {
 
 template <class S, class P = S>
 EXG_HD void law_axial(int law, const double* prm, const P* ma, const P* mb, const S* ta, const S* tb, double dt,
@@ -111,7 +118,8 @@ EXG_HD void law_wrench(int law, const double* prm, const P* ma, const P* mb, con
                        double warp, S* wa) {
   if (law <= LAW_CRITICAL) law_axial<S, P>(law, prm, ma, mb, ta, tb, dt, warp, wa);
   else if (law == LAW_PERPENDICULAR) law_perpendicular<S, P>(prm, ma, mb, ta, tb, warp, wa);
-  else law_torsional(prm, ta, tb, warp, wa);
+  else if (law == LAW_TORSIONAL) law_torsional(prm, ta, tb, warp, wa);
+  else user_law_wrench<S, P>(law - kUserLawFirst, prm, ma, mb, ta, tb, dt, warp, wa);
 }
 
 }  // namespace exg

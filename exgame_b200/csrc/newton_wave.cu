@@ -446,13 +446,14 @@ void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cu
 template <bool MIXED>
 void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_first, cudaStream_t s,
                           cudaStream_t sv) {
-  for (int L = 0; L < 4; ++L) {
+  for (int L = 0; L < 5; ++L) {
     const int first = law_first[L], n = law_first[L + 1] - first;
     if (n == 0) continue;
     if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, s, sv);
     else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, s, sv);
     else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, s, sv);
-    else launch_joints_of<MIXED, 3>(dev, a, first, n, s, sv);
+    else if (L == 3) launch_joints_of<MIXED, 3>(dev, a, first, n, s, sv);
+    else launch_joints_of<MIXED, -1>(dev, a, first, n, s, sv);  // traced laws: the law read per joint
   }
 }
 
@@ -943,6 +944,7 @@ int NewtonWorld::build_wave(cudaStream_t s) {
   for (int L = 0; L <= 4; ++L)
     wave_law_first_[L] = (int)(std::lower_bound(joint.begin(), joint.end(), L,
                                                 [&](const int2& x, int v) { return law_of(x) < v; }) - joint.begin());
+  wave_law_first_[5] = (int)joint.size();  // items from first[4] on: the traced laws, dispatched at run time
   // nodes by elimination level across the wave's islands
   std::vector<std::vector<int2>> by(max_levels);
   for (int k = 0; k < (int)isl.size(); ++k) {
@@ -1123,7 +1125,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   cudaGraphDestroy(g);
   EXG_CUDA_TRY(ie);
   int joint_kernels = 0;
-  for (int L = 0; L < 4; ++L)
+  for (int L = 0; L < 5; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels;
   wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;
@@ -1254,7 +1256,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(capture(B, {if_end}, [&] { k_w_count<<<1, 1024, 0, s>>>(a, h_loop); }));
   EXG_CUDA_TRY(cudaGraphInstantiate(&wave_graph_, G, 0));
   int joint_kernels = 0;
-  for (int L = 0; L < 4; ++L)
+  for (int L = 0; L < 5; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
   wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
   wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;

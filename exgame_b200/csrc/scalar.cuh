@@ -21,6 +21,8 @@ EXG_HD double s_exp(double x) { return exp(x); }
 EXG_HD float s_exp(float x) { return expf(x); }
 EXG_HD double s_log(double x) { return log(x); }
 EXG_HD float s_log(float x) { return logf(x); }
+EXG_HD double s_abs(double x) { return fabs(x); }
+EXG_HD float s_abs(float x) { return fabsf(x); }
 
 template <int N, class R>
 struct Dual {
@@ -91,6 +93,13 @@ template <int N, class R> EXG_HD Dual<N, R> s_atan2(const Dual<N, R>& y, const D
 #pragma unroll
   for (int i = 0; i < N; ++i) r.g[i] = y.g[i] * (x.v * inv) - x.g[i] * (y.v * inv);
   return r;
+}
+
+template <int N, class R> EXG_HD Dual<N, R> s_exp(const Dual<N, R>& a) { R e = s_exp(a.v); return a.scaled(e, e); }
+template <int N, class R> EXG_HD Dual<N, R> s_log(const Dual<N, R>& a) { return a.scaled(s_log(a.v), R(1) / a.v); }
+// |x| with the derivative sign(x) (0 at x = 0, as the reference's Tangent takes it)
+template <int N, class R> EXG_HD Dual<N, R> s_abs(const Dual<N, R>& a) {
+  return a.scaled(s_abs(a.v), a.v > R(0) ? R(1) : (a.v < R(0) ? R(-1) : R(0)));
 }
 
 template <class S> EXG_HD S sq(const S& x) { return x * x; }

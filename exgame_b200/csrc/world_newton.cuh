@@ -154,7 +154,7 @@ class NewtonWorld {
   int wave_min_dyn_ = 32, wave_max_levels_ = 64;
   int n_cta_ = 0, n_wave_ = 0;
   int wave_counts_[4] = {0, 0, 0, 0};  // body, dynamic node, joint and cell items
-  int wave_law_first_[5] = {0, 0, 0, 0, 0};  // joint items of law L: [first[L], first[L+1])
+  int wave_law_first_[6] = {0, 0, 0, 0, 0, 0};  // joint items of law L: [first[L], first[L+1]); L = 4: traced laws
   std::vector<int> wave_level_ptr_;
   DevArr<int> dw_isl_, dw_dyn_first_, dw_live_;
   DevArr<IslandDesc> dw_desc_;  // island descriptors in wave-slot order

@@ -92,7 +92,7 @@ def test_point_bushing_tree_conserves_momentum_on_both_schedules(device, precisi
     bodies["momentum"] = rng.normal(size=(len(bodies), 6)) * 0.5
     bush = np.zeros(len(joints), dtype=JOINT_DTYPE)
     bush["law"], bush["a"], bush["b"] = BUSHING, joints["a"], joints["b"]
-    # anchors at the midpoint of the two centres, in each body's frame at rest orientation
+    # anchors at the body centres: a zero-length spring between them, damped
     bush["params"][:, 6] = 200.0
     bush["params"][:, 7] = 2.0
     params = step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10, exact_jacobian=True)

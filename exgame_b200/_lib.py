@@ -226,7 +226,7 @@ class Device:
         check(lib().exg_device_stream(self.handle, ctypes.byref(s)))
         return s.value
 
-    TUNE_GRAVITY_CTAS_PER_SM, TUNE_WAVE_BLOCKS_PER_SM, TUNE_WAVE_MIN_BODIES = 1, 2, 3
+    TUNE_GRAVITY_CTAS_PER_SM, TUNE_WAVE_BLOCKS_PER_SM, TUNE_WAVE_MIN_BODIES, TUNE_WAVE_NARROW_LEVEL = 1, 2, 3, 4
 
     def set_tuning(self, key, value):
         check(lib().exg_device_set_tuning(self.handle, int(key), int(value)), "exg_device_set_tuning")

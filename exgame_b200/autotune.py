@@ -10,6 +10,9 @@ time from the library's own event profiler), keeps the fastest, and leaves it se
   gravity CTAs per SM   persistent one-warp CTAs of the mixed gravity kernel
   wave blocks per SM    grid cap of the wave schedule's data kernels
   wave threshold        dynamic bodies from which an island takes the wave schedule
+  narrow level          elimination levels up to this many nodes (over all wave islands) take one
+                        warp per node, wider ones one thread per node; tuned on a batch of trees
+                        large enough to have levels of both kinds
 """
 import numpy as np
 
@@ -19,6 +22,7 @@ from .abi import GRAVITY_PLUMMER, JOINT_DTYPE, LIE_EULER, NEWTON, PRECISION_MIXE
 GRAVITY_CTAS = (8, 12, 16, 21, 32)
 WAVE_BLOCKS = (4, 8, 16)
 WAVE_THRESHOLDS = (8, 16, 32, 256)
+NARROW_LEVELS = (8192, 32768, 1 << 30)
 
 
 def _time(dev, kinds, world, steps):
@@ -33,7 +37,7 @@ def _time(dev, kinds, world, steps):
 def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, seed=11):
     """Measure the candidates on `dev`, set the fastest, return the choices and their timings."""
     D = _lib.Device
-    out = {"gravity_ctas_per_sm": {}, "wave_blocks_per_sm": {}, "wave_min_bodies": {}}
+    out = {"gravity_ctas_per_sm": {}, "wave_blocks_per_sm": {}, "wave_min_bodies": {}, "wave_narrow_level": {}}
     g = scenarios.gravity_world(gravity_bodies, 1000.0, seed=seed)
     gw = _lib.DeviceWorld(dev, g, np.zeros(0, dtype=JOINT_DTYPE),
                           step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=PRECISION_MIXED,
@@ -63,5 +67,16 @@ def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, see
     batch.close()
     best_t = min(out["wave_min_bodies"], key=out["wave_min_bodies"].get)
     dev.set_tuning(D.TUNE_WAVE_MIN_BODIES, best_t)
+    # wide levels need many large trees at once: 48 trees of 2048 bodies
+    wide = [(*scenarios.tree_world(2048, seed=seed + 100 + k), p) for k in range(48)]
+    wb = _lib.DeviceBatch(dev, wide)
+    wb.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, best_t)
+    for nl in NARROW_LEVELS:
+        dev.set_tuning(D.TUNE_WAVE_NARROW_LEVEL, nl)
+        out["wave_narrow_level"][nl] = _time(dev, kinds, wb, steps)
+    wb.close()
+    best_n = min(out["wave_narrow_level"], key=out["wave_narrow_level"].get)
+    dev.set_tuning(D.TUNE_WAVE_NARROW_LEVEL, best_n)
     return {"gravity_ctas_per_sm": best_g, "wave_blocks_per_sm": best_b, "wave_min_bodies": best_t,
+            "wave_narrow_level": best_n,
             "ms": {k: {str(c): round(v, 4) for c, v in d.items()} for k, d in out.items()}}

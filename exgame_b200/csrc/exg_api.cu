@@ -186,6 +186,10 @@ int exg_device_set_tuning(exg_device_t dev, int32_t key, int32_t value) {
       if (value < 1) return EXG_ERR_INVALID_ARGUMENT;
       dev->tune_wave_min_bodies = value;
       return EXG_OK;
+    case EXG_TUNE_WAVE_NARROW_LEVEL:
+      if (value < 1 || value > (1 << 30)) return EXG_ERR_INVALID_ARGUMENT;
+      dev->tune_wave_narrow_level = value;
+      return EXG_OK;
     default:
       return EXG_ERR_INVALID_ARGUMENT;
   }
@@ -197,6 +201,7 @@ int exg_device_get_tuning(exg_device_t dev, int32_t key, int32_t* value) {
     case EXG_TUNE_GRAVITY_CTAS_PER_SM: *value = dev->tune_gravity_ctas_per_sm; return EXG_OK;
     case EXG_TUNE_WAVE_BLOCKS_PER_SM: *value = dev->tune_wave_blocks_per_sm; return EXG_OK;
     case EXG_TUNE_WAVE_MIN_BODIES: *value = dev->tune_wave_min_bodies; return EXG_OK;
+    case EXG_TUNE_WAVE_NARROW_LEVEL: *value = dev->tune_wave_narrow_level; return EXG_OK;
     default: return EXG_ERR_INVALID_ARGUMENT;
   }
 }

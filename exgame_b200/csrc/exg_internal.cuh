@@ -51,6 +51,7 @@ struct exg_device_s {
   std::atomic<int> tune_gravity_ctas_per_sm{32};  // persistent one-warp CTAs of the mixed gravity kernel
   std::atomic<int> tune_wave_blocks_per_sm{8};    // grid cap of the wave's 256-thread data kernels (128-thread: twice)
   std::atomic<int> tune_wave_min_bodies{32};      // default wave threshold of new world handles
+  std::atomic<int> tune_wave_narrow_level{8192};  // elimination levels up to this many nodes: a warp per node
 };
 
 // Brackets one launch with events when profiling is on (no-op otherwise).

@@ -407,12 +407,18 @@ __global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveA
       if (!((active >> (4 * j)) & 1u)) continue;  // no joint here, or its island did not evaluate slices
       const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
       const IslandDesc& d = a.wdesc[jt.x];
-      J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
-                (size_t)jt.y * 4 * kJacStride + KIND * kHalf;
-      const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
-      float4* dst4 = reinterpret_cast<float4*>(dstj);
-      constexpr int kVec = kHalf * (int)sizeof(J) / 16;
-      for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
+      J* recj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
+                (size_t)jt.y * 4 * kJacStride;
+      if (KIND == 1) {  // the twist slices, into records 2 and 3
+        const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
+        float4* dst4 = reinterpret_cast<float4*>(recj + kHalf);
+        constexpr int kVec = kHalf * (int)sizeof(J) / 16;
+        for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
+      } else {  // the pose slices meet the twist slices: records 0 and 1 become pf P + vf V
+        const WaveCtl& wj = a.ctl[jt.x];
+        const double pf = wj.pf, vf = wj.vf;
+        for (int e = lane; e < kHalf; e += 32) recj[e] = combine_term(pf, vf, stage[wib][j][e], recj[kHalf + e]);
+      }
     }
     __syncwarp();
   }
@@ -437,8 +443,8 @@ void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cu
   const int per = 2 * dev->tune_wave_blocks_per_sm;
   if (LAW != LAW_TORSIONAL) {  // the assembly knows the torsional slices in closed form
     const int g = grid_for(dev, 32LL * ((n + 7) / 8), 128, per);
-    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);
-    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);
+    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);  // twist slices first: the pose
+    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);  // launch combines them
   }
   k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, sv>>>(a, first, n);
 }
@@ -515,13 +521,13 @@ __device__ __forceinline__ void load4(const double* p, double o[4]) {
   o[0] = x.x; o[1] = x.y; o[2] = y.x; o[3] = y.y;
 }
 
-// Entries e0 .. e0+3 of one assembly term's pose (p) and velocity (v) blocks in slice precision;
-// returns whether the row end flips their sign. A torsional term has them in closed form
-// (joint_jacobian_part, value for value): zero pose columns, g = -/+ c / warp^2 on the angular
-// diagonal (entries 21, 28, 35) of the velocity columns.
+// Entries e0 .. e0+3 of one assembly term's combined block pf P + vf V (combine_term) in slice
+// precision; returns whether the row end flips their sign. A torsional term has its slices in
+// closed form (joint_jacobian_part, value for value): P = 0, V = -/+ c / warp^2 on the angular
+// diagonal (entries 21, 28, 35), combined here as the island kernel combines its slices.
 template <bool MIXED>
-__device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, typename JacType<MIXED>::T p[4],
-                                         typename JacType<MIXED>::T v[4]) {
+__device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, double pf, double vf,
+                                         typename JacType<MIXED>::T t[4]) {
   typedef typename JacType<MIXED>::T J;
   const int term = raw & ~kTermTorsional;
   const int q = term >> 2, ce = term & 1;
@@ -532,24 +538,21 @@ __device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, typename
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int e = e0 + m;
-      p[m] = J(0);
-      v[m] = (e >= 21 && e % 7 == 0) ? g : J(0);
+      t[m] = combine_term(pf, vf, J(0), (e >= 21 && e % 7 == 0) ? g : J(0));
     }
   } else {
-    load4(jac_slice<MIXED>(c, q, ce) + e0, p);
-    load4(jac_slice<MIXED>(c, q, 2 + ce) + e0, v);
+    load4(jac_slice<MIXED>(c, q, ce) + e0, t);
   }
   return (term >> 1) & 1;
 }
 
-// acc += pf p + vf v entry by entry, in FP64, with the term's sign (as op_assemble adds a term).
+// acc += the term entry by entry, in FP64, with its sign (as op_assemble adds a term).
 template <typename J>
-__device__ __forceinline__ void asm_add(double acc[4], double pf, double vf, bool re, const J p[4], const J v[4]) {
+__device__ __forceinline__ void asm_add(double acc[4], bool re, const J t[4]) {
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
-    double pv = double(p[m]), vv = double(v[m]);
-    if (re) { pv = -pv; vv = -vv; }
-    acc[m] = acc[m] + pf * pv + vf * vv;
+    const double u = double(t[m]);
+    acc[m] = acc[m] + (re ? -u : u);
   }
 }
 
@@ -582,9 +585,9 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
     for (int k = p0; k < p1; ++k) {
       const int j = (k - p0) % 9;
       if (j == 0) mine = (k + sub < p1) ? terms[k + sub] : 0;
-      J pa[4], va[4];
-      const bool ra = asm_term<MIXED>(c, __shfl_sync(gmask, mine, 9 * grp + j), e0, pa, va);
-      asm_add(acc, pf, vf, ra, pa, va);
+      J ta[4];
+      const bool ra = asm_term<MIXED>(c, __shfl_sync(gmask, mine, 9 * grp + j), e0, pf, vf, ta);
+      asm_add(acc, ra, ta);
     }
     double* dst = (kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc)) + 36 * (size_t)i + e0;
     reinterpret_cast<double2*>(dst)[0] = make_double2(acc[0], acc[1]);
@@ -748,15 +751,21 @@ __global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, 
 // warp-cooperative operations, which do per entry exactly the single-thread arithmetic, so the two
 // kernels give the same bits.
 constexpr int kSolveWarps = 4;
-constexpr int kNarrowLevel = 8192;  // nodes: levels up to this size take the warp kernel (measured:
-                                    // 2048 -> 8192 saved 1.5 %, 16384 and 32768 no more)
+// Levels of at most dev->tune_wave_narrow_level nodes (default 8192) take the warp kernel, wider
+// ones the thread kernel; the autotuner measures the threshold.
+// A narrow level is a chain of dependent loads per node; the kernel issues every load that waits
+// on no other one together at the start (the node's blocks and right-hand side, the parent
+// couplings staged into shared memory for the products, the children's range) and fetches the
+// children's finished products four at a time, subtracting them in child order.
 __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs a, int first, int count) {
-  __shared__ __align__(16) double sh[kSolveWarps][36 * 3 + 8];
+  __shared__ __align__(16) double sh[kSolveWarps][36 * 5 + 8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* Dm = sh[wib];
   double* Dinv = Dm + 36;
   double* S = Dm + 72;
-  double* b = Dm + 108;
+  double* Ap = Dm + 108;  // A_pc, staged
+  double* Ac = Dm + 144;  // A_cp, staged
+  double* b = Dm + 180;
   const int e1 = lane + 32;
   const bool has1 = e1 < 36;
   for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
@@ -765,17 +774,51 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs
     if (w.state != WS_DIR) continue;
     const Ctx c = wave_ctx_lite(a, it.x);
     const size_t i = it.y;
+    const int* chp = c.A.ch_ptr + c.d.dyn_off;
+    const int u0 = chp[i], u1 = chp[i + 1];
+    const int par = c.A.dn_parent[c.d.dyn_off + i];
     double d0 = c.s.D[36 * i + lane], d1 = has1 ? c.s.D[36 * i + e1] : 0.0;
     double bb = lane < 6 ? c.s.rhs[6 * i + lane] : 0.0;
-    const int* chp = c.A.ch_ptr + c.d.dyn_off;
-    for (int u = chp[i]; u < chp[i + 1]; ++u) {
-      const size_t ch = c.A.ch_idx[u];
-      d0 = d0 - c.s.S[36 * ch + lane];
-      if (has1) d1 = d1 - c.s.S[36 * ch + e1];
-      if (lane < 6) bb = bb - c.s.dv[6 * ch + lane];
+    // a root's coupling slots hold nothing it reads; loading them anyway keeps the loads unconditional
+    const double ap0 = c.s.Apc[36 * i + lane], ap1 = has1 ? c.s.Apc[36 * i + e1] : 0.0;
+    const double ac0 = c.s.Acp[36 * i + lane], ac1 = has1 ? c.s.Acp[36 * i + e1] : 0.0;
+    for (int ub = u0; ub < u1; ub += 32) {
+      const int nc = min(32, u1 - ub);
+      const int chl = lane < nc ? c.A.ch_idx[ub + lane] : 0;
+      int k = 0;
+      for (; k + 4 <= nc; k += 4) {
+        size_t ch[4];
+        double p0[4], p1[4], q[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) ch[h] = (size_t)__shfl_sync(0xffffffffu, chl, k + h);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          p0[h] = c.s.S[36 * ch[h] + lane];
+          p1[h] = has1 ? c.s.S[36 * ch[h] + e1] : 0.0;
+          q[h] = lane < 6 ? c.s.dv[6 * ch[h] + lane] : 0.0;
+        }
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+          d0 = d0 - p0[h];
+          if (has1) d1 = d1 - p1[h];
+          if (lane < 6) bb = bb - q[h];
+        }
+      }
+      for (; k < nc; ++k) {
+        const size_t ch = (size_t)__shfl_sync(0xffffffffu, chl, k);
+        d0 = d0 - c.s.S[36 * ch + lane];
+        if (has1) d1 = d1 - c.s.S[36 * ch + e1];
+        if (lane < 6) bb = bb - c.s.dv[6 * ch + lane];
+      }
     }
     Dm[lane] = d0;
-    if (has1) Dm[e1] = d1;
+    Ap[lane] = ap0;
+    Ac[lane] = ac0;
+    if (has1) {
+      Dm[e1] = d1;
+      Ap[e1] = ap1;
+      Ac[e1] = ac1;
+    }
     if (lane < 6) {
       b[lane] = bb;
       c.s.bvec[6 * i + lane] = bb;
@@ -784,10 +827,10 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs
     if (!warp_inverse6(Dm, Dinv) && lane == 0) atomicOr(&w.singular, 1);
     c.s.Dinv[36 * i + lane] = Dinv[lane];
     if (has1) c.s.Dinv[36 * i + e1] = Dinv[e1];
-    if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
-      warp_mm6<false>(c.s.Apc + 36 * i, Dinv, S);        // S = Apc Dinv
-      warp_mm6<false>(S, c.s.Acp + 36 * i, c.s.S + 36 * i);  // P = S Acp, in S's slot
-      warp_mv6(S, b, c.s.dv + 6 * i);                      // q = S b, in dv's slot
+    if (par >= 0) {
+      warp_mm6<false>(Ap, Dinv, S);                   // S = Apc Dinv
+      warp_mm6<false>(S, Ac, c.s.S + 36 * i);         // P = S Acp, in S's slot
+      warp_mv6(S, b, c.s.dv + 6 * i);                 // q = S b, in dv's slot
     } else {
       warp_mv6(Dinv, b, c.s.dv + 6 * i);
     }
@@ -830,17 +873,33 @@ __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
   }
 }
 
-// Back substitution with one warp per node (lanes 0..5 one row each), for narrow levels; the
-// warp operations do the single-thread arithmetic per entry.
+// Back substitution with one warp per node (lanes 0..5 one row each), for narrow levels: each lane
+// loads its rows of A_cp and D^-1 and its right-hand side entry while the parent index resolves,
+// then y = b - A_cp x_p and x = D^-1 y with y passed by shuffle; the same sums in the same order
+// as warp_mv6_sub / warp_mv6.
 __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_up_warp(WaveArgs a, int first, int count) {
+  const int lane = threadIdx.x & 31;
   for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
     const int2 it = a.level[first + t];
     if (a.ctl[it.x].state != WS_DIR) continue;
     const Ctx c = wave_ctx_lite(a, it.x);
     const size_t i = it.y;
     const size_t p = c.A.dn_parent[c.d.dyn_off + i];
-    warp_mv6_sub(c.s.Acp + 36 * i, c.s.dv + 6 * p, c.s.bvec + 6 * i);
-    warp_mv6(c.s.Dinv + 36 * i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
+    const int r = lane < 6 ? lane : 0;
+    double ar[6], dr[6], xp[6];
+    ld_n<6>(c.s.Acp + 36 * i + 6 * r, ar);
+    ld_n<6>(c.s.Dinv + 36 * i + 6 * r, dr);
+    double y = c.s.bvec[6 * i + r];
+    ld_n<6>(c.s.dv + 6 * p, xp);
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s += ar[k] * xp[k];
+    y = y - s;
+    if (lane < 6) c.s.bvec[6 * i + lane] = y;
+    double x = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) x += dr[k] * __shfl_sync(0xffffffffu, y, k);
+    if (lane < 6) c.s.dv[6 * i + lane] = x;
   }
 }
 
@@ -1031,13 +1090,15 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   if (rc != EXG_OK) return rc;
   static_assert(sizeof(WorldRef) <= sizeof(wave_graph_world_), "world snapshot too small");
   if (wave_graph_ && (std::memcmp(wave_graph_world_, &a.W, sizeof(WorldRef)) != 0 ||
-                      wave_graph_tuning_ != dev->tune_wave_blocks_per_sm || wave_graph_host_loop_ != wave_host_loop_)) {
+                      wave_graph_tuning_ != dev->tune_wave_blocks_per_sm ||
+                      wave_graph_narrow_ != dev->tune_wave_narrow_level || wave_graph_host_loop_ != wave_host_loop_)) {
     cudaGraphExecDestroy(wave_graph_);  // a world array moved since the capture
     wave_graph_ = nullptr;
   }
   if (!wave_graph_) {
     std::memcpy(wave_graph_world_, &a.W, sizeof(WorldRef));
     wave_graph_tuning_ = dev->tune_wave_blocks_per_sm;
+    wave_graph_narrow_ = dev->tune_wave_narrow_level;
     wave_graph_host_loop_ = wave_host_loop_;
     rc = wave_host_loop_ ? build_wave_round_graph(dev, &a, s) : build_wave_graph(dev, &a, s);
     if (rc != EXG_OK) return rc;
@@ -1080,6 +1141,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
+  const int narrow = dev->tune_wave_narrow_level;
   cudaGraph_t g;
   if (int rc = ensure_side()) return rc;
   EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -1094,14 +1156,14 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
   for (int L = nl - 1; L >= 0; --L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    if (count <= kNarrowLevel)
+    if (count <= narrow)
       k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
     else
       k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
   }
   for (int L = 1; L < nl; ++L) {
     int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    if (count <= kNarrowLevel)
+    if (count <= narrow)
       k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
     else
       k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
@@ -1165,6 +1227,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
+  const int narrow = dev->tune_wave_narrow_level;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
   if (int rc = ensure_side()) return rc;
   cudaGraph_t G = nullptr;
@@ -1223,7 +1286,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
     for (int L = nl - 1; L >= 0; --L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      if (count <= kNarrowLevel)
+      if (count <= narrow)
         k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
                                                                                                          count);
       else
@@ -1231,7 +1294,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
     }
     for (int L = 1; L < nl; ++L) {
       int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      if (count <= kNarrowLevel)
+      if (count <= narrow)
         k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
                                                                                                        count);
       else

@@ -176,6 +176,7 @@ class NewtonWorld {
   int wave_kernels_eval_ = 0, wave_kernels_dir_ = 0, wave_kernels_end_ = 0;
   long long seen_rounds_ = 0, seen_dir_ = 0, seen_end_ = 0;
   int wave_graph_tuning_ = 0;  // the launch-shape tuning the round graph was captured with
+  int wave_graph_narrow_ = 0;
   int last_wave_rounds_ = 0;
   std::vector<WorldSrc> src_;
   bool dirty_ = true;

@@ -177,6 +177,10 @@ EXG_API int exg_abi_version(void);
 #define EXG_TUNE_GRAVITY_CTAS_PER_SM 1
 #define EXG_TUNE_WAVE_BLOCKS_PER_SM 2
 #define EXG_TUNE_WAVE_MIN_BODIES 3
+/*   WAVE_NARROW_LEVEL   elimination levels of the wave with at most this many nodes take one warp per
+ *                       node, wider ones one thread per node (1..2^30, default 8192; the two
+ *                       kernels give the same bits) */
+#define EXG_TUNE_WAVE_NARROW_LEVEL 4
 EXG_API int exg_device_set_tuning(exg_device_t dev, int32_t key, int32_t value);
 EXG_API int exg_device_get_tuning(exg_device_t dev, int32_t key, int32_t* value);
 

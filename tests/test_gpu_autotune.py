@@ -21,10 +21,11 @@ def mixed_batch():
     return worlds
 
 
-def run(device, worlds, g, w, t):
+def run(device, worlds, g, w, t, n=8192):
     device.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, g)
     device.set_tuning(D.TUNE_WAVE_BLOCKS_PER_SM, w)
     device.set_tuning(D.TUNE_WAVE_MIN_BODIES, t)
+    device.set_tuning(D.TUNE_WAVE_NARROW_LEVEL, n)
     batch = _lib.DeviceBatch(device, worlds)
     batch.step(3)
     out = batch.bodies()
@@ -34,21 +35,22 @@ def run(device, worlds, g, w, t):
 
 def test_tuning_never_changes_results(device):
     worlds = mixed_batch()
-    defaults = [device.get_tuning(k) for k in (1, 2, 3)]
+    defaults = [device.get_tuning(k) for k in (1, 2, 3, 4)]
     try:
         ref = run(device, worlds, 32, 8, 32)
-        for g, w, t in ((8, 4, 1), (21, 16, 256), (1, 1, 1 << 20)):
-            got = run(device, worlds, g, w, t)
+        for g, w, t, n in ((8, 4, 1, 1), (21, 16, 256, 1 << 30), (1, 1, 1 << 20, 64), (32, 8, 1, 1 << 30)):
+            got = run(device, worlds, g, w, t, n)
             assert np.array_equal(got["pose"], ref["pose"]) and np.array_equal(got["momentum"], ref["momentum"])
     finally:
-        for k, v in zip((1, 2, 3), defaults):
+        for k, v in zip((1, 2, 3, 4), defaults):
             device.set_tuning(k, v)
 
 
 def test_autotune_picks_candidates(device):
-    defaults = [device.get_tuning(k) for k in (1, 2, 3)]
+    defaults = [device.get_tuning(k) for k in (1, 2, 3, 4)]
     try:
         r = autotune.autotune(device, gravity_bodies=8192, trees=8, tree_bodies=600, steps=2)
+        assert r["wave_narrow_level"] in autotune.NARROW_LEVELS
         assert r["gravity_ctas_per_sm"] in autotune.GRAVITY_CTAS
         assert r["wave_blocks_per_sm"] in autotune.WAVE_BLOCKS
         assert r["wave_min_bodies"] in autotune.WAVE_THRESHOLDS
@@ -56,5 +58,5 @@ def test_autotune_picks_candidates(device):
         with pytest.raises(_lib.ExgError):
             device.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, 0)
     finally:
-        for k, v in zip((1, 2, 3), defaults):
+        for k, v in zip((1, 2, 3, 4), defaults):
             device.set_tuning(k, v)

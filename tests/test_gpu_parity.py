@@ -417,3 +417,48 @@ def test_mixed_gravity_world_1000_steps_within_1e6_of_f64(device, oracle):
     fw.step(1000)
     pf, mf = state_error(want, fw.bodies())
     assert pf < 1e-4 and pf > pe, (pf, pe)
+
+
+def rotated_inertia(bodies, seed):
+    """Each body's diagonal box inertia turned into a full tensor R diag R^T (random R): the
+    general Inertia::Rigid path (crates/newton/src/inertia.rs:145-156, 271-345)."""
+    rng = np.random.default_rng(seed)
+    b = bodies.copy()
+    for k in range(len(b)):
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        d = np.diag([b[k]["inertia"][0], b[k]["inertia"][4], b[k]["inertia"][8]])
+        full = q @ d @ q.T
+        b[k]["inertia"] = (0.5 * (full + full.T)).reshape(9)
+        b[k]["diagonal"] = 0
+    b["momentum"][:, 3:] = rng.normal(size=(len(b), 3)) * 0.3  # spin, so the tensor matters
+    return b
+
+
+@pytest.mark.parametrize("precision", [PRECISION_F64, PRECISION_MIXED])
+def test_full_inertia_tensor_newton_both_schedules(device, oracle, precision):
+    bodies, joints = scenarios.tree_world(60, seed=91)
+    bodies = rotated_inertia(bodies, 92)
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=1e-2, tol=1e-10)
+    ow = oracle.OracleWorld(bodies, joints, params)
+    ow.step(20)
+    out = []
+    for min_bodies in (1 << 20, 1):
+        dw = _lib.DeviceWorld(device, bodies, joints, params)
+        dw.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, min_bodies)
+        dw.step(20)
+        pe, me = state_error(ow.bodies(), dw.bodies())
+        assert pe < 1e-9 and me < 1e-7, (min_bodies, pe, me)
+        out.append(dw.bodies())
+        dw.close()
+    assert np.array_equal(out[0]["pose"], out[1]["pose"])
+
+
+@pytest.mark.parametrize("scheme", [LIE_EULER, SYMPLECTIC_EULER, EXPLICIT_EULER])
+def test_full_inertia_tensor_explicit(device, oracle, scheme):
+    bodies, joints = scenarios.chain_world(24, seed=93)
+    bodies = rotated_inertia(bodies, 94)
+    params = step_params(integrator=scheme, gravity_law=GRAVITY_PLUMMER, softening=0.05, dt=1e-3)
+    ow, dw = run_both(oracle, device, bodies, joints, params, 50)
+    pe, me = state_error(ow.bodies(), dw.bodies())
+    assert pe < 1e-10 and me < 1e-9, (pe, me)
+    dw.close()

@@ -515,7 +515,7 @@ def serve_sweep(dev, rates, n_requests, pool_size, tick, rank):
             "plain_fifo": {"body_steps_per_s": bs / done, "p50_latency_s": float(np.percentile(plat, 50)),
                            "p99_latency_s": float(np.percentile(plat, 99))},
         })
-    return {"pool_worlds": len(pool), "steps_per_tick": tick, "sweep": out,
+    return {"pool_worlds": len(pool), "steps_per_tick": tick, "pools": 2, "sweep": out,
             "plain_fifo_model": "FIFO queue, one world at a time, service = steps x that world's FP64 step time "
                                 "measured alone (device time)"}
 
@@ -684,6 +684,8 @@ def main():
     if rank == 0 and world_size == 1 and args.serve_rates:
         rates = [float(x) for x in args.serve_rates.split(",") if x]
         serving = serve_sweep(r["dev"], rates, args.serve_requests, args.serve_pool, args.serve_tick, rank)
+        for s in serving["sweep"]:  # served throughput against the batch rate of the same kind of worlds
+            s["fraction_of_batch_value"] = s["body_steps_per_s"] / r["value"]
     if rank == 0:
         line = {
             "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world_size, "steps": args.steps,

@@ -526,11 +526,12 @@ class Server:
     together; results come back through poll / wait."""
 
     def __init__(self, device, hbm_budget_bytes=150 * 10**9, max_bodies=1 << 22, max_joints=1 << 22,
-                 max_worlds=4096, precision=PRECISION_F64, steps_per_tick=16):
+                 max_worlds=4096, precision=PRECISION_F64, steps_per_tick=16, pools=2):
         self.device = device
         cfg = np.zeros((), dtype=SERVER_CONFIG_DTYPE)
         cfg["hbm_budget_bytes"], cfg["max_bodies"], cfg["max_joints"] = hbm_budget_bytes, max_bodies, max_joints
         cfg["max_worlds"], cfg["precision"], cfg["steps_per_tick"] = max_worlds, precision, steps_per_tick
+        cfg["pools"] = pools
         h = ctypes.c_void_p()
         check(lib().exg_server_create(device.handle, ptr(cfg), ctypes.byref(h)), "exg_server_create")
         self.handle = h

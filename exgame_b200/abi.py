@@ -66,7 +66,7 @@ POOL_USAGE_DTYPE = np.dtype(
 
 SERVER_CONFIG_DTYPE = np.dtype(
     [("hbm_budget_bytes", "<i8"), ("max_bodies", "<i8"), ("max_joints", "<i8"), ("max_worlds", "<i4"),
-     ("precision", "<i4"), ("steps_per_tick", "<i4"), ("reserved", "<i4")],
+     ("precision", "<i4"), ("steps_per_tick", "<i4"), ("pools", "<i4")],
     align=True,
 )
 

@@ -10,6 +10,11 @@
 // their state is read back and their ranges are released for the next admissions. Every world
 // takes exactly its requested steps, with the arithmetic it would have alone.
 //
+// With cfg.pools = 2 the capacities are split between two pools, each on a CUDA stream of its own
+// (EXG_OPT_OWN_STREAM) and stepped by a worker thread of its own; both take requests from the one
+// arrival queue under the one memory budget, so one pool's admissions, state uploads and
+// read-backs run on the host and its copy engines while the other pool's tick runs on the GPU.
+//
 // The loop uses only the public C ABI, so it is also a worked example of serving on top of it.
 #include <algorithm>
 #include <chrono>
@@ -41,15 +46,23 @@ struct Request {
   int32_t left = 0;  // steps still to take (host mirror of the pool's counter)
   int64_t footprint = 0;
   int32_t slot = -1;
+  int lane = -1;  // the pool it runs in
   int status = EXG_PENDING;
   double t_submit = 0, t_admit = 0, t_done = 0;
 };
 
 }  // namespace
 
+struct ServerLane {  // one pool and the worker thread that steps it
+  exg_world_t pool = nullptr;
+  std::vector<std::shared_ptr<Request>> running;  // by pool slot (this lane's worker only)
+  int n_running = 0;                              // (under the server's mu)
+  std::thread worker;
+};
+
 struct exg_server_s {
   exg_device_t dev = nullptr;
-  exg_world_t pool = nullptr;
+  std::vector<ServerLane> lanes;
   exg_server_config_t cfg{};
   Clock::time_point t0 = Clock::now();        // request clocks
   Clock::time_point t_stats = Clock::now();   // start of the statistics window
@@ -57,14 +70,12 @@ struct exg_server_s {
   std::condition_variable cv_work, cv_done;
   std::deque<std::shared_ptr<Request>> queue;                     // submitted, not yet admitted
   std::unordered_map<uint64_t, std::shared_ptr<Request>> known;  // every request not yet collected
-  std::vector<std::shared_ptr<Request>> running;                 // by pool slot (worker only)
-  int n_running = 0;
+  int n_running = 0;                                              // over all lanes
   int64_t resident = 0;
   uint64_t next_id = 1;
   bool stop = false;
   bool worker_gone = false;
   int worker_status = EXG_OK;
-  std::thread worker;
   // statistics (under mu)
   int64_t submitted = 0, completed = 0, failed = 0, ticks = 0, steps_launched = 0, body_steps = 0;
   int32_t peak_running = 0;
@@ -88,21 +99,22 @@ void finish_locked(exg_server_s* S, const std::shared_ptr<Request>& r, int statu
 }
 
 // Release a running request's slot and publish its outcome.
-void retire(exg_server_s* S, const std::shared_ptr<Request>& r, int status) {
+void retire(exg_server_s* S, ServerLane& L, const std::shared_ptr<Request>& r, int status) {
   int st = status;
   if (st == EXG_OK && !r->bodies.empty())
-    st = exg_batch_get_world(S->pool, r->slot, r->bodies.data(), (int32_t)r->bodies.size());
-  exg_pool_release(S->pool, r->slot);
+    st = exg_batch_get_world(L.pool, r->slot, r->bodies.data(), (int32_t)r->bodies.size());
+  exg_pool_release(L.pool, r->slot);
   std::lock_guard<std::mutex> lk(S->mu);
-  S->running[r->slot].reset();
+  L.running[r->slot].reset();
+  --L.n_running;
   --S->n_running;
   S->resident -= r->footprint;
   finish_locked(S, r, st);
   S->cv_done.notify_all();
 }
 
-// Admit queued requests in arrival order while the budget and the pool allow.
-void admit(exg_server_s* S) {
+// Admit queued requests in arrival order into this lane's pool while the budget and the pool allow.
+void admit(exg_server_s* S, ServerLane& L, int lane) {
   for (;;) {
     std::shared_ptr<Request> r;
     {
@@ -120,24 +132,26 @@ void admit(exg_server_s* S) {
       continue;
     }
     int32_t slot = -1;
-    int rc = exg_pool_admit(S->pool, r->bodies.data(), (int32_t)r->bodies.size(), r->joints.data(),
+    int rc = exg_pool_admit(L.pool, r->bodies.data(), (int32_t)r->bodies.size(), r->joints.data(),
                             (int32_t)r->joints.size(), &r->params, &slot);
-    if (rc == EXG_OK) rc = exg_pool_set_steps(S->pool, slot, r->steps);
+    if (rc == EXG_OK) rc = exg_pool_set_steps(L.pool, slot, r->steps);
     std::lock_guard<std::mutex> lk(S->mu);
-    if (rc == EXG_ERR_OUT_OF_MEMORY && S->n_running > 0) {  // wait for ranges to free up
+    if (rc == EXG_ERR_OUT_OF_MEMORY && (L.n_running > 0 || S->n_running > 0)) {  // wait for ranges to free up
       S->queue.push_front(r);
       return;
     }
     if (rc != EXG_OK) {
-      if (slot >= 0) exg_pool_release(S->pool, slot);
+      if (slot >= 0) exg_pool_release(L.pool, slot);
       finish_locked(S, r, rc);
       S->cv_done.notify_all();
       continue;
     }
     r->slot = slot;
+    r->lane = lane;
     r->left = r->steps;
     r->t_admit = seconds_since(S->t0);
-    S->running[slot] = r;
+    L.running[slot] = r;
+    ++L.n_running;
     ++S->n_running;
     S->resident += r->footprint;
     S->peak_running = std::max<int32_t>(S->peak_running, S->n_running);
@@ -145,48 +159,54 @@ void admit(exg_server_s* S) {
   }
 }
 
-void run(exg_server_s* S) {
+void run(exg_server_s* S, int lane) {
+  ServerLane& L = S->lanes[lane];
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      if (S->stop) break;
-      if (S->queue.empty() && S->n_running == 0) {
+      if (S->stop || S->worker_gone) break;
+      if (S->queue.empty() && L.n_running == 0) {
         S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
         continue;
       }
     }
-    admit(S);
+    admit(S, L, lane);
     std::vector<std::shared_ptr<Request>> live;
-    for (auto& r : S->running)
+    for (auto& r : L.running)
       if (r) live.push_back(r);
-    if (live.empty()) continue;
+    if (live.empty()) {
+      std::unique_lock<std::mutex> lk(S->mu);  // the queue head waits for the other lane's memory
+      S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+      continue;
+    }
     int32_t tick = 0;
     for (auto& r : live) tick = std::max(tick, r->left);
     tick = std::min(tick, S->cfg.steps_per_tick);
     Clock::time_point t_tick = Clock::now();
-    int rc = exg_world_step(S->pool, tick);
+    int rc = exg_world_step(L.pool, tick);
     for (auto& r : live) r->left = std::max(0, r->left - tick);
     if (rc == EXG_ERR_FATAL) {
       // a guarded site fired in some worlds: those fail, the rest go on
       for (auto& r : live) {
         exg_world_stats_t st;
-        if (exg_batch_world_stats(S->pool, r->slot, &st) == EXG_OK && st.fatal) retire(S, r, EXG_ERR_FATAL);
+        if (exg_batch_world_stats(L.pool, r->slot, &st) == EXG_OK && st.fatal) retire(S, L, r, EXG_ERR_FATAL);
       }
       rc = EXG_OK;
     }
     if (rc != EXG_OK) {  // the device is unusable: fail everything and stop serving
       for (auto& r : live)
-        if (S->running[r->slot]) retire(S, r, rc);
+        if (L.running[r->slot]) retire(S, L, r, rc);
       std::lock_guard<std::mutex> lk(S->mu);
       S->worker_gone = true;
       S->worker_status = rc;
       for (auto& q : S->queue) finish_locked(S, q, EXG_ERR_WORKER_GONE);
       S->queue.clear();
       S->cv_done.notify_all();
+      S->cv_work.notify_all();
       return;
     }
     for (auto& r : live)
-      if (r->left == 0 && S->running[r->slot]) retire(S, r, EXG_OK);
+      if (r->left == 0 && L.running[r->slot]) retire(S, L, r, EXG_OK);
     std::lock_guard<std::mutex> lk(S->mu);
     ++S->ticks;
     S->steps_launched += tick;
@@ -224,26 +244,44 @@ int exg_server_create(exg_device_t dev, const exg_server_config_t* cfg, exg_serv
   if (!dev || !cfg || !out || cfg->hbm_budget_bytes <= 0 || cfg->max_worlds <= 0 || cfg->max_bodies <= 0 ||
       cfg->max_joints < 0 || cfg->steps_per_tick <= 0)
     return EXG_ERR_INVALID_ARGUMENT;
+  const int pools = cfg->pools == 0 ? 1 : cfg->pools;
+  if (pools < 1 || pools > 2 || cfg->max_worlds < pools) return EXG_ERR_INVALID_ARGUMENT;
   exg_server_s* S = new (std::nothrow) exg_server_s();
   if (!S) return EXG_ERR_OUT_OF_MEMORY;
   S->dev = dev;
   S->cfg = *cfg;
+  S->cfg.pools = pools;
+  S->lanes.resize(pools);
   exg_pool_config_t pc{};
-  pc.max_bodies = cfg->max_bodies;
-  pc.max_joints = cfg->max_joints;
-  pc.max_worlds = cfg->max_worlds;
+  pc.max_bodies = cfg->max_bodies / pools;
+  pc.max_joints = cfg->max_joints / pools;
+  pc.max_worlds = cfg->max_worlds / pools;
   pc.precision = cfg->precision;
-  int rc = exg_pool_create(dev, &pc, &S->pool);
-  if (rc != EXG_OK) {
+  int rc = EXG_OK;
+  for (int k = 0; k < pools && rc == EXG_OK; ++k) {
+    rc = exg_pool_create(dev, &pc, &S->lanes[k].pool);
+    if (rc == EXG_OK && pools > 1) rc = exg_world_set_option(S->lanes[k].pool, EXG_OPT_OWN_STREAM, 1);
+    S->lanes[k].running.resize(pc.max_worlds);
+  }
+  auto undo = [&]() {
+    for (ServerLane& L : S->lanes)
+      if (L.pool) exg_world_destroy(L.pool);
     delete S;
+  };
+  if (rc != EXG_OK) {
+    undo();
     return rc;
   }
-  S->running.resize(cfg->max_worlds);
   try {
-    S->worker = std::thread(run, S);
+    for (int k = 0; k < pools; ++k) S->lanes[k].worker = std::thread(run, S, k);
   } catch (...) {
-    exg_world_destroy(S->pool);
-    delete S;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->stop = true;
+    }
+    for (ServerLane& L : S->lanes)
+      if (L.worker.joinable()) L.worker.join();
+    undo();
     return EXG_ERR_BACKEND;
   }
   *out = S;
@@ -255,7 +293,8 @@ int exg_server_submit(exg_server_t S, const exg_body_t* bodies, int32_t n, const
   if (!S || !id || !params || n < 0 || nj < 0 || steps < 0 || (n > 0 && !bodies) || (nj > 0 && !joints))
     return EXG_ERR_INVALID_ARGUMENT;
   if (params->precision != S->cfg.precision) return EXG_ERR_INVALID_ARGUMENT;
-  if (n > S->cfg.max_bodies || nj > S->cfg.max_joints) return EXG_ERR_OUT_OF_MEMORY;  // can never fit
+  if (n > S->cfg.max_bodies / S->cfg.pools || nj > S->cfg.max_joints / S->cfg.pools)
+    return EXG_ERR_OUT_OF_MEMORY;  // can never fit a pool
   int64_t fp = 0;
   int rc = exg_world_footprint(n, nj, params, &fp);
   if (rc != EXG_OK) return rc;
@@ -274,7 +313,7 @@ int exg_server_submit(exg_server_t S, const exg_body_t* bodies, int32_t n, const
   S->queue.push_back(r);
   ++S->submitted;
   *id = r->id;
-  S->cv_work.notify_one();
+  S->cv_work.notify_all();
   return EXG_OK;
 }
 
@@ -348,8 +387,9 @@ int exg_server_destroy(exg_server_t S) {
     S->stop = true;
     S->cv_work.notify_all();
   }
-  if (S->worker.joinable()) S->worker.join();
-  exg_world_destroy(S->pool);
+  for (ServerLane& L : S->lanes)
+    if (L.worker.joinable()) L.worker.join();
+  for (ServerLane& L : S->lanes) exg_world_destroy(L.pool);
   delete S;
   return EXG_OK;
 }

@@ -287,7 +287,10 @@ typedef struct {
   int32_t max_worlds;
   int32_t precision;        /* every request must use this precision */
   int32_t steps_per_tick;   /* steps between admissions / completions */
-  int32_t reserved;
+  /* 1 (or 0): one pool. 2: the capacities split between two pools on streams of their own, each
+   * stepped by its own worker thread, so one pool's admissions, uploads and read-backs overlap the
+   * other pool's tick on the GPU. */
+  int32_t pools;
 } exg_server_config_t;
 typedef struct {
   int64_t steps;

@@ -107,14 +107,16 @@ def test_pool_capacity_errors_leave_it_usable(device):
     pool.close()
 
 
+@pytest.mark.parametrize("pools", [1, 2])
 @pytest.mark.parametrize("precision", [PRECISION_F64, PRECISION_MIXED])
-def test_served_results_are_the_same_alone_and_in_the_mix(device, precision):
+def test_served_results_are_the_same_alone_and_in_the_mix(device, precision, pools):
     """Requests of uneven size and step count submitted from two threads while others run; each
-    result equals the same world stepped alone for its step count, bit for bit."""
+    result equals the same world stepped alone for its step count, bit for bit, with one pool and
+    with two pools whose ticks overlap on the GPU."""
     worlds = world_set(precision)
     steps = [7, 31, 3, 50, 12, 1, 26, 40]
     srv = _lib.Server(device, max_bodies=8192, max_joints=8192, max_worlds=16, precision=precision,
-                      steps_per_tick=8)
+                      steps_per_tick=8, pools=pools)
     ids = [None] * len(worlds)
 
     def producer(ks):

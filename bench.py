@@ -265,9 +265,10 @@ def run_ours(args, rank, world_size, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
     dev = _lib.Device(local_rank)
-    tuning = autotune.autotune(dev) if args.autotune else None  # launch shapes only: results do not change
     parts, cfg = workload(args.workload, rank)
     worlds = make_worlds(dev, parts)
+    # launch shapes only, timed on this workload's own steps: results do not change
+    tuning = autotune.autotune(dev, workload=worlds[0], steps=2) if args.autotune else None
     n_bodies = sum(len(b) for (b, _, _) in parts)
     flush_buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 

@@ -34,10 +34,49 @@ def _time(dev, kinds, world, steps):
     return ms / steps
 
 
-def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, seed=11):
-    """Measure the candidates on `dev`, set the fastest, return the choices and their timings."""
+def _best(d):
+    return min(d, key=d.get)
+
+
+def _tune_on(dev, world, out, steps):
+    """Every knob timed on the caller's own handle, one after another, each left at its best."""
+    D = _lib.Device
+    kinds = (D.PROF_NEWTON, D.PROF_NEWTON_WAVE)
+    for c in GRAVITY_CTAS:
+        dev.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, c)
+        out["gravity_ctas_per_sm"][c] = _time(dev, (D.PROF_GRAVITY,), world, steps)
+    dev.set_tuning(D.TUNE_GRAVITY_CTAS_PER_SM, _best(out["gravity_ctas_per_sm"]))
+    for b in WAVE_BLOCKS:
+        dev.set_tuning(D.TUNE_WAVE_BLOCKS_PER_SM, b)
+        out["wave_blocks_per_sm"][b] = _time(dev, kinds, world, steps)
+    dev.set_tuning(D.TUNE_WAVE_BLOCKS_PER_SM, _best(out["wave_blocks_per_sm"]))
+    for t in WAVE_THRESHOLDS:
+        world.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, t)
+        out["wave_min_bodies"][t] = _time(dev, kinds, world, steps)
+    best_t = _best(out["wave_min_bodies"])
+    world.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, best_t)
+    dev.set_tuning(D.TUNE_WAVE_MIN_BODIES, best_t)
+    for nl in NARROW_LEVELS:
+        dev.set_tuning(D.TUNE_WAVE_NARROW_LEVEL, nl)
+        out["wave_narrow_level"][nl] = _time(dev, kinds, world, steps)
+    dev.set_tuning(D.TUNE_WAVE_NARROW_LEVEL, _best(out["wave_narrow_level"]))
+
+
+def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, seed=11, workload=None):
+    """Measure the candidates on `dev`, set the fastest, return the choices and their timings.
+
+    With `workload` (an open DeviceWorld or DeviceBatch) every candidate is timed on that handle's
+    own steps, which advance its state, and its wave threshold is left at the best candidate;
+    otherwise on the synthetic worlds above."""
     D = _lib.Device
     out = {"gravity_ctas_per_sm": {}, "wave_blocks_per_sm": {}, "wave_min_bodies": {}, "wave_narrow_level": {}}
+    if workload is not None:
+        _tune_on(dev, workload, out, steps)
+        return {"gravity_ctas_per_sm": _best(out["gravity_ctas_per_sm"]),
+                "wave_blocks_per_sm": _best(out["wave_blocks_per_sm"]),
+                "wave_min_bodies": _best(out["wave_min_bodies"]),
+                "wave_narrow_level": _best(out["wave_narrow_level"]), "timed_on": "workload",
+                "ms": {k: {str(c): round(v, 4) for c, v in d.items()} for k, d in out.items()}}
     g = scenarios.gravity_world(gravity_bodies, 1000.0, seed=seed)
     gw = _lib.DeviceWorld(dev, g, np.zeros(0, dtype=JOINT_DTYPE),
                           step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=PRECISION_MIXED,

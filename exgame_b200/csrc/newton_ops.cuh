@@ -287,15 +287,6 @@ __device__ inline void op_joint(const Ctx& c, const double* x, int q, int slice,
   if (MIXED && slice == 0) op_joint_value(c, x, q);
 }
 
-// A joint end's term of the Newton matrix, entry by entry: pf * (pose slice) + vf * (twist slice),
-// formed once in FP64 and kept in slice precision (the wave stores it in place of the pose slice;
-// the island kernel forms it on the fly from the same slices). Rounding pinned by intrinsics, so
-// both schedules produce the same bits.
-template <class J>
-__device__ __forceinline__ J combine_term(double pf, double vf, J p, J v) {
-  return J(__fma_rn(vf, double(v), __dmul_rn(pf, double(p))));
-}
-
 // Gather + POST (functions::gather_term, body_post) of dynamic node i: mass block, residual and
 // its scales; returns the node's worst relative residual^2 (newton.rs:139-151).
 __device__ inline double op_post(const Ctx& c, const double* x, double half, int i) {
@@ -383,8 +374,9 @@ __device__ inline double op_assemble(const Ctx& c, double pf, double vf, int cel
     int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
     const auto* jp = jac_slice<MIXED>(c, q, ce);
     const auto* jv = jac_slice<MIXED>(c, q, 2 + ce);
-    const double t = double(combine_term(pf, vf, jp[r * 6 + col], jv[r * 6 + col]));
-    acc = acc + (re ? -t : t);
+    double pv = double(jp[r * 6 + col]), vv = double(jv[r * 6 + col]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc = acc + pf * pv + vf * vv;
   }
   double* dst = kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc);
   dst[36 * (size_t)i + e] = acc;
@@ -411,8 +403,9 @@ __device__ inline double op_assemble_lu(const Ctx& c, double pf, double vf, int 
     int q = term >> 2, re = (term >> 1) & 1, ce = term & 1;
     const auto* jp = jac_slice<MIXED>(c, q, ce);
     const auto* jv = jac_slice<MIXED>(c, q, 2 + ce);
-    const double u = double(combine_term(pf, vf, jp[r * 6 + col], jv[r * 6 + col]));
-    acc = acc + (re ? -u : u);
+    double pv = double(jp[r * 6 + col]), vv = double(jv[r * 6 + col]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc = acc + pf * pv + vf * vv;
   }
   lu_block(c, t)[e] = acc;
   return acc;

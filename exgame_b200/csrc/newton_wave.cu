@@ -407,18 +407,12 @@ __global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveA
       if (!((active >> (4 * j)) & 1u)) continue;  // no joint here, or its island did not evaluate slices
       const int2 jt = make_int2(__shfl_sync(0xffffffffu, it.x, 4 * j), __shfl_sync(0xffffffffu, it.y, 4 * j));
       const IslandDesc& d = a.wdesc[jt.x];
-      J* recj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
-                (size_t)jt.y * 4 * kJacStride;
-      if (KIND == 1) {  // the twist slices, into records 2 and 3
-        const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
-        float4* dst4 = reinterpret_cast<float4*>(recj + kHalf);
-        constexpr int kVec = kHalf * (int)sizeof(J) / 16;
-        for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
-      } else {  // the pose slices meet the twist slices: records 0 and 1 become pf P + vf V
-        const WaveCtl& wj = a.ctl[jt.x];
-        const double pf = wj.pf, vf = wj.vf;
-        for (int e = lane; e < kHalf; e += 32) recj[e] = combine_term(pf, vf, stage[wib][j][e], recj[kHalf + e]);
-      }
+      J* dstj = reinterpret_cast<J*>(carve(a.A.scratch + d.scratch_off, d.nb, d.nj, d.m).jac) +
+                (size_t)jt.y * 4 * kJacStride + KIND * kHalf;
+      const float4* src = reinterpret_cast<const float4*>(&stage[wib][j][0]);
+      float4* dst4 = reinterpret_cast<float4*>(dstj);
+      constexpr int kVec = kHalf * (int)sizeof(J) / 16;
+      for (int v = lane; v < kVec; v += 32) dst4[v] = src[v];
     }
     __syncwarp();
   }
@@ -443,8 +437,8 @@ void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cu
   const int per = 2 * dev->tune_wave_blocks_per_sm;
   if (LAW != LAW_TORSIONAL) {  // the assembly knows the torsional slices in closed form
     const int g = grid_for(dev, 32LL * ((n + 7) / 8), 128, per);
-    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);  // twist slices first: the pose
-    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);  // launch combines them
+    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);
+    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);
   }
   k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, sv>>>(a, first, n);
 }
@@ -521,13 +515,13 @@ __device__ __forceinline__ void load4(const double* p, double o[4]) {
   o[0] = x.x; o[1] = x.y; o[2] = y.x; o[3] = y.y;
 }
 
-// Entries e0 .. e0+3 of one assembly term's combined block pf P + vf V (combine_term) in slice
-// precision; returns whether the row end flips their sign. A torsional term has its slices in
-// closed form (joint_jacobian_part, value for value): P = 0, V = -/+ c / warp^2 on the angular
-// diagonal (entries 21, 28, 35), combined here as the island kernel combines its slices.
+// Entries e0 .. e0+3 of one assembly term's pose (p) and velocity (v) blocks in slice precision;
+// returns whether the row end flips their sign. A torsional term has them in closed form
+// (joint_jacobian_part, value for value): zero pose columns, g = -/+ c / warp^2 on the angular
+// diagonal (entries 21, 28, 35) of the velocity columns.
 template <bool MIXED>
-__device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, double pf, double vf,
-                                         typename JacType<MIXED>::T t[4]) {
+__device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, typename JacType<MIXED>::T p[4],
+                                         typename JacType<MIXED>::T v[4]) {
   typedef typename JacType<MIXED>::T J;
   const int term = raw & ~kTermTorsional;
   const int q = term >> 2, ce = term & 1;
@@ -538,21 +532,24 @@ __device__ __forceinline__ bool asm_term(const Ctx& c, int raw, int e0, double p
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const int e = e0 + m;
-      t[m] = combine_term(pf, vf, J(0), (e >= 21 && e % 7 == 0) ? g : J(0));
+      p[m] = J(0);
+      v[m] = (e >= 21 && e % 7 == 0) ? g : J(0);
     }
   } else {
-    load4(jac_slice<MIXED>(c, q, ce) + e0, t);
+    load4(jac_slice<MIXED>(c, q, ce) + e0, p);
+    load4(jac_slice<MIXED>(c, q, 2 + ce) + e0, v);
   }
   return (term >> 1) & 1;
 }
 
-// acc += the term entry by entry, in FP64, with its sign (as op_assemble adds a term).
+// acc += pf p + vf v entry by entry, in FP64, with the term's sign (as op_assemble adds a term).
 template <typename J>
-__device__ __forceinline__ void asm_add(double acc[4], bool re, const J t[4]) {
+__device__ __forceinline__ void asm_add(double acc[4], double pf, double vf, bool re, const J p[4], const J v[4]) {
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
-    const double u = double(t[m]);
-    acc[m] = acc[m] + (re ? -u : u);
+    double pv = double(p[m]), vv = double(v[m]);
+    if (re) { pv = -pv; vv = -vv; }
+    acc[m] = acc[m] + pf * pv + vf * vv;
   }
 }
 
@@ -585,9 +582,9 @@ __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
     for (int k = p0; k < p1; ++k) {
       const int j = (k - p0) % 9;
       if (j == 0) mine = (k + sub < p1) ? terms[k + sub] : 0;
-      J ta[4];
-      const bool ra = asm_term<MIXED>(c, __shfl_sync(gmask, mine, 9 * grp + j), e0, pf, vf, ta);
-      asm_add(acc, ra, ta);
+      J pa[4], va[4];
+      const bool ra = asm_term<MIXED>(c, __shfl_sync(gmask, mine, 9 * grp + j), e0, pa, va);
+      asm_add(acc, pf, vf, ra, pa, va);
     }
     double* dst = (kind == 0 ? c.s.D : (kind == 1 ? c.s.Acp : c.s.Apc)) + 36 * (size_t)i + e0;
     reinterpret_cast<double2*>(dst)[0] = make_double2(acc[0], acc[1]);

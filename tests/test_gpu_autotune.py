@@ -60,3 +60,32 @@ def test_autotune_picks_candidates(device):
     finally:
         for k, v in zip((1, 2, 3, 4), defaults):
             device.set_tuning(k, v)
+
+
+def test_autotune_on_a_workload_keeps_its_results(device):
+    """Timed on the caller's own batch: the tuned batch, after the tuner's steps and as many more,
+    holds the same bits as an untuned copy stepped as often."""
+    defaults = [device.get_tuning(k) for k in (1, 2, 3, 4)]
+    p = step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10, exact_jacobian=True)
+    worlds = [(*scenarios.tree_world(n, seed=70 + k), p) for k, n in enumerate((30, 200, 900))]
+    g = scenarios.gravity_world(2048, 100.0, seed=77)
+    worlds.append((g, np.zeros(0, dtype=JOINT_DTYPE),
+                   step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=PRECISION_MIXED,
+                               softening=0.05, dt=1e-3)))
+    try:
+        tuned = _lib.DeviceBatch(device, worlds)
+        r = autotune.autotune(device, workload=tuned, steps=1)
+        assert r["timed_on"] == "workload" and r["wave_min_bodies"] in autotune.WAVE_THRESHOLDS
+        n_steps = 2 * (len(autotune.GRAVITY_CTAS) + len(autotune.WAVE_BLOCKS) + len(autotune.WAVE_THRESHOLDS) +
+                       len(autotune.NARROW_LEVELS))
+        tuned.step(3)
+        plain = _lib.DeviceBatch(device, worlds)
+        plain.step(n_steps + 3)
+        for k in range(len(worlds)):
+            a, b = tuned.world_bodies(k), plain.world_bodies(k)
+            assert np.array_equal(a["pose"], b["pose"]) and np.array_equal(a["momentum"], b["momentum"]), k
+        tuned.close()
+        plain.close()
+    finally:
+        for k, v in zip((1, 2, 3, 4), defaults):
+            device.set_tuning(k, v)

@@ -516,7 +516,7 @@ NewtonWorld::~NewtonWorld() {
   if (fork_) cudaEventDestroy(fork_);
   if (join_) cudaEventDestroy(join_);
   if (side_) cudaStreamDestroy(side_);
-  for (DevArr<int>* a : {&dw_isl_, &dw_dyn_first_, &dw_live_}) a->release();
+  for (DevArr<int>* a : {&dw_isl_, &dw_dyn_first_, &dw_live_, &dw_seg_, &dw_act_, &dw_pre_}) a->release();
   for (DevArr<int2>* a : {&dw_body_, &dw_dyn_, &dw_joint_, &dw_cell_, &dw_level_, &dw_cell_terms_}) a->release();
   dw_ctl_.release();
   dw_nodesq_.release();

@@ -65,7 +65,18 @@ struct WaveArgs {
   const int* dyn_first; // first dynamic-node item of each wave slot (n_isl + 1 entries)
   double* nodesq;       // per dynamic-node item: a sum of squares to reduce per island
   int* live;            // counters, see kLive* below
+  // Item ranges (kRange* below; the joint items of each law and the nodes of each elimination
+  // level are ranges of their own). Within a range items are ordered by slot, so slot k's items
+  // are [seg[k], seg[k + 1]) of it: seg holds n_isl + 1 offsets per range.
+  const int* seg;
+  int n_ranges;
+  int* act;             // this round's unfinished slots, ascending (k_w_round_items)
+  int* pre;             // per range, n_isl + 1 entries: item offsets of the listed slots
 };
+
+// Ranges of WaveArgs::seg: the body, dynamic-node and cell items, then the joint items of law
+// 0 .. 4 (4: the traced laws), then the nodes of elimination level 0, 1, ...
+enum { kRangeBody = 0, kRangeDyn = 1, kRangeCell = 2, kRangeJoint = 3, kRangeLevel = 8 };
 
 int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
   long long g = (items + threads - 1) / threads;
@@ -76,8 +87,10 @@ int grid_for(exg_device_s* dev, long long items, int threads, int per_sm) {
 // Device counters of the wave (a.live): islands still stepping after the last round, rounds of
 // this step, the round cap reached with islands unfinished, and cumulative rounds / direction
 // sections / end sections (for the host's count of launched kernels).
+// kLiveListed / kLiveSparse: the slots k_w_round_items listed for this round and whether the
+// data kernels walk only their items.
 enum { kLiveIslands = 0, kLiveRounds = 1, kLiveOverflow = 2, kLiveTotalRounds = 3, kLiveTotalDir = 4,
-       kLiveTotalEnd = 5, kLiveCount = 6 };
+       kLiveTotalEnd = 5, kLiveListed = 6, kLiveSparse = 7, kLiveCount = 8 };
 // Rounds one step may take before the wave gives up on it (EXG_ERR_FATAL); a step of a
 // well-formed island needs at most spans x iterations x (1 + probes), far fewer in practice.
 constexpr int kMaxRoundsPerStep = 1 << 17;
@@ -105,6 +118,7 @@ __global__ void k_w_init(WaveArgs a) {
   if (gtid() == 0) {
     a.live[kLiveRounds] = 0;
     a.live[kLiveOverflow] = 0;
+    a.live[kLiveSparse] = 0;
   }
   for (int k = gtid(); k < a.n_isl; k += gthreads()) {
     WaveCtl& c = a.ctl[k];
@@ -345,9 +359,108 @@ __global__ void k_w_count_flat(WaveArgs a) {
   }
 }
 
+// Round start: the slots still stepping (state other than WS_DONE, which no island leaves before
+// the step ends), ascending. When they are at most a sixteenth of all slots (a step's last rounds,
+// where a few islands iterate or sub-divide on after the rest have committed) the round is sparse:
+// for every range, one warp sums the listed slots' item counts into pre, and the data kernels walk
+// those items only (RoundItems). With more slots listed, the search that maps an item number to
+// its item costs more than skipping the finished islands' items. One block.
+constexpr int kListThreads = 1024;
+__global__ void __launch_bounds__(kListThreads) k_w_round_items(WaveArgs a) {
+  __shared__ int warp_sum[kListThreads / 32];
+  __shared__ int listed;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) listed = 0;
+  __syncthreads();
+  for (int k0 = 0; k0 < a.n_isl; k0 += kListThreads) {
+    const int k = k0 + threadIdx.x;
+    const int on = (k < a.n_isl && a.ctl[k].state != WS_DONE) ? 1 : 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) warp_sum[wid] = __popc(bal);
+    __syncthreads();
+    int before = listed;
+    for (int u = 0; u < wid; ++u) before += warp_sum[u];
+    if (on) a.act[before + __popc(bal & ((1u << lane) - 1u))] = k;
+    __syncthreads();
+    if (threadIdx.x == kListThreads - 1) listed = before + __popc(bal);
+    __syncthreads();
+  }
+  const int n_act = listed;
+  const int sparse = 16 * n_act <= a.n_isl ? 1 : 0;
+  if (threadIdx.x == 0) {
+    a.live[kLiveListed] = n_act;
+    a.live[kLiveSparse] = sparse;
+  }
+  if (!sparse) return;
+  const int stride = a.n_isl + 1;
+  for (int r = wid; r < a.n_ranges; r += kListThreads / 32) {
+    const int* sg = a.seg + (size_t)r * stride;
+    int* pr = a.pre + (size_t)r * stride;
+    if (lane == 0) pr[0] = 0;
+    int carry = 0;
+    for (int i0 = 0; i0 < n_act; i0 += 32) {
+      const int i = i0 + lane;
+      int c = 0;
+      if (i < n_act) {
+        const int k = a.act[i];
+        c = sg[k + 1] - sg[k];
+      }
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, c, o);
+        if (lane >= o) c += y;
+      }
+      if (i < n_act) pr[i + 1] = carry + c;
+      carry += __shfl_sync(0xffffffffu, c, 31);
+    }
+  }
+}
+
+// The items of one range that a data kernel visits this round, numbered 0 .. n-1: all of them, or
+// in a sparse round those of the listed slots in slot order (at() maps the number to the item's
+// offset in the range by a search of pre). Which items a kernel skips, and the arithmetic of those
+// it does not, are the same in both forms.
+struct RoundItems {
+  int n;
+  int n_act;
+  const int* pre;  // nullptr: every item, at(v) = v
+  const int* seg;
+  const int* act;
+  __device__ __forceinline__ int at(int v) const {
+    if (!pre) return v;
+    int lo = 0, hi = n_act - 1;  // the last listed slot whose items start at or before v
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre[mid] <= v) lo = mid;
+      else hi = mid - 1;
+    }
+    return seg[act[lo]] + (v - pre[lo]);
+  }
+};
+
+__device__ __forceinline__ RoundItems round_items(const WaveArgs& a, int range, int n) {
+  RoundItems r;
+  r.n = n;
+  r.n_act = 0;
+  r.pre = nullptr;
+  r.seg = nullptr;
+  r.act = nullptr;
+  if (a.live[kLiveSparse]) {
+    const size_t stride = (size_t)a.n_isl + 1;
+    r.n_act = a.live[kLiveListed];
+    r.pre = a.pre + range * stride;
+    r.seg = a.seg + range * stride;
+    r.act = a.act;
+    r.n = r.pre[r.n_act];
+  }
+  return r;
+}
+
 // ── data phases over all islands' items ─────────────────────────────────────
 __global__ void k_w_start(WaveArgs a) {
-  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeBody, a.n_body);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.body[t];
     if (!(a.ctl[it.x].flags & F_START)) continue;
     Ctx c = wave_ctx(a, it.x);
@@ -359,7 +472,9 @@ __global__ void k_w_start(WaveArgs a) {
 }
 
 __global__ void k_w_pre(WaveArgs a) {
-  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeBody, a.n_body);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.body[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
@@ -381,18 +496,19 @@ __global__ void k_w_pre(WaveArgs a) {
 // records into the warp's staging block in shared memory, and the warp then stores each joint's
 // two contiguous records (2 x 36 values, 16-byte aligned) with 16-byte stores.
 template <bool MIXED, int LAW, int KIND>
-__global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveArgs a, int first, int n) {
+__global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveArgs a, int first, int n, int range) {
   typedef typename JacType<MIXED>::T J;
   constexpr int kHalf = 2 * kJacStride;  // values per joint and kind
   __shared__ __align__(16) J stage[4][8][kHalf];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const long long total = 32LL * ((n + 7) / 8);
+  const RoundItems R = round_items(a, range, n);
+  const long long total = 32LL * ((R.n + 7) / 8);
   for (long long base = gtid() - lane; base < total; base += gthreads()) {  // warp-uniform loop
     const int jq = (int)(base >> 5) * 8 + (lane >> 2), slice = 2 * KIND + ((lane >> 1) & 1), half = lane & 1;
     bool on = false;
     int2 it = make_int2(0, 0);
-    if (jq < n) {
-      it = a.joint[first + jq];
+    if (jq < R.n) {
+      it = a.joint[first + R.at(jq)];
       const int ev = a.ctl[it.x].eval;
       if (ev == EV_FULL || ev == EV_JAC) {
         on = true;
@@ -419,8 +535,10 @@ __global__ void __launch_bounds__(128, KIND == 0 ? 4 : 8) k_w_joint_slices(WaveA
 }
 
 template <bool MIXED, int LAW>
-__global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, int n) {
-  for (int t = gtid(); t < n; t += gthreads()) {
+__global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, int n, int range) {
+  const RoundItems R = round_items(a, range, n);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.joint[first + t];
     const int ev = a.ctl[it.x].eval;
     // (no torsional slices are evaluated, so in FP64 the torsional values come from here too)
@@ -433,14 +551,15 @@ __global__ void __launch_bounds__(128) k_w_joint_values(WaveArgs a, int first, i
 // The slices of one law on s, its values on sv (independent work: slices write the Jacobian
 // records, values the joint wrenches).
 template <bool MIXED, int LAW>
-void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, cudaStream_t s, cudaStream_t sv) {
+void launch_joints_of(exg_device_s* dev, const WaveArgs& a, int first, int n, int range, cudaStream_t s,
+                      cudaStream_t sv) {
   const int per = 2 * dev->tune_wave_blocks_per_sm;
   if (LAW != LAW_TORSIONAL) {  // the assembly knows the torsional slices in closed form
     const int g = grid_for(dev, 32LL * ((n + 7) / 8), 128, per);
-    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n);
-    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n);
+    k_w_joint_slices<MIXED, LAW, 0><<<g, 128, 0, s>>>(a, first, n, range);
+    k_w_joint_slices<MIXED, LAW, 1><<<g, 128, 0, s>>>(a, first, n, range);
   }
-  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, sv>>>(a, first, n);
+  k_w_joint_values<MIXED, LAW><<<grid_for(dev, n, 128, per), 128, 0, sv>>>(a, first, n, range);
 }
 
 template <bool MIXED>
@@ -449,16 +568,19 @@ void launch_joints_by_law(exg_device_s* dev, const WaveArgs& a, const int* law_f
   for (int L = 0; L < 5; ++L) {
     const int first = law_first[L], n = law_first[L + 1] - first;
     if (n == 0) continue;
-    if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, s, sv);
-    else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, s, sv);
-    else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, s, sv);
-    else if (L == 3) launch_joints_of<MIXED, 3>(dev, a, first, n, s, sv);
-    else launch_joints_of<MIXED, -1>(dev, a, first, n, s, sv);  // traced laws: the law read per joint
+    const int r = kRangeJoint + L;
+    if (L == 0) launch_joints_of<MIXED, 0>(dev, a, first, n, r, s, sv);
+    else if (L == 1) launch_joints_of<MIXED, 1>(dev, a, first, n, r, s, sv);
+    else if (L == 2) launch_joints_of<MIXED, 2>(dev, a, first, n, r, s, sv);
+    else if (L == 3) launch_joints_of<MIXED, 3>(dev, a, first, n, r, s, sv);
+    else launch_joints_of<MIXED, -1>(dev, a, first, n, r, s, sv);  // traced laws: the law read per joint
   }
 }
 
 __global__ void __launch_bounds__(256, 2) k_w_post(WaveArgs a) {
-  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeDyn, a.n_dyn);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.dyn[t];
     WaveCtl& w = a.ctl[it.x];
     if (w.eval != EV_FULL && w.eval != EV_PLAIN) continue;
@@ -471,7 +593,9 @@ __global__ void __launch_bounds__(256, 2) k_w_post(WaveArgs a) {
 
 // Body copies of the control decisions, in a fixed order per body.
 __global__ void k_w_copy_bodies(WaveArgs a) {
-  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeBody, a.n_body);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.body[t];
     const WaveCtl& w = a.ctl[it.x];
     const int f = w.flags;
@@ -561,9 +685,10 @@ template <bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_w_assemble(WaveArgs a) {
   typedef typename JacType<MIXED>::T J;
   const int lane = threadIdx.x & 31, grp = lane / 9, e0 = 4 * (lane - 9 * grp);
-  for (int t0 = 3 * (gtid() >> 5); t0 < a.n_cell; t0 += 3 * (gthreads() >> 5)) {
-    const int t = t0 + grp;
-    if (grp >= 3 || t >= a.n_cell) continue;
+  const RoundItems R = round_items(a, kRangeCell, a.n_cell);
+  for (int t0 = 3 * (gtid() >> 5); t0 < R.n; t0 += 3 * (gthreads() >> 5)) {
+    if (grp >= 3 || t0 + grp >= R.n) continue;
+    const int t = R.at(t0 + grp);
     const int2 it = a.cell[t], range = a.cell_range[t];
     const WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
@@ -603,7 +728,9 @@ __device__ __forceinline__ bool wants_norms(const WaveCtl& w) {
 // Per dynamic node, a fixed-order sum of squares: of its assembled blocks (the diagonal, and the
 // two parent couplings of a non-root node) for ||A||_F^2, or of its mass0 block for ||M||_F^2.
 __global__ void k_w_node_sq(WaveArgs a, int mass) {
-  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeDyn, a.n_dyn);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.dyn[t];
     const WaveCtl& w = a.ctl[it.x];
     if (!wants_norms(w)) continue;
@@ -662,8 +789,10 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int ma
 // terms for the parent — S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's
 // slot until the back substitution writes dv) — so a parent only sums finished products; a root
 // solves for dv. The arithmetic per entry is the island kernel's (newton_ops.cuh).
-__global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, int count) {
-  for (int t = gtid(); t < count; t += gthreads()) {
+__global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, int count, int range) {
+  const RoundItems R = round_items(a, range, count);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.level[first + t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
@@ -754,7 +883,7 @@ constexpr int kSolveWarps = 4;
 // on no other one together at the start (the node's blocks and right-hand side, the parent
 // couplings staged into shared memory for the products, the children's range) and fetches the
 // children's finished products four at a time, subtracting them in child order.
-__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs a, int first, int count) {
+__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs a, int first, int count, int range) {
   __shared__ __align__(16) double sh[kSolveWarps][36 * 5 + 8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   double* Dm = sh[wib];
@@ -765,7 +894,9 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs
   double* b = Dm + 180;
   const int e1 = lane + 32;
   const bool has1 = e1 < 36;
-  for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
+  const RoundItems R = round_items(a, range, count);
+  for (int vi = gtid() >> 5; vi < R.n; vi += gthreads() >> 5) {  // warp-uniform
+    const int t = R.at(vi);
     const int2 it = a.level[first + t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
@@ -835,8 +966,10 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs
   }
 }
 
-__global__ void k_w_solve_up(WaveArgs a, int first, int count) {
-  for (int t = gtid(); t < count; t += gthreads()) {
+__global__ void k_w_solve_up(WaveArgs a, int first, int count, int range) {
+  const RoundItems R = round_items(a, range, count);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.level[first + t];
     if (a.ctl[it.x].state != WS_DIR) continue;
     Ctx c = wave_ctx_lite(a, it.x);
@@ -874,9 +1007,11 @@ __global__ void k_w_solve_up(WaveArgs a, int first, int count) {
 // loads its rows of A_cp and D^-1 and its right-hand side entry while the parent index resolves,
 // then y = b - A_cp x_p and x = D^-1 y with y passed by shuffle; the same sums in the same order
 // as warp_mv6_sub / warp_mv6.
-__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_up_warp(WaveArgs a, int first, int count) {
+__global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_up_warp(WaveArgs a, int first, int count, int range) {
   const int lane = threadIdx.x & 31;
-  for (int t = gtid() >> 5; t < count; t += gthreads() >> 5) {  // warp-uniform
+  const RoundItems R = round_items(a, range, count);
+  for (int vi = gtid() >> 5; vi < R.n; vi += gthreads() >> 5) {  // warp-uniform
+    const int t = R.at(vi);
     const int2 it = a.level[first + t];
     if (a.ctl[it.x].state != WS_DIR) continue;
     const Ctx c = wave_ctx_lite(a, it.x);
@@ -903,7 +1038,9 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_up_warp(WaveArgs a
 // A singular pivot makes the whole correction NaN (the line search then rejects it); otherwise
 // record whether any component is non-zero.
 __global__ void k_w_nz(WaveArgs a) {
-  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeDyn, a.n_dyn);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.dyn[t];
     WaveCtl& w = a.ctl[it.x];
     if (w.state != WS_DIR) continue;
@@ -927,7 +1064,9 @@ __global__ void k_w_nz(WaveArgs a) {
 
 // Span end: the best iterate back into vm, then (after the control kernel) the commit.
 __global__ void k_w_restore(WaveArgs a) {
-  for (int t = gtid(); t < a.n_body; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeBody, a.n_body);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.body[t];
     if (a.ctl[it.x].state != WS_END) continue;
     Ctx c = wave_ctx(a, it.x);
@@ -938,7 +1077,9 @@ __global__ void k_w_restore(WaveArgs a) {
 }
 
 __global__ void k_w_commit(WaveArgs a) {
-  for (int t = gtid(); t < a.n_dyn; t += gthreads()) {
+  const RoundItems R = round_items(a, kRangeDyn, a.n_dyn);
+  for (int vi = gtid(); vi < R.n; vi += gthreads()) {
+    const int t = R.at(vi);
     int2 it = a.dyn[t];
     const WaveCtl& w = a.ctl[it.x];
     if (!(w.flags & F_COMMIT)) continue;
@@ -947,6 +1088,30 @@ __global__ void k_w_commit(WaveArgs a) {
   }
 }
 
+
+// The elimination level by level (leaves to roots), then the back substitution (roots to leaves):
+// levels of at most dev->tune_wave_narrow_level nodes take the warp kernels.
+void launch_elimination(exg_device_s* dev, const WaveArgs& a, const std::vector<int>& level_ptr, cudaStream_t s) {
+  const int nl = (int)level_ptr.size() - 1;
+  const int narrow = dev->tune_wave_narrow_level;
+  const int per = 2 * dev->tune_wave_blocks_per_sm;
+  for (int L = nl - 1; L >= 0; --L) {
+    const int first = level_ptr[L], count = level_ptr[L + 1] - first, r = kRangeLevel + L;
+    if (count <= narrow)
+      k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
+                                                                                                       count, r);
+    else
+      k_w_solve_down<<<grid_for(dev, count, 128, per), 128, 0, s>>>(a, first, count, r);
+  }
+  for (int L = 1; L < nl; ++L) {
+    const int first = level_ptr[L], count = level_ptr[L + 1] - first, r = kRangeLevel + L;
+    if (count <= narrow)
+      k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
+                                                                                                     count, r);
+    else
+      k_w_solve_up<<<grid_for(dev, count, 128, per), 128, 0, s>>>(a, first, count, r);
+  }
+}
 
 }  // namespace
 
@@ -1015,6 +1180,21 @@ int NewtonWorld::build_wave(cudaStream_t s) {
     level.insert(level.end(), by[L].begin(), by[L].end());
     wave_level_ptr_.push_back((int)level.size());
   }
+  // each range's per-slot item offsets (items of a range are in slot order)
+  const int n_slots = (int)isl.size();
+  wave_ranges_ = kRangeLevel + max_levels;
+  std::vector<int> seg((size_t)wave_ranges_ * (n_slots + 1), 0);
+  auto offsets = [&](int r, const std::vector<int2>& items, int first, int count) {
+    int* o = seg.data() + (size_t)r * (n_slots + 1);
+    for (int t = first; t < first + count; ++t) ++o[items[t].x + 1];
+    for (int k = 0; k < n_slots; ++k) o[k + 1] += o[k];
+  };
+  offsets(kRangeBody, body, 0, (int)body.size());
+  offsets(kRangeDyn, dyn, 0, (int)dyn.size());
+  offsets(kRangeCell, cell, 0, (int)cell.size());
+  for (int L = 0; L < 5; ++L) offsets(kRangeJoint + L, joint, wave_law_first_[L], wave_law_first_[L + 1] - wave_law_first_[L]);
+  for (int L = 0; L < max_levels; ++L)
+    offsets(kRangeLevel + L, level, wave_level_ptr_[L], wave_level_ptr_[L + 1] - wave_level_ptr_[L]);
   int rc = EXG_OK;
   auto up = [&](auto& d, const auto& h) {
     if (rc == EXG_OK) rc = d.assign(h.data(), (long long)h.size(), s);
@@ -1030,6 +1210,9 @@ int NewtonWorld::build_wave(cudaStream_t s) {
   up(dw_cell_, cell);
   up(dw_cell_terms_, cell_range);
   up(dw_level_, level);
+  up(dw_seg_, seg);
+  if (rc == EXG_OK) rc = dw_act_.reserve(std::max(n_slots, 1), s);
+  if (rc == EXG_OK) rc = dw_pre_.reserve(std::max<long long>((long long)seg.size(), 1), s);
   if (rc == EXG_OK) rc = dw_ctl_.reserve(std::max<long long>((long long)isl.size(), 1) * (long long)sizeof(WaveCtl), s);
   if (rc == EXG_OK) rc = dw_nodesq_.reserve(std::max<long long>((long long)dyn.size(), 1), s);
   if (rc == EXG_OK && dw_live_.cap == 0) {
@@ -1071,6 +1254,10 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   a.dyn_first = dw_dyn_first_.ptr;
   a.nodesq = dw_nodesq_.ptr;
   a.live = dw_live_.ptr;
+  a.seg = dw_seg_.ptr;
+  a.n_ranges = wave_ranges_;
+  a.act = dw_act_.ptr;
+  a.pre = dw_pre_.ptr;
   const int T = 256;
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
@@ -1138,10 +1325,10 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
-  const int narrow = dev->tune_wave_narrow_level;
   cudaGraph_t g;
   if (int rc = ensure_side()) return rc;
   EXG_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  k_w_round_items<<<1, kListThreads, 0, s>>>(a);
   k_w_begin<<<g_isl, T, 0, s>>>(a);
   k_w_start<<<g_body, T, 0, s>>>(a);
   k_w_pre<<<g_body, T, 0, s>>>(a);
@@ -1151,20 +1338,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
   if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
   else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-  for (int L = nl - 1; L >= 0; --L) {
-    int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    if (count <= narrow)
-      k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
-    else
-      k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
-  }
-  for (int L = 1; L < nl; ++L) {
-    int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-    if (count <= narrow)
-      k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first, count);
-    else
-      k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
-  }
+  launch_elimination(dev, a, wave_level_ptr_, s);
   k_w_nz<<<g_dyn, T, 0, s>>>(a);
   k_w_after_solve<<<g_isl, T, 0, s>>>(a);
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
@@ -1186,7 +1360,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   int joint_kernels = 0;
   for (int L = 0; L < 5; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
-  wave_kernels_eval_ = 6 + joint_kernels;
+  wave_kernels_eval_ = 7 + joint_kernels;  // round items, begin .. copy
   wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;
   wave_kernels_end_ = 8;
   return EXG_OK;
@@ -1224,7 +1398,6 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   const int g_cell = grid_for(dev, 32LL * ((a.n_cell + 2) / 3), T, dev->tune_wave_blocks_per_sm);
   const int g_sum = std::min(a.n_isl, std::max(1, dev->sm_count) * 8);
   const int nl = (int)wave_level_ptr_.size() - 1;
-  const int narrow = dev->tune_wave_narrow_level;
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
   if (int rc = ensure_side()) return rc;
   cudaGraph_t G = nullptr;
@@ -1267,6 +1440,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(conditional(G, nullptr, 0, h_loop, cudaGraphCondTypeWhile, &loop, &B));
   // evaluation of every island at its iterate or probe
   EXG_CUDA_TRY(capture(B, {}, [&] {
+    k_w_round_items<<<1, kListThreads, 0, s>>>(a);
     k_w_begin<<<g_isl, T, 0, s>>>(a);
     k_w_start<<<g_body, T, 0, s>>>(a);
     k_w_pre<<<g_body, T, 0, s>>>(a);
@@ -1281,22 +1455,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(capture(BD, {}, [&] {
     if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-    for (int L = nl - 1; L >= 0; --L) {
-      int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      if (count <= narrow)
-        k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
-                                                                                                         count);
-      else
-        k_w_solve_down<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
-    }
-    for (int L = 1; L < nl; ++L) {
-      int first = wave_level_ptr_[L], count = wave_level_ptr_[L + 1] - first;
-      if (count <= narrow)
-        k_w_solve_up_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
-                                                                                                       count);
-      else
-        k_w_solve_up<<<grid_for(dev, count, 128, 2 * dev->tune_wave_blocks_per_sm), 128, 0, s>>>(a, first, count);
-    }
+    launch_elimination(dev, a, wave_level_ptr_, s);
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
@@ -1318,7 +1477,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   int joint_kernels = 0;
   for (int L = 0; L < 5; ++L)
     if (wave_law_first_[L + 1] > wave_law_first_[L]) joint_kernels += (L == LAW_TORSIONAL) ? 1 : 3;
-  wave_kernels_eval_ = 6 + joint_kernels + 2;  // begin .. copy, cond(dir), cond(end), count
+  wave_kernels_eval_ = 7 + joint_kernels + 2;  // round items, begin .. copy, cond(dir), cond(end), count
   wave_kernels_dir_ = 1 + nl + (nl - 1) + 3;
   wave_kernels_end_ = 7;
   return EXG_OK;

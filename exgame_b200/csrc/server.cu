@@ -71,6 +71,7 @@ struct exg_server_s {
   std::deque<std::shared_ptr<Request>> queue;                     // submitted, not yet admitted
   std::unordered_map<uint64_t, std::shared_ptr<Request>> known;  // every request not yet collected
   int n_running = 0;                                              // over all lanes
+  int n_admitting = 0;  // requests taken off the queue whose pool admission is still under way
   int64_t resident = 0;
   uint64_t next_id = 1;
   bool stop = false;
@@ -121,11 +122,18 @@ void admit(exg_server_s* S, ServerLane& L, int lane) {
       std::lock_guard<std::mutex> lk(S->mu);
       if (S->queue.empty()) return;
       r = S->queue.front();
-      if (S->n_running > 0 && S->resident + r->footprint > S->cfg.hbm_budget_bytes) return;
+      const bool others = S->n_running > 0 || S->n_admitting > 0;
+      if (others && S->resident + r->footprint > S->cfg.hbm_budget_bytes) return;
       S->queue.pop_front();
+      // the budget is taken now, under the lock, so the other lane's admission counts it
+      S->resident += r->footprint;
+      ++S->n_admitting;
+      S->peak_resident = std::max(S->peak_resident, S->resident);
     }
     if (r->steps == 0) {  // nothing to step: the result is the input
       std::lock_guard<std::mutex> lk(S->mu);
+      --S->n_admitting;
+      S->resident -= r->footprint;
       r->t_admit = seconds_since(S->t0);
       finish_locked(S, r, EXG_OK);
       S->cv_done.notify_all();
@@ -136,8 +144,10 @@ void admit(exg_server_s* S, ServerLane& L, int lane) {
                             (int32_t)r->joints.size(), &r->params, &slot);
     if (rc == EXG_OK) rc = exg_pool_set_steps(L.pool, slot, r->steps);
     std::lock_guard<std::mutex> lk(S->mu);
-    if (rc == EXG_ERR_OUT_OF_MEMORY && (L.n_running > 0 || S->n_running > 0)) {  // wait for ranges to free up
-      S->queue.push_front(r);
+    --S->n_admitting;
+    if (rc != EXG_OK) S->resident -= r->footprint;
+    if (rc == EXG_ERR_OUT_OF_MEMORY && (L.n_running > 0 || S->n_running > 0 || S->n_admitting > 0)) {
+      S->queue.push_front(r);  // wait for ranges to free up
       return;
     }
     if (rc != EXG_OK) {
@@ -153,9 +163,7 @@ void admit(exg_server_s* S, ServerLane& L, int lane) {
     L.running[slot] = r;
     ++L.n_running;
     ++S->n_running;
-    S->resident += r->footprint;
     S->peak_running = std::max<int32_t>(S->peak_running, S->n_running);
-    S->peak_resident = std::max(S->peak_resident, S->resident);
   }
 }
 

@@ -157,6 +157,10 @@ class NewtonWorld {
   int wave_law_first_[6] = {0, 0, 0, 0, 0, 0};  // joint items of law L: [first[L], first[L+1]); L = 4: traced laws
   std::vector<int> wave_level_ptr_;
   DevArr<int> dw_isl_, dw_dyn_first_, dw_live_;
+  // per item range (body, dynamic node, cell, joint law 0..4, elimination level 0..): each slot's
+  // first item in it (n_wave_ + 1 offsets); the round's listed slots and their item prefixes
+  DevArr<int> dw_seg_, dw_act_, dw_pre_;
+  int wave_ranges_ = 0;
   DevArr<IslandDesc> dw_desc_;  // island descriptors in wave-slot order
   DevArr<int2> dw_body_, dw_dyn_, dw_joint_, dw_cell_, dw_level_;
   DevArr<int2> dw_cell_terms_;  // per cell item: its term range in cell_terms (absolute)

@@ -36,12 +36,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from exgame_b200 import _lib, autotune, scenarios, sharding  # noqa: E402
-from exgame_b200.abi import (BODY_DTYPE, GRAVITY_OFF, NEWTON, PRECISION_F64, PRECISION_MIXED,  # noqa: E402
-                             PRECISION_MIXED_FAST)
+from exgame_b200.abi import (BODY_DTYPE, GRAVITY_OFF, NEWTON, NEWTON_NS_PIVOT, PRECISION_F64,  # noqa: E402
+                             PRECISION_MIXED, PRECISION_MIXED_FAST)
 
 METRIC = "body-steps/s"
 WORLDS = 4096      # config-3 batch size (--worlds)
 SHARD = False      # --shard: one batch split over the ranks instead of one batch per rank
+NS_PIVOT = False   # --ns-pivot: Newton-Schulz pivot inverses on the implicit worlds
 WORLD_SIZE = 1
 FP64_FMA_PER_SM_CLK = 64
 FP32_FMA_PER_SM_CLK = 128
@@ -53,6 +54,12 @@ def load_peaks():
         with open(path) as f:
             return json.load(f), "measured"
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def _with_flag(p, flag):
+    q = p.copy()
+    q["newton_flags"] = int(q["newton_flags"]) | flag
+    return q
 
 
 def workload(name, rank):
@@ -85,12 +92,17 @@ def workload(name, rank):
             worlds = allw
         else:  # each rank its own seeded batch (weak scaling)
             worlds = scenarios.config3_worlds(nw, seed=3 + rank, precision=prec, exact_jacobian=bool(prec))
+        if NS_PIVOT and prec:  # Newton-Schulz pivot inverses on the implicit worlds
+            worlds = [(b, j, _with_flag(p, NEWTON_NS_PIVOT) if int(p["integrator"]) == NEWTON else p)
+                      for b, j, p in worlds]
         n = sum(len(b) for b, _, _ in worlds)
         cfg = {"workload": f"{nw} independent worlds, body counts log-uniform in [8, 8192]: gravity worlds "
                            "(LieEuler, dt 1e-3) and random joint trees (Newton tol 1e-10, dt 1e-2), one batched launch "
                            "set per step, " + ("mixed precision, exact mid-point Newton matrix" if prec else "f64")
                            + " (config 3)",
-               "bodies": n, "worlds": len(worlds), "dtype": "f32 forces / f64 state" if prec else "f64"}
+               "bodies": n, "worlds": len(worlds), "dtype": "f32 forces / f64 state" if prec else "f64",
+               "pivot_inverse": ("Newton-Schulz (warm-started, FP32 steps, FP64 correction)" if NS_PIVOT and prec
+                                 else "FP64 Gauss-Jordan")}
         return worlds, cfg
     raise SystemExit(f"unknown workload {name}")
 
@@ -636,6 +648,8 @@ def main():
     ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ns-pivot", type=int, default=0,
+                    help="1: the implicit worlds invert their pivot blocks by Newton-Schulz (EXG_NEWTON_NS_PIVOT)")
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps of the sampled worlds compared with the f64 oracle after the run (0: skip)")
     args = ap.parse_args()
@@ -643,8 +657,9 @@ def main():
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     threads = os.cpu_count() or 1
-    global WORLDS, SHARD, WORLD_SIZE, WAVE_HOST_ROUNDS
+    global WORLDS, SHARD, WORLD_SIZE, WAVE_HOST_ROUNDS, NS_PIVOT
     WORLDS, SHARD, WORLD_SIZE, WAVE_HOST_ROUNDS = args.worlds, args.shard, world_size, args.wave_host_rounds
+    NS_PIVOT = bool(args.ns_pivot)
 
     if args.impl == "reference":
         if rank != 0:

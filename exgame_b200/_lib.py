@@ -98,6 +98,7 @@ SIGNATURES = {
     "exg_motor_compose_n": (ctypes.c_int, [ctypes.c_int64, _vp, _vp, _vp]),
     "exg_eval_joints": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_int32, _vp]),
+    "exg_pivot_inverse": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _vp, _vp]),
     "exg_gravity_forces": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int32, _vp]),
     "exg_gravity_forces_noalloc": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,

@@ -94,12 +94,14 @@ PRECISION_F64, PRECISION_MIXED, PRECISION_MIXED_FAST = 0, 1, 2
 
 
 NEWTON_EXACT_POSE_FACTOR = 1
+NEWTON_NS_PIVOT = 2  # mixed path: Newton-Schulz pivot inverses (warm-started, FP32 steps, FP64 correction)
 
 
 def step_params(integrator=LIE_EULER, gravity_law=GRAVITY_OFF, precision=PRECISION_F64, G=1.0, softening=0.0,
-                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32, exact_jacobian=False, field=(0.0, 0.0, 0.0)):
+                dt=1e-2, warp=1.0, tol=1e-4, max_newton=32, exact_jacobian=False, field=(0.0, 0.0, 0.0),
+                ns_pivot=False):
     p = np.zeros((), dtype=STEP_PARAMS_DTYPE)
-    p["newton_flags"] = NEWTON_EXACT_POSE_FACTOR if exact_jacobian else 0
+    p["newton_flags"] = (NEWTON_EXACT_POSE_FACTOR if exact_jacobian else 0) | (NEWTON_NS_PIVOT if ns_pivot else 0)
     p["integrator"] = integrator
     p["gravity_law"] = gravity_law
     p["precision"] = precision

@@ -1202,6 +1202,32 @@ int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t nj, c
   return EXG_OK;
 }
 
+int exg_pivot_inverse(exg_device_t dev, const double* d_blocks, int32_t n, int32_t precision, int32_t form,
+                      int32_t warm, double* d_out, int32_t* d_steps) {
+  if (!dev || n < 0 || (n > 0 && (!d_blocks || !d_out))) return EXG_ERR_INVALID_ARGUMENT;
+  if (precision != EXG_PRECISION_F64 && precision != EXG_PRECISION_MIXED && precision != EXG_PRECISION_MIXED_FAST)
+    return EXG_ERR_INVALID_ARGUMENT;
+  if (form != 0 && form != 1) return EXG_ERR_INVALID_ARGUMENT;
+  if (n == 0) return EXG_OK;
+  std::lock_guard<std::mutex> lock(dev->mu);
+  EXG_CUDA_TRY(cudaSetDevice(dev->ordinal));
+  cudaStream_t s = dev->stream;
+  int* d_singular = nullptr;
+  EXG_CUDA_TRY(cudaMallocAsync(&d_singular, sizeof(int), s));
+  int rc = EXG_OK;
+  if (cudaMemsetAsync(d_singular, 0, sizeof(int), s) != cudaSuccess) rc = EXG_ERR_BACKEND;
+  if (rc == EXG_OK)
+    rc = launch_pivot_inverse(dev, d_blocks, n, precision != EXG_PRECISION_F64, form, warm, d_out, d_steps, d_singular,
+                              s);
+  int h_singular = 0;
+  if (rc == EXG_OK && cudaMemcpyAsync(&h_singular, d_singular, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    rc = EXG_ERR_BACKEND;
+  cudaFreeAsync(d_singular, s);
+  if (rc != EXG_OK) return rc;
+  EXG_CUDA_TRY(cudaStreamSynchronize(s));
+  return h_singular ? EXG_ERR_FATAL : EXG_OK;
+}
+
 int exg_gravity_forces(exg_device_t dev, const double* d_pos_mass, const double* d_size, int32_t n, int32_t law, double G,
                        double softening, int32_t precision, double* d_force) {
   if (!dev || n < 0 || (n > 0 && (!d_pos_mass || !d_force))) return EXG_ERR_INVALID_ARGUMENT;

@@ -138,6 +138,11 @@ int launch_joints_plain_world(exg_device_s* dev, const DeviceWorld& w, cudaStrea
 int launch_joints_stage(exg_device_s* dev, const exg_joint_t* joints, int nj, const double* pose_aos, const double* vel_aos,
                         double dt, double warp, int jacobian, double* out, cudaStream_t s);
 int launch_integrate_explicit(exg_device_s* dev, const DeviceWorld& w, cudaStream_t s);
+// the elimination's pivot inverse on n row-major 6x6 blocks: mixed != 0 the Newton-Schulz inverse
+// (warm != 0: out holds earlier inverses to start from), else FP64 Gauss-Jordan; form 0 one thread
+// per block, 1 one warp
+int launch_pivot_inverse(exg_device_s* dev, const double* blocks, int n, int mixed, int form, int warm, double* out,
+                         int* steps, int* singular, cudaStream_t s);
 // records <-> rows: record k is body first + k, or body dst[k] when dst is not null
 int launch_bodies_scatter(exg_device_s* dev, const DeviceWorld& w, const exg_body_t* rec, int count, int first,
                           const int* dst, cudaStream_t s);

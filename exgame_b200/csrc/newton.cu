@@ -131,7 +131,8 @@ __device__ double phase_assemble(const Ctx& c, double half, double* red) {
 // the right-hand side follows the same updates (b_k -= S_kp y_p). Back substitution from the last
 // level: x_k = D_k^-1 (y_k - sum_j A(k, j) x_j). Returns false if a pivot block is singular (dv is
 // then NaN, which the line search rejects).
-__device__ bool phase_solve_lu(const Ctx& c, int* flag) {
+template <bool MIXED, bool NS>
+__device__ bool phase_solve_lu(const Ctx& c, int* flag, bool warm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = c.d.m;
   const int* lv = c.A.lv_ptr + c.d.lv_off;
@@ -162,7 +163,7 @@ __device__ bool phase_solve_lu(const Ctx& c, int* flag) {
     __syncthreads();
     for (int u = lv[L] + warp; u < lv[L + 1]; u += kWarps) {
       const int k = nodes[u];
-      const bool ok = warp_inverse6(lu_block(c, k), c.s.Dinv + 36 * (size_t)k);
+      const bool ok = warp_pivot_inverse6<MIXED && NS>(lu_block(c, k), c.s.Dinv + 36 * (size_t)k, c.P.ns_pivot, warm);
       if (!ok && lane == 0) *flag = 0;
       for (int s = sp[k]; s < sp[k + 1]; ++s) {
         double* lo = c.s.G + 72 * (size_t)s + 36;
@@ -191,8 +192,11 @@ __device__ bool phase_solve_lu(const Ctx& c, int* flag) {
 
 // Exact solve of A dv = rhs on the island's elimination forest. Returns false if a pivot
 // block is singular (dv is then NaN, which the line search rejects).
-__device__ bool phase_solve(const Ctx& c, int* flag) {
-  if (c.d.solver == 1) return phase_solve_lu(c, flag);
+// warm: every node's Dinv slot holds its inverse from an earlier solve of this step (the mixed
+// path's Newton-Schulz pivots start from it).
+template <bool MIXED, bool NS>
+__device__ bool phase_solve(const Ctx& c, int* flag, bool warm) {
+  if (c.d.solver == 1) return phase_solve_lu<MIXED, NS>(c, flag, warm);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m = c.d.m;
   const int* lv = c.A.lv_ptr + c.d.lv_off;
@@ -206,7 +210,7 @@ __device__ bool phase_solve(const Ctx& c, int* flag) {
   for (int L = c.d.n_levels - 1; L >= 1; --L) {
     for (int k = lv[L] + warp; k < lv[L + 1]; k += kWarps) {
       int i = nodes[k];
-      bool ok = warp_inverse6(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i);
+      bool ok = warp_pivot_inverse6<MIXED && NS>(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i, c.P.ns_pivot, warm);
       if (!ok && lane == 0) *flag = 0;
       warp_mm6<false>(c.s.Apc + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i, c.s.S + 36 * (size_t)i);
     }
@@ -223,7 +227,7 @@ __device__ bool phase_solve(const Ctx& c, int* flag) {
   }
   for (int k = lv[0] + warp; k < lv[1]; k += kWarps) {
     int i = nodes[k];
-    bool ok = warp_inverse6(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i);
+    bool ok = warp_pivot_inverse6<MIXED && NS>(c.s.D + 36 * (size_t)i, c.s.Dinv + 36 * (size_t)i, c.P.ns_pivot, warm);
     if (!ok && lane == 0) *flag = 0;
     warp_mv6(c.s.Dinv + 36 * (size_t)i, c.s.bvec + 6 * i, c.s.dv + 6 * i);
   }
@@ -264,8 +268,9 @@ __device__ void load_external(const Ctx& c) {
 
 struct SolveOut { bool converged; double best; bool assembled; double a_norm2; };
 
-template <bool MIXED>
-__device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters, PhaseTimer& tm) {
+template <bool MIXED, bool NS>
+__device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* flag, int* iters, PhaseTimer& tm,
+                                bool* warm) {
   SolveOut o{false, kHuge, false, 0.0};
   load_world_state(c);  // vmid = current world velocity; snap = P_s^n
   __syncthreads();
@@ -306,7 +311,8 @@ __device__ SolveOut newton_solve(const Ctx& c, double half, double* red, int* fl
     o.a_norm2 = phase_assemble<MIXED>(c, half, red);
     o.assembled = true;
     tm.lap(PH_ASSEMBLE);
-    phase_solve(c, flag);
+    phase_solve<MIXED, NS>(c, flag, *warm);
+    *warm = true;
     tm.lap(PH_SOLVE);
     // no correction at all -> hand over to sub-division (newton.rs:449-456)
     int nz = 0;
@@ -354,7 +360,7 @@ __device__ void commit_span(const Ctx& c, double span, double half, bool converg
   for (int i = threadIdx.x; i < c.d.m; i += blockDim.x) op_commit(c, span, half, converged, i);
 }
 
-template <bool MIXED>
+template <bool MIXED, bool NS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
                                                          int n_islands, int* __restrict__ head) {
   __shared__ double red[kWarps];
@@ -383,6 +389,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDevi
     unsigned long long remaining = 1ull << kMaxDepth;
     int depth = 0, spans = 0, iters = 0, maxdepth = 0;
     double last_best = 0.0;
+    bool warm = false;  // no solve of this step has filled the Dinv slots yet
     while (remaining > 0) {
       unsigned long long units = 1ull << (kMaxDepth - depth);
       while (units > remaining) { ++depth; units >>= 1; }
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDevi
       double half = span / 2.0;
       ++spans;
       maxdepth = max(maxdepth, depth);
-      SolveOut o = newton_solve<MIXED>(c, half, red, &flag, &iters, tm);
+      SolveOut o = newton_solve<MIXED, NS>(c, half, red, &flag, &iters, tm, &warm);
       last_best = o.best;
       bool finite = o.best < kHuge;
       bool last = depth == kMaxDepth;
@@ -534,6 +541,69 @@ NewtonWorld::~NewtonWorld() {
   d_scratch.release();
   d_residual.release();
   d_phase.release();
+}
+
+namespace {
+// Stage kernels of exg_pivot_inverse: the elimination's pivot inverse on caller-given blocks,
+// one thread per block (a wide level's form: the block staged in the thread's column of shared
+// memory, as k_w_solve_down does) or one warp per block (a narrow level's and the island kernel's).
+constexpr int kPivotThreads = 64;
+template <bool MIXED>
+__global__ void __launch_bounds__(kPivotThreads) k_pivot_thread(const double* blocks, int n, double* out, int* steps,
+                                                                int* singular, bool warm) {
+  extern __shared__ double col_base[];
+  double* col = col_base + threadIdx.x;
+  for (long long b = blockIdx.x * (long long)kPivotThreads + threadIdx.x; b < n;
+       b += (long long)gridDim.x * kPivotThreads) {
+    const double* a = blocks + 36 * b;
+    bool ok;
+    int st = 0;
+    if (MIXED) {
+      for (int e = 0; e < 36; ++e) col[e * kPivotThreads] = a[e];
+      if (warm)
+        for (int e = 0; e < 36; ++e) col[(36 + e) * kPivotThreads] = out[36 * b + e];
+      ok = thread_ns_inverse6<kPivotThreads>(col, col + 36 * kPivotThreads, warm, &st);
+      for (int e = 0; e < 36; ++e) out[36 * b + e] = col[(36 + e) * kPivotThreads];
+    } else {
+      double m[36], inv[36];
+      for (int e = 0; e < 36; ++e) m[e] = a[e];
+      ok = thread_inverse6(m, inv);
+      for (int e = 0; e < 36; ++e) out[36 * b + e] = inv[e];
+    }
+    if (steps) steps[b] = st;
+    if (!ok) atomicOr(singular, 1);
+  }
+}
+template <bool MIXED>
+__global__ void __launch_bounds__(kPivotThreads) k_pivot_warp(const double* blocks, int n, double* out, int* steps,
+                                                              int* singular, bool warm) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (kPivotThreads / 32);
+  for (long long b = (blockIdx.x * (long long)kPivotThreads + threadIdx.x) >> 5; b < n; b += warps) {
+    int st = 0;
+    const bool ok = MIXED ? warp_ns_inverse6(blocks + 36 * b, out + 36 * b, warm, &st)
+                          : warp_inverse6(blocks + 36 * b, out + 36 * b);
+    if (steps && lane == 0) steps[b] = st;
+    if (!ok && lane == 0) atomicOr(singular, 1);
+  }
+}
+}  // namespace
+
+int launch_pivot_inverse(exg_device_s* dev, const double* blocks, int n, int mixed, int form, int warm, double* out,
+                         int* steps, int* singular, cudaStream_t s) {
+  const int max_grid = std::max(1, dev->sm_count) * 8;
+  if (form == 0) {
+    const int grid = (int)std::min<long long>(max_grid, (n + kPivotThreads - 1) / kPivotThreads);
+    if (mixed) k_pivot_thread<true><<<grid, kPivotThreads, 72 * kPivotThreads * sizeof(double), s>>>(blocks, n, out,
+                                                                                                   steps, singular, warm != 0);
+    else k_pivot_thread<false><<<grid, kPivotThreads, 0, s>>>(blocks, n, out, steps, singular, false);
+  } else {
+    const int grid = (int)std::min<long long>(max_grid, (32LL * n + kPivotThreads - 1) / kPivotThreads);
+    if (mixed) k_pivot_warp<true><<<grid, kPivotThreads, 0, s>>>(blocks, n, out, steps, singular, warm != 0);
+    else k_pivot_warp<false><<<grid, kPivotThreads, 0, s>>>(blocks, n, out, steps, singular, false);
+  }
+  EXG_CUDA_TRY(cudaGetLastError());
+  return EXG_OK;
 }
 
 int NewtonWorld::add_world(exg_device_s* dev, int slot, int body_off, const exg_body_t* bodies, int n,
@@ -1062,21 +1132,30 @@ int NewtonWorld::enqueue(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
              w.grav_partial, w.wparams, w.w_poff, w.w_splits, w.w_n, w.w_body_off, w.w_active, w.n};
   int* head = d_queue.ptr + n_cta_;
   // persistent CTAs: as many as can be resident at once
-  static int resident[2] = {0, 0};
+  // variant 0 FP64, 1 mixed, 2 mixed with Newton-Schulz pivots (some world asks for them)
+  static int resident[3] = {0, 0, 0};
   const int mixed = w.precision != EXG_PRECISION_F64;
-  if (resident[mixed] == 0) {
+  bool ns = false;
+  if (mixed)
+    for (const exg_step_params_t& p : w.h_params) ns = ns || (p.newton_flags & EXG_NEWTON_NS_PIVOT) != 0;
+  const int var = mixed ? (ns ? 2 : 1) : 0;
+  if (resident[var] == 0) {
     int per_sm = 0;
-    cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<true>, kThreads, 0)
-                          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<false>, kThreads, 0);
-    resident[mixed] = (e == cudaSuccess && per_sm > 0) ? per_sm : 1;
+    cudaError_t e =
+        var == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<true, true>, kThreads, 0)
+        : var == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<true, false>, kThreads, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_newton_step<false, false>, kThreads, 0);
+    resident[var] = (e == cudaSuccess && per_sm > 0) ? per_sm : 1;
   }
-  int grid = std::min(n_cta_, std::max(1, dev->sm_count) * resident[mixed]);
+  int grid = std::min(n_cta_, std::max(1, dev->sm_count) * resident[var]);
   EXG_CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(int), s));
   int tok = prof_begin(dev, PROF_NEWTON, s);
-  if (mixed)
-    k_newton_step<true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
+  if (var == 2)
+    k_newton_step<true, true><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
+  else if (var == 1)
+    k_newton_step<true, false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
   else
-    k_newton_step<false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
+    k_newton_step<false, false><<<grid, kThreads, 0, s>>>(arr, W, d_queue.ptr, n_cta_, head);
   prof_end(dev, tok, s);
   return exg_after_launch(dev);
 }

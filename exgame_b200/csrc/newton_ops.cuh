@@ -85,6 +85,7 @@ struct WorldRef {
 struct IslandParams {
   double dt, warp, tol2, G, pose_factor_scale;
   int max_newton;
+  bool ns_pivot;  // Newton-Schulz pivot inverses (mixed path, EXG_NEWTON_NS_PIVOT)
   int splits, nw, wbody_off;
   const double* part;
 };
@@ -107,6 +108,7 @@ __device__ inline void resolve_params(Ctx& c) {
   c.P.G = wp.G;
   c.P.max_newton = wp.max_newton > 0 ? wp.max_newton : 32;
   c.P.pose_factor_scale = (wp.newton_flags & EXG_NEWTON_EXACT_POSE_FACTOR) ? 0.5 : 1.0;
+  c.P.ns_pivot = (wp.newton_flags & EXG_NEWTON_NS_PIVOT) != 0;
   c.P.splits = c.W.w_splits[c.d.world];
   c.P.nw = c.W.w_n[c.d.world];
   c.P.wbody_off = c.W.w_body_off[c.d.world];
@@ -608,12 +610,14 @@ __device__ inline void warp_mv6(const double* A, const double* x, double* y) {
 // Gauss-Jordan inverse of a (row-major 6x6) with partial pivoting into out. Returns false if a
 // pivot is zero or not finite. Only the right half of [A | I] is kept past the column being
 // eliminated: the left half's columns to the left of it are never read again.
+// STRIDE places entry e of a and of out at [e * STRIDE] (1: plain row-major arrays).
+template <int STRIDE = 1>
 __device__ __forceinline__ bool thread_inverse6(const double* a, double* out) {
   double M[6][12];
 #pragma unroll
   for (int r = 0; r < 6; ++r) {
 #pragma unroll
-    for (int c = 0; c < 6; ++c) M[r][c] = a[r * 6 + c];
+    for (int c = 0; c < 6; ++c) M[r][c] = a[(r * 6 + c) * STRIDE];
 #pragma unroll
     for (int c = 0; c < 6; ++c) M[r][6 + c] = (r == c) ? 1.0 : 0.0;
   }
@@ -653,8 +657,376 @@ __device__ __forceinline__ bool thread_inverse6(const double* a, double* out) {
 #pragma unroll
   for (int r = 0; r < 6; ++r)
 #pragma unroll
-    for (int c = 0; c < 6; ++c) out[r * 6 + c] = M[r][6 + c];
+    for (int c = 0; c < 6; ++c) out[(r * 6 + c) * STRIDE] = M[r][6 + c];
   return ok;
+}
+
+// ── the mixed path's pivot inverse: Newton-Schulz, FP32 steps and an FP64 correction ──
+// With EXG_NEWTON_NS_PIVOT set on a mixed-precision world, each 6x6 pivot block D of the
+// elimination is inverted by Newton-Schulz (the reference's iteration, newton.rs:209-327, at block
+// size), warm-started like the reference's warm path from the same node's inverse of the
+// previous solve in this step, when there is one:
+//  1. warm: R = I - D X_prev in FP64; where max|R| <= kNsWarmTol, one FP64 Newton-Schulz
+//     correction D^-1 = X_prev + X_prev R (the residual squares) and nothing else;
+//  2. otherwise FP32 Newton-Schulz steps held in registers on the symmetrically scaled block
+//     B = S D S (s_r = 1/sqrt|d_rr|, 1 where d_rr is zero or not finite, B rounded to FP32):
+//     R = I - B X, X <- X + X R, until max|R| <= kNsTol, or until the residual, once below
+//     kNsFloor, stops halving (the FP32 floor of a less well conditioned block), at most
+//     kNsMaxIter steps; seeded with the scaled previous inverse S^-1 X_prev S^-1 where its FP64
+//     residual is below 1/2, else with I where ||I - B||_inf < 1/2, else with the transposed
+//     seed B^T / (||B||_1 ||B||_inf), which converges for every non-singular B (the reference's
+//     seed_transpose, newton.rs:209-241);
+//  3. one FP64 Newton-Schulz correction of X64 = S X S against D: R = I - D X64,
+//     D^-1 = X64 + X64 R.
+// A block whose FP32 residual ends above kNsAccept (singular, not finite, or too ill-conditioned
+// for FP32) takes the FP64 Gauss-Jordan inverse instead. The thread form (a wide elimination
+// level) and the warp form (a narrow level, the island kernel) do per entry the same operations
+// in the same order with explicitly rounded FMAs, so they give the same bits.
+constexpr int kNsMaxIter = 40;
+constexpr float kNsTol = 1e-6f;
+constexpr float kNsFloor = 1.0f / 64.0f;
+constexpr float kNsAccept = 1e-3f;
+constexpr float kNsIdentitySeed = 0.5f;
+constexpr double kNsWarmTol = 1e-4;
+constexpr double kNsWarmSeed = 0.5;
+
+__device__ __forceinline__ double ns_scale(double d) {
+  const double a = fabs(d);
+  return (a > 0.0 && a < INFINITY) ? 1.0 / sqrt(a) : 1.0;
+}
+// 0: take another step, 1: stop (converged or at the FP32 floor), -1: failed
+__device__ __forceinline__ int ns_verdict(float rmax, bool nan, float prev) {
+  if (nan || !(rmax < 1e30f)) return -1;
+  if (rmax <= kNsTol) return 1;
+  if (rmax < kNsFloor && !(rmax < 0.5f * prev)) return 1;
+  return 0;
+}
+
+// One thread: out = the inverse of the block a, both row-major with entry e at [e * STRIDE] (a
+// thread's two columns of shared memory; they must not overlap). With warm set, out holds on entry
+// an earlier inverse (of this block before a small change). Returns false if the block is
+// singular (by the Gauss-Jordan fallback's test). *steps receives the FP32 steps taken (0 where
+// the warm correction sufficed), or -1 where the block fell back to Gauss-Jordan. The FP32 block
+// waits in out's slots while the iteration runs, so registers hold X and R only.
+template <int STRIDE>
+__device__ __forceinline__ bool thread_ns_inverse6(const double* a, double* out, bool warm, int* steps = nullptr) {
+  // volatile reads: a, out and B are read again where needed instead of being held in registers
+  const volatile double* av = a;
+  volatile double* ov = out;
+  bool warm_seed = false;
+  if (warm) {
+    double R[36];
+    double r = 0.0;
+    bool nan = false;
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) t = __fma_rn(av[(k * 6 + j) * STRIDE], ov[(j * 6 + c) * STRIDE], t);
+        const double v = (k == c ? 1.0 : 0.0) - t;
+        R[k * 6 + c] = v;
+        const double x = fabs(v);
+        nan = nan || (x != x);
+        r = x > r ? x : r;
+      }
+    if (!nan && r <= kNsWarmTol) {  // X_prev + X_prev R, row by row in place
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        double xr[6], o[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) xr[k] = ov[(i * 6 + k) * STRIDE];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+          double t = xr[c];
+#pragma unroll
+          for (int k = 0; k < 6; ++k) t = __fma_rn(xr[k], R[k * 6 + c], t);
+          o[c] = t;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ov[(i * 6 + c) * STRIDE] = o[c];
+      }
+      if (steps) *steps = 0;
+      return true;
+    }
+    warm_seed = !nan && r < kNsWarmSeed;
+  }
+  float* B = reinterpret_cast<float*>(out);  // entry e at B[2 * e * STRIDE]
+  const volatile float* Bv = B;
+  double s[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) s[r] = ns_scale(a[(r * 7) * STRIDE]);
+  float X[36];
+  float one = 0.0f, inf = 0.0f, off = 0.0f;
+  {
+    float colsum[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) colsum[c] = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      float row = 0.0f, rowoff = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const int e = r * 6 + c;
+        const float v = (float)((a[e * STRIDE] * s[r]) * s[c]);
+        X[e] = warm_seed ? (float)((ov[e * STRIDE] / s[r]) / s[c]) : 0.0f;  // read before B takes the slot
+        B[2 * e * STRIDE] = v;
+        row += fabsf(v);
+        rowoff += fabsf((r == c ? 1.0f : 0.0f) - v);
+        colsum[c] += fabsf(v);
+      }
+      inf = fmaxf(inf, row);
+      off = fmaxf(off, rowoff);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) one = fmaxf(one, colsum[c]);
+  }
+  if (!warm_seed) {
+    const float sc = 1.0f / (one * inf);
+    const bool eye = off < kNsIdentitySeed;
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) X[r * 6 + c] = eye ? (r == c ? 1.0f : 0.0f) : Bv[2 * (c * 6 + r) * STRIDE] * sc;
+  }
+  float prev = INFINITY, rmax = INFINITY;
+  int verdict = 0, it = 0;
+#pragma unroll 1
+  for (; it < kNsMaxIter; ++it) {
+    float R[36];
+    bool nan = false;
+    rmax = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      float br[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) br[k] = Bv[2 * (r * 6 + k) * STRIDE];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        float t = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t = __fmaf_rn(br[k], X[k * 6 + c], t);
+        const float v = (r == c ? 1.0f : 0.0f) - t;
+        R[r * 6 + c] = v;
+        const float x = fabsf(v);
+        nan = nan || (x != x);
+        rmax = x > rmax ? x : rmax;
+      }
+    }
+    verdict = ns_verdict(rmax, nan, prev);
+    if (verdict != 0) break;
+    prev = rmax;
+    // X <- X + X R, row by row in place: row r of the new X reads only row r of the old one
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      float xr[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        float t = X[r * 6 + c];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t = __fmaf_rn(X[r * 6 + k], R[k * 6 + c], t);
+        xr[c] = t;
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) X[r * 6 + c] = xr[c];
+    }
+  }
+  if (!(verdict == 1 && rmax <= kNsAccept)) {
+    if (steps) *steps = -1;
+    return thread_inverse6<STRIDE>(a, out);
+  }
+  if (steps) *steps = it;
+  // the FP64 correction, one column at a time: q = e_c - D x_c, then column c of X64 + X64 q
+  double xd[36];
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) xd[r * 6 + c] = ((double)X[r * 6 + c] * s[r]) * s[c];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double q[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      double t = 0.0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) t = __fma_rn(av[(k * 6 + j) * STRIDE], xd[j * 6 + c], t);
+      q[k] = (k == c ? 1.0 : 0.0) - t;
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      double t = xd[r * 6 + c];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) t = __fma_rn(xd[r * 6 + k], q[k], t);
+      out[(r * 6 + c) * STRIDE] = t;
+    }
+  }
+  return true;
+}
+
+// Entry idx of a block held two entries per lane (entry e in lane e, entries 32..35 in the second
+// register of lanes 0..3); every lane of the warp calls it.
+__device__ __forceinline__ float ns_get(float v0, float v1, int idx) {
+  const float x = __shfl_sync(0xffffffffu, v0, idx & 31);
+  const float y = __shfl_sync(0xffffffffu, v1, idx & 31);
+  return idx < 32 ? x : y;
+}
+__device__ __forceinline__ double ns_get(double v0, double v1, int idx) {
+  const double x = __shfl_sync(0xffffffffu, v0, idx & 31);
+  const double y = __shfl_sync(0xffffffffu, v1, idx & 31);
+  return idx < 32 ? x : y;
+}
+__device__ __forceinline__ float ns_warp_max(float m) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const float v = __shfl_xor_sync(0xffffffffu, m, o);
+    m = v > m ? v : m;
+  }
+  return m;
+}
+__device__ __forceinline__ double ns_warp_max(double m) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double v = __shfl_xor_sync(0xffffffffu, m, o);
+    m = v > m ? v : m;
+  }
+  return m;
+}
+
+// One warp: out = the inverse of the row-major block a (both in memory, not overlapping), the
+// same bits as thread_ns_inverse6; with warm set, out holds on entry an earlier inverse. Returns
+// false (to every lane) if the block is singular.
+__device__ inline bool warp_ns_inverse6(const double* a, double* out, bool warm, int* steps = nullptr) {
+  const int lane = threadIdx.x & 31;
+  const bool has1 = lane < 4;
+  const int e0 = lane, e1 = has1 ? lane + 32 : lane;  // lanes 4.. repeat e0 in their second slot
+  const int r0 = e0 / 6, c0 = e0 % 6, r1 = e1 / 6, c1 = e1 % 6;
+  bool warm_seed = false;
+  if (warm) {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      t0 = __fma_rn(a[r0 * 6 + j], out[j * 6 + c0], t0);
+      t1 = __fma_rn(a[r1 * 6 + j], out[j * 6 + c1], t1);
+    }
+    const double R0 = (r0 == c0 ? 1.0 : 0.0) - t0, R1 = (r1 == c1 ? 1.0 : 0.0) - t1;
+    const double x0 = fabs(R0), x1 = has1 ? fabs(R1) : 0.0;
+    const bool nan = __any_sync(0xffffffffu, (x0 != x0) || (x1 != x1));
+    const double r = ns_warp_max(x1 > x0 ? x1 : x0);
+    if (!nan && r <= kNsWarmTol) {  // X_prev + X_prev R
+      double o0 = out[e0], o1 = out[e1];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        o0 = __fma_rn(out[r0 * 6 + k], ns_get(R0, R1, k * 6 + c0), o0);
+        o1 = __fma_rn(out[r1 * 6 + k], ns_get(R0, R1, k * 6 + c1), o1);
+      }
+      __syncwarp();
+      out[e0] = o0;
+      if (has1) out[e1] = o1;
+      __syncwarp();
+      if (steps && lane == 0) *steps = 0;
+      return true;
+    }
+    warm_seed = !nan && r < kNsWarmSeed;
+  }
+  const double sr0 = ns_scale(a[r0 * 7]), sc0 = ns_scale(a[c0 * 7]);
+  const double sr1 = ns_scale(a[r1 * 7]), sc1 = ns_scale(a[c1 * 7]);
+  const float B0 = (float)((a[e0] * sr0) * sc0), B1 = (float)((a[e1] * sr1) * sc1);
+  float X0, X1;
+  if (warm_seed) {
+    X0 = (float)((out[e0] / sr0) / sc0);
+    X1 = (float)((out[e1] / sr1) / sc1);
+  } else {
+    float one = 0.0f, inf = 0.0f, off = 0.0f;
+    {
+      const int i = lane % 6;
+      float row = 0.0f, col = 0.0f, rowoff = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        const float v = ns_get(B0, B1, i * 6 + j);
+        row += fabsf(v);
+        rowoff += fabsf((i == j ? 1.0f : 0.0f) - v);
+        col += fabsf(ns_get(B0, B1, j * 6 + i));
+      }
+      if (lane >= 6) row = col = rowoff = 0.0f;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        row = fmaxf(row, __shfl_xor_sync(0xffffffffu, row, o));
+        col = fmaxf(col, __shfl_xor_sync(0xffffffffu, col, o));
+        rowoff = fmaxf(rowoff, __shfl_xor_sync(0xffffffffu, rowoff, o));
+      }
+      inf = row;
+      one = col;
+      off = rowoff;
+    }
+    const float sc = 1.0f / (one * inf);
+    const bool eye = off < kNsIdentitySeed;
+    X0 = eye ? (r0 == c0 ? 1.0f : 0.0f) : ns_get(B0, B1, c0 * 6 + r0) * sc;
+    X1 = eye ? (r1 == c1 ? 1.0f : 0.0f) : ns_get(B0, B1, c1 * 6 + r1) * sc;
+  }
+  float prev = INFINITY, rmax = INFINITY;
+  int verdict = 0, it = 0;
+#pragma unroll 1
+  for (; it < kNsMaxIter; ++it) {
+    float t0 = 0.0f, t1 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float b0 = ns_get(B0, B1, r0 * 6 + k), x0 = ns_get(X0, X1, k * 6 + c0);
+      const float b1 = ns_get(B0, B1, r1 * 6 + k), x1 = ns_get(X0, X1, k * 6 + c1);
+      t0 = __fmaf_rn(b0, x0, t0);
+      t1 = __fmaf_rn(b1, x1, t1);
+    }
+    const float R0 = (r0 == c0 ? 1.0f : 0.0f) - t0, R1 = (r1 == c1 ? 1.0f : 0.0f) - t1;
+    const float a0 = fabsf(R0), a1 = has1 ? fabsf(R1) : 0.0f;
+    const bool nan = __any_sync(0xffffffffu, (a0 != a0) || (a1 != a1));
+    rmax = ns_warp_max(a1 > a0 ? a1 : a0);
+    verdict = ns_verdict(rmax, nan, prev);
+    if (verdict != 0) break;
+    prev = rmax;
+    float n0 = X0, n1 = X1;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      n0 = __fmaf_rn(ns_get(X0, X1, r0 * 6 + k), ns_get(R0, R1, k * 6 + c0), n0);
+      n1 = __fmaf_rn(ns_get(X0, X1, r1 * 6 + k), ns_get(R0, R1, k * 6 + c1), n1);
+    }
+    X0 = n0;
+    X1 = n1;
+  }
+  if (!(verdict == 1 && rmax <= kNsAccept)) {
+    if (steps && lane == 0) *steps = -1;
+    __syncwarp();
+    return warp_inverse6(a, out);
+  }
+  if (steps && lane == 0) *steps = it;
+  const double xd0 = ((double)X0 * sr0) * sc0, xd1 = ((double)X1 * sr1) * sc1;
+  double q0 = 0.0, q1 = 0.0;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const double g0 = ns_get(xd0, xd1, j * 6 + c0), g1 = ns_get(xd0, xd1, j * 6 + c1);
+    q0 = __fma_rn(a[r0 * 6 + j], g0, q0);
+    q1 = __fma_rn(a[r1 * 6 + j], g1, q1);
+  }
+  const double Q0 = (r0 == c0 ? 1.0 : 0.0) - q0, Q1 = (r1 == c1 ? 1.0 : 0.0) - q1;
+  double o0 = xd0, o1 = xd1;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    o0 = __fma_rn(ns_get(xd0, xd1, r0 * 6 + k), ns_get(Q0, Q1, k * 6 + c0), o0);
+    o1 = __fma_rn(ns_get(xd0, xd1, r1 * 6 + k), ns_get(Q0, Q1, k * 6 + c1), o1);
+  }
+  __syncwarp();
+  out[e0] = o0;
+  if (has1) out[e1] = o1;
+  __syncwarp();
+  return true;
+}
+
+// The pivot inverse of the elimination: on the mixed path with Newton-Schulz pivots selected (ns),
+// warp_ns_inverse6 (warm: out holds the node's inverse from the previous solve of this step);
+// otherwise FP64 Gauss-Jordan.
+template <bool MIXED>
+__device__ __forceinline__ bool warp_pivot_inverse6(const double* a, double* out, bool ns, bool warm) {
+  if (MIXED && ns) return warp_ns_inverse6(a, out, warm);
+  return warp_inverse6(a, out);
 }
 
 // ── scalar helpers of the span budget ───────────────────────────────────────

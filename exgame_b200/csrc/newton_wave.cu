@@ -43,6 +43,8 @@ struct WaveCtl {
   int carried, lane, converged, assembled;
   int nz, singular, commit_converged, active;
   int mflip;  // 1: the scratch's mass and mass0 blocks trade places (see wave_ctx)
+  int ns;     // Newton-Schulz pivot inverses (mixed path, EXG_NEWTON_NS_PIVOT)
+  int warm;   // a solve of this step has filled every node's Dinv slot
 };
 
 struct WaveArgs {
@@ -132,6 +134,8 @@ __global__ void k_w_init(WaveArgs a) {
     c.flags = 0;
     c.eval = EV_NONE;
     c.mflip = 0;
+    c.ns = (a.W.wparams[d.world].newton_flags & EXG_NEWTON_NS_PIVOT) != 0;
+    c.warm = 0;
   }
 }
 
@@ -251,6 +255,7 @@ __global__ void k_w_after_solve(WaveArgs a) {
     c.flags &= ~(F_COPY_BEST | F_ACCEPT | F_TRIAL);  // done by the post-evaluation copy pass
     if (c.state != WS_DIR) continue;
     c.assembled = 1;
+    c.warm = 1;
     if (!c.nz) {
       c.state = WS_END;
       continue;
@@ -789,7 +794,16 @@ __global__ void __launch_bounds__(kSumThreads) k_w_island_sum(WaveArgs a, int ma
 // terms for the parent — S = Apc Dinv, then P = S Acp (kept in S's slot) and q = S b (kept in dv's
 // slot until the back substitution writes dv) — so a parent only sums finished products; a root
 // solves for dv. The arithmetic per entry is the island kernel's (newton_ops.cuh).
-__global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, int count, int range) {
+// With Newton-Schulz pivots (mixed path, EXG_NEWTON_NS_PIVOT) the pivot block passes through two
+// columns of shared memory per thread (the block, then the previous and the new inverse: 72 doubles
+// a thread, 36 KB for the 64-thread CTA), so the FP32 iteration and the FP64 correction hold only
+// their own blocks in registers; Gauss-Jordan pivots stay in registers.
+template <bool NS>
+constexpr int down_threads() { return NS ? 64 : 128; }
+template <bool MIXED, bool NS>
+__global__ void __launch_bounds__(down_threads<MIXED && NS>(), (MIXED && NS) ? 6 : 3)
+    k_w_solve_down(WaveArgs a, int first, int count, int range) {
+  extern __shared__ double w_pivot[];
   const RoundItems R = round_items(a, range, count);
   for (int vi = gtid(); vi < R.n; vi += gthreads()) {
     const int t = R.at(vi);
@@ -821,7 +835,29 @@ __global__ void __launch_bounds__(128, 3) k_w_solve_down(WaveArgs a, int first, 
     }
     st_n<6>(c.s.bvec + 6 * (size_t)i, b);
     double Dinv[36];
-    if (!thread_inverse6(D, Dinv)) atomicOr(&w.singular, 1);
+    if (MIXED && NS && w.ns) {
+      constexpr int T = down_threads<MIXED && NS>();
+      double* col = w_pivot + threadIdx.x;
+#pragma unroll
+      for (int e = 0; e < 36; ++e) col[e * T] = D[e];
+      {
+        const bool warm = w.warm != 0;
+        if (warm) {
+          const double2* xp = reinterpret_cast<const double2*>(c.s.Dinv + 36 * (size_t)i);
+#pragma unroll
+          for (int e = 0; e < 18; ++e) {
+            const double2 x = xp[e];
+            col[(36 + 2 * e) * T] = x.x;
+            col[(37 + 2 * e) * T] = x.y;
+          }
+        }
+        if (!thread_ns_inverse6<T>(col, col + 36 * T, warm)) atomicOr(&w.singular, 1);
+      }
+#pragma unroll
+      for (int e = 0; e < 36; ++e) Dinv[e] = col[(36 + e) * T];
+    } else {
+      if (!thread_inverse6(D, Dinv)) atomicOr(&w.singular, 1);
+    }
     st_n<36>(c.s.Dinv + 36 * (size_t)i, Dinv);
     if (c.A.dn_parent[c.d.dyn_off + i] >= 0) {
       double dv[6];
@@ -883,6 +919,7 @@ constexpr int kSolveWarps = 4;
 // on no other one together at the start (the node's blocks and right-hand side, the parent
 // couplings staged into shared memory for the products, the children's range) and fetches the
 // children's finished products four at a time, subtracting them in child order.
+template <bool MIXED, bool NS>
 __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs a, int first, int count, int range) {
   __shared__ __align__(16) double sh[kSolveWarps][36 * 5 + 8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -952,7 +989,12 @@ __global__ void __launch_bounds__(32 * kSolveWarps) k_w_solve_down_warp(WaveArgs
       c.s.bvec[6 * i + lane] = bb;
     }
     __syncwarp();
-    if (!warp_inverse6(Dm, Dinv) && lane == 0) atomicOr(&w.singular, 1);
+    if (MIXED && NS && w.ns && w.warm) {  // the node's inverse from the previous solve, the Newton-Schulz start
+      Dinv[lane] = c.s.Dinv[36 * i + lane];
+      if (has1) Dinv[e1] = c.s.Dinv[36 * i + e1];
+      __syncwarp();
+    }
+    if (!warp_pivot_inverse6<MIXED && NS>(Dm, Dinv, w.ns != 0, w.warm != 0) && lane == 0) atomicOr(&w.singular, 1);
     c.s.Dinv[36 * i + lane] = Dinv[lane];
     if (has1) c.s.Dinv[36 * i + e1] = Dinv[e1];
     if (par >= 0) {
@@ -1091,17 +1133,29 @@ __global__ void k_w_commit(WaveArgs a) {
 
 // The elimination level by level (leaves to roots), then the back substitution (roots to leaves):
 // levels of at most dev->tune_wave_narrow_level nodes take the warp kernels.
-void launch_elimination(exg_device_s* dev, const WaveArgs& a, const std::vector<int>& level_ptr, cudaStream_t s) {
+// NS: the kernels carry the Newton-Schulz pivot inverse (some island of the wave asks for it); without
+// it they are the plain Gauss-Jordan kernels, whose register budgets the Newton-Schulz code would raise.
+template <bool MIXED, bool NS>
+void launch_solve_down(exg_device_s* dev, const WaveArgs& a, int first, int count, int r, cudaStream_t s) {
+  constexpr int T = down_threads<MIXED && NS>();
+  if (count <= dev->tune_wave_narrow_level)
+    k_w_solve_down_warp<MIXED, NS><<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(
+        a, first, count, r);
+  else
+    k_w_solve_down<MIXED, NS><<<grid_for(dev, count, T, (256 / T) * dev->tune_wave_blocks_per_sm), T,
+                                (MIXED && NS) ? 72 * T * sizeof(double) : 0, s>>>(a, first, count, r);
+}
+
+void launch_elimination(exg_device_s* dev, const WaveArgs& a, const std::vector<int>& level_ptr, bool mixed, bool ns,
+                        cudaStream_t s) {
   const int nl = (int)level_ptr.size() - 1;
   const int narrow = dev->tune_wave_narrow_level;
   const int per = 2 * dev->tune_wave_blocks_per_sm;
   for (int L = nl - 1; L >= 0; --L) {
     const int first = level_ptr[L], count = level_ptr[L + 1] - first, r = kRangeLevel + L;
-    if (count <= narrow)
-      k_w_solve_down_warp<<<grid_for(dev, 32LL * count, 32 * kSolveWarps, 16), 32 * kSolveWarps, 0, s>>>(a, first,
-                                                                                                       count, r);
-    else
-      k_w_solve_down<<<grid_for(dev, count, 128, per), 128, 0, s>>>(a, first, count, r);
+    if (mixed && ns) launch_solve_down<true, true>(dev, a, first, count, r, s);
+    else if (mixed) launch_solve_down<true, false>(dev, a, first, count, r, s);
+    else launch_solve_down<false, false>(dev, a, first, count, r, s);
   }
   for (int L = 1; L < nl; ++L) {
     const int first = level_ptr[L], count = level_ptr[L + 1] - first, r = kRangeLevel + L;
@@ -1261,11 +1315,15 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   const int T = 256;
   const int g_isl = grid_for(dev, a.n_isl, T, 4);
   const int g_body = grid_for(dev, a.n_body, T, dev->tune_wave_blocks_per_sm);
-  if (wave_graph_ && wave_mixed_ != (w.precision != EXG_PRECISION_F64)) {
+  bool want_ns = false;  // some world asks for Newton-Schulz pivots (mixed path only)
+  if (w.precision != EXG_PRECISION_F64)
+    for (const exg_step_params_t& p : w.h_params) want_ns = want_ns || (p.newton_flags & EXG_NEWTON_NS_PIVOT) != 0;
+  if (wave_graph_ && (wave_mixed_ != (w.precision != EXG_PRECISION_F64) || wave_ns_ != want_ns)) {
     cudaGraphExecDestroy(wave_graph_);
     wave_graph_ = nullptr;
   }
   wave_mixed_ = w.precision != EXG_PRECISION_F64;
+  wave_ns_ = want_ns;
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
   k_w_init<<<g_isl, T, 0, s>>>(a);
   dev->launches.fetch_add(1, std::memory_order_relaxed);
@@ -1338,7 +1396,7 @@ int NewtonWorld::build_wave_round_graph(exg_device_s* dev, const void* args, cud
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
   if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
   else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-  launch_elimination(dev, a, wave_level_ptr_, s);
+  launch_elimination(dev, a, wave_level_ptr_, mixed, mixed && wave_ns_, s);
   k_w_nz<<<g_dyn, T, 0, s>>>(a);
   k_w_after_solve<<<g_isl, T, 0, s>>>(a);
   k_w_copy_bodies<<<g_body, T, 0, s>>>(a);
@@ -1455,7 +1513,7 @@ int NewtonWorld::build_wave_graph(exg_device_s* dev, const void* args, cudaStrea
   EXG_CUDA_TRY(capture(BD, {}, [&] {
     if (mixed) k_w_assemble<true><<<g_cell, T, 0, s>>>(a);
     else k_w_assemble<false><<<g_cell, T, 0, s>>>(a);
-    launch_elimination(dev, a, wave_level_ptr_, s);
+    launch_elimination(dev, a, wave_level_ptr_, mixed, mixed && wave_ns_, s);
     k_w_nz<<<g_dyn, T, 0, s>>>(a);
     k_w_after_solve<<<g_isl, T, 0, s>>>(a);
     k_w_copy_bodies<<<g_body, T, 0, s>>>(a);

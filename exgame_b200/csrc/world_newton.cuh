@@ -177,6 +177,7 @@ class NewtonWorld {
   cudaEvent_t fork_ = nullptr, join_ = nullptr;
   bool wave_host_loop_ = false, wave_graph_host_loop_ = false;
   bool wave_mixed_ = false;
+  bool wave_ns_ = false;  // the wave's elimination kernels carry the Newton-Schulz pivot inverse
   int wave_kernels_eval_ = 0, wave_kernels_dir_ = 0, wave_kernels_end_ = 0;
   long long seen_rounds_ = 0, seen_dir_ = 0, seen_end_ = 0;
   int wave_graph_tuning_ = 0;  // the launch-shape tuning the round graph was captured with

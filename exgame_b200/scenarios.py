@@ -217,6 +217,87 @@ def cloth_world(cols, rows, kick=0.5, k=100.0, zeta=0.7, mass_total=1.0, width=0
     return bodies, joints, params
 
 
+def camera_rig_world(n_rigs=1, r_object=2.0, linear=1.0, spacing=1000.0, dt=1.0 / 60.0, tol=1e-10,
+                     precision=PRECISION_F64, target_velocity=(0.0, 0.0, 0.0)):
+    """The hitchcock camera rig (crates/hitchcock/src/camera.rs:259-520, rig.rs:86-147) as a
+    consumer workload: per rig four bodies, in this order, the eye (`real`, at the target's
+    centre + r along z), the `intermediate` (at the centre) and the `anchor` (centre - r along y),
+    each a unit mass with unit isotropic moment moving with the target's velocity
+    (RigidBody::body_at_with_speed_and_mass), and the kinematic target tracker at the centre; 17
+    CriticallyDampedWarped axial springs between offset anchors (stiffness `linear`, softening
+    r / 1000, the rests of camera.rs:345-489: 0, 0, r sqrt2, r sqrt2 eye-intermediate; r sqrt2 x 8
+    intermediate-tracker; r x 4 intermediate-anchor; r anchor-tracker), three TorsionalDamperWarped
+    (eye-intermediate, intermediate-anchor, intermediate-tracker) and two PerpendicularDamperWarped
+    (intermediate-tracker, anchor-tracker), each with damping `linear`, connected in that order.
+    Rig k's target starts at (spacing k, 0, 0). The host moves each tracker between steps
+    (camera.rs:55-76: pose = translation to the target, momentum = the target's velocity), see
+    track_targets. Gravity off; implicit Newton."""
+    r, z = float(r_object), 0.0
+    s1 = r * math.sqrt(2.0)
+    soft = r / 1000.0
+    springs = [  # (a, a_local, b, b_local, rest) with 0 eye, 1 intermediate, 2 anchor, 3 tracker
+        (0, (r, z, -r), 1, (r, z, z), z), (0, (-r, z, -r), 1, (-r, z, z), z),
+        (0, (z, r, z), 1, (z, z, z), s1), (0, (z, -r, z), 1, (z, z, z), s1),
+        (1, (r, -r, z), 3, (z, z, z), s1), (1, (-r, -r, z), 3, (z, z, z), s1),
+        (1, (z, -r, -r), 3, (z, z, z), s1), (1, (z, -r, r), 3, (z, z, z), s1),
+        (1, (r, r, z), 3, (z, z, z), s1), (1, (-r, r, z), 3, (z, z, z), s1),
+        (1, (z, r, -r), 3, (z, z, z), s1), (1, (z, r, r), 3, (z, z, z), s1),
+        (1, (r, -r, z), 2, (z, z, z), r), (1, (-r, -r, z), 2, (z, z, z), r),
+        (1, (z, -r, -r), 2, (z, z, z), r), (1, (z, -r, r), 2, (z, z, z), r),
+        (2, (z, z, z), 3, (z, z, z), r),
+    ]
+    torsional = [(0, 1), (1, 2), (1, 3)]
+    transverse = [(1, 3), (2, 3)]
+    nb, nj = 4 * n_rigs, (len(springs) + len(torsional) + len(transverse)) * n_rigs
+    bodies = np.zeros(nb, dtype=BODY_DTYPE)
+    joints = np.zeros(nj, dtype=JOINT_DTYPE)
+    tw = np.zeros((nb, 6))
+    v = np.asarray(target_velocity, dtype=np.float64)
+    q = 0
+    for k in range(n_rigs):
+        c = np.array([spacing * k, 0.0, 0.0])
+        o = 4 * k
+        for i, off in enumerate(((z, z, r), (z, z, z), (z, -r, z), (z, z, z))):
+            tw[o + i, :3] = c + np.array(off)
+        for i in range(3):
+            bodies[o + i]["mass"] = 1.0
+            bodies[o + i]["momentum"][:3] = v
+        bodies[o + 3]["kinematic"] = 1
+        bodies[o + 3]["mass"] = 0.0
+        bodies[o + 3]["momentum"][:3] = v  # Inertia::Kinematic: the momentum is the twist
+        for a, al, b, bl, rest in springs:
+            joints[q]["law"], joints[q]["a"], joints[q]["b"] = 1, o + a, o + b
+            joints[q]["params"][:10] = (*al, *bl, rest, linear, 0.0, soft)
+            q += 1
+        for a, b in torsional:
+            joints[q]["law"], joints[q]["a"], joints[q]["b"] = 3, o + a, o + b
+            joints[q]["params"][0] = linear
+            q += 1
+        for a, b in transverse:
+            joints[q]["law"], joints[q]["a"], joints[q]["b"] = 2, o + a, o + b
+            joints[q]["params"][:2] = (linear, soft)
+            q += 1
+    bodies["pose"] = motors_np.twist_exp_n(tw, 1.0)
+    bodies["inertia"][:, 0] = bodies["inertia"][:, 4] = bodies["inertia"][:, 8] = 1.0
+    bodies["diagonal"] = 1
+    bodies["size"] = 1.0
+    params = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=dt, tol=tol)
+    return bodies, joints, params
+
+
+def track_targets(state, n_rigs, centres, velocities):
+    """The tracker's pre_step (crates/hitchcock/src/camera.rs:55-76) on an (n, 14) state array
+    (pose, momentum per body, as exg_world_get_state returns it): tracker k (body 4k + 3) moves to
+    centres[k] with velocity velocities[k]."""
+    out = state.copy()
+    tw = np.zeros((n_rigs, 6))
+    tw[:, :3] = centres
+    out[3::4, :8] = motors_np.twist_exp_n(tw, 1.0)
+    out[3::4, 8:11] = velocities
+    out[3::4, 11:14] = 0.0
+    return out
+
+
 def concat_worlds(parts):
     """Concatenate (bodies, joints) pairs into one world, re-indexing the joints."""
     bodies, joints, off = [], [], 0

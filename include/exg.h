@@ -117,6 +117,12 @@ typedef enum { EXG_PRECISION_F64 = 0, EXG_PRECISION_MIXED = 1, EXG_PRECISION_MIX
  * (crates/newton/src/integrator/implicit/cache.rs:509-520). Either matrix leads to the same
  * converged step; the exact one converges in fewer iterations. */
 #define EXG_NEWTON_EXACT_POSE_FACTOR 1
+/* newton_flags bit 1 (mixed precisions only): invert the elimination's 6x6 pivot blocks by
+ * Newton-Schulz (the reference's iteration, crates/newton/src/integrator/implicit/newton.rs:209-327,
+ * at block size): warm-started from the node's inverse of the previous solve in the step, FP32
+ * steps where the block moved, one FP64 correction (exg_pivot_inverse states the details); without
+ * it the pivots take FP64 Gauss-Jordan. Both converge to the same step. */
+#define EXG_NEWTON_NS_PIVOT 2
 
 typedef struct {
   int32_t integrator;
@@ -223,9 +229,9 @@ EXG_API int exg_batch_world_stats(exg_world_t w, int32_t world, exg_world_stats_
  * crates/newton/src/mechanism/islands.rs:166-299; Mechanism::split / merge,
  * crates/newton/src/mechanism/mechanism.rs:326-434); the islands and the solver's structure are
  * rebuilt before the next step (cache.rs:689-788). The bodies keep their state on the device.
- * All or nothing: EXG_ERR_UNSUPPORTED (a dynamic cycle), EXG_ERR_OUT_OF_MEMORY (no room in the
- * handle's joint capacity: a world or batch handle holds the joint count it was created with, a
- * pool max_joints) or a bad record leaves the world as it was. */
+ * An island whose dynamic bodies form a cycle takes the block-LU solve. All or nothing:
+ * EXG_ERR_OUT_OF_MEMORY (no room in the handle's joint capacity: a world or batch handle holds the
+ * joint count it was created with, a pool max_joints) or a bad record leaves the world as it was. */
 EXG_API int exg_batch_set_joints(exg_world_t w, int32_t world, const exg_joint_t* joints, int32_t n_joints);
 /* The epoch of one world (world 0 of a single world) for the following steps: its dt and warp
  * (Epoch::standalone(dt, warp), crates/aristotle/src/epoch.rs:17-60; the reference passes the
@@ -450,6 +456,22 @@ EXG_API int exg_motor_compose_n(int64_t count, const double* a, const double* b,
  * pose B, vel A, vel B; each lin xyz then ang xyz) when jacobian != 0. */
 EXG_API int exg_eval_joints(exg_device_t dev, const exg_joint_t* d_joints, int32_t n_joints, const double* d_pose,
                     const double* d_vel, double dt, double warp, int32_t jacobian, double* d_out);
+/* The implicit solve's 6x6 pivot inverse on n row-major blocks d_blocks[36*k] -> d_out[36*k]
+ * (the block inverse of the reference's Newton-Schulz solve, crates/newton/src/integrator/implicit/
+ * newton.rs:209-327: seed_transpose, refine_inverse, the warm start). precision MIXED or
+ * MIXED_FAST: the inverse the mixed path takes with EXG_NEWTON_NS_PIVOT. With warm != 0, d_out
+ * holds on entry an earlier inverse of each block (the block before a small change): where its
+ * FP64 residual max|I - D X| is at most 1e-4, one FP64 Newton-Schulz correction; otherwise FP32
+ * Newton-Schulz steps held in registers on the diagonally scaled block (seeded with the earlier
+ * inverse where its residual is below 1/2, else with the identity or the reference's transposed
+ * seed) and one FP64 correction, FP64 Gauss-Jordan for a block whose FP32 residual stays above
+ * 1e-3. F64: FP64 Gauss-Jordan with partial pivoting (the plain path's). form 0 runs one thread
+ * per block (a wide elimination level's form), 1 one warp per block (a narrow level's and the
+ * island kernel's); both give the same bits. d_steps (may be NULL) receives per block the FP32
+ * steps taken (0 where the warm correction sufficed), -1 where the block fell back to Gauss-Jordan,
+ * 0 on F64. EXG_ERR_FATAL if a block is singular (its output is then not finite). */
+EXG_API int exg_pivot_inverse(exg_device_t dev, const double* d_blocks, int32_t n, int32_t precision, int32_t form,
+                              int32_t warm, double* d_out, int32_t* d_steps);
 /* All-pairs gravity (crates/newton/src/gravity.rs:110-140, 438-450): d_pos_mass holds
  * [x, y, z, m] per body, d_size the core radius (SIZE_CORE law), output d_force[3*i] is the
  * world force on body i. precision MIXED runs the FP32 kernel on double-single separations,

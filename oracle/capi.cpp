@@ -87,6 +87,16 @@ void orc_world_get_bodies(void* h, exg_body_t* out) {
   OWorld* w = static_cast<OWorld*>(h);
   for (size_t i = 0; i < w->bodies.size(); ++i) from_obody(w->bodies[i], out[i]);
 }
+// Overwrite every body's pose and momentum (a host moving kinematic bodies between steps, as the
+// camera rig's target tracker does in pre_step, crates/hitchcock/src/camera.rs:55-76); the islands
+// and their solver state stay.
+void orc_world_set_state(void* h, const exg_body_t* bodies) {
+  OWorld* w = static_cast<OWorld*>(h);
+  for (size_t i = 0; i < w->bodies.size(); ++i) {
+    std::memcpy(w->bodies[i].pose, bodies[i].pose, sizeof w->bodies[i].pose);
+    std::memcpy(w->bodies[i].mom, bodies[i].momentum, sizeof w->bodies[i].mom);
+  }
+}
 double orc_world_energy(void* h) { return static_cast<OWorld*>(h)->energy(); }
 // spans / Newton iterations of island k's last step
 int orc_world_island_count(void* h) { return (int)static_cast<OWorld*>(h)->islands.size(); }

@@ -32,6 +32,7 @@ def lib():
         L.orc_world_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_worlds_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_world_get_bodies.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_world_set_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_world_energy.restype = ctypes.c_double
         L.orc_world_energy.argtypes = [ctypes.c_void_p]
         L.orc_world_island_count.argtypes = [ctypes.c_void_p]
@@ -83,6 +84,12 @@ class OracleWorld:
         out = np.zeros_like(self._b)
         lib().orc_world_get_bodies(self.h, p(out))
         return out
+
+    def set_state(self, bodies):
+        """Overwrite every body's pose and momentum from records (the islands stay)."""
+        b = np.ascontiguousarray(bodies)
+        assert len(b) == self.n
+        lib().orc_world_set_state(self.h, p(b))
 
     def energy(self):
         return lib().orc_world_energy(self.h)

@@ -82,10 +82,11 @@ def test_wave_exact_pose_factor_matches_oracle(device, oracle):
     assert pe < 1e-9 and me < 1e-7, (pe, me)
 
 
-@pytest.mark.parametrize("precision", [0, PRECISION_MIXED])
-def test_wave_agrees_with_island_kernel(device, precision):
+@pytest.mark.parametrize("precision,ns", [(0, False), (PRECISION_MIXED, False), (PRECISION_MIXED, True)])
+def test_wave_agrees_with_island_kernel(device, precision, ns):
     bodies, joints = scenarios.tree_world(700, seed=71)
-    params = step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10, exact_jacobian=True)
+    params = step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10, exact_jacobian=True,
+                         ns_pivot=ns)
     a = _lib.DeviceWorld(device, bodies, joints, params)
     a.set_option(W.OPT_WAVE_MIN_BODIES, 1 << 20)  # island kernel
     a.step(5)
@@ -99,14 +100,14 @@ def test_wave_agrees_with_island_kernel(device, precision):
     assert sa["last_spans"] == sb["last_spans"]
 
 
-@pytest.mark.parametrize("precision", [0, PRECISION_MIXED])
-def test_wave_batch_is_bitwise_identical_to_worlds_alone(device, precision):
+@pytest.mark.parametrize("precision,ns", [(0, False), (PRECISION_MIXED, False), (PRECISION_MIXED, True)])
+def test_wave_batch_is_bitwise_identical_to_worlds_alone(device, precision, ns):
     worlds = []
     for k, n in enumerate([3, 50, 300, 900]):
         b, j = scenarios.tree_world(n, seed=80 + k)
-        worlds.append((b, j, step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10)))
+        worlds.append((b, j, step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10, ns_pivot=ns)))
     b, j = scenarios.chain_world(40, seed=90)
-    worlds.append((b, j, step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10)))
+    worlds.append((b, j, step_params(integrator=NEWTON, precision=precision, dt=1e-2, tol=1e-10, ns_pivot=ns)))
     worlds.append((scenarios.gravity_world(500, 30.0, seed=91), np.zeros(0, dtype=JOINT_DTYPE),
                    step_params(integrator=LIE_EULER, gravity_law=GRAVITY_PLUMMER, precision=precision,
                                softening=0.05, dt=1e-3)))
@@ -163,15 +164,16 @@ def test_host_driven_rounds_equal_the_conditional_graph(device):
     assert np.array_equal(out[0]["pose"], out[1]["pose"]) and np.array_equal(out[0]["momentum"], out[1]["momentum"])
 
 
-def test_wide_and_narrow_elimination_levels_agree_with_island_kernel(device):
+@pytest.mark.parametrize("ns", [False, True])
+def test_wide_and_narrow_elimination_levels_agree_with_island_kernel(device, ns):
     """A batch whose widest elimination levels hold more than 8192 nodes, so the wave eliminates
     them one thread per node and the narrow levels one warp per node: every world ends bit for bit
-    as the island kernel leaves it."""
+    as the island kernel leaves it (with Gauss-Jordan and with Newton-Schulz pivot inverses)."""
     worlds = []
     for k in range(64):
         b, j = scenarios.tree_world(2048, seed=400 + k)
         worlds.append((b, j, step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10,
-                                         exact_jacobian=True)))
+                                         exact_jacobian=True, ns_pivot=ns)))
     a = _lib.DeviceBatch(device, worlds)
     a.set_option(W.OPT_WAVE_MIN_BODIES, 1 << 20)  # island kernel
     a.step(3)

@@ -44,6 +44,14 @@ WORLDS = 4096      # config-3 batch size (--worlds)
 SHARD = False      # --shard: one batch split over the ranks instead of one batch per rank
 NS_PIVOT = False   # --ns-pivot: Newton-Schulz pivot inverses on the implicit worlds
 WORLD_SIZE = 1
+# DRAM bytes (read + write) of the Newton step over its algorithmic bytes, measured by ncu on one
+# step of the 1024-world batch (28.33 GB against 15.62 GB); the Newton step's traffic grows with the
+# islands' Newton iterations as its algorithmic bytes do, so roofline.traffic is this ratio times the
+# timed step's algorithmic bytes.
+NEWTON_TRAFFIC_RATIO = 28.33 / 15.62
+NEWTON_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one Newton step of the first 1024 "
+                         "worlds of this batch: 28.33 GB against its 15.62 GB of algorithmic bytes, ratio 1.81, "
+                         "times this step's algorithmic bytes")
 FP64_FMA_PER_SM_CLK = 64
 FP32_FMA_PER_SM_CLK = 128
 
@@ -397,7 +405,8 @@ def run_ours(args, rank, world_size, local_rank):
         nbytes, iters = newton_bytes_last_step(worlds[0], parts)
         hbm = float(peaks["hbm_gbs"])
         roofline = {"bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
-                    "frac": nbytes / avg_s / 1e9 / hbm, "traffic": None, "kernel": label,
+                    "frac": nbytes / avg_s / 1e9 / hbm, "traffic": NEWTON_TRAFFIC_RATIO * nbytes,
+                    "traffic_source": NEWTON_TRAFFIC_SOURCE, "kernel": label,
                     "algorithmic_bytes_per_launch": nbytes, "newton_iterations_summed_over_islands": iters,
                     "avg_launch_us": avg_s * 1e6, "launches": nl, "device_ms_by_kernel": shares,
                     "peak_source": f"{src} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs), of {src}"}

@@ -49,7 +49,7 @@ struct exg_device_s {
   long long prof_count[PROF_KINDS] = {0};
   // launch-shape tuning (exg_device_set_tuning; results do not depend on any of these)
   std::atomic<int> tune_gravity_ctas_per_sm{32};  // persistent one-warp CTAs of the mixed gravity kernel
-  std::atomic<int> tune_wave_blocks_per_sm{8};    // grid cap of the wave's 256-thread data kernels (128-thread: twice)
+  std::atomic<int> tune_wave_blocks_per_sm{16};   // grid cap of the wave's 256-thread data kernels (128-thread: twice)
   std::atomic<int> tune_wave_min_bodies{32};      // default wave threshold of new world handles
   std::atomic<int> tune_wave_narrow_level{8192};  // elimination levels up to this many nodes: a warp per node
 };

@@ -504,7 +504,7 @@ def serve_sweep(dev, rates, n_requests, pool_size, tick, rank):
         picks = rng.integers(0, len(pool), n_requests)
         steps = np.exp(rng.uniform(math.log(10), math.log(1000), n_requests)).astype(np.int64)
         srv = _lib.Server(dev, hbm_budget_bytes=150 * 10**9, max_bodies=max(4 << 20, 2 * max_b),
-                          max_joints=max(12 << 20, 6 * max_b), max_worlds=1024, precision=PRECISION_MIXED,
+                          max_joints=max(12 << 20, 6 * max_b), max_worlds=2048, precision=PRECISION_MIXED,
                           steps_per_tick=tick)
         ids, lag = [], []
         t0 = time.perf_counter()
@@ -652,7 +652,7 @@ def main():
                     help="split one batch over the ranks by body count (strong scaling) instead of one batch per rank")
     ap.add_argument("--serve-rates", default="100,1000,10000",
                     help="request rates (req/s) of the served sweep at N=1; empty to skip")
-    ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-requests", type=int, default=1000)
     ap.add_argument("--serve-pool", type=int, default=256)
     ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")

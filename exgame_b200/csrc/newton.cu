@@ -364,6 +364,9 @@ template <bool MIXED, bool NS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDeviceArrays A, WorldRef W, const int* __restrict__ queue,
                                                          int n_islands, int* __restrict__ head) {
   __shared__ double red[kWarps];
+  __shared__ double frame[kFrameDoubles];
+  __shared__ double frame_sh[4 * kFrameThreads];
+  static_assert(kThreads == kFrameThreads, "the island frame sums over a CTA of kFrameThreads threads");
   __shared__ int flag;
   __shared__ int item;
   __shared__ long long phase_acc[kPhases];
@@ -384,6 +387,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_newton_step(NewtonDevi
     const int island = queue[k];
     if (!W.w_active[A.desc[island].world]) continue;  // the world holds this step
     Ctx c = make_ctx(A, W, island);
+    island_frame(A, W, c.d, frame_sh, frame);  // the step's frame: the island's centre of mass
+    c.frame = frame;
     load_external(c);
     __syncthreads();
     unsigned long long remaining = 1ull << kMaxDepth;

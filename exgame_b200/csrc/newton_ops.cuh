@@ -90,12 +90,86 @@ struct IslandParams {
   const double* part;
 };
 
+// An island's frame for one step: its poses are read relative to an anchor near the island's centre
+// of mass at the step's start, and written back to world coordinates. The reference keeps each
+// island's poses local to an origin re-bound to its centre of mass after every step
+// (Island::recompute_centroid, crates/newton/src/mechanism/island.rs:206-243;
+// crates/newton/tests/precision_seam.rs measures why): world-origin twists (v = v_body - w x p)
+// cancel catastrophically far from the origin. Here the anchor is the centre of mass rounded to a
+// multiple of kFrameGrid in each component, so an island within kFrameGrid / 2 of the origin steps
+// in world coordinates exactly as before: the Newton residual's per-body angular scale
+// (functions/src/lib.rs:170-247) is taken about the frame's origin and has a floor of 1e-9, which a
+// small island's bodies at its own centre of mass reach, and a 1e-10 tolerance then cannot be met.
+// Layout (doubles): [0, 3) the anchor a, [4, 12) the translator by -a, [12, 20) the one by +a.
+constexpr double kFrameGrid = 1024.0;
+constexpr int kFrameDoubles = 20;
+__device__ inline void frame_make(const double* a, double* f) {
+  double t6[6] = {-a[0], -a[1], -a[2], 0.0, 0.0, 0.0}, b[6];
+  f[0] = a[0]; f[1] = a[1]; f[2] = a[2]; f[3] = 0.0;
+  screw_from6(t6, b);
+  twist_exp(b, 1.0, f + 4);
+  t6[0] = a[0]; t6[1] = a[1]; t6[2] = a[2];
+  screw_from6(t6, b);
+  twist_exp(b, 1.0, f + 12);
+}
+
+// The frame of island d for this step, by a CTA of kFrameThreads threads (the wave and the island
+// kernel both call this, so both get the same bits): thread t sums m p over the island's bodies
+// t, t + kFrameThreads, ... in island order (kinematic bodies weigh nothing), then a fixed tree over
+// the threads; the centre of mass is the sum over the mass (the island's first body where the
+// island has no dynamic mass), and the anchor that point on the kFrameGrid grid. sh:
+// 4 * kFrameThreads doubles of shared memory; f receives the frame.
+constexpr int kFrameThreads = 256;
+__device__ inline void island_frame(const NewtonDeviceArrays& A, const WorldRef& W, const IslandDesc& d, double* sh,
+                                    double* f) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int q = threadIdx.x; q < d.nb; q += kFrameThreads) {
+    const int g = A.isl_body[d.body_off + q];
+    const double m = W.kinematic[g] ? 0.0 : W.mass[g];
+    double pose[8], p3[3];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) pose[e] = W.pose[(size_t)e * W.n + g];
+    body_position(pose, p3);
+    acc[0] += p3[0] * m;
+    acc[1] += p3[1] * m;
+    acc[2] += p3[2] * m;
+    acc[3] += m;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) sh[4 * threadIdx.x + k] = acc[k];
+  __syncthreads();
+  for (int h = kFrameThreads / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sh[4 * threadIdx.x + k] += sh[4 * (threadIdx.x + h) + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double a[3];
+    if (sh[3] > 0.0) {
+      const double inv = 1.0 / sh[3];
+      a[0] = sh[0] * inv; a[1] = sh[1] * inv; a[2] = sh[2] * inv;
+    } else {
+      const int g = A.isl_body[d.body_off];
+      double pose[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) pose[e] = W.pose[(size_t)e * W.n + g];
+      body_position(pose, a);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a[k] = kFrameGrid * rint(a[k] / kFrameGrid);
+    frame_make(a, f);
+  }
+  __syncthreads();
+}
+
 struct Ctx {
   NewtonDeviceArrays A;
   IslandDesc d;
   WorldRef W;
   IslandParams P;
   Scratch s;
+  const double* frame;  // kFrameDoubles: the island's frame for this step (see frame_make)
   int island;
   EXG_HD int gbody(int q) const { return A.isl_body[d.body_off + q]; }
 };
@@ -122,6 +196,7 @@ __device__ inline Ctx make_ctx(const NewtonDeviceArrays& A, const WorldRef& W, i
   c.island = island;
   c.d = A.desc[island];
   c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
+  c.frame = nullptr;
   resolve_params(c);
   return c;
 }
@@ -136,6 +211,7 @@ __device__ __forceinline__ Ctx make_ctx_desc(const NewtonDeviceArrays& A, const 
   c.island = -1;
   c.d = d;
   c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
+  c.frame = nullptr;
   if (params) resolve_params(c);
   return c;
 }
@@ -148,6 +224,7 @@ __device__ inline Ctx make_ctx_lite(const NewtonDeviceArrays& A, const WorldRef&
   c.island = island;
   c.d = A.desc[island];
   c.s = carve(A.scratch + c.d.scratch_off, c.d.nb, c.d.nj, c.d.m, c.d.n_slots);
+  c.frame = nullptr;
   return c;
 }
 
@@ -173,11 +250,18 @@ __device__ __forceinline__ void st_n(double* p, const double* v) {
 
 // ── per-item operations ─────────────────────────────────────────────────────
 // PRE (functions::pre): mid = exp(half/2 x) * pose of island body q.
+// Pose of world body g in the island's frame.
+__device__ __forceinline__ void local_pose(const Ctx& c, int g, double* pose) {
+  double w[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w[k] = c.W.pose[(size_t)k * c.W.n + g];
+  motor_compose(w, c.frame + 4, pose);
+}
+
 __device__ inline void op_pre(const Ctx& c, const double* x, double half, int q) {
   int g = c.gbody(q);
   double pose[8], xv[6], vb[6], e[8], m[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+  local_pose(c, g, pose);
   ld_n<6>(x + 6 * (size_t)q, xv);
   screw_from6(xv, vb);
   twist_exp(vb, half, e);
@@ -425,8 +509,7 @@ __device__ inline void op_trial(const Ctx& c, double alpha, int t) {
 __device__ inline void op_load_world_state(const Ctx& c, int q) {
   int g = c.gbody(q);
   double pose[8], mom[6], I9[9];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) pose[k] = c.W.pose[(size_t)k * c.W.n + g];
+  local_pose(c, g, pose);
 #pragma unroll
   for (int k = 0; k < 6; ++k) mom[k] = c.W.mom[(size_t)k * c.W.n + g];
 #pragma unroll
@@ -448,6 +531,9 @@ __device__ inline void op_load_external(const Ctx& c, int q) {
   double e[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   int g = c.gbody(q);
   double4 pm = reinterpret_cast<const double4*>(c.W.pos_mass)[g];
+  pm.x = pm.x - c.frame[0];  // the moment arm from the island's anchor
+  pm.y = pm.y - c.frame[1];
+  pm.z = pm.z - c.frame[2];
   if (c.P.splits > 0) {
     int il = g - c.P.wbody_off;
     double f[3];
@@ -471,8 +557,7 @@ __device__ inline void op_commit(const Ctx& c, double span, double half, bool co
   int q = c.A.dn_body[c.d.dyn_off + i];
   int g = c.gbody(q);
   double m0[8], vb[6], e[8], pm[8], inv[8], vbody[6], v6[6], I9[9];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) m0[k] = c.W.pose[(size_t)k * c.W.n + g];
+  local_pose(c, g, m0);
 #pragma unroll
   for (int k = 0; k < 9; ++k) I9[k] = c.W.inertia[(size_t)k * c.W.n + g];
   double vq[6], snap[6];
@@ -499,8 +584,10 @@ __device__ inline void op_commit(const Ctx& c, double span, double half, bool co
   screw_from6(pnew, pnb);
   wrench_transport(pnb, minv, pbody);
   screw_to6(pbody, out6);
+  double mw[8];
+  motor_compose(mnew, c.frame + 12, mw);  // back to world coordinates
 #pragma unroll
-  for (int k = 0; k < 8; ++k) c.W.pose[(size_t)k * c.W.n + g] = mnew[k];
+  for (int k = 0; k < 8; ++k) c.W.pose[(size_t)k * c.W.n + g] = mw[k];
 #pragma unroll
   for (int k = 0; k < 6; ++k) c.W.mom[(size_t)k * c.W.n + g] = out6[k];
 }

@@ -45,6 +45,7 @@ struct WaveCtl {
   int mflip;  // 1: the scratch's mass and mass0 blocks trade places (see wave_ctx)
   int ns;     // Newton-Schulz pivot inverses (mixed path, EXG_NEWTON_NS_PIVOT)
   int warm;   // a solve of this step has filled every node's Dinv slot
+  double frame[kFrameDoubles];  // the island's frame for this step (frame_make)
 };
 
 struct WaveArgs {
@@ -106,6 +107,7 @@ __device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 __device__ __forceinline__ Ctx wave_ctx(const WaveArgs& a, int k) {
   Ctx c = make_ctx_desc(a.A, a.W, a.wdesc[k], true);
   if (a.ctl[k].mflip) { double* t = c.s.mass; c.s.mass = c.s.mass0; c.s.mass0 = t; }
+  c.frame = a.ctl[k].frame;
   return c;
 }
 __device__ __forceinline__ Ctx wave_ctx_lite(const WaveArgs& a, int k) {
@@ -136,6 +138,16 @@ __global__ void k_w_init(WaveArgs a) {
     c.mflip = 0;
     c.ns = (a.W.wparams[d.world].newton_flags & EXG_NEWTON_NS_PIVOT) != 0;
     c.warm = 0;
+  }
+}
+
+// Step start, after k_w_init: every active island's frame for the step (its centre of mass), one
+// CTA per island, the island kernel's arithmetic.
+__global__ void __launch_bounds__(kFrameThreads) k_w_frame(WaveArgs a) {
+  __shared__ double sh[4 * kFrameThreads];
+  for (int k = blockIdx.x; k < a.n_isl; k += gridDim.x) {
+    if (!a.ctl[k].active) continue;  // uniform over the CTA
+    island_frame(a.A, a.W, a.wdesc[k], sh, a.ctl[k].frame);
   }
 }
 
@@ -1326,7 +1338,8 @@ int NewtonWorld::run_wave(exg_device_s* dev, DeviceWorld& w, cudaStream_t s) {
   wave_ns_ = want_ns;
   int tok = prof_begin(dev, PROF_NEWTON_WAVE, s);
   k_w_init<<<g_isl, T, 0, s>>>(a);
-  dev->launches.fetch_add(1, std::memory_order_relaxed);
+  k_w_frame<<<std::min(a.n_isl, std::max(1, dev->sm_count) * 8), kFrameThreads, 0, s>>>(a);
+  dev->launches.fetch_add(2, std::memory_order_relaxed);
   k_w_external<<<g_body, T, 0, s>>>(a);
   int rc = exg_after_launch(dev);
   if (rc != EXG_OK) return rc;

@@ -45,6 +45,7 @@ struct OJoint { int law, a, b; double p[10]; };
 enum Integrator { EXPLICIT_EULER = 0, SYMPLECTIC_EULER = 1, LIE_EULER = 2, NEWTON = 3 };
 enum GravityLaw { GRAVITY_OFF = 0, GRAVITY_SIZE_CORE = 1, GRAVITY_PLUMMER = 2 };
 enum Solver { SOLVER_EXACT = 0, SOLVER_REFERENCE_NS = 1 };
+constexpr double kFrameGrid = 1024.0;  // island frames' anchors lie on this grid (NewtonIsland::make_frame)
 
 // body.rs:70-77
 inline double effective_size(double mass) { return std::pow(mass / 4.0, 1.0 / 3.0); }
@@ -400,8 +401,52 @@ struct NewtonIsland {
   bool have_A = false;
   int newton_iterations = 0;
 
+  // The step's frame: the island's poses are taken relative to an anchor near its centre of mass at
+  // the step's start, delta = sum m_i r_i / M (kinematic bodies weigh nothing; the first body's
+  // position where the island has no dynamic mass) rounded to a multiple of kFrameGrid in each
+  // component, and written back in world coordinates. The reference re-binds each island's origin
+  // to its centre of mass after every step (Island::recompute_centroid, mechanism/island.rs:206-243);
+  // the rounding keeps islands within kFrameGrid / 2 of the world origin in world coordinates, where
+  // the Newton residual's per-body angular scale (functions/src/lib.rs:170-247) has the lever arms
+  // the tolerances here are set for: at the centre of mass itself a small island's angular scale
+  // falls to the residual's 1e-9 floor and a 1e-10 tolerance is out of reach.
+  std::vector<Motor<double>> lpose;   // per island body, in the island's frame
+  std::vector<Wrench<double>> lext;   // external wrenches about the anchor
+  Motor<double> to_world;
+
   NewtonIsland(std::vector<OBody>& b, const std::vector<OJoint>& j, Island& i, const WorldParams& w, const std::vector<Wrench<double>>& e)
       : bodies(b), joints(j), isl(i), wp(w), external(e) {}
+
+  void make_frame() {
+    double wx[3] = {0.0, 0.0, 0.0}, total = 0.0;
+    for (int q = 0; q < nb(); ++q) {
+      const OBody& b = bodies[isl.bodies[q]];
+      const double m = b.kinematic ? 0.0 : b.mass;
+      const V3<double> r = body_position(b);
+      for (int k = 0; k < 3; ++k) wx[k] += r[k] * m;
+      total += m;
+    }
+    V3<double> a = body_position(bodies[isl.bodies[0]]);
+    if (total > 0.0) {
+      const double inv = 1.0 / total;
+      a = V3<double>(wx[0] * inv, wx[1] * inv, wx[2] * inv);
+    }
+    for (int k = 0; k < 3; ++k) a[k] = kFrameGrid * std::nearbyint(a[k] / kFrameGrid);
+    const double neg[6] = {-a[0], -a[1], -a[2], 0.0, 0.0, 0.0}, pos[6] = {a[0], a[1], a[2], 0.0, 0.0, 0.0};
+    const Motor<double> to_local = twist_exp(Twist<double>::from6(neg), 1.0);
+    to_world = twist_exp(Twist<double>::from6(pos), 1.0);
+    lpose.resize(nb());
+    lext.resize(nb());
+    for (int q = 0; q < nb(); ++q) {
+      lpose[q] = body_pose(bodies[isl.bodies[q]]).compose(to_local);
+      const Wrench<double>& e = external[isl.bodies[q]];
+      double w6[6];
+      e.to6(w6);
+      const V3<double> f(w6[0], w6[1], w6[2]);
+      const V3<double> m = V3<double>(w6[3], w6[4], w6[5]) - a.cross(f);
+      lext[q] = Wrench<double>::make(f, m);
+    }
+  }
 
   int nb() const { return (int)isl.bodies.size(); }
   int local_of(int global) const { return int(std::lower_bound(isl.bodies.begin(), isl.bodies.end(), global) - isl.bodies.begin()); }
@@ -411,7 +456,7 @@ struct NewtonIsland {
                   std::vector<Block>& mass_out, std::vector<double>& rhs_out, std::vector<double>& scale_out) {
     int n = nb();
     mid.resize(n);
-    for (int q = 0; q < n; ++q) mid[q] = body_pose(bodies[isl.bodies[q]]).compose(twist_exp(vmid[q], half));  // functions::pre
+    for (int q = 0; q < n; ++q) mid[q] = lpose[q].compose(twist_exp(vmid[q], half));  // functions::pre
     size_t nj = isl.joints.size();
     std::vector<double> conn(nj * 12);
     if (with_jac) jac.resize(nj * 300);
@@ -432,7 +477,7 @@ struct NewtonIsland {
       }
     }
     std::vector<Wrench<double>> total(n);
-    for (int q = 0; q < n; ++q) total[q] = external[isl.bodies[q]];
+    for (int q = 0; q < n; ++q) total[q] = lext[q];
     for (size_t q = 0; q < nj; ++q) {
       const OJoint& j = joints[isl.joints[q]];
       int la = local_of(j.a), lb = local_of(j.b);
@@ -666,7 +711,7 @@ struct NewtonIsland {
     const double tol2 = wp.tol * wp.tol;
     int n = nb(), m = isl.m;
     std::vector<Twist<double>> vmid(n);
-    for (int q = 0; q < n; ++q) vmid[q] = world_velocity(bodies[isl.bodies[q]]);
+    for (int q = 0; q < n; ++q) vmid[q] = body_velocity(bodies[isl.bodies[q]]).transport_contra(lpose[q]);
     auto read_vals = [&]() { return vmid; };
     double best = huge;
     std::vector<Twist<double>> best_vals = read_vals();
@@ -728,13 +773,14 @@ struct NewtonIsland {
     for (int q = 0; q < nb(); ++q) {
       if (isl.order[q] < 0) continue;
       OBody& b = bodies[isl.bodies[q]];
-      Motor<double> m_start = body_pose(b);
+      Motor<double> m_start = lpose[q];
       Motor<double> pose_mid = m_start.compose(twist_exp(vmid[q], half));
       Twist<double> v_body = vmid[q].transport_contra(pose_mid.inverse());
       Wrench<double> p_s_mid = inertia_apply(b, v_body).transport_co(pose_mid);
       Wrench<double> p_new = converged ? p_s_mid.scale(2.0) - snap[q] : p_s_mid;
       Motor<double> m_new = m_start.compose(twist_exp(vmid[q], span));
-      m_new.to_components(b.pose);
+      lpose[q] = m_new;
+      m_new.compose(to_world).to_components(b.pose);
       p_new.transport_co(m_new.inverse()).to6(b.mom);
     }
   }
@@ -758,6 +804,7 @@ struct NewtonIsland {
     const int MAX_DEPTH = 8, THRESHOLD_LOG2 = 8, PER_HALVING_LOG2 = 4;
     const double huge = 1e9;
     build_sparsity();
+    make_frame();
     if (wp.solver == SOLVER_REFERENCE_NS && (int)isl.X.size() != isl.m * isl.m) {
       isl.X.assign((size_t)isl.m * isl.m, zero_block()); isl.X_accepted = isl.X; isl.seeded = isl.accepted_seeded = false;
     }
@@ -772,7 +819,7 @@ struct NewtonIsland {
       double half = span / 2.0;
       ++spans;
       std::vector<Wrench<double>> snap(nb());
-      for (int q = 0; q < nb(); ++q) snap[q] = world_momentum(bodies[isl.bodies[q]]);
+      for (int q = 0; q < nb(); ++q) snap[q] = body_mom(bodies[isl.bodies[q]]).transport_co(lpose[q]);
       SolveResult res = newton_solve(snap, half);
       bool finite = res.best < huge;
       bool last = depth == MAX_DEPTH;

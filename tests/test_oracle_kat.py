@@ -396,11 +396,13 @@ def test_uniform_field_applies_m_times_accel_and_ignores_kinematic(oracle):
     out = w.bodies()
     assert np.allclose(out[0]["momentum"][:3], np.array(a) * m * dt, rtol=0, atol=1e-15)
     assert np.array_equal(out[1]["momentum"], bs[1]["momentum"]) and np.array_equal(out[1]["pose"], bs[1]["pose"])
-    # a free body in the field falls as p = 1/2 a t^2 under the implicit step too
+    # a free body in the field falls as p = 1/2 a t^2 under the implicit step too (tol 1e-10: the
+    # body sits at its island's centre of mass, so its angular residual is measured against the
+    # residual's floor, 1e-9, functions/src/lib.rs:170-247, which a tolerance of 1e-12 cannot meet)
     from exgame_b200.abi import NEWTON
     bs2 = np.array([body((1, 2, 3), (0, 0, 0), mass=m)])
     w2 = oracle.OracleWorld(bs2, np.zeros(0, dtype=JOINT_DTYPE),
-                            step_params(integrator=NEWTON, dt=dt, tol=1e-12, field=a))
+                            step_params(integrator=NEWTON, dt=dt, tol=1e-10, field=a))
     w2.step(10)
     mom = w2.bodies()[0]["momentum"]
     assert np.allclose(mom[:3], np.array(a) * m * dt * 10, rtol=1e-9, atol=1e-12)

@@ -287,8 +287,15 @@ def run_ours(args, rank, world_size, local_rank):
     dev = _lib.Device(local_rank)
     parts, cfg = workload(args.workload, rank)
     worlds = make_worlds(dev, parts)
-    # launch shapes only, timed on this workload's own steps: results do not change
-    tuning = autotune.autotune(dev, workload=worlds[0], steps=2) if args.autotune else None
+    # launch shapes only, timed on this workload's own steps: results do not change. Tuning
+    # advances the worlds, so their initial state is put back afterwards: the warm-up and timed
+    # steps are then steps 1..W+K from the initial state, the steps the reference arm times.
+    tuning = None
+    if args.autotune:
+        initial = worlds[0].state()
+        tuning = autotune.autotune(dev, workload=worlds[0], steps=2)
+        worlds[0].set_state(initial)
+        del initial
     n_bodies = sum(len(b) for (b, _, _) in parts)
     flush_buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 

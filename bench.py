@@ -351,11 +351,13 @@ def run_ours(args, rank, world_size, local_rank):
                 "d2h_bytes_per_step": int(nbytes), "steps": args.steps}
 
     def end_to_end_overlapped():
-        # the same state loop on three handles with streams of their own (EXG_OPT_OWN_STREAM): the
-        # explicit worlds, and the implicit ones in two halves; each handle is driven by its own
-        # host thread, so one handle's copies run while the others step
+        # the same state loop on --e2e-handles handles with streams of their own
+        # (EXG_OPT_OWN_STREAM): the explicit worlds, and the implicit ones in the remaining parts;
+        # each handle is driven by its own host thread, so one handle's copies run while the others
+        # step
         implicit = [p for p in parts if int(p[2]["integrator"]) == NEWTON]
-        groups = [[p for p in parts if int(p[2]["integrator"]) != NEWTON], implicit[0::2], implicit[1::2]]
+        k = max(1, args.e2e_handles - 1)  # the explicit worlds on one handle, the implicit ones in k parts
+        groups = [[p for p in parts if int(p[2]["integrator"]) != NEWTON]] + [implicit[i::k] for i in range(k)]
         if not all(groups):
             return None
         hs = [_lib.DeviceBatch(dev, g) for g in groups]
@@ -391,8 +393,8 @@ def run_ours(args, rank, world_size, local_rank):
         nbytes = sum(b.nbytes for b in bufs)
         return {"value": total_bodies * args.steps / t_e, "unit": METRIC, "h2d_bytes_per_step": int(nbytes),
                 "d2h_bytes_per_step": int(nbytes), "steps": args.steps,
-                "transfer": "dynamic state in and out every step; three handles on their own streams (the "
-                            "explicit worlds, the implicit ones in two halves), one host thread each"}
+                "transfer": f"dynamic state in and out every step; {len(hs)} handles on their own streams (the "
+                            f"explicit worlds, the implicit ones in {len(hs) - 1} parts), one host thread each"}
 
     one = end_to_end(_lib.host_state, lambda w, h: w.state(out=h), lambda w, h: w.set_state(h))
     one["transfer"] = "dynamic state (pose, momentum: 112 B per body) in and out every step, one handle"
@@ -664,6 +666,9 @@ def main():
     ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--e2e-handles", type=int, default=4,
+                    help="handles of the overlapped end-to-end loop (one for the explicit worlds, the rest split the "
+                         "implicit ones)")
     ap.add_argument("--ns-pivot", type=int, default=0,
                     help="1: the implicit worlds invert their pivot blocks by Newton-Schulz (EXG_NEWTON_NS_PIVOT)")
     ap.add_argument("--error-steps", type=int, default=1000,

@@ -10,7 +10,7 @@ the same seeded inputs, each quantity's error stated.
 Error measures (per world): pose, per body, max |d pose| / max(1, max |pose|) over the motor's
 eight components, then the worst body; momentum, max |d p| over the world's largest |p|; energy,
 |E(device state) - E(oracle state)| / |E(oracle state)| with one energy function (the oracle's)
-applied to both. The north star's bound is 1e-6 relative pose error after 1000 steps. Set
+applied to both. The accuracy bound of the mixed path is 1e-6 relative pose error after 1000 steps. Set
 EXG_ERROR_LOG to a file path to have each test append its measured errors there as JSON lines.
 """
 import json
@@ -77,8 +77,8 @@ def test_config2_full_size_mixed_each_quantity(device, orc):
     converges linearly there, so whether a chain's first span converges or is sub-divided depends
     on rounding; the oracle itself sub-divides one chain of the sixteen, and the device path (FP64 as
     well as mixed) sub-divides a different set. Two valid integrations of that step then differ by
-    the mid-point rule's own error: about 1e-5 of the largest momentum, 1e-9 in pose (the bound the
-    north star sets is 1e-6 relative pose error)."""
+    the mid-point rule's own error: about 1e-5 of the largest momentum, 1e-9 in pose (the mixed
+    path's accuracy bound is 1e-6 relative pose error)."""
     (gb, gj, gp), (cb, cj, cp), _ = scenarios.config2_parts(precision=PRECISION_MIXED, exact_jacobian=True)
     assert len(gb) == 65536 and len(cb) == 16 * 256
     steps = 3

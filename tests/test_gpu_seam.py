@@ -46,12 +46,16 @@ def grid_chain(offset, h=64.0):
     return b, j
 
 
-def relative_positions(device, offset, precision):
+def relative_positions(device, offset, precision, wave=False):
     b, j = grid_chain(offset)
     p = step_params(integrator=NEWTON, gravity_law=GRAVITY_OFF, precision=precision, dt=DT, tol=1e-10,
                     field=(0.0, 0.0, -9.81))
     w = _lib.DeviceWorld(device, b, j, p)
+    if wave:
+        w.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, 1)
     w.step(STEPS)
+    if wave:
+        assert w.get_option(_lib.DeviceWorld.OPT_LAST_WAVE_ROUNDS) > 0
     out = w.bodies()
     assert w.stats()["fatal"] == 0
     w.close()
@@ -59,13 +63,15 @@ def relative_positions(device, offset, precision):
     return pos - pos[0]
 
 
+@pytest.mark.parametrize("wave", [False, True])
 @pytest.mark.parametrize("offset", [2.0 ** 10, 2.0 ** 20, 2.0 ** 30])
-def test_far_offset_keeps_the_shape_fp64(device, offset):
-    ref = relative_positions(device, 0.0, 0)
-    far = relative_positions(device, offset, 0)
+def test_far_offset_keeps_the_shape_fp64(device, offset, wave):
+    ref = relative_positions(device, 0.0, 0, wave)
+    far = relative_positions(device, offset, 0, wave)
     div = np.abs(far - ref).max()
     ulp = np.spacing(offset)  # FP64 spacing at the offset: positions are rounded to it
-    print(f"FP64 offset {offset:.0e}: relative divergence {div:.3e} (FP64 ulp {ulp:.1e})")
+    print(f"FP64 offset {offset:.0e} ({'wave' if wave else 'island kernel'}): relative divergence {div:.3e} "
+          f"(FP64 ulp {ulp:.1e})")
     assert div <= 64.0 * ulp, (div, ulp)
 
 

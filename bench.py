@@ -661,7 +661,7 @@ def main():
                     help="split one batch over the ranks by body count (strong scaling) instead of one batch per rank")
     ap.add_argument("--serve-rates", default="100,1000,10000",
                     help="request rates (req/s) of the served sweep at N=1; empty to skip")
-    ap.add_argument("--serve-requests", type=int, default=1000)
+    ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-pool", type=int, default=256)
     ap.add_argument("--serve-tick", type=int, default=16)
     ap.add_argument("--plain", type=int, default=1, help="also time the plain one-world-per-launch FP64 path")

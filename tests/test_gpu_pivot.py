@@ -203,3 +203,27 @@ def test_ns_pivots_on_a_curtain_match_the_oracle(device, oracle):
     ow.step(30)
     pe, me = state_error(ow.bodies(), got)
     assert pe < 1e-8 and me < 1e-6, (pe, me)
+
+
+def test_worlds_with_and_without_ns_pivots_in_one_batch_step_as_alone(device):
+    """One world asking for Newton-Schulz pivots makes the batch launch the kernels that carry them;
+    the other worlds still take Gauss-Jordan inside them. Every world of such a batch (both
+    schedules) ends bit for bit as it does alone."""
+    from exgame_b200 import scenarios
+    from exgame_b200.abi import NEWTON, step_params
+    worlds = []
+    for k, (n, ns) in enumerate([(60, True), (60, False), (900, True), (900, False), (12, False)]):
+        b, j = scenarios.tree_world(n, seed=500 + k)
+        worlds.append((b, j, step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10,
+                                         exact_jacobian=True, ns_pivot=ns)))
+    batch = _lib.DeviceBatch(device, worlds)
+    batch.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, 32)
+    batch.step(4)
+    for k, (b, j, p) in enumerate(worlds):
+        alone = _lib.DeviceWorld(device, b, j, p)
+        alone.set_option(_lib.DeviceWorld.OPT_WAVE_MIN_BODIES, 32)
+        alone.step(4)
+        got, want = batch.world_bodies(k), alone.bodies()
+        assert np.array_equal(got["pose"], want["pose"]) and np.array_equal(got["momentum"], want["momentum"]), k
+        alone.close()
+    batch.close()

@@ -34,7 +34,7 @@ def test_every_entry_point_is_bound():
         consts, structs, handles, funcs = g.parse(f.read())
     with open(g.HEADER) as f:
         declared = re.findall(r"EXG_API\s+[\w\s\*]*?\b(exg_\w+)\s*\(", g.strip_comments(f.read()))
-    assert len(declared) == len(funcs) == 70
+    assert len(declared) == len(funcs) > 0 and sorted(declared) == sorted(f[0] for f in funcs)
     with open(LIB_RS) as f:
         rs = f.read()
     for name, _, params in funcs:

@@ -293,7 +293,7 @@ def run_ours(args, rank, world_size, local_rank):
     tuning = None
     if args.autotune:
         initial = worlds[0].state()
-        tuning = autotune.autotune(dev, workload=worlds[0], steps=2)
+        tuning = autotune.autotune(dev, workload=worlds[0], steps=2, cache=args.tuning_cache)
         worlds[0].set_state(initial)
         del initial
     n_bodies = sum(len(b) for (b, _, _) in parts)
@@ -655,6 +655,8 @@ def main():
     ap.add_argument("--workload", default="c3", choices=["c0", "c1", "c2", "c3", "c3-f64"])
     ap.add_argument("--worlds", type=int, default=4096, help="worlds of the config-3 batch")
     ap.add_argument("--autotune", type=int, default=1, help="tune launch shapes on this GPU first")
+    ap.add_argument("--tuning-cache", default=None,
+                    help="JSON file of tuned launch shapes per GPU and batch-shape bucket: reused on a hit, written on a miss")
     ap.add_argument("--wave-host-rounds", type=int, default=0,
                     help="drive the wave's rounds from the host (for profilers that skip conditional graph nodes)")
     ap.add_argument("--shard", action="store_true",

@@ -89,3 +89,32 @@ def test_autotune_on_a_workload_keeps_its_results(device):
     finally:
         for k, v in zip((1, 2, 3, 4), defaults):
             device.set_tuning(k, v)
+
+
+def test_tuning_cache_hit_sets_the_tuned_values(device, tmp_path):
+    """A second process-like call on a batch of the same shape reads the cache instead of timing:
+    same choices, set on the device and the handle, and the handle's state untouched."""
+    defaults = [device.get_tuning(k) for k in (1, 2, 3, 4)]
+    p = step_params(integrator=NEWTON, precision=PRECISION_MIXED, dt=1e-2, tol=1e-10, exact_jacobian=True)
+    worlds = [(*scenarios.tree_world(n, seed=90 + k), p) for k, n in enumerate((40, 300))]
+    path = str(tmp_path / "tuning.json")
+    try:
+        first = _lib.DeviceBatch(device, worlds)
+        r1 = autotune.autotune(device, workload=first, steps=1, cache=path)
+        first.close()
+        assert r1["timed_on"] == "workload"
+        for k, v in zip((1, 2, 3, 4), defaults):
+            device.set_tuning(k, v)
+        second = _lib.DeviceBatch(device, worlds)
+        before = second.bodies()
+        launches = device.kernel_launches()
+        r2 = autotune.autotune(device, workload=second, steps=1, cache=path)
+        assert r2["timed_on"] == "cache" and device.kernel_launches() == launches
+        for name, key, _ in autotune.KNOBS:
+            assert r2[name] == r1[name] and device.get_tuning(key) == r1[name]
+        after = second.bodies()
+        assert np.array_equal(before["pose"], after["pose"])
+        second.close()
+    finally:
+        for k, v in zip((1, 2, 3, 4), defaults):
+            device.set_tuning(k, v)

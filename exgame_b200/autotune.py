@@ -231,8 +231,10 @@ class TuningCache:
     """The JSON file of tuned choices: {"version": 1, "entries": {"<gpu>|<bucket>": {knob: value, ...}}}.
 
     Reads tolerate a missing, unreadable or other-version file (empty cache) and drop entries whose
-    values are not candidates of this tuner. Writes go through a temporary file and an atomic
-    rename, so concurrent processes never see half a file (the last writer's entries win)."""
+    values are not candidates of this tuner. A write holds an exclusive lock on a sidecar file
+    (`<path>.lock`, flock) across its read, merge and write, and replaces the file through a
+    temporary file and an atomic rename: concurrent processes (one per rank) keep each other's
+    entries, and a reader never sees half a file."""
 
     def __init__(self, path):
         self.path = str(path)
@@ -268,22 +270,28 @@ class TuningCache:
         import json
         import os
         import tempfile
+        import fcntl
         entry = {name: int(result[name]) for name, _, _ in KNOBS}
         if "ms" in result:
             entry["ms"] = result["ms"]
-        entries = self._load()
-        entries[f"{gpu}|{bucket}"] = entry
         folder = os.path.dirname(os.path.abspath(self.path))
         os.makedirs(folder, exist_ok=True)
-        fd, tmp = tempfile.mkstemp(prefix=".tuning.", dir=folder)
-        try:
-            with os.fdopen(fd, "w") as f:
-                json.dump({"version": CACHE_VERSION, "entries": entries}, f, indent=1, sort_keys=True)
-            os.replace(tmp, self.path)
-        except BaseException:
-            if os.path.exists(tmp):
-                os.unlink(tmp)
-            raise
+        with open(self.path + ".lock", "a") as lock:
+            fcntl.flock(lock, fcntl.LOCK_EX)
+            try:
+                entries = self._load()
+                entries[f"{gpu}|{bucket}"] = entry
+                fd, tmp = tempfile.mkstemp(prefix=".tuning.", dir=folder)
+                try:
+                    with os.fdopen(fd, "w") as f:
+                        json.dump({"version": CACHE_VERSION, "entries": entries}, f, indent=1, sort_keys=True)
+                    os.replace(tmp, self.path)
+                except BaseException:
+                    if os.path.exists(tmp):
+                        os.unlink(tmp)
+                    raise
+            finally:
+                fcntl.flock(lock, fcntl.LOCK_UN)
 
     def entries(self):
         return dict(self._load())

@@ -131,7 +131,7 @@ def test_missing_folder_is_created_and_no_temporary_left(tmp_path, timed):
     path = tmp_path / "a" / "b" / "tuning.json"
     autotune.autotune(FakeDevice(), workload=batch(), cache=str(path), device_key="gpuA")
     assert path.exists()
-    assert [p.name for p in path.parent.iterdir()] == ["tuning.json"]
+    assert sorted(p.name for p in path.parent.iterdir()) == ["tuning.json", "tuning.json.lock"]
 
 
 def test_bucket_edges():
@@ -168,3 +168,25 @@ def test_library_build_id_tracks_file_content(tmp_path):
     assert a == autotune.library_build_id(str(p)) and len(a) == 12
     p.write_bytes(b"b" * 101)
     assert autotune.library_build_id(str(p)) != a
+
+
+def _put_many(path, worker, n):
+    cache = autotune.TuningCache(path)
+    for k in range(n):
+        cache.put(f"gpu{worker}", f"bucket{k}", BEST)
+
+
+def test_concurrent_writers_keep_every_entry(tmp_path):
+    """Processes writing different buckets at once (ranks sharing one file) lose none of them."""
+    import multiprocessing as mp
+    path = str(tmp_path / "tuning.json")
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_put_many, args=(path, w, 15)) for w in range(4)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    entries = autotune.TuningCache(path).entries()
+    assert len(entries) == 60
+    assert all(autotune.TuningCache(path).get(f"gpu{w}", f"bucket{k}") == BEST for w in range(4) for k in range(15))

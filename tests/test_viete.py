@@ -1,5 +1,5 @@
 """viete, the tracer and CUDA C emitter of joint force laws (crates/viete/src/api.rs, ir.rs,
-glsl.rs; the CUDA C emitter is this build's addition). The traced laws of
+glsl.rs; the reference emits GLSL, this package emits CUDA C). The traced laws of
 exgame_b200/user_laws.py are compiled for the host from the generated header together with the
 device algebra and checked: the traced restatement of SimpleSpringDamper against the oracle's law
 (plain values and the 24-axis Jacobian), the new PointBushing against its own float evaluation and

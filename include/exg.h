@@ -168,7 +168,8 @@ EXG_API const char* exg_status_string(int status);
 EXG_API int exg_device_stream(exg_device_t dev, void** out);
 /* In-library profiler: when enabled, each kernel launch is bracketed by CUDA events on the device
  * stream (worlds then launch directly instead of through a CUDA graph). Kinds: 0 gravity,
- * 1 joints, 2 explicit integrate, 3 Newton step, 4 body pre. Enabling or disabling resets the
+ * 1 joints, 2 explicit integrate, 3 Newton step (island kernel), 4 body pre, 5 Newton step (wave
+ * schedule). Enabling or disabling resets the
  * totals; read returns the summed device time and the launch count of one kind. */
 EXG_API int exg_device_profile(exg_device_t dev, int32_t enable);
 EXG_API int exg_device_profile_read(exg_device_t dev, int32_t kind, double* total_ms, int64_t* launches);
@@ -177,7 +178,7 @@ EXG_API int exg_abi_version(void);
 /* Launch-shape tuning of a device (exgame_b200.autotune measures and sets these). No result
  * depends on them: they change how work is spread over the SMs, not the arithmetic.
  *   GRAVITY_CTAS_PER_SM  persistent CTAs per SM of the mixed gravity kernel (1..64, default 32)
- *   WAVE_BLOCKS_PER_SM   grid cap per SM of the wave schedule's data kernels (1..32, default 8)
+ *   WAVE_BLOCKS_PER_SM   grid cap per SM of the wave schedule's data kernels (1..32, default 16)
  *   WAVE_MIN_BODIES      wave threshold given to world handles created afterwards (default 32;
  *                        the island kernel and the wave give identical results) */
 #define EXG_TUNE_GRAVITY_CTAS_PER_SM 1

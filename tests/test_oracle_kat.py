@@ -255,6 +255,41 @@ def test_lie_euler_conserves_world_momentum(oracle):
     assert world_momentum_drift(oracle, LIE_EULER, 0.01, 2000) < 1e-9
 
 
+def test_lie_world_momentum_independent_of_dt(oracle):
+    # lie_euler.rs:104-114: coarse (dt 0.01, 200 steps) and fine (dt 0.0005, 4000 steps) both stay
+    # at round-off (f32 bounds 1e-4 and 1e-2 there; f64 here)
+    coarse = world_momentum_drift(oracle, LIE_EULER, 0.01, 200)
+    fine = world_momentum_drift(oracle, LIE_EULER, 0.0005, 4000)
+    assert coarse < 1e-4 and fine < 1e-2
+    assert coarse < 1e-11 and fine < 1e-10, (coarse, fine)
+
+
+def test_lie_off_axis_spinning_body_keeps_com_in_place(oracle):
+    # lie_euler.rs:116-160: a body at x = 10 spinning about its own z axis (isotropic 0.4, omega_z 1)
+    # keeps its centre of mass over 100 steps of 0.01: the body-frame increment composes on the
+    # right of the pose (f32 bound 1e-4 there)
+    from exgame_b200 import _lib
+    b = body(moments=(0.4, 0.4, 0.4))
+    b["pose"] = _lib.motor_exp(np.array([10.0, 0, 0, 0, 0, 0]), 1.0)
+    b["momentum"][3:] = [0.0, 0.0, 0.4]
+    w = oracle.OracleWorld(np.array([b]), np.zeros(0, dtype=JOINT_DTYPE), step_params(integrator=LIE_EULER, dt=0.01))
+    p0 = position(w.bodies()[0])
+    w.step(100)
+    p1 = position(w.bodies()[0])
+    assert np.allclose(p0, [10.0, 0.0, 0.0], rtol=0, atol=1e-15)
+    assert np.abs(p1 - p0).max() < 1e-12, (p0, p1)
+
+
+def test_lie_free_linear_motion_is_uniform(oracle):
+    # lie_euler.rs:162-180: mass 2, v = (3, 0, 0), 100 steps of 0.01: v stays 3 and x = v t = 3
+    b = body(mass=2.0, vel=(3.0, 0.0, 0.0))
+    w = oracle.OracleWorld(np.array([b]), np.zeros(0, dtype=JOINT_DTYPE), step_params(integrator=LIE_EULER, dt=0.01))
+    w.step(100)
+    bb = w.bodies()[0]
+    assert np.allclose(bb["momentum"][:3] / 2.0, [3.0, 0.0, 0.0], rtol=0, atol=1e-13)
+    assert np.allclose(position(bb), [3.0, 0.0, 0.0], rtol=0, atol=1e-12)
+
+
 def test_euler_schemes_drift_more_than_lie(oracle):
     lie = world_momentum_drift(oracle, LIE_EULER, 0.01, 200)
     sym = world_momentum_drift(oracle, SYMPLECTIC_EULER, 0.01, 200)

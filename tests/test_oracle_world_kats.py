@@ -1,0 +1,338 @@
+"""Pins the oracle's joint laws and explicit integrators to the reference's pair-of-bodies tests
+(crates/newton/src/body.rs `tests_with_joints`, crates/newton/src/integrator/explicit/
+symplectic_euler.rs and explicit_euler.rs, crates/newton/src/gravity.rs): every case restates one
+of those tests, cited by line, on the oracle's world step (the joint wrench from the step's start
+state, then each body integrated) or on its single law evaluation. The reference runs in f32 and
+asserts f32 bounds; each case asserts that bound and, where the quantity is exact up to rounding,
+a tight f64 bound too. These run on the CPU."""
+import math
+
+import numpy as np
+
+from exgame_b200.abi import (BODY_DTYPE, EXPLICIT_EULER, GRAVITY_OFF, GRAVITY_SIZE_CORE, JOINT_DTYPE, SYMPLECTIC_EULER,
+                             step_params)
+
+AXIAL, CRIT, PERP, TORS = 0, 1, 2, 3
+
+
+def rec(oracle, pos=(0.0, 0.0, 0.0), rot=(0.0, 0.0, 0.0), vel=(0.0, 0.0, 0.0), omega=(0.0, 0.0, 0.0), mass=1.0,
+        moments=(1.0, 1.0, 1.0)):
+    """A body record: pose Twist(pos, rot).exp(1), body-frame velocity (vel, omega), diagonal inertia."""
+    b = np.zeros((), dtype=BODY_DTYPE)
+    b["pose"] = oracle.twist_exp(np.r_[pos, rot], 1.0)
+    b["momentum"][:3] = mass * np.asarray(vel, float)
+    b["momentum"][3:] = np.asarray(moments, float) * np.asarray(omega, float)
+    b["mass"] = mass
+    b["inertia"][[0, 4, 8]] = moments
+    b["diagonal"] = 1
+    b["size"] = (mass / 4.0) ** (1.0 / 3.0)
+    return b
+
+
+def axial(a, b, rest, k, c=0.0, anchor_a=(0.0, 0.0, 0.0), anchor_b=(0.0, 0.0, 0.0), law=AXIAL):
+    j = np.zeros((), dtype=JOINT_DTYPE)
+    j["law"], j["a"], j["b"] = law, a, b
+    j["params"][:10] = [*anchor_a, *anchor_b, rest, k, c, 1e-6]  # softening: the builder's default 1e-6
+    return j
+
+
+def transport(oracle, s, pose, covariant):
+    out = np.zeros(6)
+    oracle.lib().orc_twist_transport(oracle.p(oracle.arr(s)), oracle.p(oracle.arr(pose)), int(covariant),
+                                     oracle.p(out))
+    return out
+
+
+def spatial_twist(oracle, b):
+    """World twist of a body: Ad_pose of its body-frame twist (momentum through the inverse inertia)."""
+    t = np.r_[b["momentum"][:3] / b["mass"], b["momentum"][3:] / b["inertia"][[0, 4, 8]]]
+    return transport(oracle, t, b["pose"], 0)
+
+
+def power(oracle, w, t):
+    return oracle.lib().orc_power(oracle.p(oracle.arr(w)), oracle.p(oracle.arr(t)))
+
+
+def point(oracle, pose, local=(0.0, 0.0, 0.0)):
+    from exgame_b200 import _lib
+    return _lib.motor_apply_point(pose, np.asarray(local, float))
+
+
+def separation(oracle, bodies):
+    return float(np.linalg.norm(point(oracle, bodies[0]["pose"]) - point(oracle, bodies[1]["pose"])))
+
+
+def pair_world(oracle, a, b, joints, integrator=SYMPLECTIC_EULER, dt=0.01, **kw):
+    js = np.array(joints, dtype=JOINT_DTYPE) if len(joints) else np.zeros(0, dtype=JOINT_DTYPE)
+    return oracle.OracleWorld(np.array([a, b]), js, step_params(integrator=integrator, dt=dt, **kw))
+
+
+# ── body.rs tests_with_joints: worlds of two unit bodies stepped by SymplecticEuler ──
+
+def test_stretched_critically_damped_spring_pulls_inward(oracle):
+    # body.rs:375-405: rest 2, k 10, bodies 4 apart, 50 steps of 0.01 -> closer
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 2.0, 10.0, law=CRIT)])
+    d0 = separation(oracle, w.bodies())
+    w.step(50)
+    assert separation(oracle, w.bodies()) < d0
+
+
+def test_critically_damped_spring_settles_to_rest_length(oracle):
+    # body.rs:407-433: 4000 steps of 0.01 -> |d - 2| < 0.05
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 2.0, 10.0, law=CRIT)])
+    w.step(4000)
+    assert abs(separation(oracle, w.bodies()) - 2.0) < 0.05
+
+
+def _offset_spinning_pair(oracle):
+    # A at (0, 2, 0) spinning about +z, B at rest at the origin; anchor of A at local (1, 0, 0)
+    a = rec(oracle, pos=(0, 2, 0), omega=(0, 0, 1))
+    b = rec(oracle)
+    prm = axial(0, 1, math.sqrt(5.0), 10.0, 3.0, anchor_a=(1, 0, 0))["params"]
+    va, vb = spatial_twist(oracle, a), spatial_twist(oracle, b)
+    pa, pb = point(oracle, a["pose"], (1, 0, 0)), point(oracle, b["pose"])
+    vel = np.zeros(3)
+    oracle.lib().orc_velocity_at(oracle.p(oracle.arr(va)), oracle.p(oracle.arr(pa)), oracle.p(vel))
+    d_dot = float((pa - pb) @ vel / np.linalg.norm(pa - pb))
+    return a, b, prm, va, vb, d_dot
+
+
+def test_damped_offset_spring_dissipates_true_closing_rate(oracle):
+    # body.rs:447-503: at rest length the pair receives exactly -c d_dot^2, d_dot from world twists
+    a, b, prm, va, vb, d_dot = _offset_spinning_pair(oracle)
+    assert abs(d_dot) > 1e-6 and abs(d_dot - 2.0 / math.sqrt(5.0)) < 1e-15
+    w = oracle.plain_eval(AXIAL, prm, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    pw = power(oracle, w[:6], va) + power(oracle, w[6:], vb)
+    expected = -3.0 * d_dot * d_dot
+    assert abs(pw - expected) < 1e-5
+    assert abs(pw - expected) < 1e-10, (pw, expected)
+
+
+def test_damped_offset_spring_dissipates_true_closing_rate_for_jacobian(oracle):
+    # body.rs:505-571: the same through the dual-number (Jacobian) evaluation's value part
+    a, b, prm, va, vb, d_dot = _offset_spinning_pair(oracle)
+    J = oracle.jacobian_eval(AXIAL, prm, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    plain = oracle.plain_eval(AXIAL, prm, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    assert np.array_equal(J[:, 0], plain)
+    pw = power(oracle, J[:6, 0], va) + power(oracle, J[6:, 0], vb)
+    assert abs(pw + 3.0 * d_dot * d_dot) < 1e-10
+
+
+def test_at_rest_length_no_force(oracle):
+    # body.rs:579-615: anchors 2 apart at rest length 2 (k 10, c 1, dt 0.1, warp 0.1): only the
+    # softening residual k eps^2 / (2 L0) remains (f32 bound 1e-5)
+    a, b = rec(oracle), rec(oracle, pos=(2, 0, 0))
+    z = np.zeros(6)
+    w = oracle.plain_eval(AXIAL, axial(0, 1, 2.0, 10.0, 1.0)["params"], a["pose"], b["pose"], z, z, 0.1, 0.1)
+    forces = np.r_[w[0:3], w[6:9]]
+    assert np.abs(forces).max() < 1e-5
+    assert np.abs(forces).max() < 1e-10, forces
+
+
+def test_conserves_total_linear_momentum(oracle):
+    # body.rs:617-651: rest 2, k 8, c 0.5, dt 0.005; the pair's world linear momentum stays 0 at
+    # every one of 2000 steps (f32 bound |p|^2 < 1e-12)
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 2.0, 8.0, 0.5)], dt=0.005)
+    worst = 0.0
+    for _ in range(2000):
+        w.step(1)
+        bs = w.bodies()
+        total = sum(transport(oracle, x["momentum"], x["pose"], 1)[:3] for x in bs)
+        worst = max(worst, float(total @ total))
+    assert worst < 1e-12
+    assert worst < 1e-28, worst
+
+
+def test_damped_spring_settles_to_rest_length(oracle):
+    # body.rs:653-688: rest 2, k 10, c 4, 4000 steps of 0.005 -> |d - 2| < 0.05
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 2.0, 10.0, 4.0)], dt=0.005)
+    w.step(4000)
+    assert abs(separation(oracle, w.bodies()) - 2.0) < 0.05
+
+
+def test_stretched_spring_pulls_inward(oracle):
+    # body.rs:690-726: undamped, 100 steps of 0.005 -> the distance shrinks
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 2.0, 10.0)], dt=0.005)
+    d0 = separation(oracle, w.bodies())
+    w.step(100)
+    assert separation(oracle, w.bodies()) < d0
+
+
+def test_offset_anchor_induces_rotation(oracle):
+    # body.rs:728-770: anchor of A at local (0, 1, 0), stretched along x -> A spins about z
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(4, 0, 0)), [axial(0, 1, 1.0, 10.0, anchor_a=(0, 1, 0))],
+                   dt=0.005)
+    w.step(50)
+    omega = w.bodies()[0]["momentum"][3:]  # unit isotropic inertia: body angular velocity
+    assert omega @ omega > 1e-6
+    assert abs(omega[2]) > 10 * max(abs(omega[0]), abs(omega[1]), 1e-300)
+
+
+def _energy_run(oracle, integrator, k, c, dt, steps, each=True):
+    w = pair_world(oracle, rec(oracle), rec(oracle, pos=(3.5, 0, 0)), [axial(0, 1, 2.0, k, c)], integrator=integrator,
+                   dt=dt)
+    e = [w.energy()]
+    for _ in range(steps):
+        w.step(1)
+        e.append(w.energy())
+    return np.array(e)
+
+
+def test_undamped_spring_conserves_total_energy(oracle):
+    # body.rs:777-822: k 6, 8000 steps of 0.005: energy within a 5 % band and no drift
+    e = _energy_run(oracle, SYMPLECTIC_EULER, 6.0, 0.0, 0.005, 8000)
+    assert (e.max() - e.min()) / e[0] < 0.05
+    assert abs(e[-1] - e[0]) / e[0] < 0.05
+
+
+def test_damped_spring_dissipates_monotonically(oracle):
+    # body.rs:824-872: k 6, c 2, 5000 steps of 0.002: never up by more than 1e-6, ends below half
+    e = _energy_run(oracle, SYMPLECTIC_EULER, 6.0, 2.0, 0.002, 5000)
+    assert np.all(np.diff(e) <= 1e-6)
+    assert e[-1] < 0.5 * e[0] and e[-1] >= 0.0
+
+
+def test_explicit_euler_drifts_energy_on_spring(oracle):
+    # body.rs:874-913: the same spring under ExplicitEuler gains more than 5 % at some point
+    e = _energy_run(oracle, EXPLICIT_EULER, 6.0, 0.0, 0.005, 8000)
+    assert (e.max() - e[0]) / e[0] > 0.05
+
+
+# ── perpendicular and torsional dampers (body.rs:922-1080): single evaluations ──
+
+def test_brakes_transverse_velocity_in_world_frame(oracle):
+    # body.rs:922-962: A rotated 90 deg about z with body velocity +x (world +y), B at (10, 0, 0):
+    # the brake force on A is -3 (0, 1, 0), on B +3 (0, 1, 0)
+    a = rec(oracle, rot=(0, 0, math.pi / 2), vel=(1, 0, 0))
+    b = rec(oracle, pos=(10, 0, 0))
+    va, vb = spatial_twist(oracle, a), spatial_twist(oracle, b)
+    w = oracle.plain_eval(PERP, [3.0, 1e-6] + [0] * 8, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    assert np.allclose(w[0:3], [0, -3, 0], rtol=0, atol=1e-5) and np.allclose(w[6:9], [0, 3, 0], rtol=0, atol=1e-5)
+    assert np.allclose(w[0:3], [0, -3, 0], rtol=0, atol=1e-12) and np.allclose(w[6:9], [0, 3, 0], rtol=0, atol=1e-12)
+
+
+def test_ignores_radial_velocity(oracle):
+    # body.rs:964-990: A moving +x along the line to B: no transverse force
+    a = rec(oracle, vel=(1, 0, 0))
+    b = rec(oracle, pos=(10, 0, 0))
+    va, vb = spatial_twist(oracle, a), spatial_twist(oracle, b)
+    w = oracle.plain_eval(PERP, [3.0, 1e-6] + [0] * 8, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    assert np.abs(w[0:3]).max() < 1e-5
+    # the softened unit (eps 1e-6) leaks c v eps^2 / d^2 = 3e-14 along the line
+    assert np.abs(w[0:3]).max() < 1e-12, w[0:3]
+
+
+def test_perpendicular_damper_dissipative_under_rotation_offset_from_origin(oracle):
+    # body.rs:992-1034: both bodies offset, rotated and moving: the pair's power is <= 0
+    a = rec(oracle, pos=(0, 3, 0), rot=(0, 0, math.pi / 2), vel=(0.4, 0.1, 0), omega=(0, 0, 1))
+    b = rec(oracle, pos=(5, 0, 0), vel=(0, -0.2, 0), omega=(0, 1, 0))
+    va, vb = spatial_twist(oracle, a), spatial_twist(oracle, b)
+    w = oracle.plain_eval(PERP, [4.0, 1e-6] + [0] * 8, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    pw = power(oracle, w[:6], va) + power(oracle, w[6:], vb)
+    assert pw <= 1e-5
+    assert pw < 0.0, pw  # the relative velocity has a transverse part here
+
+
+def test_pure_couple_dissipates_relative_angular_velocity(oracle):
+    # body.rs:1036-1080: A rotated 90 deg about z spinning about body x (world +y), B at rest:
+    # zero force, third law on the couple, power exactly -b |omega_rel|^2
+    a = rec(oracle, rot=(0, 0, math.pi / 2), omega=(1, 0, 0))
+    b = rec(oracle)
+    va, vb = spatial_twist(oracle, a), spatial_twist(oracle, b)
+    assert np.allclose(va[3:], [0, 1, 0], rtol=0, atol=1e-15)
+    w = oracle.plain_eval(TORS, [3.0] + [0] * 9, a["pose"], b["pose"], va, vb, 0.01, 1.0)
+    assert np.abs(w[0:3]).max() < 1e-12 and np.abs(w[6:9]).max() < 1e-12
+    assert np.allclose(w[9:12], -w[3:6], rtol=0, atol=1e-12)
+    w_rel = va[3:] - vb[3:]
+    expected = -3.0 * float(w_rel @ w_rel)
+    pw = power(oracle, w[:6], va) + power(oracle, w[6:], vb)
+    assert abs(expected) > 1e-6 and abs(pw - expected) < 1e-5
+    assert abs(pw - expected) < 1e-12, (pw, expected)
+
+
+# ── explicit schemes on a single body (symplectic_euler.rs, explicit_euler.rs) ──
+
+def one_body(oracle, b, integrator, dt, **kw):
+    return oracle.OracleWorld(np.array([b]), np.zeros(0, dtype=JOINT_DTYPE),
+                              step_params(integrator=integrator, dt=dt, **kw))
+
+
+def test_symplectic_free_linear_motion_is_uniform(oracle):
+    # symplectic_euler.rs:54-76: mass 2, v = (3, 0, 0), 100 steps of 0.01: v unchanged, x = 3
+    w = one_body(oracle, rec(oracle, vel=(3, 0, 0), mass=2.0), SYMPLECTIC_EULER, 0.01)
+    w.step(100)
+    bb = w.bodies()[0]
+    assert np.allclose(bb["momentum"] / np.r_[2.0, 2.0, 2.0, 1.0, 1.0, 1.0], [3, 0, 0, 0, 0, 0], rtol=0, atol=1e-9)
+    assert abs(point(oracle, bb["pose"])[0] - 3.0) < 1e-12
+
+
+def test_symplectic_constant_force_accelerates(oracle):
+    # symplectic_euler.rs:78-95: a constant push of 5 along y (here a uniform field on a unit
+    # mass) for 50 steps of 0.01: p_y = 2.5
+    w = one_body(oracle, rec(oracle), SYMPLECTIC_EULER, 0.01, field=(0.0, 5.0, 0.0))
+    w.step(50)
+    bb = w.bodies()[0]
+    assert abs(bb["momentum"][1] - 2.5) < 1e-5 and abs(bb["momentum"][1] - 2.5) < 1e-12
+    assert point(oracle, bb["pose"])[1] > 0.0
+
+
+def test_symplectic_free_precession_energy_bounded_short_run(oracle):
+    # symplectic_euler.rs:97-115: inertia (2, 3, 4), v (0.5, -0.3, 0.2), omega (1, 1.5, 0.7),
+    # 2000 steps of 0.001: kinetic energy within 1 %
+    w = one_body(oracle, rec(oracle, vel=(0.5, -0.3, 0.2), omega=(1.0, 1.5, 0.7), moments=(2.0, 3.0, 4.0)),
+                 SYMPLECTIC_EULER, 0.001)
+    e0 = w.energy()
+    w.step(2000)
+    assert abs(w.energy() - e0) / e0 < 1e-2
+
+
+def _precession_drift(oracle, integrator, dt, steps):
+    w = one_body(oracle, rec(oracle, omega=(1.0, 1.5, 0.7), moments=(2.0, 3.0, 4.0)), integrator, dt)
+    b0 = w.bodies()[0]
+    l0 = transport(oracle, b0["momentum"], b0["pose"], 1)[3:]
+    w.step(steps)
+    b1 = w.bodies()[0]
+    return float(np.linalg.norm(transport(oracle, b1["momentum"], b1["pose"], 1)[3:] - l0))
+
+
+def test_symplectic_free_precession_world_momentum_converges(oracle):
+    # symplectic_euler.rs:139-152: drift at dt 0.002 over that at 0.001 (t = 2) is about 2
+    coarse = _precession_drift(oracle, SYMPLECTIC_EULER, 0.002, 1000)
+    fine = _precession_drift(oracle, SYMPLECTIC_EULER, 0.001, 2000)
+    assert fine < 1e-2 and 1.6 <= coarse / fine <= 2.4, (coarse, fine)
+
+
+def test_explicit_euler_is_first_order_too(oracle):
+    # explicit_euler.rs:64-78
+    coarse = _precession_drift(oracle, EXPLICIT_EULER, 0.002, 1000)
+    fine = _precession_drift(oracle, EXPLICIT_EULER, 0.001, 2000)
+    assert fine < 1e-2 and 1.6 <= coarse / fine <= 2.4, (coarse, fine)
+
+
+# ── gravity (gravity.rs) ──
+
+def test_two_body_infall_momentum_conserved(oracle):
+    # gravity.rs:905-945: unit masses at -1 and +1, G 1, SymplecticEuler dt 0.001, 500 steps:
+    # the pair's linear momentum stays 0 at every step and the bodies fall together. The
+    # reference's forces lag its charges by one publication; here each step takes the charges
+    # of its own start state, which changes neither property.
+    a, b = rec(oracle, pos=(-1, 0, 0)), rec(oracle, pos=(1, 0, 0))
+    w = oracle.OracleWorld(np.array([a, b]), np.zeros(0, dtype=JOINT_DTYPE),
+                           step_params(integrator=SYMPLECTIC_EULER, gravity_law=GRAVITY_SIZE_CORE, G=1.0, dt=0.001))
+    worst = 0.0
+    for _ in range(500):
+        w.step(1)
+        bs = w.bodies()
+        total = sum(transport(oracle, x["momentum"], x["pose"], 1)[:3] for x in bs)
+        worst = max(worst, float(total @ total))
+    assert worst < 1e-12 and worst < 1e-28, worst
+    assert separation(oracle, w.bodies()) < 2.0
+
+
+def test_gravity_off_pair_stays_at_rest(oracle):
+    # the field switch of the same world: without gravity nothing moves (GRAVITY_OFF)
+    a, b = rec(oracle, pos=(-1, 0, 0)), rec(oracle, pos=(1, 0, 0))
+    w = oracle.OracleWorld(np.array([a, b]), np.zeros(0, dtype=JOINT_DTYPE),
+                           step_params(integrator=SYMPLECTIC_EULER, gravity_law=GRAVITY_OFF, dt=0.001))
+    w.step(10)
+    assert separation(oracle, w.bodies()) == 2.0

@@ -98,6 +98,13 @@ void orc_world_set_state(void* h, const exg_body_t* bodies) {
   }
 }
 double orc_world_energy(void* h) { return static_cast<OWorld*>(h)->energy(); }
+// The epoch of the following steps (Epoch::standalone(dt, warp), crates/aristotle/src/epoch.rs:17-60):
+// a host with a variable frame time passes a new dt to every Mechanism::step; the islands stay.
+void orc_world_set_epoch(void* h, double dt, double warp) {
+  OWorld* w = static_cast<OWorld*>(h);
+  w->wp.dt = dt;
+  w->wp.warp = warp;
+}
 // spans / Newton iterations of island k's last step
 int orc_world_island_count(void* h) { return (int)static_cast<OWorld*>(h)->islands.size(); }
 void orc_world_island_stats(void* h, int k, int* spans, int* iters) {

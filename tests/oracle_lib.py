@@ -33,6 +33,7 @@ def lib():
         L.orc_worlds_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
         L.orc_world_get_bodies.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_world_set_state.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_world_set_epoch.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         L.orc_world_energy.restype = ctypes.c_double
         L.orc_world_energy.argtypes = [ctypes.c_void_p]
         L.orc_world_island_count.argtypes = [ctypes.c_void_p]
@@ -93,6 +94,10 @@ class OracleWorld:
 
     def energy(self):
         return lib().orc_world_energy(self.h)
+
+    def set_epoch(self, dt, warp=1.0):
+        """dt and warp of the following steps (a variable frame time); the islands stay."""
+        lib().orc_world_set_epoch(self.h, float(dt), float(warp))
 
     def island_stats(self):
         out = []

@@ -8,9 +8,10 @@ a tight f64 bound too. These run on the CPU."""
 import math
 
 import numpy as np
+import pytest
 
-from exgame_b200.abi import (BODY_DTYPE, EXPLICIT_EULER, GRAVITY_OFF, GRAVITY_SIZE_CORE, JOINT_DTYPE, SYMPLECTIC_EULER,
-                             step_params)
+from exgame_b200.abi import (BODY_DTYPE, EXPLICIT_EULER, GRAVITY_OFF, GRAVITY_SIZE_CORE, JOINT_DTYPE, NEWTON,
+                             SYMPLECTIC_EULER, step_params)
 
 AXIAL, CRIT, PERP, TORS = 0, 1, 2, 3
 
@@ -336,3 +337,86 @@ def test_gravity_off_pair_stays_at_rest(oracle):
                            step_params(integrator=SYMPLECTIC_EULER, gravity_law=GRAVITY_OFF, dt=0.001))
     w.step(10)
     assert separation(oracle, w.bodies()) == 2.0
+
+
+# ── implicit Newton regressions (crates/newton/src/integrator/implicit/newton.rs tests) ──
+# Bodies as body_at_with_speed_and_mass builds them (body.rs:112-130): isotropic unit moment, pose
+# a translation; joints as the tests' `spring(world, rest, k, c)` (newton.rs:882-888). Each runs
+# on both of the oracle's linear solvers: the exact elimination and the reference's Newton-Schulz.
+
+SOLVERS = (0, 1)  # OracleWorld.SOLVER_EXACT, SOLVER_REFERENCE_NS
+
+
+def newton_world(oracle, bodies, springs, dt, solver, ns_warm=2):
+    js = np.array([axial(a, b, rest, k, c) for a, b, rest, k, c in springs], dtype=JOINT_DTYPE)
+    return oracle.OracleWorld(np.array(bodies), js, step_params(integrator=NEWTON, dt=dt), solver=solver,
+                              ns_warm=ns_warm)
+
+
+def positions(oracle, w):
+    return np.array([point(oracle, b["pose"]) for b in w.bodies()])
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_newton_diverging_step_does_not_poison_later_steps(oracle, solver):
+    # newton.rs:1262-1325: cloth-node pair (mass 1/18, k 100, c 0.5, rest 0.1): 10 steps of 1/60,
+    # one frame drop of 0.1 (deep in the regime where the mass-block seed diverges), 60 steps of
+    # 1/60: positions stay finite and the pair stays together
+    m = 1.0 / 18.0
+    w = newton_world(oracle, [rec(oracle, pos=(0.05, 0, 0), mass=m), rec(oracle, pos=(-0.05, 0, 0), mass=m)],
+                     [(0, 1, 0.1, 100.0, 0.5)], 1.0 / 60.0, solver)
+    w.step(10)
+    w.set_epoch(0.1)
+    w.step(1)
+    w.set_epoch(1.0 / 60.0)
+    w.step(60)
+    p = positions(oracle, w)
+    assert np.all(np.isfinite(p))
+    assert np.linalg.norm(p[0] - p[1]) < 1.0
+
+
+def test_newton_accuracy_improves_with_the_iteration_budget(oracle):
+    # newton.rs:1377-1430: a stretched pair with transverse velocities (k 500, c 1) for 60 steps;
+    # with warm Newton-Schulz budgets 1, 2, 3, 5, 8 every result is finite and one comes within
+    # 1e-4 of the generous budget 12
+    def run_with(warm):
+        w = newton_world(oracle, [rec(oracle, pos=(1.5, 0, 0), vel=(0, 4, 0)), rec(oracle, pos=(-1.5, 0, 0), vel=(0, -4, 0))],
+                         [(0, 1, 2.0, 500.0, 1.0)], 1.0 / 60.0, solver=1, ns_warm=warm)
+        w.step(60)
+        return float(positions(oracle, w)[0, 0])
+    generous = run_with(12)
+    errs = []
+    for warm in (1, 2, 3, 5, 8):
+        x = run_with(warm)
+        assert math.isfinite(x), warm
+        errs.append(abs(x - generous))
+    assert min(errs) < 1e-4, errs
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_newton_topology_change_causes_no_visible_jolt(oracle, solver):
+    # newton.rs:1478-1530: a-b spring (k 500) and c-b spring (k 200); c detached after 30 of 60
+    # steps or before the first: both runs finite. A detach is the joint list without c's spring,
+    # the bodies keeping their state (the oracle rebuilds its islands from the new list).
+    bodies = [rec(oracle, pos=(1, 0, 0)), rec(oracle, pos=(-1, 0, 0)), rec(oracle, pos=(0, 3, 0))]
+    both = [(0, 1, 2.0, 500.0, 1.0), (2, 1, 3.0, 200.0, 1.0)]
+    w = newton_world(oracle, bodies, both, 1.0 / 60.0, solver)
+    w.step(30)
+    late = newton_world(oracle, list(w.bodies()), both[:1], 1.0 / 60.0, solver)
+    late.step(30)
+    never = newton_world(oracle, bodies, both[:1], 1.0 / 60.0, solver)
+    never.step(60)
+    for ww in (late, never):
+        assert np.all(np.isfinite(positions(oracle, ww)))
+
+
+@pytest.mark.parametrize("solver", SOLVERS)
+def test_newton_stale_warm_hint_is_reseeded_not_followed(oracle, solver):
+    # newton.rs:1532-1575: a stiff pair (k 5e4, c 5, v +-5) whose step alternates between 0.2 and
+    # 1/600 (every third step the large one) for 40 steps: positions finite after every step
+    w = newton_world(oracle, [rec(oracle, pos=(1, 0, 0), vel=(0, 5, 0)), rec(oracle, pos=(-1, 0, 0), vel=(0, -5, 0))],
+                     [(0, 1, 2.0, 5.0e4, 5.0)], 0.2, solver)
+    for step in range(40):
+        w.set_epoch(0.2 if step % 3 == 0 else 1.0 / 600.0)
+        w.step(1)
+        assert np.all(np.isfinite(positions(oracle, w))), step

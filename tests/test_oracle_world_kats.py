@@ -420,3 +420,70 @@ def test_newton_stale_warm_hint_is_reseeded_not_followed(oracle, solver):
         w.set_epoch(0.2 if step % 3 == 0 else 1.0 / 600.0)
         w.step(1)
         assert np.all(np.isfinite(positions(oracle, w))), step
+
+
+# ── perpendicular damper unit cases (crates/joints/src/perpendicular_damper_warped.rs:164-300):
+# damping 1, softening 1e-3, dt 1/60, bodies at their poses with world twists as given ──
+
+def _perp(oracle, pa, pb, va, vb):
+    qa, qb = oracle.twist_exp(np.r_[pa, 0, 0, 0], 1.0), oracle.twist_exp(np.r_[pb, 0, 0, 0], 1.0)
+    return oracle.plain_eval(PERP, [1.0, 1e-3] + [0] * 8, qa, qb, va, vb, 1.0 / 60.0, 1.0)
+
+
+def test_perpendicular_reaction_cancels_force_and_moment(oracle):
+    # perpendicular_damper_warped.rs:193-227: A at (0, 1, 0) sliding along z, B still at (2, 0, 0)
+    w = _perp(oracle, (0, 1, 0), (2, 0, 0), [0, 0, 1, 0, 0, 0], np.zeros(6))
+    assert w[0:3] @ w[0:3] > 1e-6
+    assert np.abs(w[0:6] + w[6:12]).max() < 1e-6 and np.abs(w[0:6] + w[6:12]).max() < 1e-15
+
+
+def test_perpendicular_dissipates_when_the_far_end_spins(oracle):
+    # perpendicular_damper_warped.rs:229-247: B spins at (0, 0, -1) about its centre (2, 0, 0),
+    # which moves at (0, -1, 0): spatial linear part v_com - omega x p_com = (0, 1, 0)
+    vb = np.r_[0.0, 1.0, 0.0, 0.0, 0.0, -1.0]
+    w = _perp(oracle, (0, 0, 0), (2, 0, 0), np.zeros(6), vb)
+    assert power(oracle, w[:6], np.zeros(6)) + power(oracle, w[6:], vb) < 0.0
+
+
+def test_perpendicular_dissipates_in_pure_translation(oracle):
+    # perpendicular_damper_warped.rs:249-266
+    va = np.r_[0.0, 1.0, 0.0, 0.0, 0.0, 0.0]
+    w = _perp(oracle, (0, 0, 0), (2, 0, 0), va, np.zeros(6))
+    assert power(oracle, w[:6], va) + power(oracle, w[6:], np.zeros(6)) < 0.0
+
+
+def test_perpendicular_ignores_motion_along_the_line(oracle):
+    # perpendicular_damper_warped.rs:268-285 (the softened unit leaves a force of
+    # c v eps^2 / d^2 = 2.5e-7, so |F|^2 ~ 6e-14: far below the reference's bound of 1e-6)
+    w = _perp(oracle, (0, 0, 0), (2, 0, 0), [1, 0, 0, 0, 0, 0], np.zeros(6))
+    assert w[0:3] @ w[0:3] < 1e-6
+
+
+# ── inertia (crates/newton/src/inertia.rs:352-470): kinetic energy 1/2 <P, V> through the oracle
+# world's energy (gravity off, no joints), P = inertia . V ──
+
+def _one_body_energy(oracle, mass, tensor, v, omega):
+    b = np.zeros((), dtype=BODY_DTYPE)
+    b["pose"] = oracle.twist_exp(np.zeros(6), 1.0)
+    t = np.asarray(tensor, float).reshape(3, 3)
+    b["momentum"][:3] = mass * np.asarray(v, float)
+    b["momentum"][3:] = t @ np.asarray(omega, float)
+    b["mass"] = mass
+    b["inertia"] = t.reshape(-1)
+    b["diagonal"] = int(np.count_nonzero(t - np.diag(np.diag(t))) == 0)
+    b["size"] = 1.0
+    w = oracle.OracleWorld(np.array([b]), np.zeros(0, dtype=JOINT_DTYPE), step_params(integrator=SYMPLECTIC_EULER))
+    return w.energy()
+
+
+def test_kinetic_energy_includes_linear_and_angular(oracle):
+    # inertia.rs:405-426: m 2, I diag(3, 4, 5), v (1, 2, 3), omega (0.5, 1.5, 2.5): E = 34.5
+    e = _one_body_energy(oracle, 2.0, np.diag([3.0, 4.0, 5.0]), (1, 2, 3), (0.5, 1.5, 2.5))
+    assert abs(e - 34.5) < 1e-12
+
+
+def test_full_tensor_kinetic_energy(oracle):
+    # inertia.rs:428-466: the off-diagonal tensor [[4,1,0],[1,3,1],[0,1,5]]: E = 38 (the velocity
+    # comes back through the tensor's inverse, so this also checks full_inverse_recovers_twist)
+    e = _one_body_energy(oracle, 2.0, [[4, 1, 0], [1, 3, 1], [0, 1, 5]], (1, 2, 3), (0.5, 1.5, 2.5))
+    assert abs(e - 38.0) < 1e-12

@@ -1,8 +1,10 @@
 """Batches: many independent worlds of uneven size stepped together.
 
 Pins: every world of a batch is bit-identical to the same world stepped alone (the reference's
-driver-vs-solo property, crates/newton/tests/ar0103_epoch_driver.rs:115-158, and its batch-policy
-independence, crates/newton/tests/ar0104_batch_determinism.rs:140-153), and matches the oracle.
+driver-vs-solo property, crates/newton/tests/ar0103_epoch_driver.rs:115-158; mechanisms of different
+sizes sharing one accelerator, crates/newton/tests/concurrent_mechanisms.rs:84-137; and its
+batch-policy independence, crates/newton/tests/ar0104_batch_determinism.rs:140-153), and matches the
+oracle.
 """
 import numpy as np
 import pytest

@@ -54,3 +54,16 @@ def test_reference_arm_under_two_ranks_prints_once_from_rank_zero():
     lines = json_lines(out.stdout)
     assert len(lines) == 1
     check_line(lines[0], 2)
+
+
+def test_our_arm_without_a_gpu_fails_instead_of_falling_back():
+    """The product arm has no CPU path: on a machine without a GPU it exits non-zero and prints no
+    result line (skipped where CUDA is present, where it would run the full bench)."""
+    import pytest
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    out = subprocess.run([sys.executable, "bench.py", "--steps", "1", "--warmup", "3"], cwd=ROOT, capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode != 0
+    assert json_lines(out.stdout) == []

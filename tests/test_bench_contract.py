@@ -8,6 +8,8 @@ import socket
 import subprocess
 import sys
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ARGS = ["--impl", "reference", "--workload", "c0", "--steps", "1", "--warmup", "3"]
 REQUIRED = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
@@ -59,7 +61,6 @@ def test_reference_arm_under_two_ranks_prints_once_from_rank_zero():
 def test_our_arm_without_a_gpu_fails_instead_of_falling_back():
     """The product arm has no CPU path: on a machine without a GPU it exits non-zero and prints no
     result line (skipped where CUDA is present, where it would run the full bench)."""
-    import pytest
     torch = pytest.importorskip("torch")
     if torch.cuda.is_available():
         pytest.skip("a GPU is present")

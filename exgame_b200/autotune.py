@@ -77,8 +77,9 @@ def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, see
     With `cache` (a TuningCache or a file path) the choices are looked up first under this GPU's
     key and the workload's shape bucket: a hit sets them without timing anything (the workload's
     state is left alone) and returns them with `timed_on` "cache"; a miss measures as above and
-    stores the result. `device_key` overrides the GPU's key (its name, SM count and the library
-    build)."""
+    stores the result (a file that cannot be written leaves the measured choices set and is
+    reported under `cache_error`). `device_key` overrides the GPU's key (its name, SM count and the
+    library build)."""
     if cache is None:
         return _measure(dev, gravity_bodies, trees, tree_bodies, steps, seed, workload)
     if not isinstance(cache, TuningCache):
@@ -93,7 +94,10 @@ def autotune(dev, gravity_bodies=32768, trees=24, tree_bodies=1500, steps=3, see
         apply(dev, hit, workload)
         return dict(hit, timed_on="cache", bucket=bucket)
     res = _measure(dev, gravity_bodies, trees, tree_bodies, steps, seed, workload)
-    cache.put(key, bucket, res)
+    try:
+        cache.put(key, bucket, res)
+    except OSError as e:  # the choices are measured and set; only keeping them failed
+        return dict(res, bucket=bucket, cache_error=f"{type(e).__name__}: {e}")
     return dict(res, bucket=bucket)
 
 

@@ -190,3 +190,14 @@ def test_concurrent_writers_keep_every_entry(tmp_path):
     entries = autotune.TuningCache(path).entries()
     assert len(entries) == 60
     assert all(autotune.TuningCache(path).get(f"gpu{w}", f"bucket{k}") == BEST for w in range(4) for k in range(15))
+
+
+def test_unwritable_cache_keeps_the_measured_choices(tmp_path, timed):
+    """A cache path that cannot be written (its folder is a file) does not undo the tuning."""
+    blocker = tmp_path / "not_a_folder"
+    blocker.write_text("x")
+    dev = FakeDevice()
+    r = autotune.autotune(dev, workload=batch(), cache=str(blocker / "tuning.json"), device_key="gpuA")
+    assert r["timed_on"] == "workload" and "cache_error" in r
+    assert {k: r[k] for k in BEST} == BEST
+    assert dev.tuning == {key: BEST[name] for name, key, _ in autotune.KNOBS}

@@ -48,7 +48,12 @@ typedef enum {
   EXG_ERR_FATAL = -3,           /* Fatal: a guarded site fired (non-finite state) */
   EXG_ERR_WORKER_GONE = -4,     /* WorkerGone: the request loop has shut down */
   EXG_ERR_BACKEND = -5,         /* Backend: a CUDA call failed */
-  /* StructureError (crates/newton/src/mechanism/mechanism.rs:21-58) */
+  /* StructureError (crates/newton/src/mechanism/mechanism.rs:21-58), kept so that a host's mapping
+   * of the reference's errors stays total. This library returns none of the four: calls on one
+   * handle exclude each other, so a structural change (exg_batch_set_joints, a kinematic flip in
+   * exg_world_set_bodies, exg_pool_admit/release) waits for a step in flight on the handle instead
+   * of being refused mid-epoch; body records are copied into a handle, so no body belongs to two;
+   * a handle is bound to its device when created; and no call registers a world twice. */
   EXG_ERR_EPOCH_IN_PROGRESS = -10,
   EXG_ERR_ALREADY_OWNED = -11,
   EXG_ERR_FOREIGN_ACCELERATOR = -12,

@@ -44,7 +44,9 @@ typedef enum {
   EXG_OK = 0,
   /* EvalError (crates/newton/src/error.rs:11-28) */
   EXG_ERR_NO_SHADER = -1,       /* NoShader: unknown joint-law name or id */
-  EXG_ERR_TRAP = -2,            /* Trap: a kernel refused its input */
+  EXG_ERR_TRAP = -2,            /* Trap: a kernel refused its input. Not returned here: records a
+                                 * kernel would refuse are checked before any kernel runs and
+                                 * refused with EXG_ERR_INVALID_ARGUMENT */
   EXG_ERR_FATAL = -3,           /* Fatal: a guarded site fired (non-finite state) */
   EXG_ERR_WORKER_GONE = -4,     /* WorkerGone: the request loop has shut down */
   EXG_ERR_BACKEND = -5,         /* Backend: a CUDA call failed */

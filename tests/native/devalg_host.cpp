@@ -67,4 +67,32 @@ void dh_jacobian_slices_f32(int law, const double* prm, const float* pa, const f
     }
   }
 }
+// One first-order dual-number operation of the device scalar carrier (exg::Dual<1, double>) on
+// a = (av, ad) and b = (bv, bd): out = (value, derivative).
+void dh_dual1(int op, double av, double ad, double bv, double bd, double* out2) {
+  using D = exg::Dual<1, double>;
+  D a, b, r;
+  a.v = av; a.g[0] = ad;
+  b.v = bv; b.g[0] = bd;
+  switch (op) {
+    case 0: r = a + b; break;
+    case 1: r = a - b; break;
+    case 2: r = a * b; break;
+    case 3: r = a / b; break;
+    case 4: r = a.recip(); break;
+    case 5: r = exg::s_sqrt(a); break;
+    case 6: r = exg::s_sin(a); break;
+    case 7: r = exg::s_cos(a); break;
+    case 8: r = exg::s_atan2(a, b); break;
+    case 9: r = exg::s_exp(a); break;
+    case 10: r = exg::s_log(a); break;
+    case 11: r = exg::s_abs(a); break;
+    case 12: r = a * b + a / b; break;
+    case 13: r = exg::s_sin(a * a); break;
+    case 14: r = exg::s_exp(exg::s_log(a)); break;
+    default: out2[0] = out2[1] = 0.0; return;
+  }
+  out2[0] = r.v;
+  out2[1] = r.g[0];
+}
 }

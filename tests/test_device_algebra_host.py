@@ -100,3 +100,67 @@ def test_half_slices_equal_whole_slices_bit_for_bit(dh):
             dh.dh_jacobian_slices_f32(law, P(prm), *[P(x) for x in f], ctypes.c_double(0.016), ctypes.c_double(1.3), 1,
                                       P(o3))
             assert np.array_equal(o6, o3), law
+
+
+# ── the device's dual-number carrier (exg::Dual, csrc/scalar.cuh) against the reference's
+# first-order Tangent tests (crates/clifford/src/tangent.rs:340-510) ──
+
+ADD, SUB, MUL, DIV, RECIP, SQRT, SIN, COS, ATAN2, EXP, LOG, ABS, FOO, SIN_SQ, EXP_LOG = range(15)
+
+
+def dual(dh, op, a, da=1.0, b=0.0, db=0.0):
+    out = np.zeros(2)
+    dh.dh_dual1.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4 + [ctypes.c_void_p]
+    dh.dh_dual1(op, a, da, b, db, P(out))
+    return out
+
+
+def test_dual_simple_and_product_rules(dh):
+    # tangent.rs:383-391 `simple`: a = (10, 2), b = (2, 2), a b + a / b = (25, 20)
+    assert list(dual(dh, FOO, 10.0, 2.0, 2.0, 2.0)) == [25.0, 20.0]
+    # tangent.rs:421-439: constant, x^2 at 3 -> (9, 6), 1/x at 2 -> (0.5, -0.25)
+    assert list(dual(dh, MUL, 7.0, 0.0, 3.0, 0.0)) == [21.0, 0.0]
+    assert list(dual(dh, MUL, 3.0, 1.0, 3.0, 1.0)) == [9.0, 6.0]
+    assert list(dual(dh, RECIP, 2.0)) == [0.5, -0.25]
+    assert list(dual(dh, DIV, 1.0, 0.0, 2.0, 1.0)) == [0.5, -0.25]
+
+
+def test_dual_transcendentals(dh):
+    # tangent.rs:441-470: sqrt at 4 -> (2, 1/4); exp(ln x) at 3 -> (3, 1); sin, cos at 0; sin(x^2) at 1
+    v, d = dual(dh, SQRT, 4.0)
+    assert abs(v - 2.0) < 1e-12 and abs(d - 0.25) < 1e-12
+    v, d = dual(dh, EXP_LOG, 3.0)
+    assert abs(v - 3.0) < 1e-12 and abs(d - 1.0) < 1e-12
+    assert np.allclose(dual(dh, SIN, 0.0), [0.0, 1.0], rtol=0, atol=1e-15)
+    assert np.allclose(dual(dh, COS, 0.0), [1.0, 0.0], rtol=0, atol=1e-15)
+    v, d = dual(dh, SIN_SQ, 1.0)
+    assert abs(v - np.sin(1.0)) < 1e-12 and abs(d - 2.0 * np.cos(1.0)) < 1e-12
+    v, d = dual(dh, EXP, 0.5)
+    assert abs(v - np.exp(0.5)) < 1e-12 and abs(d - np.exp(0.5)) < 1e-12
+    v, d = dual(dh, LOG, 2.0)
+    assert abs(v - np.log(2.0)) < 1e-12 and abs(d - 0.5) < 1e-12
+
+
+def test_dual_atan2(dh):
+    # tangent.rs:490-505: atan2(sin t, cos t) at t = 0.7 -> (0.7, 1); d/dy atan2(y, x) at (1, 2) = x / (x^2 + y^2)
+    t = 0.7
+    s, ds = dual(dh, SIN, t)
+    c, dc = dual(dh, COS, t)
+    v, d = dual(dh, ATAN2, s, ds, c, dc)
+    assert abs(v - 0.7) < 1e-12 and abs(d - 1.0) < 1e-12
+    v, d = dual(dh, ATAN2, 1.0, 1.0, 2.0, 0.0)
+    assert abs(v - np.arctan2(1.0, 2.0)) < 1e-15 and abs(d - 2.0 / 5.0) < 1e-15
+    # and the x partial: -y / (x^2 + y^2)
+    v, d = dual(dh, ATAN2, 1.0, 0.0, 2.0, 1.0)
+    assert abs(d + 1.0 / 5.0) < 1e-15
+
+
+def test_dual_singular_points_stay_finite_in_value(dh):
+    # tangent.rs:347-360: sqrt and ln at 0 must not abort; the value of sqrt is clean, only the
+    # derivative is non-finite (a downstream guard on the standard part discards it)
+    v, d = dual(dh, SQRT, 0.0)
+    assert v == 0.0 and not np.isfinite(d)
+    v, d = dual(dh, LOG, 0.0)
+    assert v == -np.inf
+    # |x| takes derivative sign(x), 0 at 0
+    assert list(dual(dh, ABS, -2.0)) == [2.0, -1.0] and list(dual(dh, ABS, 0.0)) == [0.0, 0.0]

@@ -95,4 +95,12 @@ void dh_dual1(int op, double av, double ad, double bv, double bd, double* out2) 
   out2[0] = r.v;
   out2[1] = r.g[0];
 }
+// The Study forms of the device's exp (sin(sqrt u)/sqrt u, cos(sqrt u), its u-derivative), each
+// with its Taylor arm below the scalar's effective-zero threshold.
+void dh_study_forms(double u, double* out3) {
+  out3[0] = exg::sinc_sq(u); out3[1] = exg::cos_sq(u); out3[2] = exg::dsinc_sq(u);
+}
+void dh_study_forms_f32(float u, float* out3) {
+  out3[0] = exg::sinc_sq(u); out3[1] = exg::cos_sq(u); out3[2] = exg::dsinc_sq(u);
+}
 }

@@ -164,3 +164,24 @@ def test_dual_singular_points_stay_finite_in_value(dh):
     assert v == -np.inf
     # |x| takes derivative sign(x), 0 at 0
     assert list(dual(dh, ABS, -2.0)) == [2.0, -1.0] and list(dual(dh, ABS, 0.0)) == [0.0, 0.0]
+
+
+def test_study_forms_match_the_oracle_across_the_seams(dh, oracle):
+    """The device's Study forms (the exp of a twist goes through them) against the oracle's
+    restatement of crates/peano/src/scalar.rs:67-131 with the thresholds of support.rs:39-49,
+    on both sides of every seam (f64: |u| < 1e-9, and 1e-4 for the derivative's arm; f32: 1e-5
+    and 1), bit for bit: the same arms, the same operation order."""
+    dh.dh_study_forms.argtypes = [ctypes.c_double, ctypes.c_void_p]
+    dh.dh_study_forms_f32.argtypes = [ctypes.c_float, ctypes.c_void_p]
+    L = oracle.lib()
+    us = np.r_[0.0, np.logspace(-14, 1.5, 400), 0.999e-9, 1.001e-9, 0.999e-4, 1.001e-4, 0.999e-5, 1.001e-5, 0.999,
+               1.001]
+    for u in us:
+        d, o = np.zeros(3), np.zeros(3)
+        dh.dh_study_forms(float(u), P(d))
+        L.orc_study_forms(ctypes.c_double(u), oracle.p(o))
+        assert np.array_equal(d, o), (u, d, o)
+        df, of = np.zeros(3, dtype=np.float32), np.zeros(3, dtype=np.float32)
+        dh.dh_study_forms_f32(np.float32(u), P(df))
+        L.orc_study_forms_f32(ctypes.c_float(u), ctypes.c_void_p(of.ctypes.data))
+        assert np.array_equal(df, of), (u, df, of)

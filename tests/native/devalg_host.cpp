@@ -1,6 +1,9 @@
 // Test harness: compiles the device algebra and force-law headers of the CUDA path for the
 // host so the CPU test suite can compare them with the oracle without a GPU.
 #include "../../exgame_b200/csrc/joint_eval.cuh"
+// body.cuh names CUDA's double4 (a device vector type); the host build gets a plain stand-in
+struct double4 { double x, y, z, w; };
+#include "../../exgame_b200/csrc/body.cuh"
 
 extern "C" {
 void dh_joint_plain(int law, const double* prm, const double* pa, const double* pb, const double* va, const double* vb,
@@ -102,5 +105,15 @@ void dh_study_forms(double u, double* out3) {
 }
 void dh_study_forms_f32(float u, float* out3) {
   out3[0] = exg::sinc_sq(u); out3[1] = exg::cos_sq(u); out3[2] = exg::dsinc_sq(u);
+}
+// Body helpers: momentum <-> body twist through the inertia (diagonal, full tensor or kinematic),
+// and the world twist of a body from its pose and momentum.
+void dh_inertia(const double* I9, int diag, int kin, double mass, int inverse, const double* in6, double* out6) {
+  if (inverse) exg::inertia_inverse<double>(I9, diag != 0, kin != 0, mass, in6, out6);
+  else exg::inertia_apply<double>(I9, diag != 0, kin != 0, mass, in6, out6);
+}
+void dh_world_velocity(const double* pose8, const double* mom6, const double* I9, int diag, int kin, double mass,
+                       double* out6) {
+  exg::world_velocity(pose8, mom6, I9, diag != 0, kin != 0, mass, out6);
 }
 }

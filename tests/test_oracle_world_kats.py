@@ -512,3 +512,25 @@ def test_lagged_gravity_must_not_pump_energy(oracle):
     assert e_max <= e0 + 0.05 * abs(e0)
     assert e_max <= e0 + 1e-9 * abs(e0), (e0, e_max)  # here: never above E0 at all
     assert e_end < 0.0 and e_end < e0
+
+
+def test_set_epoch_is_the_epoch_of_the_following_steps(oracle):
+    """The oracle's epoch change (the reference passes a new Epoch to every Mechanism::step):
+    setting the same dt changes nothing, and a new dt gives the bits of a world built with it
+    from the same state."""
+    bodies = [rec(oracle, pos=(1.5, 0, 0), vel=(0, 4, 0)), rec(oracle, pos=(-1.5, 0, 0), vel=(0, -4, 0))]
+    springs = [(0, 1, 2.0, 500.0, 1.0)]
+    a = newton_world(oracle, bodies, springs, 1.0 / 60.0, 0)
+    b = newton_world(oracle, bodies, springs, 1.0 / 60.0, 0)
+    a.step(5)
+    b.step(5)
+    b.set_epoch(1.0 / 60.0)
+    a.step(5)
+    b.step(5)
+    assert np.array_equal(a.bodies()["pose"], b.bodies()["pose"])
+    b.set_epoch(0.005)
+    c = newton_world(oracle, list(a.bodies()), springs, 0.005, 0)
+    b.step(7)
+    c.step(7)
+    assert np.array_equal(b.bodies()["pose"], c.bodies()["pose"])
+    assert np.array_equal(b.bodies()["momentum"], c.bodies()["momentum"])

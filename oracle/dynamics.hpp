@@ -1,4 +1,7 @@
 // ORACLE — test infrastructure only (CPU restatement the CUDA path is checked against).
+// Pinned against the reference's own known-answer tests and test properties, restated with their
+// file:line in tests/test_oracle_kat.py, tests/test_oracle_world_kats.py and
+// tests/test_seam_oracle.py (the reference keeps no golden vectors and cannot be built here).
 //
 // f64 restatement of the per-step dynamics path, composed in the reference's order:
 //   * RigidBody state: pose motor + BODY-frame momentum (crates/newton/src/body.rs:32-205),
